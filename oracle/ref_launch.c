@@ -1,0 +1,65 @@
+/*
+ * Launchers for the reference's OpenCL kernels compiled as C (TEST
+ * INFRASTRUCTURE ONLY).  Linked with binary_pursuit.cl (compiled through
+ * clshim.h) into oracle/_ref/libbp_ref.so.  Each launch runs work-items
+ * offset..offset+gsize-1 one at a time with a work-group size of 1.  Arguments
+ * arrive as an array of 64-bit words in kernel-argument order: a buffer or
+ * local-memory argument is its address, a scalar argument its value.  The
+ * prototypes restate the kernel signatures of binary_pursuit.cl.
+ */
+#include <stddef.h>
+#include <stdint.h>
+typedef unsigned int uint;
+typedef unsigned char uchar;
+_Thread_local size_t clshim_gid, clshim_lid, clshim_lsz = 1;
+
+void compute_residual(float *, uint, uint, const float *, uint, uint, const uint *, const uint *, uint);                           /* .cl:57 */
+void compute_full_likelihood(float *, uint, uint, const float *, uint, uint, const float *, const uint *, uint, float *);          /* .cl:255 */
+void compute_template_maximum_likelihood(uint, uint, uint, const uint *, uint, uint *, uint *, float *, uchar *, uchar *,
+                                         uint *, uint *, float *, const float *);                                                 /* .cl:350 */
+void overlap_recheck_indices(float *, uint, uint, const float *, uint, uint, const uint *, uint, uint *, uint *, float *, uint,
+                             float *, uint *, float *, uint *, const float *);                                                     /* .cl:444 */
+void parse_overlap_recheck_indices(uint, uint, const uint *, uint, uint *, uint *, float *, uint *, uint *, float *, uint,
+                                   const float *, float *, uint *, uchar *);                                                       /* .cl:657 */
+void check_overlap_reassignments(uint, uint, const uint *, uint, uint *, uint *, uchar *, uint *, uint *, uchar *);              /* .cl:822 */
+void binary_pursuit(uint, uint, uint, const float *, uint *, uint, const uint *, const uint *, const float *, uint *, uint *,
+                    uint *, uint *, uchar *, uchar *);                                                                             /* .cl:918 */
+void get_adjusted_clips(const float *, uint, uint, const float *, uint, uint, const uint *, const uint *, uint, float *);        /* .cl:1088 */
+
+#define P(i, T) ((T)(uintptr_t)a[i])
+#define U(i) ((uint)a[i])
+
+/* kernel ids follow the order of the .cl file */
+int bpref_launch(int kernel, uint64_t offset, uint64_t gsize, uint64_t lsize, const uint64_t *a)
+{
+    if (lsize != 1) return -1;
+    clshim_lsz = 1;
+    clshim_lid = 0;
+    for (uint64_t g = offset; g < offset + gsize; g++) {
+        clshim_gid = (size_t)g;
+        switch (kernel) {
+        case 0: compute_residual(P(0, float *), U(1), U(2), P(3, const float *), U(4), U(5), P(6, const uint *),
+                                 P(7, const uint *), U(8)); break;
+        case 1: compute_full_likelihood(P(0, float *), U(1), U(2), P(3, const float *), U(4), U(5), P(6, const float *),
+                                        P(7, const uint *), U(8), P(9, float *)); break;
+        case 2: compute_template_maximum_likelihood(U(0), U(1), U(2), P(3, const uint *), U(4), P(5, uint *), P(6, uint *),
+                                                    P(7, float *), P(8, uchar *), P(9, uchar *), P(10, uint *),
+                                                    P(11, uint *), P(12, float *), P(13, const float *)); break;
+        case 3: overlap_recheck_indices(P(0, float *), U(1), U(2), P(3, const float *), U(4), U(5), P(6, const uint *), U(7),
+                                        P(8, uint *), P(9, uint *), P(10, float *), U(11), P(12, float *), P(13, uint *),
+                                        P(14, float *), P(15, uint *), P(16, const float *)); break;
+        case 4: parse_overlap_recheck_indices(U(0), U(1), P(2, const uint *), U(3), P(4, uint *), P(5, uint *), P(6, float *),
+                                              P(7, uint *), P(8, uint *), P(9, float *), U(10), P(11, const float *),
+                                              P(12, float *), P(13, uint *), P(14, uchar *)); break;
+        case 5: check_overlap_reassignments(U(0), U(1), P(2, const uint *), U(3), P(4, uint *), P(5, uint *), P(6, uchar *),
+                                            P(7, uint *), P(8, uint *), P(9, uchar *)); break;
+        case 6: binary_pursuit(U(0), U(1), U(2), P(3, const float *), P(4, uint *), U(5), P(6, const uint *),
+                               P(7, const uint *), P(8, const float *), P(9, uint *), P(10, uint *), P(11, uint *),
+                               P(12, uint *), P(13, uchar *), P(14, uchar *)); break;
+        case 7: get_adjusted_clips(P(0, const float *), U(1), U(2), P(3, const float *), U(4), U(5), P(6, const uint *),
+                                   P(7, const uint *), U(8), P(9, float *)); break;
+        default: return -2;
+        }
+    }
+    return 0;
+}
