@@ -1,0 +1,342 @@
+"""Benchmark: pursuit sample*template/s of Full Binary Pursuit on B200.
+
+One step = one complete binary pursuit (all passes until convergence,
+overlap recheck and residuals included) of one synthetic recording segment.
+Default workload: 16-channel linear probe, 10 min at 40 kHz (24M samples per
+channel), 64 templates of 101 samples on all channels, Poisson 1-80 Hz with
+15% forced overlaps, n_max_shift_inds = L-1 (the production setting,
+full_binary_pursuit.py:145).  Inputs are seeded synthetic data: the voltage
+(1.5 GB) and the likelihood buffer (6.1 GB) are both far larger than L2.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+N > 1 runs under torchrun, one process per GPU; each rank pursues its own
+segment (segments are independent units; no data-path collective), and the
+reported value is the total over ranks divided by the slowest rank's time.
+"""
+import argparse
+import ctypes
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+REPO = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, REPO)
+
+METRIC = "pursuit sample*template/s"
+UNIT = "sample*template/s"
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=3)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--workload", choices=["linear16", "tetrode", "hd384"], default="linear16")
+    ap.add_argument("--duration", type=float, default=None,
+                    help="override the segment length in seconds (development only)")
+    ap.add_argument("--precision", choices=["fp32", "bf16"], default="fp32")
+    ap.add_argument("--cpu-sample-s", type=float, default=0.05,
+                    help="seconds of recording timed on the CPU baseline")
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-cpu", action="store_true")
+    return ap.parse_args()
+
+
+def workload(name, duration, seed):
+    from spikesorting_fullpursuit_b200 import synthetic
+    fn = {"linear16": synthetic.linear16, "tetrode": synthetic.tetrode, "hd384": synthetic.hd384}[name]
+    kw = {"seed": seed}
+    if duration is not None:
+        kw["duration_s"] = duration
+    return fn(**kw)
+
+
+def template_channels(templates, C, L):
+    """Mean number of channels a template is non-zero on (C_t)."""
+    t = templates.reshape(templates.shape[0], C, L)
+    return float(np.mean(np.sum(np.any(t != 0, axis=2), axis=1)))
+
+
+class ClockSampler:
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index):
+        self.gpu = gpu_index
+        self.proc = None
+        self.path = None
+
+    def start(self):
+        try:
+            fd, self.path = tempfile.mkstemp(suffix=".csv")
+            os.close(fd)
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.gpu), "--query-gpu=" + self.FIELDS, "--format=csv,noheader,nounits",
+                 "-lms", "200"], stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+
+    def stop(self):
+        if self.proc is None:
+            return None
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        rows = []
+        for line in open(self.path):
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) >= 9:
+                rows.append(parts)
+        os.unlink(self.path)
+        if not rows:
+            return None
+        sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in rows if r[2].replace(".", "").isdigit()]
+        reasons = set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for r in rows:
+            for nm, v in zip(names, r[5:9]):
+                if v.strip().lower() == "active":
+                    reasons.add(nm)
+        loaded = [x for x in sm if x > 0.5 * (max(mx) if mx else 1)] or sm
+        return {"sm_mhz": statistics.median(loaded) if loaded else None,
+                "sm_max_mhz": max(mx) if mx else None, "reasons": sorted(reasons),
+                "samples": len(rows)}
+
+
+def measured_peaks():
+    p = os.path.join(REPO, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        d = json.load(open(p))
+        return d["hbm_gbs"], d["bf16_tflops"], d["bf16_tflops_sustained"], "measured"
+    return 6650.0, 1590.0, 1400.0, "fallback"
+
+
+# ---------------------------------------------------------------- reference arm
+
+def run_reference_arm(args, rank, world):
+    """The reference's CPU implementation of the path (the oracle: kernels and
+    host loop of binary_pursuit.cl / binary_pursuit_parallel.py restated in C,
+    pinned to the reference) on the host cores, one bounded sample per step."""
+    if rank != 0:
+        return
+    from oracle import oracle as O
+    rec = workload(args.workload, max(args.cpu_sample_s, 0.01) if args.duration is None else
+                   min(args.duration, args.cpu_sample_s), seed=1)
+    L = rec.n_samples_per_chan
+    si = rec.sort_info()
+    threads = os.cpu_count() or 1
+    times = []
+    for i in range(args.warmup + args.steps):
+        t0 = time.perf_counter()
+        O.binary_pursuit_oracle(rec.voltage, rec.voltage.dtype, si, rec.fresh_metrics(),
+                                n_max_shift_inds=L - 1, nthreads=threads)
+        dt = time.perf_counter() - t0
+        if i >= args.warmup:
+            times.append(dt)
+    sec = float(np.median(times))
+    units = rec.n_samples * rec.n_templates
+    value = units / sec
+    sample = ("first %.3f s (%d samples) of the %s workload, all passes, n_max_shift=L-1"
+              % (rec.n_samples / rec.sampling_rate, rec.n_samples, args.workload))
+    line = {"impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": sec * 1e3,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic (seeded)",
+            "config": {"workload": args.workload, "n_chans": rec.n_chans, "n_samples": rec.n_samples,
+                       "n_templates": rec.n_templates, "template_len": L, "n_max_shift": L - 1},
+            "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "port",
+                             "sample": sample},
+            "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+# ---------------------------------------------------------------- our arm
+
+def main():
+    args = parse()
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        run_reference_arm(args, rank, world)
+        return
+
+    import torch
+    import torch.distributed as dist
+    from spikesorting_fullpursuit_b200 import _lib, binary_pursuit
+    from spikesorting_fullpursuit_b200 import build as B
+
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    if world > 1:
+        import datetime
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600),
+                                device_id=dev)
+    lib = _lib.lib() if not B.needs_build() else (B.build(), _lib.lib())[1]
+
+    rec = workload(args.workload, args.duration, seed=1 + rank)
+    C, n, K, L = rec.n_chans, rec.n_samples, rec.n_templates, rec.n_samples_per_chan
+    nmax = L - 1
+    prec = 0 if args.precision == "fp32" else 1
+    metrics = rec.fresh_metrics()
+    T = np.ascontiguousarray(np.float32(metrics["templates"]).reshape(-1))
+    tss = np.ascontiguousarray(np.float32(-0.5 * metrics["template_SS"]))
+    thr = np.ascontiguousarray(np.float32(metrics["neuron_lower_thresholds"]))
+    stream = torch.cuda.current_stream(dev)
+    sp = _lib.stream_ptr(stream)
+    pristine = torch.from_numpy(np.ascontiguousarray(rec.voltage)).to(dev).to(torch.float32)
+    v = torch.empty_like(pristine)
+    T_d, tss_d, thr_d = (torch.from_numpy(x).to(dev) for x in (T, tss, thr))
+    wsb = ctypes.c_size_t(0)
+    _lib.check(lib.fbp_pursuit_workspace_bytes(n, C, K, L, nmax, prec, ctypes.byref(wsb)))
+    ws = torch.empty(wsb.value, dtype=torch.uint8, device=dev)
+    W = (n + L - 1) // L
+    cap = 16 * W + 4096
+    out_i = torch.empty(cap, dtype=torch.int32, device=dev)
+    out_l = torch.empty(cap, dtype=torch.int32, device=dev)
+
+    def step(profile):
+        v.copy_(pristine)
+        nspk, npass = ctypes.c_uint32(0), ctypes.c_uint32(0)
+        st = _lib.StageStats()
+        _lib.check(lib.fbp_pursuit_chunk(
+            _lib.ptr(v), n, C, _lib.ptr(T_d), K, L, _lib.ptr(tss_d), _lib.ptr(thr_d), nmax, 1, prec,
+            1000000, _lib.ptr(ws), ws.numel(), _lib.ptr(out_i), _lib.ptr(out_l), cap, None,
+            ctypes.byref(nspk), ctypes.byref(npass), int(profile), ctypes.byref(st), sp))
+        return st
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+
+    for _ in range(args.warmup):
+        step(False)
+    torch.cuda.synchronize()
+
+    clocks = ClockSampler(local)
+    barrier()
+    torch.cuda.synchronize()
+    clocks.start()
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    stats = []
+    ev0.record(stream)
+    for _ in range(args.steps):
+        stats.append(step(True))
+    ev1.record(stream)
+    torch.cuda.synchronize()
+    clock_info = clocks.stop()
+    barrier()
+    ms_total = ev0.elapsed_time(ev1)
+    t = torch.tensor([ms_total], dtype=torch.float64, device=dev)
+    if world > 1:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    ms_step = float(t.item()) / args.steps
+    units_per_step = world * n * K
+    value = units_per_step / (ms_step / 1e3)
+
+    # per-stage CUDA-event times inside the timed steps -> dominant stage roofline
+    stage_ms = np.zeros(_lib.N_STAGES)
+    work = np.zeros(_lib.N_STAGES)
+    launches = np.zeros(_lib.N_STAGES)
+    for s in stats:
+        stage_ms += np.array(s.ms[:])
+        work += np.array(s.work[:], dtype=np.float64)
+        launches += np.array(s.launches[:], dtype=np.float64)
+    Ct = template_channels(T.reshape(K, -1), C, L)
+    hbm, tf_burst, tf_sust, peak_src = measured_peaks()
+    per_unit = {  # name: (bound, algorithmic units -> flops or bytes)
+        0: ("tensor", 2.0 * Ct * L, "TFLOP/s"),       # likelihood: 2*C_t*L flops per sample*template
+        1: ("hbm", 4.0, "GB/s"),                       # argmax: each scanned fp32 likelihood read once
+        2: ("tensor", 5.0 * C * L, "TFLOP/s"),        # overlap: 5*C*L flops per evaluated item
+        5: ("hbm", 8.0 * Ct * L, "GB/s"),             # residual: 8*C_t*L bytes per spike
+    }
+    dom = max(per_unit, key=lambda i: stage_ms[i])
+    bound, per, unit = per_unit[dom]
+    alg = work[dom] * per
+    secs = stage_ms[dom] / 1e3
+    if bound == "tensor":
+        achieved = alg / secs / 1e12 if secs > 0 else 0.0
+        peak = tf_sust
+    else:
+        achieved = alg / secs / 1e9 if secs > 0 else 0.0
+        peak = hbm
+    roofline = {"bound": bound, "achieved": achieved, "peak": peak, "unit": unit,
+                "frac": achieved / peak if peak else None, "traffic": None,
+                "kernel": _lib.STAGE_NAMES[dom], "peak_source": peak_src + (" sustained" if bound == "tensor" else ""),
+                "launches_in_timed_region": int(launches[dom]),
+                "stage_ms_per_step": {_lib.STAGE_NAMES[i]: stage_ms[i] / args.steps for i in range(_lib.N_STAGES)}}
+    gpu_launches = int(launches.sum())
+
+    # end to end through the public API: host voltage (pinned) -> spikes on the host
+    e2e = None
+    if not args.no_e2e:
+        pinned = torch.empty(rec.voltage.shape, dtype=torch.from_numpy(rec.voltage[:1, :1]).dtype).pin_memory()
+        pinned.numpy()[...] = rec.voltage
+        host_v = pinned.numpy()
+        si = rec.sort_info()
+        binary_pursuit(host_v, host_v.dtype, si, rec.fresh_metrics(), n_max_shift_inds=nmax,
+                       precision=args.precision)
+        barrier()
+        e_times = []
+        d2h = 0
+        for _ in range(args.steps):
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            out = binary_pursuit(host_v, host_v.dtype, si, rec.fresh_metrics(), n_max_shift_inds=nmax,
+                                 precision=args.precision)
+            e_times.append(time.perf_counter() - t0)
+            d2h = 8 * len(out[0])
+        te = torch.tensor([float(np.mean(e_times))], dtype=torch.float64, device=dev)
+        if world > 1:
+            dist.all_reduce(te, op=dist.ReduceOp.MAX)
+        e2e = {"value": units_per_step / float(te.item()), "unit": UNIT,
+               "h2d_bytes_per_step": int(host_v.nbytes + T.nbytes + tss.nbytes + thr.nbytes),
+               "d2h_bytes_per_step": int(d2h)}
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu:
+        from oracle import oracle as O
+        sample_s = args.cpu_sample_s
+        m = int(round(sample_s * rec.sampling_rate))
+        sl = np.ascontiguousarray(rec.voltage[:, :m])
+        threads = os.cpu_count() or 1
+        t0 = time.perf_counter()
+        O.binary_pursuit_oracle(sl, sl.dtype, rec.sort_info(), rec.fresh_metrics(), n_max_shift_inds=nmax,
+                                nthreads=threads)
+        dt = time.perf_counter() - t0
+        cpu = {"value": m * K / dt, "unit": UNIT, "cores": threads, "kind": "port",
+               "sample": "first %.3f s (%d samples) of the same recording, all passes" % (sample_s, m)}
+
+    if rank == 0:
+        line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+                "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True,
+                "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+                "data": "synthetic (seeded; one independent segment per rank)",
+                "config": {"workload": rec.name, "n_chans": C, "n_samples": n, "n_templates": K,
+                           "template_len": L, "n_max_shift": nmax, "precision": args.precision,
+                           "l2": "inputs larger than L2 (voltage %.2f GB, likelihood %.2f GB)"
+                                 % (C * n * 4 / 1e9, K * n * 4 / 1e9),
+                           "passes": int(stats[-1].passes), "spikes": int(stats[-1].spikes),
+                           "overlap_candidates": int(stats[-1].candidates),
+                           "parallelism": "segment-parallel x%d" % world},
+                "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": gpu_launches,
+                "clocks": clock_info}
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

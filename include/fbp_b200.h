@@ -1,0 +1,224 @@
+/*
+ * fbp_b200.h -- C ABI of the B200-native Full Binary Pursuit library
+ * (libfbp_b200.so, built from spikesorting_fullpursuit_b200/csrc).
+ *
+ * The reference drives eight OpenCL kernels of
+ * spikesorting_fullpursuit/kernels/binary_pursuit.cl from Python through
+ * pyopencl (spikesorting_fullpursuit/parallel/binary_pursuit_parallel.py).
+ * Each entry point below replaces one kernel, or the whole per-chunk loop,
+ * and names the reference code it stands in for.
+ *
+ * Conventions
+ *  - All array arguments are DEVICE pointers unless the name says `host`.
+ *  - voltage is channel-major [C][n] float32; templates are [K][C][L]
+ *    float32 (the packing described at binary_pursuit.cl:11-29).
+ *  - Window `w` covers samples [w*L, (w+1)*L); W = ceil(n / L).
+ *  - Per-window state arrays hold at least W + FBP_WINDOW_PAD entries.
+ *  - `stream` is a cudaStream_t passed as void* (NULL = legacy default).
+ *  - Every entry point returns an fbp_status; fbp_last_error() gives text.
+ *  - Results are those of the reference kernels executed with a work-group
+ *    size of 1, work-items in global-id order: the one schedule under which
+ *    the reference is deterministic.
+ */
+#ifndef FBP_B200_H
+#define FBP_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define FBP_WINDOW_PAD 4
+
+typedef enum fbp_status {
+    FBP_OK = 0,
+    FBP_ERR_BAD_ARG = 1,     /* invalid size, null pointer, mis-sized workspace */
+    FBP_ERR_CUDA = 2,        /* a CUDA runtime call failed                      */
+    FBP_ERR_ITER_CAP = 3,    /* the pursuit did not converge within max_passes  */
+    FBP_ERR_CAPACITY = 4,    /* the spike output buffer is too small            */
+    FBP_ERR_NO_DEVICE = 5,   /* no CUDA device                                  */
+    FBP_ERR_OOM = 6          /* reserved: allocation failure in a caller layer  */
+} fbp_status;
+
+/* Arithmetic of the full-pass likelihood (path (a)).  Both modes produce
+ * the same spikes; FBP_PREC_FP32 evaluates every likelihood in the
+ * reference's order on the FP32 pipes. */
+typedef enum fbp_precision {
+    FBP_PREC_FP32 = 0,
+    FBP_PREC_BF16_REFINE = 1
+} fbp_precision;
+
+/* Stages of a pass, for fbp_stage_stats. */
+enum {
+    FBP_STAGE_LIKELIHOOD = 0,   /* path (a): full-pass likelihood          */
+    FBP_STAGE_ARGMAX = 1,       /* per-window argmax over templates        */
+    FBP_STAGE_OVERLAP = 2,      /* overlap recheck + parse                 */
+    FBP_STAGE_CHECK = 3,        /* check_overlap_reassignments             */
+    FBP_STAGE_ACCEPT = 4,       /* accept, flags, spike compaction         */
+    FBP_STAGE_RESIDUAL = 5,     /* path (c): residual subtract             */
+    FBP_STAGE_LISTS = 6,        /* window/candidate list compaction, resets */
+    FBP_N_STAGES = 7
+};
+
+/* Per-stage counters of one fbp_pursuit_chunk call.  `ms` holds CUDA-event
+ * time per stage (filled only when profiling is requested); `launches` the
+ * kernels launched per stage; `work` the algorithmic units per stage:
+ *  LIKELIHOOD  sample x template likelihoods evaluated
+ *  ARGMAX      likelihood values scanned
+ *  OVERLAP     (a, b, t) items evaluated after the reference's skip rules
+ *  ACCEPT      windows examined
+ *  RESIDUAL    spikes subtracted
+ *  CHECK       candidate windows */
+typedef struct fbp_stage_stats {
+    double ms[FBP_N_STAGES];
+    uint64_t launches[FBP_N_STAGES];
+    uint64_t work[FBP_N_STAGES];
+    uint64_t candidates;        /* overlap-recheck candidates over all passes */
+    uint32_t passes;
+    uint32_t spikes;
+} fbp_stage_stats;
+
+/* Library version (major*10000 + minor*100 + patch). */
+int fbp_version(void);
+
+/* Text of the last error raised on the calling thread ("" if none). */
+const char *fbp_last_error(void);
+
+/* ------------------------------------------------------------------------
+ * Whole per-chunk pursuit.
+ * Replaces the iterate-until-converged loop of
+ * binary_pursuit_parallel.py:386-736 (and the K+6 kernel launches plus the
+ * host round trips of each pass) for one chunk that is already resident on
+ * the device.
+ * ---------------------------------------------------------------------- */
+
+/* Bytes of device workspace fbp_pursuit_chunk needs for these sizes. */
+int fbp_pursuit_workspace_bytes(uint32_t n_samples, uint32_t n_chans, uint32_t n_templates,
+                                uint32_t template_len, uint32_t n_max_shift, int precision,
+                                size_t *bytes_out);
+
+/* Run binary pursuit on one chunk.
+ *  voltage      [C][n] float32, turned into the residual in place
+ *  templates    [K][C][L] float32
+ *  neg_half_ss  [K] float32, float32(-0.5 * template_SS)   (.py:199)
+ *  thresholds   [K] float32, float32(neuron_lower_thresholds) (.py:201)
+ *  n_max_shift  overlap shift range, S = 2*n_max_shift + 1   (.py:294-298)
+ *  spike_idx/spike_lab  [spike_cap] uint32 outputs: window-relative clip
+ *               starts and labels, in pass order and window order inside a
+ *               pass (the order the reference's loop concatenates them)
+ *  pass_counts  [max_passes] uint32 device array (may be NULL): spikes per pass
+ *  n_spikes_host, n_passes_host  host outputs
+ *  profile      1: time every stage with CUDA events (into stats->ms)
+ *  stats        host fbp_stage_stats (may be NULL)
+ * Returns FBP_ERR_CAPACITY if spike_cap is too small (n_spikes_host then
+ * holds the number found before the buffer filled), FBP_ERR_ITER_CAP after
+ * max_passes passes without convergence. */
+int fbp_pursuit_chunk(float *voltage, uint32_t n_samples, uint32_t n_chans,
+                      const float *templates, uint32_t n_templates, uint32_t template_len,
+                      const float *neg_half_ss, const float *thresholds,
+                      uint32_t n_max_shift, int do_overlap_recheck, int precision,
+                      uint32_t max_passes, void *workspace, size_t workspace_bytes,
+                      uint32_t *spike_idx, uint32_t *spike_lab, uint32_t spike_cap,
+                      uint32_t *pass_counts, uint32_t *n_spikes_host,
+                      uint32_t *n_passes_host, int profile, fbp_stage_stats *stats,
+                      void *stream);
+
+/* ------------------------------------------------------------------------
+ * Single stages (the reference kernels one by one).
+ * ---------------------------------------------------------------------- */
+
+/* compute_residual, binary_pursuit.cl:57-102: voltage[c, idx+i] -= t[lab,c,i]
+ * for every listed spike, in list order where spikes overlap.  Labels >= K
+ * are skipped, as in the reference.  max_overlap_neighbours bounds how many
+ * list positions apart two overlapping spikes can be (a pass's spikes, one
+ * per window in window order, need 3 + ceil(2*n_max_shift/L)); spikes
+ * farther apart in the list must not overlap. */
+int fbp_compute_residual(float *voltage, uint32_t n_samples, uint32_t n_chans,
+                         const float *templates, uint32_t n_templates, uint32_t template_len,
+                         const uint32_t *spike_idx, const uint32_t *spike_lab,
+                         uint32_t n_spikes, uint32_t max_overlap_neighbours, void *stream);
+
+/* get_adjusted_clips, binary_pursuit.cl:1088-1130: clips[s, c*L+i] =
+ * voltage[c, idx+i] + t[lab,c,i]; entries past the end of the voltage are
+ * left untouched (callers pass zeroed clips, as the reference does). */
+int fbp_get_adjusted_clips(const float *voltage, uint32_t n_samples, uint32_t n_chans,
+                           const float *templates, uint32_t n_templates, uint32_t template_len,
+                           const uint32_t *spike_idx, const uint32_t *spike_lab,
+                           uint32_t n_spikes, float *clips, void *stream);
+
+/* compute_full_likelihood, binary_pursuit.cl:255-300: likelihood[k, s] for
+ * every sample s of every window in window_list (device count n_windows_dev,
+ * a device uint32), 0 where s + L >= n. */
+int fbp_compute_full_likelihood(const float *voltage, uint32_t n_samples, uint32_t n_chans,
+                                const float *templates, uint32_t n_templates,
+                                uint32_t template_len, const float *neg_half_ss,
+                                const uint32_t *window_list, const uint32_t *n_windows_dev,
+                                uint32_t max_windows, float *likelihood, int precision,
+                                void *stream);
+
+/* Per-window state shared by the stage entry points below (all device
+ * arrays of W + FBP_WINDOW_PAD entries). */
+typedef struct fbp_window_state {
+    uint32_t *best_idx;       /* best_spike_indices          */
+    uint32_t *best_lab;       /* best_spike_labels           */
+    float *best_ll;           /* best_spike_likelihoods      */
+    uint32_t *ov_idx;         /* overlap_best_spike_indices  */
+    uint32_t *ov_lab;         /* overlap_best_spike_labels   */
+    uint8_t *flags;           /* check_window_on_next_pass   */
+    uint8_t *overlap_recheck; /* overlap_recheck             */
+} fbp_window_state;
+
+/* compute_template_maximum_likelihood, binary_pursuit.cl:350-441, for all
+ * K templates in template order (the reference's K launches per pass,
+ * binary_pursuit_parallel.py:551-562, fused into one). */
+int fbp_window_argmax(uint32_t n_samples, uint32_t template_len, uint32_t n_templates,
+                      const uint32_t *window_list, const uint32_t *n_windows_dev,
+                      uint32_t max_windows, const fbp_window_state *st,
+                      const float *likelihood, void *stream);
+
+/* overlap_recheck_indices + parse_overlap_recheck_indices,
+ * binary_pursuit.cl:444-815, for the candidate windows in cand_list (device
+ * count n_cand_dev), ascending. */
+int fbp_overlap_recheck(const float *voltage, uint32_t n_samples, uint32_t n_chans,
+                        const float *templates, uint32_t n_templates, uint32_t template_len,
+                        const uint32_t *cand_list, const uint32_t *n_cand_dev,
+                        uint32_t max_cand, const fbp_window_state *st,
+                        const float *likelihood, uint32_t n_max_shift,
+                        const float *thresholds, void *stream);
+
+/* check_overlap_reassignments, binary_pursuit.cl:822-875, for the candidate
+ * windows in cand_list.  scratch: W + FBP_WINDOW_PAD bytes. */
+int fbp_check_overlap_reassignments(uint32_t n_samples, uint32_t template_len,
+                                    const uint32_t *cand_list, const uint32_t *n_cand_dev,
+                                    uint32_t max_cand, const fbp_window_state *st,
+                                    uint8_t *scratch, void *stream);
+
+/* binary_pursuit kernel, binary_pursuit.cl:918-1063: accept spikes of the
+ * windows in window_list, update the flags, append spikes (window order).
+ *  active   [W+pad] uint8, 1 for windows in window_list (others 0)
+ *  has      [W+pad] uint8 scratch
+ *  flags_out[W+pad] uint8: the flags after the kernel (flags in st are read only)
+ *  spike_idx/spike_lab/spike_win [>= number of listed windows] outputs
+ *  n_spikes_dev  device uint32 count of appended spikes
+ *  scan_scratch  fbp_scan_scratch_bytes(W) bytes */
+int fbp_binary_pursuit_accept(uint32_t n_samples, uint32_t n_chans, uint32_t template_len,
+                              const float *thresholds, const uint32_t *window_list,
+                              const uint32_t *n_windows_dev, uint32_t max_windows,
+                              const fbp_window_state *st, const uint8_t *active, uint8_t *has,
+                              uint8_t *flags_out, uint32_t *spike_idx, uint32_t *spike_lab,
+                              uint32_t *spike_win, uint32_t *n_spikes_dev, void *scan_scratch,
+                              void *stream);
+
+/* Scratch bytes the ordered compaction in fbp_binary_pursuit_accept needs. */
+size_t fbp_scan_scratch_bytes(uint32_t n_windows);
+
+/* Bytes of a uint8 per-window array that an ordered compaction reads
+ * (active, has, flags_out): W + FBP_WINDOW_PAD rounded up to 4096. */
+size_t fbp_window_u8_bytes(uint32_t n_windows);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* FBP_B200_H */

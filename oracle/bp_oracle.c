@@ -38,6 +38,15 @@
 typedef uint32_t u32;
 typedef uint8_t u8;
 
+/* Work counters (for profiling the algorithm, not part of its semantics):
+ * [0] likelihood samples x templates evaluated, [1] overlap candidates,
+ * [2] overlap (a, b, t) items that survive the skip rules, [3] passes. */
+static unsigned long long g_counters[8];
+void bpo_counters(unsigned long long *out, int reset)
+{
+    for (int i = 0; i < 8; i++) { out[i] = g_counters[i]; if (reset) g_counters[i] = 0; }
+}
+
 /* compute_maximum_likelihood, binary_pursuit.cl:216-252.  Start from
  * -0.5*SS (already scaled on the host, binary_pursuit_parallel.py:199), then
  * channel-outer, sample-inner accumulation of t*v. */
@@ -64,6 +73,7 @@ void bpo_compute_full_likelihood(const float *v, u32 n, u32 C, const float *T,
 {
     if (C == 0) return;
     long long total = (long long)nwin * K;
+    __atomic_fetch_add(&g_counters[0], (unsigned long long)total * L, __ATOMIC_RELAXED);
 #pragma omp parallel for schedule(dynamic, 64) num_threads(nthreads > 0 ? nthreads : 1)
     for (long long g = 0; g < total; g++) {
         u32 w = (u32)(g / K), k = (u32)(g % K);
@@ -161,6 +171,7 @@ void bpo_overlap_recheck(const float *v, u32 n, u32 C, const float *T, u32 K, u3
         if (bidx >= n - L) skip_all = 1;                     /* .cl:524-527 */
         float best_group = best_ll[id];                      /* .cl:690-694 */
         size_t best_item = 0;
+        unsigned long long evaluated = 0;
         if (!skip_all) {
             for (size_t it = 0; it < items; it++) {
                 u32 t = (u32)(it % K);                       /* .cl:530-532 */
@@ -175,9 +186,12 @@ void bpo_overlap_recheck(const float *v, u32 n, u32 C, const float *T, u32 K, u3
                 float ls = Lk[(size_t)t * n + ashift];
                 if (lf <= 0 && ls <= 0) continue;            /* .cl:572-576 */
                 float ll = overlap_pair_ll(v, n, C, T, L, lab, bidx, t, afix, ashift);
+                evaluated++;
                 if (ll > best_group) { best_group = ll; best_item = it; }
             }
         }
+        __atomic_fetch_add(&g_counters[1], 1ULL, __ATOMIC_RELAXED);
+        __atomic_fetch_add(&g_counters[2], evaluated, __ATOMIC_RELAXED);
         /* parse_overlap_recheck_indices, .cl:707-814 */
         if (best_group <= best_ll[id] || best_group <= 0.0f) { ovr[id] = 0; continue; }
         u32 t = (u32)(best_item % K);
@@ -327,6 +341,7 @@ long long bpo_pursuit_chunk(float *v, u32 n, u32 C, const float *T, u32 K, u32 L
     u32 passes = 0;
     for (;;) {
         passes++;
+        g_counters[3]++;
         bpo_compute_full_likelihood(v, n, C, T, K, L, tss, win, nwin, Lk, nthreads);
         bpo_template_maximum_likelihood(n, L, K, win, nwin, best_idx, best_lab, best_ll,
                                         flags, ovr, ov_idx, ov_lab, Lk);

@@ -45,6 +45,7 @@ def lib():
         L.bpo_binary_pursuit.restype = U
         L.bpo_binary_pursuit.argtypes = [U, U, U, f32p, u32p, U, u32p, u32p, f32p, u32p, u32p, u8p, u8p]
         L.bpo_compute_residual.argtypes = [f32p, U, U, f32p, U, U, u32p, u32p, U]
+        L.bpo_counters.argtypes = [ctypes.POINTER(ctypes.c_ulonglong), ctypes.c_int]
         L.bpo_get_adjusted_clips.argtypes = [f32p, U, U, f32p, U, U, u32p, u32p, U, f32p]
         _lib = L
     return _lib
@@ -75,6 +76,62 @@ def pursuit_chunk(chunk_v, templates_vec, K, L, tss, thr, n_max_shift, do_overla
             raise MemoryError("oracle allocation failed")
         chunk_v[...] = work
         return out_i[:r].copy(), out_l[:r].copy(), passes.value, pc[:min(passes.value, max_passes)].copy()
+
+
+# --- single stages (restated kernels), for stage-level parity tests --------
+
+def stage_full_likelihood(v, T, K, L, tss, win, Lk, nthreads=4):
+    C, n = v.shape
+    lib().bpo_compute_full_likelihood(np.ascontiguousarray(v, np.float32).reshape(-1), n, C, T, K, L,
+                                      tss, np.ascontiguousarray(win, np.uint32), len(win), Lk.reshape(-1),
+                                      nthreads)
+
+
+def stage_template_max(n, L, K, win, st, Lk):
+    lib().bpo_template_maximum_likelihood(n, L, K, np.ascontiguousarray(win, np.uint32), len(win),
+                                          st["best_idx"], st["best_lab"], st["best_ll"], st["flags"],
+                                          st["ovr"], st["ov_idx"], st["ov_lab"], Lk.reshape(-1))
+
+
+def stage_overlap(v, T, K, L, cand, st, Lk, nmax, thr, nthreads=4):
+    C, n = v.shape
+    lib().bpo_overlap_recheck(np.ascontiguousarray(v, np.float32).reshape(-1), n, C, T, K, L,
+                              np.ascontiguousarray(cand, np.uint32), len(cand), st["best_idx"],
+                              st["best_lab"], st["best_ll"], st["ov_idx"], st["ov_lab"], Lk.reshape(-1),
+                              nmax, thr, st["ovr"], nthreads)
+
+
+def stage_check_overlap(n, L, cand, st):
+    lib().bpo_check_overlap_reassignments(n, L, np.ascontiguousarray(cand, np.uint32), len(cand),
+                                          st["best_idx"], st["best_lab"], st["flags"], st["ov_idx"],
+                                          st["ov_lab"], st["ovr"])
+
+
+def stage_accept(n, C, L, thr, win, st):
+    W = len(st["flags"])
+    oi = np.zeros(W, np.uint32)
+    ol = np.zeros(W, np.uint32)
+    cnt = lib().bpo_binary_pursuit(n, C, L, thr, np.ascontiguousarray(win, np.uint32), len(win),
+                                   st["best_idx"], st["best_lab"], st["best_ll"], oi, ol, st["ovr"],
+                                   st["flags"])
+    return oi[:cnt], ol[:cnt]
+
+
+def stage_residual(v, T, K, L, idx, lab):
+    C, n = v.shape
+    flat = np.ascontiguousarray(v, np.float32).reshape(-1).copy()
+    lib().bpo_compute_residual(flat, n, C, T, K, L, np.ascontiguousarray(idx, np.uint32),
+                               np.ascontiguousarray(lab, np.uint32), len(idx))
+    return flat.reshape(C, n)
+
+
+def counters(reset=True):
+    """Work counters: likelihood sample*templates, overlap candidates,
+    overlap items surviving the skip rules, passes."""
+    out = (ctypes.c_ulonglong * 8)()
+    lib().bpo_counters(out, int(reset))
+    return {"likelihood_st": out[0], "overlap_candidates": out[1],
+            "overlap_items": out[2], "passes": out[3]}
 
 
 def adjusted_clips(resid_v, templates_vec, K, L, idx, lab):
@@ -153,7 +210,10 @@ def binary_pursuit_oracle(voltage, v_dtype, sort_info, separability_metrics,
         event_indices += clip_init_samples
     else:
         event_indices, neuron_labels, bp_bool, adjusted = [], [], [], []
-    separability_metrics["n_spikes"] = np.zeros(K)
-    for k in range(K):
+    # add_n_spikes (neuron_separability.py:264-273) sizes the array by the
+    # dict's templates entry, so 1-D templates give C*L entries.
+    nt = separability_metrics["templates"].shape[0]
+    separability_metrics["n_spikes"] = np.zeros(nt)
+    for k in range(nt):
         separability_metrics["n_spikes"][k] = np.count_nonzero(neuron_labels == k)
     return event_indices, neuron_labels, bp_bool, adjusted

@@ -1,0 +1,525 @@
+// C ABI and per-chunk driver of the Full Binary Pursuit library (sm_100a).
+//
+// fbp_pursuit_chunk replaces the iterate-until-converged loop of the
+// reference host driver (spikesorting_fullpursuit/parallel/
+// binary_pursuit_parallel.py:386-736): the window lists that the reference
+// builds on the host with np.nonzero after every pass are compacted on the
+// device, and the host reads back one count per pass.
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "../../include/fbp_b200.h"
+#include "fbp_kernels.cuh"
+
+using namespace fbp;
+
+namespace {
+
+thread_local std::string g_last_error;
+
+int fail(int code, const char *fmt, ...) {
+    char buf[512];
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(buf, sizeof(buf), fmt, ap);
+    va_end(ap);
+    g_last_error = buf;
+    return code;
+}
+
+#define FBP_CUDA(call)                                                                     \
+    do {                                                                                   \
+        cudaError_t e_ = (call);                                                           \
+        if (e_ != cudaSuccess)                                                             \
+            return fail(FBP_ERR_CUDA, "%s failed: %s", #call, cudaGetErrorString(e_));     \
+    } while (0)
+
+#define FBP_LAUNCH_CHECK()                                                                 \
+    do {                                                                                   \
+        cudaError_t e_ = cudaGetLastError();                                               \
+        if (e_ != cudaSuccess)                                                             \
+            return fail(FBP_ERR_CUDA, "kernel launch failed at %s:%d: %s", __FILE__,       \
+                        __LINE__, cudaGetErrorString(e_));                                 \
+    } while (0)
+
+int sm_count() {
+    static int cached = 0;
+    if (!cached) {
+        int dev = 0;
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&cached, cudaDevAttrMultiProcessorCount, dev);
+        if (cached <= 0) cached = 148;
+    }
+    return cached;
+}
+
+// Device workspace of one chunk: sub-buffers at 256-byte boundaries.
+struct Workspace {
+    float *Lk;
+    u32 *best_idx, *best_lab, *ov_idx, *ov_lab, *win, *cand, *acc_list;
+    u32 *spk_idx, *spk_lab, *spk_win, *tile_counts;
+    float *best_ll;
+    u8 *flags, *flags_out, *ovr, *ovr2, *active, *has;
+    Counters *cnt;
+    size_t bytes;
+};
+
+size_t window_bytes_u8(u32 W) { return align_up((size_t)W + FBP_WINDOW_PAD, kCompactTile); }
+
+Workspace layout(char *base, u32 n, u32 K, u32 L) {
+    Workspace w{};
+    const u32 W = ceil_div(n, L);
+    const size_t Wp = (size_t)W + FBP_WINDOW_PAD;
+    size_t off = 0;
+    auto take = [&](size_t bytes) {
+        char *p = base ? base + off : nullptr;
+        off = align_up(off + bytes, 256);
+        return p;
+    };
+    w.cnt = (Counters *)take(sizeof(Counters));
+    w.Lk = (float *)take((size_t)K * n * sizeof(float));
+    w.best_idx = (u32 *)take(Wp * 4);
+    w.best_lab = (u32 *)take(Wp * 4);
+    w.best_ll = (float *)take(Wp * 4);
+    w.ov_idx = (u32 *)take(Wp * 4);
+    w.ov_lab = (u32 *)take(Wp * 4);
+    w.win = (u32 *)take(Wp * 4);
+    w.cand = (u32 *)take(Wp * 4);
+    w.acc_list = (u32 *)take(Wp * 4);
+    w.spk_idx = (u32 *)take(Wp * 4);
+    w.spk_lab = (u32 *)take(Wp * 4);
+    w.spk_win = (u32 *)take(Wp * 4);
+    w.tile_counts = (u32 *)take((size_t)(ceil_div(W, kCompactTile) + 1) * 4);
+    const size_t wb = window_bytes_u8(W);
+    w.flags = (u8 *)take(wb);
+    w.flags_out = (u8 *)take(wb);
+    w.ovr = (u8 *)take(wb);
+    w.ovr2 = (u8 *)take(wb);
+    w.active = (u8 *)take(wb);
+    w.has = (u8 *)take(wb);
+    w.bytes = off;
+    return w;
+}
+
+int grid_for(u64 items, int threads, int per_sm = 8) {
+    u64 b = (items + threads - 1) / threads;
+    u64 cap = (u64)sm_count() * per_sm;
+    if (b > cap) b = cap;
+    if (b < 1) b = 1;
+    return (int)b;
+}
+
+// Ordered compaction of f[0..W) into list; count written to *count_dev.
+int compact(const u8 *f, u32 W, u32 *list, u32 *count_dev, u32 *tile_counts, cudaStream_t st) {
+    const u32 tiles = ceil_div(W, kCompactTile);
+    if (tiles == 0) {
+        FBP_CUDA(cudaMemsetAsync(count_dev, 0, 4, st));
+        return FBP_OK;
+    }
+    k_compact_count<<<tiles, kCompactThreads, 0, st>>>(f, W, tile_counts);
+    k_compact_scan<<<1, kCompactThreads, 0, st>>>(tile_counts, tiles, count_dev);
+    k_compact_write<<<tiles, kCompactThreads, 0, st>>>(f, W, tile_counts, list);
+    FBP_LAUNCH_CHECK();
+    return FBP_OK;
+}
+
+int launch_likelihood(const float *v, u32 n, u32 C, const float *T, u32 K, u32 L, const float *tss,
+                      const u32 *win, const u32 *n_win_dev, u32 max_windows, float *Lk,
+                      cudaStream_t st) {
+    const size_t smem = (size_t)kLikChanChunk * (kLikTile + L) * sizeof(float);
+    static size_t configured = 0;
+    if (smem > 48 * 1024 && smem > configured) {
+        FBP_CUDA(cudaFuncSetAttribute(k_likelihood_fp32, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                      (int)smem));
+        configured = smem;
+    }
+    const u64 items = (u64)max_windows * ceil_div(K, kLikTplPerBlock);
+    const int grid = grid_for(items * kLikThreads, kLikThreads, 16);
+    k_likelihood_fp32<<<grid, kLikThreads, smem, st>>>(v, n, C, T, K, L, tss, win, n_win_dev, Lk);
+    FBP_LAUNCH_CHECK();
+    return FBP_OK;
+}
+
+int launch_argmax(u32 n, u32 L, u32 K, const u32 *win, const u32 *n_win_dev, u32 max_windows,
+                  const fbp_window_state &s, const float *Lk, cudaStream_t st) {
+    const int threads = 256;
+    const int grid = grid_for((u64)max_windows * 32, threads, 8);
+    k_window_argmax<<<grid, threads, 0, st>>>(n, L, K, win, n_win_dev, s.best_idx, s.best_lab, s.best_ll,
+                                              s.flags, s.overlap_recheck, s.ov_idx, s.ov_lab, Lk);
+    FBP_LAUNCH_CHECK();
+    return FBP_OK;
+}
+
+int launch_overlap(const float *v, u32 n, u32 C, const float *T, u32 K, u32 L, const u32 *cand,
+                   const u32 *n_cand_dev, u32 max_cand, const fbp_window_state &s, const float *Lk,
+                   u32 nmax, const float *thr, u64 *items_evaluated, cudaStream_t st) {
+    const size_t smem = (size_t)2 * C * L * sizeof(float);
+    if (smem > 227 * 1024)
+        return fail(FBP_ERR_BAD_ARG, "overlap recheck: C*L = %u too large for shared memory", C * L);
+    static size_t configured = 0;
+    if (smem > 48 * 1024 && smem > configured) {
+        FBP_CUDA(cudaFuncSetAttribute(k_overlap_exact, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                      (int)smem));
+        configured = smem;
+    }
+    const int grid = grid_for((u64)max_cand * kOvThreads, kOvThreads, 4);
+    k_overlap_exact<<<grid, kOvThreads, smem, st>>>(v, n, C, T, K, L, cand, n_cand_dev, s.best_idx,
+                                                    s.best_lab, s.best_ll, s.ov_idx, s.ov_lab,
+                                                    s.overlap_recheck, Lk, nmax, thr, items_evaluated);
+    FBP_LAUNCH_CHECK();
+    return FBP_OK;
+}
+
+int launch_check_overlap(u32 n, u32 L, const u32 *cand, const u32 *n_cand_dev, u32 max_cand,
+                         const fbp_window_state &s, u8 *scratch, cudaStream_t st) {
+    const int threads = 256;
+    const int grid = grid_for(max_cand, threads, 8);
+    k_check_overlap<<<grid, threads, 0, st>>>(n, L, cand, n_cand_dev, s.best_idx, s.best_lab, s.flags,
+                                              s.ov_idx, s.ov_lab, s.overlap_recheck, scratch);
+    k_copy_ovr<<<grid, threads, 0, st>>>(cand, n_cand_dev, scratch, s.overlap_recheck);
+    FBP_LAUNCH_CHECK();
+    return FBP_OK;
+}
+
+int launch_accept(u32 n, u32 C, u32 L, const float *thr, const u32 *win, const u32 *n_win_dev,
+                  u32 max_windows, const fbp_window_state &s, const u8 *active, u8 *has, u8 *flags_out,
+                  u32 *acc_list, u32 *spk_idx, u32 *spk_lab, u32 *spk_win, u32 *n_spk_dev,
+                  u32 *tile_counts, cudaStream_t st) {
+    const u32 W = ceil_div(n, L);
+    const int threads = 256;
+    FBP_CUDA(cudaMemsetAsync(has, 0, window_bytes_u8(W), st));
+    k_accept_has<<<grid_for(max_windows, threads), threads, 0, st>>>(
+        n, C, L, thr, win, n_win_dev, s.best_idx, s.best_lab, s.best_ll, s.overlap_recheck, has);
+    AcceptView a{n, C, L, W, n / L, thr, s.best_idx, s.best_lab, s.best_ll, active, has, s.flags};
+    k_accept_flags<<<grid_for(W, threads), threads, 0, st>>>(a, flags_out);
+    FBP_LAUNCH_CHECK();
+    int rc = compact(has, W, acc_list, n_spk_dev, tile_counts, st);
+    if (rc) return rc;
+    k_gather_spikes<<<grid_for(W, threads), threads, 0, st>>>(n, C, L, acc_list, n_spk_dev, s.best_idx,
+                                                              s.best_lab, spk_idx, spk_lab, spk_win);
+    FBP_LAUNCH_CHECK();
+    return FBP_OK;
+}
+
+// CUDA-event timing of the stages of a pass.  Events come from a pool that
+// is drained after every host synchronisation (collect()).
+class StageTimer {
+  public:
+    StageTimer(bool on, cudaStream_t st, fbp_stage_stats *s) : on_(on), st_(st), s_(s) {}
+    ~StageTimer() {
+        for (auto &e : pool_) cudaEventDestroy(e);
+    }
+    void begin(int stage) {
+        if (!on_) return;
+        cur_stage_ = stage;
+        cur_begin_ = next();
+        cudaEventRecord(cur_begin_, st_);
+    }
+    void end(int stage) {
+        if (!on_) return;
+        cudaEvent_t e = next();
+        cudaEventRecord(e, st_);
+        pending_.push_back({stage, cur_begin_, e});
+    }
+    void collect() {
+        if (!on_) return;
+        for (auto &p : pending_) {
+            float ms = 0.f;
+            if (cudaEventElapsedTime(&ms, p.b, p.e) == cudaSuccess) s_->ms[p.stage] += ms;
+        }
+        pending_.clear();
+        used_ = 0;
+    }
+
+  private:
+    struct Pending { int stage; cudaEvent_t b, e; };
+    cudaEvent_t next() {
+        if (used_ == pool_.size()) {
+            cudaEvent_t e;
+            cudaEventCreate(&e);
+            pool_.push_back(e);
+        }
+        return pool_[used_++];
+    }
+    bool on_;
+    cudaStream_t st_;
+    fbp_stage_stats *s_;
+    std::vector<cudaEvent_t> pool_;
+    std::vector<Pending> pending_;
+    size_t used_ = 0;
+    int cur_stage_ = 0;
+    cudaEvent_t cur_begin_ = nullptr;
+};
+
+u32 overlap_neighbours(u32 L, u32 nmax) {
+    // spikes of one pass lie within n_max_shift of their window; two of them
+    // can overlap only if their windows are fewer than 2 + 2*nmax/L apart.
+    return 3 + ceil_div(2 * nmax, L);
+}
+
+}  // namespace
+
+extern "C" {
+
+int fbp_version(void) { return 100; }
+
+const char *fbp_last_error(void) { return g_last_error.c_str(); }
+
+size_t fbp_scan_scratch_bytes(uint32_t n_windows) {
+    return (size_t)(ceil_div(n_windows, kCompactTile) + 1) * 4;
+}
+
+size_t fbp_window_u8_bytes(uint32_t n_windows) { return window_bytes_u8(n_windows); }
+
+int fbp_pursuit_workspace_bytes(uint32_t n, uint32_t C, uint32_t K, uint32_t L, uint32_t nmax,
+                                int precision, size_t *bytes_out) {
+    if (!bytes_out || n == 0 || C == 0 || K == 0 || L == 0)
+        return fail(FBP_ERR_BAD_ARG, "workspace size: bad arguments");
+    (void)nmax;
+    (void)precision;
+    *bytes_out = layout(nullptr, n, K, L).bytes;
+    return FBP_OK;
+}
+
+int fbp_pursuit_chunk(float *voltage, uint32_t n, uint32_t C, const float *templates, uint32_t K,
+                      uint32_t L, const float *neg_half_ss, const float *thresholds, uint32_t nmax,
+                      int do_overlap_recheck, int precision, uint32_t max_passes, void *workspace,
+                      size_t workspace_bytes, uint32_t *spike_idx, uint32_t *spike_lab,
+                      uint32_t spike_cap, uint32_t *pass_counts, uint32_t *n_spikes_host,
+                      uint32_t *n_passes_host, int profile, fbp_stage_stats *stats, void *stream) {
+    g_last_error.clear();
+    if (!voltage || !templates || !neg_half_ss || !thresholds || !workspace || !spike_idx ||
+        !spike_lab || !n_spikes_host || !n_passes_host)
+        return fail(FBP_ERR_BAD_ARG, "fbp_pursuit_chunk: null pointer argument");
+    if (n == 0 || C == 0 || K == 0 || L == 0)
+        return fail(FBP_ERR_BAD_ARG, "fbp_pursuit_chunk: zero size (n=%u C=%u K=%u L=%u)", n, C, K, L);
+    if (precision != FBP_PREC_FP32 && precision != FBP_PREC_BF16_REFINE)
+        return fail(FBP_ERR_BAD_ARG, "fbp_pursuit_chunk: unknown precision %d", precision);
+    if ((u64)2 * nmax + 1 > 0xffffffffull)
+        return fail(FBP_ERR_BAD_ARG, "fbp_pursuit_chunk: n_max_shift too large");
+    Workspace w = layout((char *)workspace, n, K, L);
+    if (workspace_bytes < w.bytes)
+        return fail(FBP_ERR_BAD_ARG, "fbp_pursuit_chunk: workspace has %zu bytes, needs %zu",
+                    workspace_bytes, w.bytes);
+    cudaStream_t st = (cudaStream_t)stream;
+    const u32 W = ceil_div(n, L);
+    const size_t Wp = (size_t)W + FBP_WINDOW_PAD;
+    const size_t wb = window_bytes_u8(W);
+    fbp_window_state s{w.best_idx, w.best_lab, w.best_ll, w.ov_idx, w.ov_lab, w.flags, w.ovr};
+    fbp_stage_stats local_stats;
+    fbp_stage_stats &S = stats ? *stats : local_stats;
+    memset(&S, 0, sizeof(S));
+    StageTimer timer(profile != 0, st, &S);
+
+    // reference buffers start zeroed (.py:387, :412-423)
+    timer.begin(FBP_STAGE_LISTS);
+    FBP_CUDA(cudaMemsetAsync(w.cnt, 0, sizeof(Counters), st));
+    FBP_CUDA(cudaMemsetAsync(w.Lk, 0, (size_t)K * n * sizeof(float), st));
+    FBP_CUDA(cudaMemsetAsync(w.best_idx, 0, Wp * 4, st));
+    FBP_CUDA(cudaMemsetAsync(w.best_lab, 0, Wp * 4, st));
+    FBP_CUDA(cudaMemsetAsync(w.best_ll, 0, Wp * 4, st));
+    FBP_CUDA(cudaMemsetAsync(w.ov_idx, 0, Wp * 4, st));
+    FBP_CUDA(cudaMemsetAsync(w.ov_lab, 0, Wp * 4, st));
+    FBP_CUDA(cudaMemsetAsync(w.flags, 0, wb, st));
+    FBP_CUDA(cudaMemsetAsync(w.ovr, 0, wb, st));
+    FBP_CUDA(cudaMemsetAsync(w.ovr2, 0, wb, st));
+    FBP_CUDA(cudaMemsetAsync(w.active, 0, wb, st));
+    k_iota_windows<<<grid_for(W, 256), 256, 0, st>>>(w.win, w.active, W, w.cnt);
+    FBP_LAUNCH_CHECK();
+    S.launches[FBP_STAGE_LISTS] += 1;
+    timer.end(FBP_STAGE_LISTS);
+
+    u32 *h_counts = nullptr;
+    FBP_CUDA(cudaMallocHost(&h_counts, sizeof(Counters)));
+    const u32 R = overlap_neighbours(L, nmax);
+    int rc = FBP_OK;
+    u32 passes = 0;
+    for (;;) {
+        if (passes >= max_passes) { rc = fail(FBP_ERR_ITER_CAP, "no convergence after %u passes", passes); break; }
+        passes++;
+        // 1. likelihood over the listed windows (.py:538-549)
+        timer.begin(FBP_STAGE_LIKELIHOOD);
+        if ((rc = launch_likelihood(voltage, n, C, templates, K, L, neg_half_ss, w.win, &w.cnt->n_win, W,
+                                    w.Lk, st)))
+            break;
+        S.launches[FBP_STAGE_LIKELIHOOD] += 1;
+        timer.end(FBP_STAGE_LIKELIHOOD);
+        // 2. per-window argmax over all templates (.py:551-562)
+        timer.begin(FBP_STAGE_ARGMAX);
+        if ((rc = launch_argmax(n, L, K, w.win, &w.cnt->n_win, W, s, w.Lk, st))) break;
+        S.launches[FBP_STAGE_ARGMAX] += 1;
+        timer.end(FBP_STAGE_ARGMAX);
+        // 3. candidates = nonzero(overlap_recheck) (.py:565-569), 4. recheck (.py:570-661)
+        if (do_overlap_recheck) {
+            timer.begin(FBP_STAGE_LISTS);
+            if ((rc = compact(w.ovr, W, w.cand, &w.cnt->n_cand, w.tile_counts, st))) break;
+            S.launches[FBP_STAGE_LISTS] += 3;
+            timer.end(FBP_STAGE_LISTS);
+            timer.begin(FBP_STAGE_OVERLAP);
+            if ((rc = launch_overlap(voltage, n, C, templates, K, L, w.cand, &w.cnt->n_cand, W, s, w.Lk,
+                                     nmax, thresholds, &w.cnt->ov_items, st)))
+                break;
+            S.launches[FBP_STAGE_OVERLAP] += 1;
+            timer.end(FBP_STAGE_OVERLAP);
+            timer.begin(FBP_STAGE_CHECK);
+            if ((rc = launch_check_overlap(n, L, w.cand, &w.cnt->n_cand, W, s, w.ovr2, st))) break;
+            S.launches[FBP_STAGE_CHECK] += 2;
+            timer.end(FBP_STAGE_CHECK);
+        }
+        // 5. accept (.py:663-671)
+        timer.begin(FBP_STAGE_ACCEPT);
+        if ((rc = launch_accept(n, C, L, thresholds, w.win, &w.cnt->n_win, W, s, w.active, w.has,
+                                w.flags_out, w.acc_list, w.spk_idx, w.spk_lab, w.spk_win, &w.cnt->n_spk,
+                                w.tile_counts, st)))
+            break;
+        S.launches[FBP_STAGE_ACCEPT] += 6;
+        timer.end(FBP_STAGE_ACCEPT);
+        // 6. count; stop when nothing was added (.py:673-676)
+        FBP_CUDA(cudaMemcpyAsync(h_counts, w.cnt, sizeof(Counters), cudaMemcpyDeviceToHost, st));
+        FBP_CUDA(cudaStreamSynchronize(st));
+        timer.collect();
+        const u32 added = h_counts[2];
+        const u32 nwin = h_counts[0];
+        S.work[FBP_STAGE_LIKELIHOOD] += (u64)nwin * L * K;
+        S.work[FBP_STAGE_ARGMAX] += (u64)nwin * 3 * L * K;
+        S.work[FBP_STAGE_ACCEPT] += nwin;
+        if (do_overlap_recheck) {
+            S.work[FBP_STAGE_CHECK] += h_counts[1];
+            S.candidates += h_counts[1];
+        }
+        if (pass_counts)
+            FBP_CUDA(cudaMemcpyAsync(pass_counts + passes - 1, &w.cnt->n_spk, 4, cudaMemcpyDeviceToDevice, st));
+        if (added == 0) break;
+        // 7. reset overlap flags, next list = nonzero(flags), reset flags (.py:678-700)
+        timer.begin(FBP_STAGE_LISTS);
+        FBP_CUDA(cudaMemsetAsync(w.ovr, 0, wb, st));
+        if ((rc = compact(w.flags_out, W, w.win, &w.cnt->n_win, w.tile_counts, st))) break;
+        k_mark_active<<<grid_for(W, 256), 256, 0, st>>>(w.flags_out, w.active, W);
+        FBP_CUDA(cudaMemsetAsync(w.flags, 0, wb, st));
+        // 8. keep the spikes (.py:702-710)
+        k_append_spikes<<<grid_for(added, 256), 256, 0, st>>>(w.spk_idx, w.spk_lab, w.cnt, spike_idx,
+                                                               spike_lab, spike_cap);
+        k_commit_total<<<1, 1, 0, st>>>(w.cnt, spike_cap);
+        FBP_LAUNCH_CHECK();
+        S.launches[FBP_STAGE_LISTS] += 6;
+        timer.end(FBP_STAGE_LISTS);
+        // 9. subtract them (.py:712-731)
+        timer.begin(FBP_STAGE_RESIDUAL);
+        k_residual<<<grid_for((u64)added * 256, 256, 16), 256, 0, st>>>(
+            voltage, n, C, templates, K, L, w.spk_idx, w.spk_lab, nullptr, added, R);
+        FBP_LAUNCH_CHECK();
+        S.launches[FBP_STAGE_RESIDUAL] += 1;
+        S.work[FBP_STAGE_RESIDUAL] += added;
+        timer.end(FBP_STAGE_RESIDUAL);
+    }
+    if (rc == FBP_OK || rc == FBP_ERR_ITER_CAP) {
+        cudaError_t e = cudaMemcpyAsync(h_counts, w.cnt, sizeof(Counters), cudaMemcpyDeviceToHost, st);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+        if (e != cudaSuccess) rc = fail(FBP_ERR_CUDA, "final readback: %s", cudaGetErrorString(e));
+        else {
+            timer.collect();
+            *n_spikes_host = h_counts[3];
+            S.spikes = h_counts[3];
+            S.work[FBP_STAGE_OVERLAP] = *(const u64 *)(h_counts + 8);
+            if (h_counts[4]) rc = fail(FBP_ERR_CAPACITY, "spike output holds %u spikes; more were found", spike_cap);
+        }
+    }
+    *n_passes_host = passes;
+    S.passes = passes;
+    cudaFreeHost(h_counts);
+    return rc;
+}
+
+int fbp_compute_residual(float *voltage, uint32_t n, uint32_t C, const float *templates, uint32_t K,
+                         uint32_t L, const uint32_t *spike_idx, const uint32_t *spike_lab,
+                         uint32_t n_spikes, uint32_t max_overlap_neighbours, void *stream) {
+    g_last_error.clear();
+    if (n_spikes == 0 || C == 0) return FBP_OK;
+    if (!voltage || !templates || !spike_idx || !spike_lab)
+        return fail(FBP_ERR_BAD_ARG, "fbp_compute_residual: null pointer argument");
+    k_residual<<<grid_for((u64)n_spikes * 256, 256, 16), 256, 0, (cudaStream_t)stream>>>(
+        voltage, n, C, templates, K, L, spike_idx, spike_lab, nullptr, n_spikes, max_overlap_neighbours);
+    FBP_LAUNCH_CHECK();
+    return FBP_OK;
+}
+
+int fbp_get_adjusted_clips(const float *voltage, uint32_t n, uint32_t C, const float *templates,
+                           uint32_t K, uint32_t L, const uint32_t *spike_idx, const uint32_t *spike_lab,
+                           uint32_t n_spikes, float *clips, void *stream) {
+    g_last_error.clear();
+    if (n_spikes == 0 || C == 0) return FBP_OK;
+    if (!voltage || !templates || !spike_idx || !spike_lab || !clips)
+        return fail(FBP_ERR_BAD_ARG, "fbp_get_adjusted_clips: null pointer argument");
+    k_adjusted_clips<<<grid_for((u64)n_spikes * 256, 256, 16), 256, 0, (cudaStream_t)stream>>>(
+        voltage, n, C, templates, K, L, spike_idx, spike_lab, n_spikes, clips);
+    FBP_LAUNCH_CHECK();
+    return FBP_OK;
+}
+
+int fbp_compute_full_likelihood(const float *voltage, uint32_t n, uint32_t C, const float *templates,
+                                uint32_t K, uint32_t L, const float *neg_half_ss,
+                                const uint32_t *window_list, const uint32_t *n_windows_dev,
+                                uint32_t max_windows, float *likelihood, int precision, void *stream) {
+    g_last_error.clear();
+    if (!voltage || !templates || !neg_half_ss || !window_list || !n_windows_dev || !likelihood)
+        return fail(FBP_ERR_BAD_ARG, "fbp_compute_full_likelihood: null pointer argument");
+    if (C == 0 || max_windows == 0) return FBP_OK;
+    (void)precision;
+    return launch_likelihood(voltage, n, C, templates, K, L, neg_half_ss, window_list, n_windows_dev,
+                             max_windows, likelihood, (cudaStream_t)stream);
+}
+
+int fbp_window_argmax(uint32_t n, uint32_t L, uint32_t K, const uint32_t *window_list,
+                      const uint32_t *n_windows_dev, uint32_t max_windows, const fbp_window_state *st,
+                      const float *likelihood, void *stream) {
+    g_last_error.clear();
+    if (!st || !window_list || !n_windows_dev || !likelihood)
+        return fail(FBP_ERR_BAD_ARG, "fbp_window_argmax: null pointer argument");
+    if (max_windows == 0) return FBP_OK;
+    return launch_argmax(n, L, K, window_list, n_windows_dev, max_windows, *st, likelihood,
+                         (cudaStream_t)stream);
+}
+
+int fbp_overlap_recheck(const float *voltage, uint32_t n, uint32_t C, const float *templates, uint32_t K,
+                        uint32_t L, const uint32_t *cand_list, const uint32_t *n_cand_dev, uint32_t max_cand,
+                        const fbp_window_state *st, const float *likelihood, uint32_t nmax,
+                        const float *thresholds, void *stream) {
+    g_last_error.clear();
+    if (!voltage || !templates || !cand_list || !n_cand_dev || !st || !likelihood || !thresholds)
+        return fail(FBP_ERR_BAD_ARG, "fbp_overlap_recheck: null pointer argument");
+    if (max_cand == 0) return FBP_OK;
+    return launch_overlap(voltage, n, C, templates, K, L, cand_list, n_cand_dev, max_cand, *st, likelihood,
+                          nmax, thresholds, nullptr, (cudaStream_t)stream);
+}
+
+int fbp_check_overlap_reassignments(uint32_t n, uint32_t L, const uint32_t *cand_list,
+                                    const uint32_t *n_cand_dev, uint32_t max_cand,
+                                    const fbp_window_state *st, uint8_t *scratch, void *stream) {
+    g_last_error.clear();
+    if (!cand_list || !n_cand_dev || !st || !scratch)
+        return fail(FBP_ERR_BAD_ARG, "fbp_check_overlap_reassignments: null pointer argument");
+    if (max_cand == 0) return FBP_OK;
+    return launch_check_overlap(n, L, cand_list, n_cand_dev, max_cand, *st, scratch, (cudaStream_t)stream);
+}
+
+int fbp_binary_pursuit_accept(uint32_t n, uint32_t C, uint32_t L, const float *thresholds,
+                              const uint32_t *window_list, const uint32_t *n_windows_dev,
+                              uint32_t max_windows, const fbp_window_state *st, const uint8_t *active,
+                              uint8_t *has, uint8_t *flags_out, uint32_t *spike_idx, uint32_t *spike_lab,
+                              uint32_t *spike_win, uint32_t *n_spikes_dev, void *scan_scratch,
+                              void *stream) {
+    g_last_error.clear();
+    if (!thresholds || !window_list || !n_windows_dev || !st || !active || !has || !flags_out ||
+        !spike_idx || !spike_lab || !n_spikes_dev || !scan_scratch)
+        return fail(FBP_ERR_BAD_ARG, "fbp_binary_pursuit_accept: null pointer argument");
+    // the compaction list reuses spike_win when given, else spike_idx as scratch is unsafe
+    if (!spike_win) return fail(FBP_ERR_BAD_ARG, "fbp_binary_pursuit_accept: spike_win is required");
+    return launch_accept(n, C, L, thresholds, window_list, n_windows_dev, max_windows, *st, active, has,
+                         flags_out, spike_win, spike_idx, spike_lab, nullptr, n_spikes_dev,
+                         (u32 *)scan_scratch, (cudaStream_t)stream);
+}
+
+}  // extern "C"

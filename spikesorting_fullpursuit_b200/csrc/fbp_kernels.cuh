@@ -1,0 +1,562 @@
+// Full Binary Pursuit kernels for sm_100a.
+//
+// Each kernel restates one kernel of the reference
+// (spikesorting_fullpursuit/kernels/binary_pursuit.cl) with the results a
+// work-group size of 1 gives when work-items run in global-id order.  Where
+// the reference's outcome depends on that order (neighbour flags, the
+// overlap_recheck[id-2] read, overlapping residual subtractions), the order
+// is resolved explicitly so that any thread schedule gives the same answer.
+//
+// Exact-order floating point: the likelihoods are accumulated with
+// __fmul_rn/__fadd_rn (never contracted into FMA) in the reference's order,
+// so every value is bit-identical to the reference's IEEE binary32 result.
+#pragma once
+#include "fbp_common.cuh"
+
+namespace fbp {
+
+// ---------------------------------------------------------------------------
+// Ordered compaction: list of indices j < W with f[j] != 0, ascending.
+// Three launches: per-tile counts, one-block scan of the tile counts, write.
+// f must be readable up to align_up(W, kCompactTile) bytes.
+// ---------------------------------------------------------------------------
+__global__ void k_compact_count(const u8 *__restrict__ f, u32 W, u32 *__restrict__ tile_counts) {
+    const u32 base = blockIdx.x * kCompactTile + threadIdx.x * kCompactPerThread;
+    uint4 q = *reinterpret_cast<const uint4 *>(f + base);
+    const u8 *b = reinterpret_cast<const u8 *>(&q);
+    u32 c = 0;
+#pragma unroll
+    for (u32 i = 0; i < kCompactPerThread; i++) c += (base + i < W && b[i] != 0);
+    u32 tot;
+    block_excl_scan(c, &tot);
+    if (threadIdx.x == 0) tile_counts[blockIdx.x] = tot;
+}
+
+// One block of kCompactThreads threads: exclusive scan of tile_counts in place.
+__global__ void k_compact_scan(u32 *__restrict__ tile_counts, u32 n_tiles, u32 *__restrict__ total_out) {
+    u32 carry = 0;
+    for (u32 base = 0; base < n_tiles; base += kCompactThreads) {
+        u32 i = base + threadIdx.x;
+        u32 v = i < n_tiles ? tile_counts[i] : 0;
+        u32 tot;
+        u32 ex = block_excl_scan(v, &tot);
+        if (i < n_tiles) tile_counts[i] = ex + carry;
+        carry += tot;
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) *total_out = carry;
+}
+
+__global__ void k_compact_write(const u8 *__restrict__ f, u32 W, const u32 *__restrict__ tile_offsets,
+                                u32 *__restrict__ out) {
+    const u32 base = blockIdx.x * kCompactTile + threadIdx.x * kCompactPerThread;
+    uint4 q = *reinterpret_cast<const uint4 *>(f + base);
+    const u8 *b = reinterpret_cast<const u8 *>(&q);
+    u32 c = 0;
+#pragma unroll
+    for (u32 i = 0; i < kCompactPerThread; i++) c += (base + i < W && b[i] != 0);
+    u32 off = tile_offsets[blockIdx.x] + block_excl_scan(c, nullptr);
+#pragma unroll
+    for (u32 i = 0; i < kCompactPerThread; i++)
+        if (base + i < W && b[i] != 0) out[off++] = base + i;
+}
+
+// ---------------------------------------------------------------------------
+// Pass setup.
+// ---------------------------------------------------------------------------
+__global__ void k_iota_windows(u32 *__restrict__ win, u8 *__restrict__ active, u32 W, Counters *cnt) {
+    for (u32 i = blockIdx.x * blockDim.x + threadIdx.x; i < W; i += gridDim.x * blockDim.x) {
+        win[i] = i;
+        active[i] = 1;
+    }
+    if (blockIdx.x == 0 && threadIdx.x == 0) cnt->n_win = W;
+}
+
+// active[j] = (flags[j] != 0) for the next pass.
+__global__ void k_mark_active(const u8 *__restrict__ flags, u8 *__restrict__ active, u32 W) {
+    for (u32 i = blockIdx.x * blockDim.x + threadIdx.x; i < W; i += gridDim.x * blockDim.x)
+        active[i] = flags[i] != 0;
+}
+
+// ---------------------------------------------------------------------------
+// Path (a): full likelihood, exact reference order on the FP32 pipes.
+// compute_full_likelihood / compute_maximum_likelihood, binary_pursuit.cl:216-300.
+//
+// Work item = (listed window, group of 16 templates).  Block = 4 warps; warp
+// q handles templates 4q..4q+3 of the group; lane l handles samples
+// l + 32r (r < 4) of a 128-sample tile starting at the window.  The voltage
+// strip of a channel chunk is staged in shared memory.  Each of the 16
+// accumulators of a thread is an independent chain in (channel, lag) order,
+// starting from float32(-0.5*SS) -- exactly the reference's sequence.
+// ---------------------------------------------------------------------------
+constexpr int kLikThreads = 128;
+constexpr int kLikQ = 4;             // templates per warp
+constexpr int kLikR = 4;             // samples per lane
+constexpr int kLikTile = 32 * kLikR; // 128 samples
+constexpr int kLikTplPerBlock = (kLikThreads / 32) * kLikQ;   // 16
+constexpr int kLikChanChunk = 8;
+
+__global__ void __launch_bounds__(kLikThreads)
+k_likelihood_fp32(const float *__restrict__ v, u32 n, u32 C, const float *__restrict__ T, u32 K, u32 L,
+                  const float *__restrict__ tss, const u32 *__restrict__ win,
+                  const u32 *__restrict__ n_win_dev, float *__restrict__ Lk) {
+    extern __shared__ float strip[];   // kLikChanChunk x (kLikTile + L)
+    const u32 n_win = *n_win_dev;
+    const u32 kgroups = ceil_div(K, kLikTplPerBlock);
+    const u32 stride = kLikTile + L;
+    const u32 lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const u64 total = (u64)n_win * kgroups;
+    for (u64 item = blockIdx.x; item < total; item += gridDim.x) {
+        const u32 w = win[item / kgroups];
+        const u32 kg = (u32)(item % kgroups);
+        const u32 sw = w * L;
+        const u32 ew = min((w + 1) * L, n);
+        const u32 t0 = kg * kLikTplPerBlock + warp * kLikQ;
+        for (u32 s0 = sw; s0 < ew; s0 += kLikTile) {
+            float acc[kLikQ][kLikR];
+#pragma unroll
+            for (int q = 0; q < kLikQ; q++)
+#pragma unroll
+                for (int r = 0; r < kLikR; r++) acc[q][r] = (t0 + q < K) ? tss[t0 + q] : 0.0f;
+            for (u32 c0 = 0; c0 < C; c0 += kLikChanChunk) {
+                const u32 cc = min((u32)kLikChanChunk, C - c0);
+                __syncthreads();
+                for (u32 e = threadIdx.x; e < cc * stride; e += blockDim.x) {
+                    const u32 c = e / stride, x = e % stride;
+                    const u32 g = s0 + x;
+                    strip[c * stride + x] = g < n ? v[(size_t)(c0 + c) * n + g] : 0.0f;
+                }
+                __syncthreads();
+                for (u32 c = 0; c < cc; c++) {
+                    const float *sp = strip + c * stride + lane;
+                    const float *tp[kLikQ];
+#pragma unroll
+                    for (int q = 0; q < kLikQ; q++)
+                        tp[q] = T + ((size_t)min(t0 + q, K - 1) * C + (c0 + c)) * L;
+                    for (u32 i = 0; i < L; i++) {
+                        float tv[kLikQ], vv[kLikR];
+#pragma unroll
+                        for (int q = 0; q < kLikQ; q++) tv[q] = __ldg(tp[q] + i);
+#pragma unroll
+                        for (int r = 0; r < kLikR; r++) vv[r] = sp[32 * r + i];
+#pragma unroll
+                        for (int q = 0; q < kLikQ; q++)
+#pragma unroll
+                            for (int r = 0; r < kLikR; r++)
+                                acc[q][r] = __fadd_rn(acc[q][r], __fmul_rn(tv[q], vv[r]));
+                    }
+                }
+            }
+#pragma unroll
+            for (int q = 0; q < kLikQ; q++) {
+                if (t0 + q >= K) continue;
+#pragma unroll
+                for (int r = 0; r < kLikR; r++) {
+                    const u32 s = s0 + lane + 32 * r;
+                    if (s < ew && s < s0 + kLikTile)
+                        Lk[(size_t)(t0 + q) * n + s] = (s + L >= n) ? 0.0f : acc[q][r];
+                }
+            }
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Path (b): per-window argmax over all templates.
+// compute_template_maximum_likelihood, binary_pursuit.cl:350-441, with the K
+// per-template launches fused: one warp per listed window walks templates in
+// order; within a template the warp finds the first sample holding the
+// template's maximum, and the running best is replaced only on a strictly
+// larger value -- the sequential scan's result.
+// ---------------------------------------------------------------------------
+__global__ void k_window_argmax(u32 n, u32 L, u32 K, const u32 *__restrict__ win,
+                                const u32 *__restrict__ n_win_dev, u32 *__restrict__ best_idx,
+                                u32 *__restrict__ best_lab, float *__restrict__ best_ll,
+                                u8 *__restrict__ flags, u8 *__restrict__ ovr,
+                                u32 *__restrict__ ov_idx, u32 *__restrict__ ov_lab,
+                                const float *__restrict__ Lk) {
+    const u32 n_win = *n_win_dev;
+    const u32 lane = threadIdx.x & 31;
+    const u32 warps_per_block = blockDim.x >> 5;
+    for (u32 g = blockIdx.x * warps_per_block + (threadIdx.x >> 5); g < n_win;
+         g += gridDim.x * warps_per_block) {
+        const u32 id = win[g];
+        const u32 sw = id * L, ew = (id + 1) * L;
+        const u32 start = (L > sw) ? 0 : sw - L;
+        const u32 stop = (ew + L) > n ? n : ew + L;
+        if (ew >= n - L) continue;                       // .cl:380-383
+        float bl = 0.0f;                                 // .cl:389-393 (template 0 resets)
+        u32 blab = best_lab[id], bidx = best_idx[id];
+        bool check = false;
+        for (u32 t = 0; t < K; t++) {
+            const float *row = Lk + (size_t)t * n;
+            float lv = -INFINITY;
+            u32 li = 0xffffffffu;
+            for (u32 s = start + lane; s < stop; s += 32) {
+                const float cur = row[s];
+                if (cur > lv) { lv = cur; li = s; }
+                check |= (cur > 0.0f) && s >= sw && s < ew;
+            }
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) {
+                const float ov = __shfl_xor_sync(0xffffffffu, lv, o);
+                const u32 oi = __shfl_xor_sync(0xffffffffu, li, o);
+                if (ov > lv || (ov == lv && oi < li)) { lv = ov; li = oi; }
+            }
+            if (lv > bl) { bl = lv; blab = t; bidx = li; }
+        }
+        check = __any_sync(0xffffffffu, check);
+        if (lane == 0) {
+            if (check) flags[id] = 1;                    // .cl:419-422
+            ovr[id] = (bl > 0.0f && bidx >= sw && bidx < ew) ? 1 : 0;   // .cl:423-433
+            best_ll[id] = bl; best_lab[id] = blab; best_idx[id] = bidx;
+            ov_idx[id] = bidx; ov_lab[id] = blab;        // .cl:435-439
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Overlap recheck, exact: overlap_recheck_indices + parse_overlap_recheck_indices
+// (binary_pursuit.cl:444-815).  One block per candidate window; every
+// (a, b, t) item is evaluated in the reference's order of operations; the
+// block keeps the first item (lowest id) with the largest likelihood above
+// the window's current best, which is what the parse kernel's strict-greater
+// scan over single-item groups returns.
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ float overlap_pair_exact(const float *__restrict__ vwin,   // [C][L] at bidx
+                                                    const float *__restrict__ tk0,    // [C][L]
+                                                    const float *__restrict__ tt,     // [C][L]
+                                                    u32 C, u32 L, int fa, int sa) {
+    float cml = 0.0f;
+    const u32 ffj = fa < 0 ? (u32)(-fa) : 0u;
+    const u32 sfj = sa < 0 ? (u32)(-sa) : 0u;
+    for (u32 c = 0; c < C; c++) {
+        const float *f = tk0 + (size_t)c * L;
+        const float *s = tt + (size_t)c * L;
+        const float *vv = vwin + (size_t)c * L;
+        float ss = 0.0f;
+        for (u32 j = 0; j < L; j++) {
+            float fv = 0.0f, sv = 0.0f;
+            if (j >= ffj && (u32)(fa + (int)j) < L) fv = f[fa + (int)j];
+            if (j >= sfj && (u32)(sa + (int)j) < L) sv = __ldg(s + sa + (int)j);
+            const float sum = __fadd_rn(fv, sv);
+            ss = __fadd_rn(ss, __fmul_rn(sum, sum));
+            cml = __fadd_rn(cml, __fmul_rn(sum, vv[j]));
+        }
+        if ((double)ss > 0.0)                                          // .cl:627-630
+            cml = __double2float_rn(__dsub_rn((double)cml, __dmul_rn(0.5, (double)ss)));
+    }
+    return cml;
+}
+
+// parse_overlap_recheck_indices' decision, binary_pursuit.cl:707-814, given
+// the winning item (best_group > best_ll[id] already established or not).
+__device__ __forceinline__ void overlap_parse(u32 id, u32 n, u32 K, u32 S, u32 nmax, float best_group,
+                                              u64 best_item, u32 *best_idx, u32 *best_lab,
+                                              float *best_ll, u32 *ov_idx, u32 *ov_lab, u8 *ovr,
+                                              const float *Lk, const float *thr) {
+    if (best_group <= best_ll[id] || best_group <= 0.0f) { ovr[id] = 0; return; }
+    const u32 lab = best_lab[id], bidx = best_idx[id];
+    const u32 t = (u32)(best_item % K);
+    const u32 a = (u32)((best_item / K) % S);
+    const u32 b = (u32)((best_item / ((u64)S * K)) % S);
+    const u32 afix = bidx + a - nmax, ashift = bidx + b - nmax;
+    const float lf = Lk[(size_t)lab * n + afix];
+    const float ls = Lk[(size_t)t * n + ashift];
+    if (best_group < lf || best_group < ls) { ovr[id] = 0; return; }
+    if (lf <= 0.0f || ls <= 0.0f) { ovr[id] = 0; return; }
+    if (lf >= ls && lf > thr[lab]) {
+        best_ll[id] = lf; ov_lab[id] = lab; ov_idx[id] = afix;
+    } else if (ls > lf && ls > thr[t]) {
+        best_ll[id] = ls; ov_lab[id] = t; ov_idx[id] = ashift;
+    } else if (lf > thr[lab]) {
+        best_ll[id] = lf; ov_lab[id] = lab; ov_idx[id] = afix;
+    } else {
+        ov_idx[id] = best_idx[id]; ov_lab[id] = best_lab[id]; ovr[id] = 0;
+    }
+}
+
+constexpr int kOvThreads = 256;
+
+__global__ void __launch_bounds__(kOvThreads)
+k_overlap_exact(const float *__restrict__ v, u32 n, u32 C, const float *__restrict__ T, u32 K, u32 L,
+                const u32 *__restrict__ cand, const u32 *__restrict__ n_cand_dev,
+                u32 *__restrict__ best_idx, u32 *__restrict__ best_lab, float *__restrict__ best_ll,
+                u32 *__restrict__ ov_idx, u32 *__restrict__ ov_lab, u8 *__restrict__ ovr,
+                const float *__restrict__ Lk, u32 nmax, const float *__restrict__ thr,
+                u64 *__restrict__ items_evaluated) {
+    extern __shared__ float sm[];          // vwin [C*L], tk0 [C*L]
+    __shared__ float red_v[kOvThreads / 32];
+    __shared__ u64 red_i[kOvThreads / 32];
+    const u32 n_cand = *n_cand_dev;
+    const u32 S = 2 * nmax + 1;
+    const u64 items = (u64)S * S * K;
+    float *vwin = sm, *tk0 = sm + (size_t)C * L;
+    for (u32 g = blockIdx.x; g < n_cand; g += gridDim.x) {
+        const u32 id = cand[g];
+        const u32 lab = best_lab[id], bidx = best_idx[id];
+        const float start_ll = best_ll[id];
+        const float bll = Lk[(size_t)lab * n + bidx];
+        const bool skip_all = (bll < thr[lab]) || (bidx >= n - L);   // .cl:518-527
+        float bv = start_ll;
+        u64 bi = ~0ull;
+        u32 evaluated = 0;
+        __syncthreads();
+        if (!skip_all) {
+            for (u32 e = threadIdx.x; e < C * L; e += blockDim.x) {
+                const u32 c = e / L, j = e % L;
+                vwin[e] = v[(size_t)c * n + bidx + j];
+                tk0[e] = T[(size_t)lab * C * L + e];
+            }
+        }
+        __syncthreads();
+        if (!skip_all) {
+            for (u64 it = threadIdx.x; it < items; it += blockDim.x) {
+                const u32 t = (u32)(it % K);
+                const u32 a = (u32)((it / K) % S);
+                const u32 b = (u32)((it / ((u64)S * K)) % S);
+                if (a + bidx < nmax || a + bidx >= n - L + nmax) continue;   // .cl:534-537
+                if (b + bidx < nmax || b + bidx >= n - L + nmax) continue;   // .cl:538-541
+                if (a > b && a - b > L) continue;                             // .cl:543-549
+                if (b > a && b - a > L) continue;                             // .cl:550-556
+                const u32 afix = bidx + a - nmax, ashift = bidx + b - nmax;
+                const float lf = Lk[(size_t)lab * n + afix];
+                const float ls = Lk[(size_t)t * n + ashift];
+                if (lf <= 0.0f && ls <= 0.0f) continue;                       // .cl:572-576
+                const float ll = overlap_pair_exact(vwin, tk0, T + (size_t)t * C * L, C, L,
+                                                    (int)bidx - (int)afix, (int)bidx - (int)ashift);
+                evaluated++;
+                if (ll > bv) { bv = ll; bi = it; }
+            }
+        }
+        if (items_evaluated) {
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) evaluated += __shfl_xor_sync(0xffffffffu, evaluated, o);
+            if ((threadIdx.x & 31) == 0 && evaluated) atomicAdd(items_evaluated, (u64)evaluated);
+        }
+        // block argmax: larger value, then lower item id
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+            const float ov = __shfl_xor_sync(0xffffffffu, bv, o);
+            const u64 oi = __shfl_xor_sync(0xffffffffu, bi, o);
+            if (ov > bv || (ov == bv && oi < bi)) { bv = ov; bi = oi; }
+        }
+        if ((threadIdx.x & 31) == 0) { red_v[threadIdx.x >> 5] = bv; red_i[threadIdx.x >> 5] = bi; }
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            for (u32 w = 1; w < blockDim.x / 32; w++)
+                if (red_v[w] > bv || (red_v[w] == bv && red_i[w] < bi)) { bv = red_v[w]; bi = red_i[w]; }
+            overlap_parse(id, n, K, S, nmax, bv, bi == ~0ull ? 0 : bi, best_idx, best_lab, best_ll,
+                          ov_idx, ov_lab, ovr, Lk, thr);
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------
+// check_overlap_reassignments, binary_pursuit.cl:822-875.  Window id reads
+// overlap_recheck[id-2] after candidate id-2 has been processed; that value
+// is reconstructed by walking the stride-2 chain of candidates that moved
+// left.  The final overlap_recheck values go to ovr_out.
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ u8 ovr_final(u32 k, u32 L, const u8 *ovr_in, const u32 *ov_idx) {
+    u32 m = 0;
+    while (ovr_in[k] == 1 && ov_idx[k] < k * L && k > 1) { k -= 2; m++; }
+    const u8 base = ovr_in[k] == 1 ? 1 : 0;
+    return (m & 1) ? (u8)(1 - base) : base;
+}
+
+__global__ void k_check_overlap(u32 n, u32 L, const u32 *__restrict__ cand, const u32 *__restrict__ n_cand_dev,
+                                u32 *__restrict__ best_idx, u32 *__restrict__ best_lab,
+                                u8 *__restrict__ flags, const u32 *__restrict__ ov_idx,
+                                const u32 *__restrict__ ov_lab, const u8 *__restrict__ ovr,
+                                u8 *__restrict__ ovr_out) {
+    const u32 n_cand = *n_cand_dev;
+    for (u32 g = blockIdx.x * blockDim.x + threadIdx.x; g < n_cand; g += gridDim.x * blockDim.x) {
+        const u32 id = cand[g];
+        const u32 sw = id * L, ew = (id + 1) * L;
+        if (ovr[id] == 0) { ovr_out[id] = 0; continue; }
+        best_idx[id] = ov_idx[id];
+        best_lab[id] = ov_lab[id];
+        u8 fin = 1;
+        if (ov_idx[id] < sw && id > 1) {
+            if (ovr_final(id - 2, L, ovr, ov_idx) == 1) {
+                fin = 0;
+                best_idx[id] = 0;
+                flags[id - 1] = 2; flags[id] = 2; flags[id + 1] = 2;
+            } else {
+                flags[id - 2] = 2;
+            }
+        }
+        if (ov_idx[id] >= ew && id + 2 < n / L) flags[id + 2] = 2;
+        ovr_out[id] = fin;
+    }
+}
+
+__global__ void k_copy_ovr(const u32 *__restrict__ cand, const u32 *__restrict__ n_cand_dev,
+                           const u8 *__restrict__ src, u8 *__restrict__ dst) {
+    const u32 n_cand = *n_cand_dev;
+    for (u32 g = blockIdx.x * blockDim.x + threadIdx.x; g < n_cand; g += gridDim.x * blockDim.x)
+        dst[cand[g]] = src[cand[g]];
+}
+
+// ---------------------------------------------------------------------------
+// binary_pursuit kernel, binary_pursuit.cl:918-1063.
+// k_accept_has: phase one (the accept decision) for every listed window.
+// k_accept_flags: the flags after the kernel, for every window, reproducing
+// the sequential reads of the neighbours' flags in phase two.
+// ---------------------------------------------------------------------------
+__global__ void k_accept_has(u32 n, u32 C, u32 L, const float *__restrict__ thr,
+                             const u32 *__restrict__ win, const u32 *__restrict__ n_win_dev,
+                             const u32 *__restrict__ best_idx, const u32 *__restrict__ best_lab,
+                             const float *__restrict__ best_ll, const u8 *__restrict__ ovr,
+                             u8 *__restrict__ has) {
+    const u32 n_win = *n_win_dev;
+    for (u32 g = blockIdx.x * blockDim.x + threadIdx.x; g < n_win; g += gridDim.x * blockDim.x) {
+        const u32 id = win[g];
+        const u32 sw = id * L, ew = (id + 1) * L;
+        u32 lab = 0, idx = 0;
+        float ml = 0.0f;
+        if (ew < n - L && C > 0) { ml = best_ll[id]; lab = best_lab[id]; idx = best_idx[id]; }
+        const bool o = ovr[id] == 1;
+        has[id] = ((ml > thr[lab]) || o) && ((idx >= sw && idx < ew) || o);   // .cl:982-999
+    }
+}
+
+struct AcceptView {
+    u32 n, C, L, W, nfloor;
+    const float *thr;
+    const u32 *best_idx, *best_lab;
+    const float *best_ll;
+    const u8 *active, *has, *F0;
+};
+
+__device__ __forceinline__ bool acc_valid(const AcceptView &a, u32 k) {
+    return ((k + 1) * a.L < a.n - a.L) && a.C > 0;
+}
+// flags[k] at the start of window k's phase two: window k-1's phase one may
+// have set it to 3 (.cl:994-997); window k+1 has not run yet.
+__device__ __forceinline__ u8 acc_f0(const AcceptView &a, u32 k) {
+    return (k >= 1 && a.active[k - 1] && a.has[k - 1] && k < a.nfloor) ? (u8)3 : a.F0[k];
+}
+__device__ __forceinline__ bool acc_step3(const AcceptView &a, u32 k) {
+    return a.best_ll[k] <= a.thr[a.best_lab[k]];
+}
+// Window k's left-prune (.cl:1024-1031) reads the final flag of window k-1.
+__device__ __forceinline__ bool acc_left_dependent(const AcceptView &a, u32 k) {
+    return k > 0 && a.active[k] && !a.has[k] && acc_valid(a, k) && acc_f0(a, k) == 1 &&
+           a.best_idx[k] < k * a.L;
+}
+// flags[k] after windows 0..k ran, for a window that is not left-dependent.
+__device__ __forceinline__ u8 acc_direct(const AcceptView &a, u32 k) {
+    u8 f = acc_f0(a, k);
+    if (!a.active[k]) return f;
+    if (a.has[k]) return 3;
+    if (!acc_valid(a, k)) return f;
+    if (f == 1 && a.best_idx[k] >= (k + 1) * a.L && k + 1 < a.nfloor)     // .cl:1032-1039
+        if (a.F0[k + 1] == 0) f = 0;
+    if (acc_step3(a, k) && f < 3) f = 0;                                   // .cl:1040-1044
+    return f;
+}
+
+__global__ void k_accept_flags(AcceptView a, u8 *__restrict__ flags_out) {
+    for (u32 j = blockIdx.x * blockDim.x + threadIdx.x; j < a.W; j += gridDim.x * blockDim.x) {
+        u8 P;
+        if (!acc_left_dependent(a, j)) {
+            P = acc_direct(a, j);
+        } else {
+            u32 k = j;
+            while (acc_left_dependent(a, k)) k--;
+            bool z = acc_direct(a, k) == 0;
+            for (u32 q = k + 1; q <= j; q++) z = z || acc_step3(a, q);
+            P = z ? 0 : 1;
+        }
+        // window j+1's phase one sets flags[j] = 3 (.cl:990-993)
+        if (j + 1 < a.W && a.active[j + 1] && a.has[j + 1]) P = 3;
+        flags_out[j] = P;
+    }
+}
+
+// Spike payload of an accepting window (.cl:971-976, 1057-1061).
+__global__ void k_gather_spikes(u32 n, u32 C, u32 L, const u32 *__restrict__ list,
+                                const u32 *__restrict__ n_list_dev, const u32 *__restrict__ best_idx,
+                                const u32 *__restrict__ best_lab, u32 *__restrict__ out_idx,
+                                u32 *__restrict__ out_lab, u32 *__restrict__ out_win) {
+    const u32 m = *n_list_dev;
+    for (u32 g = blockIdx.x * blockDim.x + threadIdx.x; g < m; g += gridDim.x * blockDim.x) {
+        const u32 id = list[g];
+        const bool valid = ((id + 1) * L < n - L) && C > 0;
+        out_idx[g] = valid ? best_idx[id] : 0;
+        out_lab[g] = valid ? best_lab[id] : 0;
+        if (out_win) out_win[g] = id;
+    }
+}
+
+// Append this pass's spikes to the chunk output (device-side offset).
+__global__ void k_append_spikes(const u32 *__restrict__ idx, const u32 *__restrict__ lab, Counters *cnt,
+                                u32 *__restrict__ out_idx, u32 *__restrict__ out_lab, u32 cap) {
+    const u32 m = cnt->n_spk, base = cnt->total;
+    if (base + m > cap) {
+        if (blockIdx.x == 0 && threadIdx.x == 0) cnt->overflow = 1;
+        return;
+    }
+    for (u32 g = blockIdx.x * blockDim.x + threadIdx.x; g < m; g += gridDim.x * blockDim.x) {
+        out_idx[base + g] = idx[g];
+        out_lab[base + g] = lab[g];
+    }
+}
+
+__global__ void k_commit_total(Counters *cnt, u32 cap) {
+    if (cnt->total + cnt->n_spk <= cap) cnt->total += cnt->n_spk;
+}
+
+// ---------------------------------------------------------------------------
+// Path (c): residual subtract, compute_residual (binary_pursuit.cl:57-102).
+// Spikes of one pass can overlap (an overlap-recheck spike may move up to
+// n_max_shift samples).  Each sample is written by the last listed spike
+// covering it, which applies every covering spike's subtraction in list
+// order -- the sequential reference's result, with no atomics.
+// ---------------------------------------------------------------------------
+__global__ void k_residual(float *__restrict__ v, u32 n, u32 C, const float *__restrict__ T, u32 K, u32 L,
+                           const u32 *__restrict__ idx, const u32 *__restrict__ lab,
+                           const u32 *__restrict__ n_spk_dev, u32 n_spk_host, u32 R) {
+    const u32 m = n_spk_dev ? *n_spk_dev : n_spk_host;
+    for (u32 s = blockIdx.x; s < m; s += gridDim.x) {
+        const u32 p = idx[s];
+        if (lab[s] >= K) continue;                                       // .cl:78-81
+        const u32 jlo = s > R ? s - R : 0;
+        const u32 jhi = min(m - 1, s + R);
+        for (u32 e = threadIdx.x; e < C * L; e += blockDim.x) {
+            const u32 c = e / L, i = e % L;
+            const u32 x = p + i;
+            if (x >= n) continue;                                        // .cl:93-96
+            bool owner = true;
+            for (u32 j = s + 1; j <= jhi; j++)
+                if (lab[j] < K && idx[j] <= x && x < idx[j] + L) { owner = false; break; }
+            if (!owner) continue;
+            float val = v[(size_t)c * n + x];
+            for (u32 j = jlo; j <= s; j++) {
+                const u32 pj = idx[j];
+                if (lab[j] < K && pj <= x && x < pj + L)
+                    val = __fsub_rn(val, T[((size_t)lab[j] * C + c) * L + (x - pj)]);
+            }
+            v[(size_t)c * n + x] = val;
+        }
+    }
+}
+
+// get_adjusted_clips, binary_pursuit.cl:1088-1130.
+__global__ void k_adjusted_clips(const float *__restrict__ v, u32 n, u32 C, const float *__restrict__ T,
+                                 u32 K, u32 L, const u32 *__restrict__ idx, const u32 *__restrict__ lab,
+                                 u32 m, float *__restrict__ clips) {
+    for (u32 s = blockIdx.x; s < m; s += gridDim.x) {
+        const u32 p = idx[s], k = lab[s];
+        if (k >= K) continue;
+        for (u32 e = threadIdx.x; e < C * L; e += blockDim.x) {
+            const u32 c = e / L, i = e % L;
+            if (p + i >= n) continue;
+            clips[(size_t)s * C * L + e] = __fadd_rn(v[(size_t)c * n + p + i], T[(size_t)k * C * L + e]);
+        }
+    }
+}
+
+}  // namespace fbp

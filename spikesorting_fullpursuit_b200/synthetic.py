@@ -85,17 +85,22 @@ def clip_width_for(L: int, pre_fraction: float, fs: float):
     return [-pre / fs, post / fs]
 
 
-def bandlimited_noise(rng, n_chans, n, fs, f_lo=300.0, f_hi=8000.0, dtype=np.float32):
+def bandlimited_noise(rng, n_chans, n, fs, f_lo=300.0, f_hi=8000.0, dtype=np.float32,
+                      batch=16):
+    import scipy.fft as sfft
     out = np.empty((n_chans, n), dtype=dtype)
     freqs = np.fft.rfftfreq(n, 1.0 / fs)
-    keep = (freqs >= f_lo) & (freqs <= f_hi)
-    for c in range(n_chans):
-        x = rng.standard_normal(n, dtype=np.float32)
-        X = np.fft.rfft(x)
-        X[~keep] = 0
-        y = np.fft.irfft(X, n)
-        y /= np.std(y)
-        out[c] = y.astype(dtype)
+    drop = ~((freqs >= f_lo) & (freqs <= f_hi))
+    for c0 in range(0, n_chans, batch):
+        c1 = min(n_chans, c0 + batch)
+        x = rng.standard_normal((c1 - c0, n), dtype=np.float32)
+        X = sfft.rfft(x, axis=1, workers=-1)
+        del x
+        X[:, drop] = 0
+        y = sfft.irfft(X, n, axis=1, workers=-1)
+        del X
+        y /= np.std(y, axis=1, keepdims=True)
+        out[c0:c1] = y.astype(dtype)
     return out
 
 
@@ -142,6 +147,41 @@ def poisson_train(rng, rate, n, fs, refractory_s=1.5e-3, edge_s=5e-3):
         t = np.concatenate([t, t[-1] + np.cumsum(more)])
     t = t[(t >= edge_s) & (t < dur - edge_s)]
     return np.unique(np.round(t * fs).astype(np.int64))
+
+
+def _refractory(s, ref):
+    """Drop the later spike of every pair closer than `ref` samples."""
+    while s.size > 1:
+        bad = np.nonzero(np.diff(s) <= ref)[0]
+        if bad.size == 0:
+            break
+        s = np.delete(s, bad + 1)
+    return s
+
+
+def _insert_spikes(volt, templates, spikes, align, L, n):
+    """volt[c, t_k + i - align] += templates[k, c, i] for every spike; spikes
+    whose clip would leave the recording are dropped.  Uses torch's
+    index_add_ on the CPU, which accumulates duplicates one by one."""
+    import torch
+    C = volt.shape[0]
+    V = torch.from_numpy(volt)
+    offs = torch.arange(L, dtype=torch.int64)
+    for k in range(len(spikes)):
+        s = spikes[k]
+        if s.size == 0:
+            continue
+        starts = s - align
+        ok = (starts >= 0) & (starts + L <= n)
+        spikes[k] = s[ok]
+        st = torch.from_numpy(starts[ok].astype(np.int64))
+        if st.numel() == 0:
+            continue
+        flat = (st[:, None] + offs[None, :]).reshape(-1)
+        tk = templates[k].reshape(C, L)
+        for c in np.nonzero(np.any(tk != 0, axis=1))[0]:
+            src = torch.from_numpy(np.ascontiguousarray(tk[c], dtype=volt.dtype)).repeat(st.numel())
+            V[c].index_add_(0, flat, src)
 
 
 def separability(templates, chan_cov, n_chans, L, sigma_bp_noise=1.645, sigma_bp_CI=4.0):
@@ -229,37 +269,16 @@ def make_recording(*, n_chans, duration_s, fs, n_templates, L, pre_fraction,
             pick = rng.choice(s.size, size=nmove, replace=False)
             others = rng.integers(0, K - 1, size=nmove)
             others = others + (others >= k)
-            for j, o in zip(pick, others):
+            jit = rng.integers(-win, win + 1, size=nmove)
+            for o in np.unique(others):
+                sel = np.nonzero(others == o)[0]
                 if spikes[o].size:
-                    anchor = spikes[o][rng.integers(spikes[o].size)]
-                    s[j] = anchor + rng.integers(-win, win + 1)
-            s = np.unique(np.clip(s, L, n - L))
-            # restore the refractory period inside the unit
-            keep = np.ones(s.size, dtype=bool)
-            last = -10 ** 12
-            ref = int(1.5e-3 * fs)
-            for i in range(s.size):
-                if s[i] - last <= ref:
-                    keep[i] = False
-                else:
-                    last = s[i]
-            spikes[k] = s[keep]
+                    anchors = spikes[o][rng.integers(0, spikes[o].size, size=sel.size)]
+                    s[pick[sel]] = anchors + jit[sel]
+            spikes[k] = _refractory(np.unique(np.clip(s, L, n - L)), int(1.5e-3 * fs))
 
     volt = noise.astype(np.float64) if int16_scale else noise
-    Lr = np.arange(L)
-    for k in range(K):
-        s = spikes[k]
-        if s.size == 0:
-            continue
-        starts = s - align
-        ok = (starts >= 0) & (starts + L <= n)
-        starts = starts[ok]
-        spikes[k] = s[ok]
-        tk = templates[k].reshape(C, L)
-        nz = np.nonzero(np.any(tk != 0, axis=1))[0]
-        for i in Lr:
-            col = starts + i
-            volt[np.ix_(nz, col)] += tk[nz, i][:, None].astype(volt.dtype)
+    _insert_spikes(volt, templates, spikes, align, L, n)
 
     if int16_scale:
         q = np.clip(np.round(volt * int16_scale), -32768, 32767).astype(np.int16)
