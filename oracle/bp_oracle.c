@@ -373,3 +373,17 @@ done:
     free(flags); free(ovr); free(win); free(cand); free(add_idx); free(add_lab);
     return total;
 }
+
+/* Reference value (binary_pursuit.cl:578-632) of listed overlap items of one
+ * candidate, whatever the skip rules say: item = t + K*(a + S*b). */
+void bpo_overlap_items(const float *v, u32 n, u32 C, const float *T, u32 K, u32 L, u32 lab,
+                       u32 bidx, u32 nmax, const unsigned long long *items, u32 count, float *out)
+{
+    const size_t S = 2 * (size_t)nmax + 1;
+    for (u32 q = 0; q < count; q++) {
+        unsigned long long it = items[q];
+        u32 t = (u32)(it % K), a = (u32)((it / K) % S), b = (u32)((it / (S * K)) % S);
+        u32 afix = bidx + a - nmax, ashift = bidx + b - nmax;
+        out[q] = overlap_pair_ll(v, n, C, T, L, lab, bidx, t, afix, ashift);
+    }
+}

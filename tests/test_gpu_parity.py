@@ -31,12 +31,26 @@ def lib():
     return _lib.lib()
 
 
+_KEEP = []
+
+
 def D(a):
-    """numpy -> cuda tensor (uint32 carried as int32 bits)."""
+    """numpy -> cuda tensor (uint32 carried as int32 bits).  The tensor is
+    kept alive until the test ends: a pointer handed to the C ABI must not
+    outlive its tensor (the caching allocator would reuse the block)."""
     a = np.ascontiguousarray(a)
     if a.dtype == np.uint32:
         a = a.view(np.int32)
-    return torch.from_numpy(a.copy()).cuda()
+    t = torch.from_numpy(a.copy()).cuda()
+    _KEEP.append(t)
+    return t
+
+
+@pytest.fixture(autouse=True)
+def _release_kept():
+    yield
+    torch.cuda.synchronize()
+    _KEEP.clear()
 
 
 def H(t, dtype=None):
