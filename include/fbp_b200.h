@@ -211,6 +211,30 @@ int fbp_binary_pursuit_accept(uint32_t n_samples, uint32_t n_chans, uint32_t tem
                               uint32_t *spike_win, uint32_t *n_spikes_dev, void *scan_scratch,
                               void *stream);
 
+/* Allocation-free variant of fbp_binary_pursuit_accept (no counterpart in
+ * the reference).  For callers that cannot call cudaMalloc: for example a
+ * host framework that has reserved the whole device heap for its own pool,
+ * or a real-time acquisition loop where an allocation's implicit device
+ * synchronisation and unbounded latency are not allowed.  The `has` and
+ * `scan_scratch` buffers of fbp_binary_pursuit_accept live instead in one
+ * file-scope device array of FBP_NOALLOC_SCRATCH_BYTES (about 4.2 MB), which
+ * every GPU that loads the library keeps until the process exits; the
+ * caller still passes every input and output.  Limit: at most
+ * FBP_NOALLOC_MAX_WINDOWS windows (n_samples <= FBP_NOALLOC_MAX_WINDOWS * L);
+ * larger inputs return FBP_ERR_BAD_ARG.  The first call on a device looks up
+ * the array's device address (cudaGetSymbolAddress), so make that first call
+ * before any stream capture.  All calls share the one array: calls whose GPU
+ * work overlaps (other streams, other threads) race on it; it is cleared
+ * at the start of every call, so its leftover contents do not matter. */
+#define FBP_NOALLOC_MAX_WINDOWS 4194300u
+#define FBP_NOALLOC_SCRATCH_BYTES (4194304u + 8192u)
+int fbp_binary_pursuit_accept_noalloc(uint32_t n_samples, uint32_t n_chans, uint32_t template_len,
+                                      const float *thresholds, const uint32_t *window_list,
+                                      const uint32_t *n_windows_dev, uint32_t max_windows,
+                                      const fbp_window_state *st, const uint8_t *active,
+                                      uint8_t *flags_out, uint32_t *spike_idx, uint32_t *spike_lab,
+                                      uint32_t *spike_win, uint32_t *n_spikes_dev, void *stream);
+
 /* Scratch bytes the ordered compaction in fbp_binary_pursuit_accept needs. */
 size_t fbp_scan_scratch_bytes(uint32_t n_windows);
 

@@ -17,6 +17,7 @@ FBP_ERR_ITER_CAP = 3
 FBP_ERR_CAPACITY = 4
 FBP_ERR_NO_DEVICE = 5
 FBP_ERR_OOM = 6
+NOALLOC_MAX_WINDOWS = 4194300
 PREC_FP32 = 0
 PREC_BF16_REFINE = 1
 
@@ -41,6 +42,7 @@ SIGNATURES = {
     "fbp_overlap_recheck": (I, [P, U32, U32, P, U32, U32, P, P, U32, P, P, U32, P, P]),
     "fbp_check_overlap_reassignments": (I, [U32, U32, P, P, U32, P, P, P]),
     "fbp_binary_pursuit_accept": (I, [U32, U32, U32, P, P, P, U32, P, P, P, P, P, P, P, P, P, P]),
+    "fbp_binary_pursuit_accept_noalloc": (I, [U32, U32, U32, P, P, P, U32, P, P, P, P, P, P, P, P]),
     "fbp_scan_scratch_bytes": (SZ, [U32]),
     "fbp_window_u8_bytes": (SZ, [U32]),
 }

@@ -8,6 +8,7 @@
 #include <cstdarg>
 #include <cstdio>
 #include <cstring>
+#include <mutex>
 #include <string>
 #include <vector>
 
@@ -523,3 +524,72 @@ int fbp_binary_pursuit_accept(uint32_t n, uint32_t C, uint32_t L, const float *t
 }
 
 }  // extern "C"
+
+// ---------------------------------------------------------------------------
+// Allocation-free accept: the scratch of fbp_binary_pursuit_accept (the
+// per-window accept bytes and the compaction's tile offsets) in a file-scope
+// device array, for callers that cannot allocate device memory.
+// ---------------------------------------------------------------------------
+namespace {
+
+static __device__ __align__(256) unsigned char g_accept_scratch[FBP_NOALLOC_SCRATCH_BYTES];
+
+constexpr size_t kNoallocHasBytes = 4194304;   // align_up(FBP_NOALLOC_MAX_WINDOWS + pad, 4096)
+constexpr int kMaxDevices = 64;
+std::mutex g_noalloc_mutex;
+unsigned char *g_noalloc_ptr[kMaxDevices] = {nullptr};
+
+// Device address of g_accept_scratch on the current device, looked up once
+// per device.  Host code must not use the symbol itself as a pointer.
+int noalloc_scratch(unsigned char **out) {
+    int dev = 0;
+    FBP_CUDA(cudaGetDevice(&dev));
+    if (dev < 0 || dev >= kMaxDevices) return fail(FBP_ERR_BAD_ARG, "device index %d out of range", dev);
+    std::lock_guard<std::mutex> lock(g_noalloc_mutex);
+    if (!g_noalloc_ptr[dev]) {
+        void *p = nullptr;
+        cudaError_t e = cudaGetSymbolAddress(&p, g_accept_scratch);
+        if (e != cudaSuccess || !p)
+            return fail(FBP_ERR_CUDA, "cudaGetSymbolAddress(accept scratch) failed: %s", cudaGetErrorString(e));
+        g_noalloc_ptr[dev] = (unsigned char *)p;
+    }
+    *out = g_noalloc_ptr[dev];
+    return FBP_OK;
+}
+
+}  // namespace
+
+static_assert(kNoallocHasBytes >= ((size_t)FBP_NOALLOC_MAX_WINDOWS + FBP_WINDOW_PAD + kCompactTile - 1) /
+                                       kCompactTile * kCompactTile,
+              "accept bytes do not fit the no-alloc scratch");
+static_assert(FBP_NOALLOC_SCRATCH_BYTES - kNoallocHasBytes >=
+                  (size_t)((FBP_NOALLOC_MAX_WINDOWS + kCompactTile - 1) / kCompactTile + 1) * 4,
+              "tile offsets do not fit the no-alloc scratch");
+
+extern "C" int fbp_binary_pursuit_accept_noalloc(uint32_t n, uint32_t C, uint32_t L, const float *thresholds,
+                                                 const uint32_t *window_list, const uint32_t *n_windows_dev,
+                                                 uint32_t max_windows, const fbp_window_state *st,
+                                                 const uint8_t *active, uint8_t *flags_out, uint32_t *spike_idx,
+                                                 uint32_t *spike_lab, uint32_t *spike_win, uint32_t *n_spikes_dev,
+                                                 void *stream) {
+    g_last_error.clear();
+    if (!thresholds || !window_list || !n_windows_dev || !st || !active || !flags_out || !spike_idx ||
+        !spike_lab || !spike_win || !n_spikes_dev)
+        return fail(FBP_ERR_BAD_ARG, "fbp_binary_pursuit_accept_noalloc: null pointer argument");
+    if (L == 0) return fail(FBP_ERR_BAD_ARG, "fbp_binary_pursuit_accept_noalloc: template_len is 0");
+    const u32 W = ceil_div(n, L);
+    if (W > FBP_NOALLOC_MAX_WINDOWS)
+        return fail(FBP_ERR_BAD_ARG,
+                    "fbp_binary_pursuit_accept_noalloc: %u windows exceed the fixed scratch limit of %u "
+                    "windows (use fbp_binary_pursuit_accept with caller-provided scratch)",
+                    W, FBP_NOALLOC_MAX_WINDOWS);
+    unsigned char *scratch = nullptr;
+    int rc = noalloc_scratch(&scratch);
+    if (rc) return rc;
+    u8 *has = scratch;                                        // cleared by launch_accept
+    u32 *tile_offsets = (u32 *)(scratch + kNoallocHasBytes);  // fully rewritten by the compaction
+    return launch_accept(n, C, L, thresholds, window_list, n_windows_dev, max_windows, *st, active, has, flags_out,
+                         spike_win, spike_idx, spike_lab, nullptr, n_spikes_dev, tile_offsets,
+                         (cudaStream_t)stream);
+}
+
