@@ -43,6 +43,7 @@ def parse():
     ap.add_argument("--duration", type=float, default=None,
                     help="override the segment length in seconds (development only)")
     ap.add_argument("--precision", choices=["fp32", "bf16"], default="fp32")
+    ap.add_argument("--overlap", choices=["fast", "exact"], default="fast")
     ap.add_argument("--cpu-sample-s", type=float, default=0.05,
                     help="seconds of recording timed on the CPU baseline")
     ap.add_argument("--no-e2e", action="store_true")
@@ -213,7 +214,7 @@ def main():
         st = _lib.StageStats()
         _lib.check(lib.fbp_pursuit_chunk(
             _lib.ptr(v), n, C, _lib.ptr(T_d), K, L, _lib.ptr(tss_d), _lib.ptr(thr_d), nmax, 1, prec,
-            1000000, _lib.ptr(ws), ws.numel(), _lib.ptr(out_i), _lib.ptr(out_l), cap, None,
+            0 if args.overlap == "fast" else 1, 1000000, _lib.ptr(ws), ws.numel(), _lib.ptr(out_i), _lib.ptr(out_l), cap, None,
             ctypes.byref(nspk), ctypes.byref(npass), int(profile), ctypes.byref(st), sp))
         return st
 
@@ -287,7 +288,7 @@ def main():
         host_v = pinned.numpy()
         si = rec.sort_info()
         binary_pursuit(host_v, host_v.dtype, si, rec.fresh_metrics(), n_max_shift_inds=nmax,
-                       precision=args.precision)
+                       precision=args.precision, overlap=args.overlap)
         barrier()
         e_times = []
         d2h = 0
@@ -295,7 +296,7 @@ def main():
             torch.cuda.synchronize()
             t0 = time.perf_counter()
             out = binary_pursuit(host_v, host_v.dtype, si, rec.fresh_metrics(), n_max_shift_inds=nmax,
-                                 precision=args.precision)
+                                 precision=args.precision, overlap=args.overlap)
             e_times.append(time.perf_counter() - t0)
             d2h = 8 * len(out[0])
         te = torch.tensor([float(np.mean(e_times))], dtype=torch.float64, device=dev)
@@ -326,6 +327,7 @@ def main():
                 "data": "synthetic (seeded; one independent segment per rank)",
                 "config": {"workload": rec.name, "n_chans": C, "n_samples": n, "n_templates": K,
                            "template_len": L, "n_max_shift": nmax, "precision": args.precision,
+                           "overlap": args.overlap,
                            "l2": "inputs larger than L2 (voltage %.2f GB, likelihood %.2f GB)"
                                  % (C * n * 4 / 1e9, K * n * 4 / 1e9),
                            "passes": int(stats[-1].passes), "spikes": int(stats[-1].spikes),

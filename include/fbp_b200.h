@@ -50,6 +50,17 @@ typedef enum fbp_precision {
     FBP_PREC_BF16_REFINE = 1
 } fbp_precision;
 
+/* How the overlap recheck (binary_pursuit.cl:444-815) is evaluated.  Both
+ * give the reference's result.  FAST splits each item's likelihood into
+ * per-candidate correlations and template-pair prefix sums, bounds the
+ * reference's rounding, and re-evaluates exactly (in the reference's order)
+ * only the items that can be the maximum; EXACT evaluates every item in the
+ * reference's order.  FAST falls back to EXACT for shift ranges above 4L+1. */
+typedef enum fbp_overlap_method {
+    FBP_OVERLAP_FAST = 0,
+    FBP_OVERLAP_EXACT = 1
+} fbp_overlap_method;
+
 /* Stages of a pass, for fbp_stage_stats. */
 enum {
     FBP_STAGE_LIKELIHOOD = 0,   /* path (a): full-pass likelihood          */
@@ -105,6 +116,7 @@ int fbp_pursuit_workspace_bytes(uint32_t n_samples, uint32_t n_chans, uint32_t n
  *  neg_half_ss  [K] float32, float32(-0.5 * template_SS)   (.py:199)
  *  thresholds   [K] float32, float32(neuron_lower_thresholds) (.py:201)
  *  n_max_shift  overlap shift range, S = 2*n_max_shift + 1   (.py:294-298)
+ *  overlap_method  fbp_overlap_method
  *  spike_idx/spike_lab  [spike_cap] uint32 outputs: window-relative clip
  *               starts and labels, in pass order and window order inside a
  *               pass (the order the reference's loop concatenates them)
@@ -119,7 +131,7 @@ int fbp_pursuit_chunk(float *voltage, uint32_t n_samples, uint32_t n_chans,
                       const float *templates, uint32_t n_templates, uint32_t template_len,
                       const float *neg_half_ss, const float *thresholds,
                       uint32_t n_max_shift, int do_overlap_recheck, int precision,
-                      uint32_t max_passes, void *workspace, size_t workspace_bytes,
+                      int overlap_method, uint32_t max_passes, void *workspace, size_t workspace_bytes,
                       uint32_t *spike_idx, uint32_t *spike_lab, uint32_t spike_cap,
                       uint32_t *pass_counts, uint32_t *n_spikes_host,
                       uint32_t *n_passes_host, int profile, fbp_stage_stats *stats,

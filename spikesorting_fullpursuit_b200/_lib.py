@@ -20,6 +20,8 @@ FBP_ERR_OOM = 6
 NOALLOC_MAX_WINDOWS = 4194300
 PREC_FP32 = 0
 PREC_BF16_REFINE = 1
+OVERLAP_FAST = 0
+OVERLAP_EXACT = 1
 
 _lib = None
 
@@ -33,7 +35,7 @@ SIGNATURES = {
     "fbp_version": (I, []),
     "fbp_last_error": (ctypes.c_char_p, []),
     "fbp_pursuit_workspace_bytes": (I, [U32, U32, U32, U32, U32, I, ctypes.POINTER(SZ)]),
-    "fbp_pursuit_chunk": (I, [P, U32, U32, P, U32, U32, P, P, U32, I, I, U32, P, SZ, P, P, U32, P,
+    "fbp_pursuit_chunk": (I, [P, U32, U32, P, U32, U32, P, P, U32, I, I, I, U32, P, SZ, P, P, U32, P,
                               ctypes.POINTER(U32), ctypes.POINTER(U32), I, P, P]),
     "fbp_compute_residual": (I, [P, U32, U32, P, U32, U32, P, P, U32, U32, P]),
     "fbp_get_adjusted_clips": (I, [P, U32, U32, P, U32, U32, P, P, U32, P, P]),

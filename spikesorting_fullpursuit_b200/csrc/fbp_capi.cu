@@ -13,7 +13,7 @@
 #include <vector>
 
 #include "../../include/fbp_b200.h"
-#include "fbp_kernels.cuh"
+#include "fbp_overlap_fast.cuh"
 
 using namespace fbp;
 
@@ -65,12 +65,30 @@ struct Workspace {
     float *best_ll;
     u8 *flags, *flags_out, *ovr, *ovr2, *active, *has;
     Counters *cnt;
+    // fast overlap recheck (present when `fast`)
+    bool fast;
+    u32 slots;
+    float *NT, *sNT, *tnorm, *Q, *H, *vn, *res_lb, *res_hi;
+    OvConst *oc;
+    u8 *cskip, *fallback;
+    u32 *k0_count, *k0_cursor, *k0_offset, *k0_active, *n_k0_active, *order, *res_cnt, *res_item;
+    u32 *ref_cnt, *ref_item, *fb_slots, *fb_list, *fb_count;
     size_t bytes;
 };
 
+// The fast overlap recheck is used when its shared-memory tiles fit and the
+// shift range is at most 4L+1 (production uses S = 2L-1).
+bool fast_overlap_fits(u32 K, u32 L, u32 nmax) {
+    const u64 S = 2 * (u64)nmax + 1;
+    if (S > 4 * (u64)L + 1 || S > 65535) return false;
+    if (sweep_smem_bytes((u32)S, L) > 227 * 1024) return false;
+    if (tables_smem_bytes((u32)S, K, L) > 227 * 1024) return false;
+    return true;
+}
+
 size_t window_bytes_u8(u32 W) { return align_up((size_t)W + FBP_WINDOW_PAD, kCompactTile); }
 
-Workspace layout(char *base, u32 n, u32 K, u32 L) {
+Workspace layout(char *base, u32 n, u32 K, u32 L, u32 nmax, bool want_fast) {
     Workspace w{};
     const u32 W = ceil_div(n, L);
     const size_t Wp = (size_t)W + FBP_WINDOW_PAD;
@@ -101,6 +119,38 @@ Workspace layout(char *base, u32 n, u32 K, u32 L) {
     w.ovr2 = (u8 *)take(wb);
     w.active = (u8 *)take(wb);
     w.has = (u8 *)take(wb);
+    w.fast = want_fast && fast_overlap_fits(K, L, nmax);
+    if (w.fast) {
+        const u32 S = 2 * nmax + 1;
+        // at most every other window is a candidate (their bests cannot
+        // both lie in their own windows)
+        w.slots = W / 2 + 2;
+        const size_t sl = w.slots;
+        w.oc = (OvConst *)take(sizeof(OvConst));
+        w.NT = (float *)take((size_t)K * S * 4);
+        w.sNT = (float *)take((size_t)K * S * 4);
+        w.tnorm = (float *)take((size_t)K * 4);
+        w.Q = (float *)take((size_t)K * K * (2 * L - 1) * (L + 1) * 4);
+        w.H = (float *)take(sl * K * S * 4);
+        w.vn = (float *)take(sl * 4);
+        w.cskip = (u8 *)take(sl);
+        w.fallback = (u8 *)take(align_up(sl + FBP_WINDOW_PAD, kCompactTile));
+        w.k0_count = (u32 *)take((size_t)K * 4);
+        w.k0_cursor = (u32 *)take((size_t)K * 4);
+        w.k0_offset = (u32 *)take((size_t)K * 4);
+        w.k0_active = (u32 *)take((size_t)K * 4);
+        w.n_k0_active = (u32 *)take(4);
+        w.order = (u32 *)take(sl * 4);
+        w.res_lb = (float *)take(sl * K * 4);
+        w.res_cnt = (u32 *)take(sl * K * 4);
+        w.res_item = (u32 *)take(sl * K * kOvOutCap * 4);
+        w.res_hi = (float *)take(sl * K * kOvOutCap * 4);
+        w.ref_cnt = (u32 *)take(sl * 4);
+        w.ref_item = (u32 *)take(sl * kOvRefCap * 4);
+        w.fb_slots = (u32 *)take(sl * 4);
+        w.fb_list = (u32 *)take(sl * 4);
+        w.fb_count = (u32 *)take(4);
+    }
     w.bytes = off;
     return w;
 }
@@ -205,6 +255,74 @@ int launch_accept(u32 n, u32 C, u32 L, const float *thr, const u32 *win, const u
     return FBP_OK;
 }
 
+OvArgs ov_args(const Workspace &w, const float *v, u32 n, u32 C, const float *T, u32 K, u32 L, u32 nmax,
+               const float *thr, const fbp_window_state &s, const float *Lk, const u32 *cand,
+               const u32 *n_cand, u64 *items) {
+    OvArgs A{};
+    A.n = n; A.C = C; A.K = K; A.L = L; A.nmax = nmax; A.S = 2 * nmax + 1;
+    A.v = v; A.T = T; A.Lk = Lk; A.thr = thr;
+    A.NT = w.NT; A.sNT = w.sNT; A.tnorm = w.tnorm; A.Q = w.Q; A.oc = w.oc;
+    A.cand = cand; A.n_cand = n_cand;
+    A.best_idx = s.best_idx; A.best_lab = s.best_lab; A.ov_idx = s.ov_idx; A.ov_lab = s.ov_lab;
+    A.best_ll = s.best_ll; A.ovr = s.overlap_recheck;
+    A.H = w.H; A.vn = w.vn; A.cskip = w.cskip;
+    A.k0_count = w.k0_count; A.k0_cursor = w.k0_cursor; A.k0_offset = w.k0_offset;
+    A.k0_active = w.k0_active; A.n_k0_active = w.n_k0_active; A.order = w.order;
+    A.res_lb = w.res_lb; A.res_cnt = w.res_cnt; A.res_item = w.res_item; A.res_hi = w.res_hi;
+    A.ref_cnt = w.ref_cnt; A.ref_item = w.ref_item; A.fallback = w.fallback;
+    A.items_evaluated = items;
+    return A;
+}
+
+// Per-chunk tables of the fast overlap recheck (templates are fixed).
+int ov_chunk_setup(const Workspace &w, const float *T, u32 K, u32 C, u32 L, u32 nmax, cudaStream_t st) {
+    const u32 S = 2 * nmax + 1;
+    k_ov_chunk_tables<<<grid_for((u64)K * S, 256), 256, 0, st>>>(T, K, C, L, nmax, w.NT, w.sNT, w.tnorm, w.oc);
+    const u64 rows = (u64)K * K * (2 * L - 1);
+    k_ov_q_table<<<grid_for(rows, 128, 16), 128, 0, st>>>(T, K, C, L, w.Q);
+    FBP_LAUNCH_CHECK();
+    return FBP_OK;
+}
+
+// One pass of the fast overlap recheck over the candidate list (device count
+// n_cand).  Returns the number of kernels launched in *launches.
+int ov_fast_pass(const Workspace &w, const OvArgs &A, u32 W, cudaStream_t st, int *launches) {
+    const u32 slots = w.slots;
+    const u32 S = A.S;
+    FBP_CUDA(cudaMemsetAsync(w.k0_count, 0, (size_t)A.K * 4, st));
+    FBP_CUDA(cudaMemsetAsync(w.fallback, 0, align_up((size_t)slots + FBP_WINDOW_PAD, kCompactTile), st));
+    k_ov_prep<<<grid_for((u64)slots * 32, 256), 256, 0, st>>>(A);
+    k_ov_group<<<1, 32, 0, st>>>(A);
+    k_ov_scatter<<<grid_for(slots, 256), 256, 0, st>>>(A);
+    FBP_LAUNCH_CHECK();
+    {
+        const size_t smem = tables_smem_bytes(S, A.K, A.L);
+        if (smem > 48 * 1024)
+            FBP_CUDA(cudaFuncSetAttribute(k_ov_tables, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        k_ov_tables<<<grid_for((u64)slots * kTabThreads, kTabThreads, 4), kTabThreads, smem, st>>>(A);
+        FBP_LAUNCH_CHECK();
+    }
+    {
+        const size_t smem = sweep_smem_bytes(S, A.L);
+        if (smem > 48 * 1024)
+            FBP_CUDA(cudaFuncSetAttribute(k_ov_sweep, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        k_ov_sweep<<<sm_count(), kSweepThreads, smem, st>>>(A);
+        FBP_LAUNCH_CHECK();
+    }
+    k_ov_merge<<<grid_for((u64)slots * 32, 256), 256, 0, st>>>(A);
+    k_ov_refine<<<grid_for((u64)slots * 32, 256), 256, 0, st>>>(A);
+    FBP_LAUNCH_CHECK();
+    int rc = compact(w.fallback, slots, w.fb_slots, w.fb_count, w.tile_counts, st);
+    if (rc) return rc;
+    k_ov_fallback_list<<<grid_for(slots, 256), 256, 0, st>>>(A, w.fb_slots, w.fb_count, w.fb_list);
+    FBP_LAUNCH_CHECK();
+    fbp_window_state s{A.best_idx, A.best_lab, A.best_ll, A.ov_idx, A.ov_lab, nullptr, A.ovr};
+    rc = launch_overlap(A.v, A.n, A.C, A.T, A.K, A.L, w.fb_list, w.fb_count, slots, s, A.Lk, A.nmax, A.thr,
+                        A.items_evaluated, st);
+    *launches = 14;
+    return rc;
+}
+
 // CUDA-event timing of the stages of a pass.  Events come from a pool that
 // is drained after every host synchronisation (collect()).
 class StageTimer {
@@ -279,16 +397,15 @@ int fbp_pursuit_workspace_bytes(uint32_t n, uint32_t C, uint32_t K, uint32_t L, 
                                 int precision, size_t *bytes_out) {
     if (!bytes_out || n == 0 || C == 0 || K == 0 || L == 0)
         return fail(FBP_ERR_BAD_ARG, "workspace size: bad arguments");
-    (void)nmax;
     (void)precision;
-    *bytes_out = layout(nullptr, n, K, L).bytes;
+    *bytes_out = layout(nullptr, n, K, L, nmax, true).bytes;
     return FBP_OK;
 }
 
 int fbp_pursuit_chunk(float *voltage, uint32_t n, uint32_t C, const float *templates, uint32_t K,
                       uint32_t L, const float *neg_half_ss, const float *thresholds, uint32_t nmax,
-                      int do_overlap_recheck, int precision, uint32_t max_passes, void *workspace,
-                      size_t workspace_bytes, uint32_t *spike_idx, uint32_t *spike_lab,
+                      int do_overlap_recheck, int precision, int overlap_method, uint32_t max_passes,
+                      void *workspace, size_t workspace_bytes, uint32_t *spike_idx, uint32_t *spike_lab,
                       uint32_t spike_cap, uint32_t *pass_counts, uint32_t *n_spikes_host,
                       uint32_t *n_passes_host, int profile, fbp_stage_stats *stats, void *stream) {
     g_last_error.clear();
@@ -301,7 +418,9 @@ int fbp_pursuit_chunk(float *voltage, uint32_t n, uint32_t C, const float *templ
         return fail(FBP_ERR_BAD_ARG, "fbp_pursuit_chunk: unknown precision %d", precision);
     if ((u64)2 * nmax + 1 > 0xffffffffull)
         return fail(FBP_ERR_BAD_ARG, "fbp_pursuit_chunk: n_max_shift too large");
-    Workspace w = layout((char *)workspace, n, K, L);
+    if (overlap_method != FBP_OVERLAP_FAST && overlap_method != FBP_OVERLAP_EXACT)
+        return fail(FBP_ERR_BAD_ARG, "fbp_pursuit_chunk: unknown overlap method %d", overlap_method);
+    Workspace w = layout((char *)workspace, n, K, L, nmax, overlap_method == FBP_OVERLAP_FAST);
     if (workspace_bytes < w.bytes)
         return fail(FBP_ERR_BAD_ARG, "fbp_pursuit_chunk: workspace has %zu bytes, needs %zu",
                     workspace_bytes, w.bytes);
@@ -332,6 +451,13 @@ int fbp_pursuit_chunk(float *voltage, uint32_t n, uint32_t C, const float *templ
     FBP_LAUNCH_CHECK();
     S.launches[FBP_STAGE_LISTS] += 1;
     timer.end(FBP_STAGE_LISTS);
+    if (w.fast && do_overlap_recheck) {
+        timer.begin(FBP_STAGE_OVERLAP);
+        int rc0 = ov_chunk_setup(w, templates, K, C, L, nmax, st);
+        if (rc0) return rc0;
+        S.launches[FBP_STAGE_OVERLAP] += 2;
+        timer.end(FBP_STAGE_OVERLAP);
+    }
 
     u32 *h_counts = nullptr;
     FBP_CUDA(cudaMallocHost(&h_counts, sizeof(Counters)));
@@ -360,10 +486,18 @@ int fbp_pursuit_chunk(float *voltage, uint32_t n, uint32_t C, const float *templ
             S.launches[FBP_STAGE_LISTS] += 3;
             timer.end(FBP_STAGE_LISTS);
             timer.begin(FBP_STAGE_OVERLAP);
-            if ((rc = launch_overlap(voltage, n, C, templates, K, L, w.cand, &w.cnt->n_cand, W, s, w.Lk,
-                                     nmax, thresholds, &w.cnt->ov_items, st)))
-                break;
-            S.launches[FBP_STAGE_OVERLAP] += 1;
+            if (w.fast) {
+                int nl = 0;
+                OvArgs A = ov_args(w, voltage, n, C, templates, K, L, nmax, thresholds, s, w.Lk, w.cand,
+                                   &w.cnt->n_cand, &w.cnt->ov_items);
+                if ((rc = ov_fast_pass(w, A, W, st, &nl))) break;
+                S.launches[FBP_STAGE_OVERLAP] += nl;
+            } else {
+                if ((rc = launch_overlap(voltage, n, C, templates, K, L, w.cand, &w.cnt->n_cand, W, s, w.Lk,
+                                         nmax, thresholds, &w.cnt->ov_items, st)))
+                    break;
+                S.launches[FBP_STAGE_OVERLAP] += 1;
+            }
             timer.end(FBP_STAGE_OVERLAP);
             timer.begin(FBP_STAGE_CHECK);
             if ((rc = launch_check_overlap(n, L, w.cand, &w.cnt->n_cand, W, s, w.ovr2, st))) break;

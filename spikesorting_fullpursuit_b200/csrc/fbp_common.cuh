@@ -6,6 +6,7 @@
 
 typedef uint32_t u32;
 typedef uint8_t u8;
+typedef uint16_t u16;
 typedef unsigned long long u64;
 
 namespace fbp {

@@ -1,0 +1,598 @@
+// Fast overlap recheck with exact refinement (sm_100a).
+//
+// The reference's overlap_recheck_indices (binary_pursuit.cl:444-654)
+// evaluates, for each candidate window and every (a, b, t) item, the
+// likelihood of the clipped sum of the best template k0 shifted by
+// da = a - n_max and template t shifted by db = b - n_max, over the window
+// [i0, i0+L), with C*L multiply-adds per item.  In exact arithmetic that
+// value splits into
+//
+//     LL(t,a,b) = G(a) + H(t,b) - X(k0,t,a,b)
+//     H(t,b)    = <t_t shifted by db, window>  - 0.5 * ||t_t clipped||^2   (G(a) = H(k0,a))
+//     X         = <t_k0 shifted by da, t_t shifted by db>, both clipped to the window
+//
+// H is a small per-candidate correlation; X depends only on the templates
+// and is read from prefix sums Q[k0][t][r][m] of the channel-summed product
+// t_k0[m] * t_t[m+r] (r = da - db):  X = Q[hi] - Q[lo] with
+// lo = max(0, -r, -da), hi = min(L, L-r, L-da).
+//
+// Each item gets an interval [lo, hi] guaranteed to contain the
+// reference's IEEE-binary32 value: the reference's own rounding is bounded by
+// gamma_n * (sum |s_j v_j| + sum s_j^2) with n the number of non-zero terms,
+// and sum |s_j v_j| <= (||F_a|| + ||T_b||) * ||window||,
+// sum s_j^2 <= ||F_a||^2 + ||T_b||^2 + 2|X|; kappa below covers twice that
+// (the reference's error plus this approximation's).  Only items whose
+// interval can reach the best one are re-evaluated exactly, in the
+// reference's order; the parse kernel's strict-greater scan over single-item
+// groups (.cl:699-706) then picks the same item as the reference.
+#pragma once
+#include "fbp_kernels.cuh"
+
+namespace fbp {
+
+constexpr int kOvListCap = 32;      // per-warp contender list during the sweep
+constexpr int kOvOutCap = 8;        // contenders kept per (candidate, template)
+constexpr int kOvRefCap = 64;       // contenders refined per candidate
+constexpr u32 kOvOverflow = 0xffffffffu;
+constexpr float kUnitRoundoff = 5.9604644775390625e-08f;   // 2^-24
+
+// Constants of one chunk (computed on the device once per call).
+struct OvConst {
+    float kappa;          // interval half-width multiplier
+    u32 cnz_max;          // max non-zero channels of a template
+};
+
+struct OvArgs {
+    u32 n, C, K, L, nmax, S;
+    const float *v, *T, *Lk, *thr;
+    const float *NT, *sNT, *tnorm;   // [K][S], [K][S], [K]
+    const float *Q;                  // [K][K][2L-1][L+1]
+    const OvConst *oc;
+    const u32 *cand, *n_cand;
+    u32 *best_idx, *best_lab, *ov_idx, *ov_lab;
+    float *best_ll;
+    u8 *ovr;
+    float *H;                        // [slot][K][S]
+    float *vn;                       // [slot]
+    u8 *cskip;                       // [slot]
+    u32 *k0_count, *k0_cursor, *k0_offset, *k0_active, *n_k0_active;
+    u32 *order;                      // [slot]
+    float *res_lb;                   // [slot][K]
+    u32 *res_cnt;                    // [slot][K]
+    u32 *res_item;                   // [slot][K][kOvOutCap]
+    float *res_hi;                   // [slot][K][kOvOutCap]
+    u32 *ref_cnt;                    // [slot]
+    u32 *ref_item;                   // [slot][kOvRefCap]
+    u8 *fallback;                    // [slot]
+    u64 *items_evaluated;
+};
+
+__device__ __forceinline__ float warp_max_f(float x) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) x = fmaxf(x, __shfl_xor_sync(0xffffffffu, x, o));
+    return x;
+}
+
+// ---------------------------------------------------------------- per chunk
+
+// NT[t][b] = sum_c sum_{j in J(db)} T[t][c][j-db]^2 (clipped energy), sNT its
+// square root, tnorm[t] = ||t||; kappa from the number of non-zero channels.
+__global__ void k_ov_chunk_tables(const float *__restrict__ T, u32 K, u32 C, u32 L, u32 nmax,
+                                  float *__restrict__ NT, float *__restrict__ sNT,
+                                  float *__restrict__ tnorm, OvConst *oc) {
+    const u32 S = 2 * nmax + 1;
+    for (u32 e = blockIdx.x * blockDim.x + threadIdx.x; e < K * S; e += gridDim.x * blockDim.x) {
+        const u32 t = e / S, b = e % S;
+        const int d = (int)b - (int)nmax;
+        const int j0 = max(0, d), j1 = min((int)L, (int)L + d);
+        double acc = 0.0;
+        for (u32 c = 0; c < C; c++) {
+            const float *tp = T + ((size_t)t * C + c) * L;
+            for (int j = j0; j < j1; j++) {
+                const double x = tp[j - d];
+                acc += x * x;
+            }
+        }
+        NT[e] = (float)(acc * (1.0 + 1e-6));
+        sNT[e] = (float)(sqrt(acc) * (1.0 + 1e-6));
+    }
+    if (blockIdx.x == 0) {
+        __shared__ u32 cmax;
+        if (threadIdx.x == 0) cmax = 0;
+        __syncthreads();
+        for (u32 t = threadIdx.x; t < K; t += blockDim.x) {
+            double ss = 0.0;
+            u32 nz = 0;
+            for (u32 c = 0; c < C; c++) {
+                const float *tp = T + ((size_t)t * C + c) * L;
+                bool any = false;
+                for (u32 j = 0; j < L; j++) {
+                    ss += (double)tp[j] * tp[j];
+                    any |= tp[j] != 0.0f;
+                }
+                nz += any;
+            }
+            tnorm[t] = (float)(sqrt(ss) * (1.0 + 1e-6));
+            atomicMax(&cmax, nz);
+        }
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            oc->cnz_max = cmax;
+            // twice gamma_n for the reference's sum plus this approximation
+            const double nterms = 2.0 * cmax * L + C + L + 8.0;
+            oc->kappa = (float)(4.0 * nterms * (double)kUnitRoundoff);
+        }
+    }
+}
+
+// Q[k0][t][ri][m] = sum_{m' < m} sum_c T[k0][c][m'] * T[t][c][m'+r], r = ri-(L-1).
+// One thread per (k0, t, ri) row, accumulated in double, stored in float.
+__global__ void k_ov_q_table(const float *__restrict__ T, u32 K, u32 C, u32 L, float *__restrict__ Q) {
+    const u32 R = 2 * L - 1;
+    const u64 rows = (u64)K * K * R;
+    for (u64 e = (u64)blockIdx.x * blockDim.x + threadIdx.x; e < rows; e += (u64)gridDim.x * blockDim.x) {
+        const u32 ri = (u32)(e % R);
+        const u32 t = (u32)((e / R) % K);
+        const u32 k0 = (u32)(e / ((u64)R * K));
+        const int r = (int)ri - (int)(L - 1);
+        float *q = Q + e * (L + 1);
+        double acc = 0.0;
+        q[0] = 0.0f;
+        for (u32 m = 0; m < L; m++) {
+            const int mt = (int)m + r;
+            if (mt >= 0 && mt < (int)L) {
+                for (u32 c = 0; c < C; c++)
+                    acc += (double)T[((size_t)k0 * C + c) * L + m] * (double)T[((size_t)t * C + c) * L + mt];
+            }
+            q[m + 1] = (float)acc;
+        }
+    }
+}
+
+// ---------------------------------------------------------------- per pass
+
+// One warp per candidate slot: skip rules of .cl:518-527, window energy,
+// label histogram.
+__global__ void k_ov_prep(OvArgs A) {
+    const u32 nc = *A.n_cand;
+    const u32 lane = threadIdx.x & 31;
+    for (u32 g = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); g < nc;
+         g += gridDim.x * (blockDim.x >> 5)) {
+        const u32 id = A.cand[g];
+        const u32 lab = A.best_lab[id], bidx = A.best_idx[id];
+        const float bll = A.Lk[(size_t)lab * A.n + bidx];
+        const bool skip = (bll < A.thr[lab]) || (bidx >= A.n - A.L);
+        double e = 0.0;
+        if (!skip)
+            for (u32 q = lane; q < A.C * A.L; q += 32) {
+                const double x = A.v[(size_t)(q / A.L) * A.n + bidx + q % A.L];
+                e += x * x;
+            }
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) e += __shfl_xor_sync(0xffffffffu, e, o);
+        if (lane == 0) {
+            A.cskip[g] = skip;
+            A.vn[g] = (float)(sqrt(e) * (1.0 + 1e-6));
+            A.fallback[g] = 0;
+            A.ref_cnt[g] = 0;
+            if (!skip) atomicAdd(&A.k0_count[lab], 1u);
+        }
+    }
+}
+
+// One block: offsets of the label groups and the list of labels present.
+__global__ void k_ov_group(OvArgs A) {
+    if (threadIdx.x == 0) {
+        u32 off = 0, na = 0;
+        for (u32 k = 0; k < A.K; k++) {
+            A.k0_offset[k] = off;
+            A.k0_cursor[k] = 0;
+            off += A.k0_count[k];
+            if (A.k0_count[k]) A.k0_active[na++] = k;
+        }
+        *A.n_k0_active = na;
+    }
+}
+
+__global__ void k_ov_scatter(OvArgs A) {
+    const u32 nc = *A.n_cand;
+    for (u32 g = blockIdx.x * blockDim.x + threadIdx.x; g < nc; g += gridDim.x * blockDim.x) {
+        if (A.cskip[g]) continue;
+        const u32 lab = A.best_lab[A.cand[g]];
+        A.order[A.k0_offset[lab] + atomicAdd(&A.k0_cursor[lab], 1u)] = g;
+    }
+}
+
+// H[g][t][b] for every template t and shift b of candidate g: correlation of
+// t shifted by db with the window voltage (zero outside [i0, i0+L)), minus
+// half the clipped energy.  FP32 FMA; its error is inside kappa.
+// Thread tile: 8 shifts x 8 templates; per channel the window strip and the
+// templates' channel slab ([m][t], t contiguous) are staged in shared memory.
+constexpr int kTabThreads = 256;
+__global__ void __launch_bounds__(kTabThreads)
+k_ov_tables(OvArgs A) {
+    extern __shared__ float sm[];
+    const u32 S = A.S, K = A.K, L = A.L, C = A.C, nmax = A.nmax;
+    const u32 Lp = (L + 7) & ~7u;                  // lags padded to 8
+    const u32 Sg = (S + 7) / 8, Kg = (K + 7) / 8;  // output groups
+    const u32 Sp = Sg * 8, Kp = Kg * 8;
+    const u32 strip_len = Sp + Lp + 8;
+    float *strip = sm;                             // [strip_len]
+    float *slab = sm + strip_len;                  // [Lp][Kp]
+    const u32 nc = *A.n_cand;
+    const u32 groups = Sg * Kg;
+    for (u32 g = blockIdx.x; g < nc; g += gridDim.x) {
+        if (A.cskip[g]) continue;
+        const u32 id = A.cand[g];
+        const u32 bidx = A.best_idx[id];
+        for (u32 gb = 0; gb < groups; gb += blockDim.x) {
+            const u32 my = gb + threadIdx.x;
+            const bool active = my < groups;
+            const u32 sg = active ? my % Sg : 0, kg = active ? my / Sg : 0;
+            float acc[8][8];
+#pragma unroll
+            for (int i = 0; i < 8; i++)
+#pragma unroll
+                for (int j = 0; j < 8; j++) acc[i][j] = 0.0f;
+            for (u32 c = 0; c < C; c++) {
+                __syncthreads();
+                // strip[x] = window voltage at position i0 - nmax + x (zero outside [i0, i0+L))
+                for (u32 x = threadIdx.x; x < strip_len; x += blockDim.x) {
+                    const int rel = (int)x - (int)nmax;   // position relative to i0
+                    strip[x] = (rel >= 0 && rel < (int)L) ? A.v[(size_t)c * A.n + bidx + rel] : 0.0f;
+                }
+                for (u32 e = threadIdx.x; e < Lp * Kp; e += blockDim.x) {
+                    const u32 m = e / Kp, t = e % Kp;
+                    slab[e] = (m < L && t < K) ? A.T[((size_t)t * C + c) * L + m] : 0.0f;
+                }
+                __syncthreads();
+                if (!active) continue;
+                const float *sp = strip + sg * 8;
+                const float *tp = slab + kg * 8;
+                for (u32 m0 = 0; m0 < Lp; m0 += 8) {
+                    float w[16];
+#pragma unroll
+                    for (int q = 0; q < 16; q++) w[q] = sp[m0 + q];
+#pragma unroll
+                    for (int mm = 0; mm < 8; mm++) {
+                        const float4 t0 = *reinterpret_cast<const float4 *>(tp + (m0 + mm) * Kp);
+                        const float4 t1 = *reinterpret_cast<const float4 *>(tp + (m0 + mm) * Kp + 4);
+                        const float tv[8] = {t0.x, t0.y, t0.z, t0.w, t1.x, t1.y, t1.z, t1.w};
+#pragma unroll
+                        for (int i = 0; i < 8; i++)
+#pragma unroll
+                            for (int j = 0; j < 8; j++) acc[i][j] = fmaf(tv[j], w[i + mm], acc[i][j]);
+                    }
+                }
+            }
+            if (active) {
+#pragma unroll
+                for (int j = 0; j < 8; j++) {
+                    const u32 t = kg * 8 + j;
+                    if (t >= K) continue;
+#pragma unroll
+                    for (int i = 0; i < 8; i++) {
+                        const u32 b = sg * 8 + i;
+                        if (b < S)
+                            A.H[((size_t)g * K + t) * S + b] = acc[i][j] - 0.5f * A.NT[(size_t)t * S + b];
+                    }
+                }
+            }
+        }
+    }
+}
+
+// Warp-shared contender list during the sweep.
+struct OvList {
+    u32 item[kOvListCap];
+    float hi[kOvListCap];
+};
+
+// Drop entries whose upper bound fell below lb (warp-cooperative).
+__device__ __forceinline__ u32 ov_list_prune(OvList &Ls, u32 cnt, float lb, u32 lane) {
+    u32 it = 0;
+    float hv = -INFINITY;
+    bool keep = false;
+    if (lane < cnt) {
+        it = Ls.item[lane];
+        hv = Ls.hi[lane];
+        keep = hv >= lb;
+    }
+    const u32 m = __ballot_sync(0xffffffffu, keep);
+    __syncwarp();
+    if (keep) {
+        const u32 p = __popc(m & ((1u << lane) - 1u));
+        Ls.item[p] = it;
+        Ls.hi[p] = hv;
+    }
+    __syncwarp();
+    return __popc(m);
+}
+
+// Sweep: one task per (label k0 present this pass, template t).  Q[k0][t]
+// is staged once; each warp walks the candidates of label k0 and enumerates
+// the items that survive the reference's skip rules (.cl:534-576): a with
+// L[k0][afix] not <= 0 (all b within L of a), or (t, b) with L[t][ashift]
+// not <= 0 (all other a within L of b).
+constexpr int kSweepThreads = 512;
+// Per-warp scratch of the sweep: ga_lo, ga_hi, hb_lo, hb_hi (S floats each),
+// the a and b row lists (S u16 each), then the contender list.
+__host__ __device__ inline size_t sweep_warp_bytes(u32 S) {
+    return align_up(align_up((size_t)20 * S, 16) + sizeof(OvList), 16);
+}
+__host__ __device__ inline size_t sweep_smem_bytes(u32 S, u32 L) {
+    return align_up((size_t)(2 * L - 1) * (L + 1) * 4 + (size_t)4 * S * 4, 16) +
+           (size_t)(kSweepThreads / 32) * sweep_warp_bytes(S);
+}
+__host__ __device__ inline size_t tables_smem_bytes(u32 S, u32 K, u32 L) {
+    const size_t Lp = (L + 7) & ~7u, Sp = (size_t)(S + 7) / 8 * 8, Kp = (size_t)(K + 7) / 8 * 8;
+    return (Sp + Lp + 8 + Lp * Kp) * 4;
+}
+__global__ void __launch_bounds__(kSweepThreads)
+k_ov_sweep(OvArgs A) {
+    extern __shared__ float sm[];
+    const u32 S = A.S, K = A.K, L = A.L, nmax = A.nmax, n = A.n;
+    const u32 R = 2 * L - 1;
+    const u32 nwarps = blockDim.x >> 5, warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    float *q = sm;                                  // [R][L+1]
+    float *nt0 = q + (size_t)R * (L + 1);           // NT[k0][S], sNT[k0][S], NT[t][S], sNT[t][S]
+    float *snt0 = nt0 + S, *ntt = snt0 + S, *sntt = ntt + S;
+    char *wbase = (char *)sm + align_up((size_t)R * (L + 1) * 4 + (size_t)4 * S * 4, 16);
+    const size_t per_warp = sweep_warp_bytes(S);
+    const u32 ntasks = *A.n_k0_active * K;
+    const float kappa = A.oc->kappa;
+    for (u32 task = blockIdx.x; task < ntasks; task += gridDim.x) {
+        const u32 k0 = A.k0_active[task / K], t = task % K;
+        __syncthreads();
+        const float *qg = A.Q + ((size_t)k0 * K + t) * R * (L + 1);
+        for (u32 e = threadIdx.x; e < R * (L + 1); e += blockDim.x) q[e] = qg[e];
+        for (u32 b = threadIdx.x; b < S; b += blockDim.x) {
+            nt0[b] = A.NT[(size_t)k0 * S + b];
+            snt0[b] = A.sNT[(size_t)k0 * S + b];
+            ntt[b] = A.NT[(size_t)t * S + b];
+            sntt[b] = A.sNT[(size_t)t * S + b];
+        }
+        __syncthreads();
+        // per-warp scratch
+        float *ga_lo = (float *)(wbase + (size_t)warp * per_warp);
+        float *ga_hi = ga_lo + S, *hb_lo = ga_hi + S, *hb_hi = hb_lo + S;
+        u16 *alist = (u16 *)(hb_hi + S);
+        u16 *blist = alist + S;
+        OvList &Ls = *(OvList *)((char *)ga_lo + align_up((size_t)20 * S, 16));
+        const float eq = 4.0f * kUnitRoundoff * A.tnorm[k0] * A.tnorm[t];
+        const u32 gcount = A.k0_count[k0], goff = A.k0_offset[k0];
+        u32 evaluated = 0;
+        for (u32 ci = warp; ci < gcount; ci += nwarps) {
+            const u32 g = A.order[goff + ci];
+            const u32 id = A.cand[g];
+            const u32 bidx = A.best_idx[id];
+            const float lbest = A.best_ll[id];
+            const float vn = A.vn[g];
+            const float *Hg = A.H + (size_t)g * K * S;
+            // rows for a (label k0) and b (template t), and the surviving-item lists
+            u32 na = 0, nb = 0;
+            for (u32 x0 = 0; x0 < S; x0 += 32) {
+                const u32 x = x0 + lane;
+                bool ap = false, bp = false;
+                if (x < S) {
+                    const float G = Hg[(size_t)k0 * S + x];
+                    const float ea = kappa * (snt0[x] * vn + nt0[x] + fabsf(G));
+                    ga_lo[x] = G - ea;
+                    ga_hi[x] = G + ea;
+                    const float Hv = Hg[(size_t)t * S + x];
+                    const float eb = kappa * (sntt[x] * vn + ntt[x] + fabsf(Hv)) + eq;
+                    hb_lo[x] = Hv - eb;
+                    hb_hi[x] = Hv + eb;
+                    const bool inb = !(x + bidx < nmax || x + bidx >= n - L + nmax);
+                    if (inb) {
+                        const u32 pos = bidx + x - nmax;
+                        ap = !(A.Lk[(size_t)k0 * n + pos] <= 0.0f);
+                        bp = !(A.Lk[(size_t)t * n + pos] <= 0.0f);
+                    }
+                }
+                const u32 ma = __ballot_sync(0xffffffffu, ap), mb = __ballot_sync(0xffffffffu, bp);
+                if (ap) alist[na + __popc(ma & ((1u << lane) - 1u))] = (u16)x;
+                if (bp) blist[nb + __popc(mb & ((1u << lane) - 1u))] = (u16)x;
+                na += __popc(ma);
+                nb += __popc(mb);
+            }
+            __syncwarp();
+            float lb = -INFINITY;
+            u32 cnt = 0;
+            bool overflow = false;
+            // enumerate items: phase 0 rows a in alist (all b), phase 1 rows b in blist (a not in alist)
+            for (int phase = 0; phase < 2; phase++) {
+                const u32 nrows = phase == 0 ? na : nb;
+                for (u32 ri = 0; ri < nrows; ri++) {
+                    const u32 fixed = phase == 0 ? alist[ri] : blist[ri];
+                    const u32 lo_x = fixed > L ? fixed - L : 0;
+                    const u32 hi_x = min(S - 1, fixed + L);
+                    for (u32 x0 = lo_x; x0 <= hi_x; x0 += 32) {
+                        const u32 x = x0 + lane;
+                        const u32 a = phase == 0 ? fixed : x;
+                        const u32 b = phase == 0 ? x : fixed;
+                        bool valid = x <= hi_x;
+                        if (valid) {
+                            // bounds of the moving index (.cl:534-541)
+                            valid = !(x + bidx < nmax || x + bidx >= n - L + nmax);
+                            if (valid && phase == 1) {
+                                // rows a with L[k0][afix] > 0 were enumerated in phase 0
+                                const u32 pos = bidx + a - nmax;
+                                valid = (A.Lk[(size_t)k0 * n + pos] <= 0.0f);
+                            }
+                        }
+                        float lo = -INFINITY, hi = -INFINITY;
+                        u32 item = 0;
+                        if (valid) {
+                            const int r = (int)a - (int)b;
+                            float X = 0.0f;
+                            if (r > -(int)L && r < (int)L) {
+                                const int da = (int)a - (int)nmax;
+                                const int lo_m = max(max(0, -r), -da);
+                                const int hi_m = min(min((int)L, (int)L - r), (int)L - da);
+                                if (lo_m < hi_m) {
+                                    const float *qr = q + (size_t)(r + (int)L - 1) * (L + 1);
+                                    X = qr[hi_m] - qr[lo_m];
+                                }
+                            }
+                            const float ex = 2.0f * kappa * fabsf(X);
+                            hi = ga_hi[a] + hb_hi[b] - X + ex;
+                            lo = ga_lo[a] + hb_lo[b] - X - ex;
+                            item = t + K * (a + S * b);
+                            evaluated++;
+                        }
+                        lb = fmaxf(lb, warp_max_f(lo));
+                        const bool keep = valid && hi > lbest && hi >= lb;
+                        const u32 mk = __ballot_sync(0xffffffffu, keep);
+                        if (mk) {
+                            const u32 add = __popc(mk);
+                            if (cnt + add > kOvListCap) cnt = ov_list_prune(Ls, cnt, lb, lane);
+                            if (cnt + add > kOvListCap) {
+                                overflow = true;
+                            } else {
+                                if (keep) {
+                                    const u32 p = cnt + __popc(mk & ((1u << lane) - 1u));
+                                    Ls.item[p] = item;
+                                    Ls.hi[p] = hi;
+                                }
+                                cnt += add;
+                                __syncwarp();
+                            }
+                        }
+                    }
+                }
+            }
+            cnt = ov_list_prune(Ls, cnt, lb, lane);
+            const size_t slot = (size_t)g * K + t;
+            if (lane == 0) {
+                A.res_lb[slot] = lb;
+                A.res_cnt[slot] = (overflow || cnt > kOvOutCap) ? kOvOverflow : cnt;
+            }
+            if (!overflow && lane < cnt && lane < kOvOutCap) {
+                A.res_item[slot * kOvOutCap + lane] = Ls.item[lane];
+                A.res_hi[slot * kOvOutCap + lane] = Ls.hi[lane];
+            }
+            __syncwarp();
+        }
+        if (A.items_evaluated) {
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) evaluated += __shfl_xor_sync(0xffffffffu, evaluated, o);
+            if (lane == 0 && evaluated) atomicAdd(A.items_evaluated, (u64)evaluated);
+        }
+    }
+}
+
+// One warp per candidate slot: the best lower bound over all templates and
+// the contenders whose upper bound reaches it.
+__global__ void k_ov_merge(OvArgs A) {
+    const u32 nc = *A.n_cand;
+    const u32 lane = threadIdx.x & 31, K = A.K;
+    for (u32 g = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); g < nc;
+         g += gridDim.x * (blockDim.x >> 5)) {
+        if (A.cskip[g]) continue;
+        const float lbest = A.best_ll[A.cand[g]];
+        float lb = -INFINITY;
+        bool ov = false;
+        for (u32 t = lane; t < K; t += 32) {
+            lb = fmaxf(lb, A.res_lb[(size_t)g * K + t]);
+            ov |= A.res_cnt[(size_t)g * K + t] == kOvOverflow;
+        }
+        lb = warp_max_f(lb);
+        ov = __any_sync(0xffffffffu, ov);
+        u32 cnt = 0;
+        if (!ov) {
+            for (u32 t0 = 0; t0 < K; t0 += 32) {
+                const u32 t = t0 + lane;
+                const u32 c = t < K ? A.res_cnt[(size_t)g * K + t] : 0;
+                for (u32 e = 0; e < kOvOutCap; e++) {
+                    bool keep = false;
+                    u32 it = 0;
+                    if (e < c) {
+                        const size_t s = ((size_t)g * K + t) * kOvOutCap + e;
+                        keep = A.res_hi[s] >= lb && A.res_hi[s] > lbest;
+                        it = A.res_item[s];
+                    }
+                    const u32 m = __ballot_sync(0xffffffffu, keep);
+                    if (keep) {
+                        const u32 p = cnt + __popc(m & ((1u << lane) - 1u));
+                        if (p < kOvRefCap) A.ref_item[(size_t)g * kOvRefCap + p] = it;
+                    }
+                    cnt += __popc(m);
+                }
+            }
+        }
+        if (lane == 0) {
+            A.ref_cnt[g] = cnt;
+            A.fallback[g] = (ov || cnt > kOvRefCap) ? 1 : 0;
+        }
+    }
+}
+
+// Exact value of one item (reference order), window read from global memory.
+__device__ float overlap_item_exact_global(const OvArgs &A, u32 lab, u32 bidx, u32 t, u32 a, u32 b) {
+    const u32 L = A.L, C = A.C;
+    const u32 afix = bidx + a - A.nmax, ashift = bidx + b - A.nmax;
+    const int fa = (int)bidx - (int)afix, sa = (int)bidx - (int)ashift;
+    const u32 ffj = fa < 0 ? (u32)(-fa) : 0u, sfj = sa < 0 ? (u32)(-sa) : 0u;
+    float cml = 0.0f;
+    for (u32 c = 0; c < C; c++) {
+        const float *f = A.T + ((size_t)lab * C + c) * L;
+        const float *s = A.T + ((size_t)t * C + c) * L;
+        const float *vv = A.v + (size_t)c * A.n + bidx;
+        float ss = 0.0f;
+        for (u32 j = 0; j < L; j++) {
+            float fv = 0.0f, sv = 0.0f;
+            if (j >= ffj && (u32)(fa + (int)j) < L) fv = __ldg(f + fa + (int)j);
+            if (j >= sfj && (u32)(sa + (int)j) < L) sv = __ldg(s + sa + (int)j);
+            const float sum = __fadd_rn(fv, sv);
+            ss = __fadd_rn(ss, __fmul_rn(sum, sum));
+            cml = __fadd_rn(cml, __fmul_rn(sum, __ldg(vv + j)));
+        }
+        if ((double)ss > 0.0) cml = __double2float_rn(__dsub_rn((double)cml, __dmul_rn(0.5, (double)ss)));
+    }
+    return cml;
+}
+
+// One warp per candidate slot: exact values of the contenders, the first
+// (lowest item id) maximum above the current best, and the parse decision.
+__global__ void k_ov_refine(OvArgs A) {
+    const u32 nc = *A.n_cand;
+    const u32 lane = threadIdx.x & 31, K = A.K, S = A.S;
+    for (u32 g = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); g < nc;
+         g += gridDim.x * (blockDim.x >> 5)) {
+        if (A.fallback[g]) continue;
+        const u32 id = A.cand[g];
+        const float start = A.best_ll[id];
+        float bv = start;
+        u64 bi = ~0ull;
+        if (!A.cskip[g]) {
+            const u32 lab = A.best_lab[id], bidx = A.best_idx[id];
+            const u32 cnt = A.ref_cnt[g];
+            for (u32 e = lane; e < cnt; e += 32) {
+                const u32 it = A.ref_item[(size_t)g * kOvRefCap + e];
+                const u32 t = it % K, a = (it / K) % S, b = it / (K * S);
+                const float ll = overlap_item_exact_global(A, lab, bidx, t, a, b);
+                if (ll > bv || (ll == bv && ll > start && it < bi)) { bv = ll; bi = it; }
+            }
+        }
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+            const float ov = __shfl_xor_sync(0xffffffffu, bv, o);
+            const u64 oi = __shfl_xor_sync(0xffffffffu, bi, o);
+            if (ov > bv || (ov == bv && oi < bi)) { bv = ov; bi = oi; }
+        }
+        if (lane == 0)
+            overlap_parse(id, A.n, K, S, A.nmax, bv, bi == ~0ull ? 0 : bi, A.best_idx, A.best_lab, A.best_ll,
+                          A.ov_idx, A.ov_lab, A.ovr, A.Lk, A.thr);
+    }
+}
+
+// Window ids of the candidates that overflowed a contender list.
+__global__ void k_ov_fallback_list(OvArgs A, const u32 *__restrict__ slots, const u32 *__restrict__ n_slots,
+                                   u32 *__restrict__ out) {
+    const u32 m = *n_slots;
+    for (u32 i = blockIdx.x * blockDim.x + threadIdx.x; i < m; i += gridDim.x * blockDim.x)
+        out[i] = A.cand[slots[i]];
+}
+
+}  // namespace fbp

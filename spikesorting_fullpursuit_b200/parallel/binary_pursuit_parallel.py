@@ -50,7 +50,8 @@ def _to_device_f32(torch, host_chunk, dev, stream):
 
 def binary_pursuit(voltage, v_dtype, sort_info, separability_metrics, n_max_shift_inds=None,
                    kernels_path=None, max_gpu_memory=None, *, precision="fp32",
-                   chunk_samples=None, device=None, max_passes=1000000, stats=None, profile=False):
+                   chunk_samples=None, device=None, max_passes=1000000, stats=None, profile=False,
+                   overlap="fast"):
     """Full Binary Pursuit over `voltage` ([channels, samples], any real dtype).
 
     Returns (event_indices int64, neuron_labels int64, binary_pursuit_spike_bool
@@ -66,6 +67,9 @@ def binary_pursuit(voltage, v_dtype, sort_info, separability_metrics, n_max_shif
                      device memory, :276-341); needed to reproduce a given
                      chunking exactly.
       device         CUDA device index (default: current device).
+      overlap        "fast" (decomposed overlap recheck with exact refinement)
+                     or "exact" (every item in the reference's order); both
+                     give the reference's result.
       stats          a list; one dict per chunk is appended (passes, spikes,
                      per-stage launches, work and, with profile=True, CUDA-event
                      milliseconds).
@@ -80,6 +84,9 @@ def binary_pursuit(voltage, v_dtype, sort_info, separability_metrics, n_max_shif
     if precision not in _PRECISIONS:
         raise ValueError("precision must be one of %s" % sorted(_PRECISIONS))
     prec = _PRECISIONS[precision]
+    if overlap not in ("fast", "exact"):
+        raise ValueError("overlap must be 'fast' or 'exact'")
+    ov_method = _lib.OVERLAP_FAST if overlap == "fast" else _lib.OVERLAP_EXACT
 
     n_chans = int(voltage.shape[0])
     n_samples = int(voltage.shape[1])
@@ -138,7 +145,7 @@ def binary_pursuit(voltage, v_dtype, sort_info, separability_metrics, n_max_shif
             sst = _lib.StageStats()
             rc = lib.fbp_pursuit_chunk(
                 _lib.ptr(v_d), n, n_chans, _lib.ptr(T_d), K, L, _lib.ptr(tss_d), _lib.ptr(thr_d),
-                n_max_shift_inds, int(bool(sort_info['do_overlap_recheck'])), prec, int(max_passes),
+                n_max_shift_inds, int(bool(sort_info['do_overlap_recheck'])), prec, ov_method, int(max_passes),
                 _lib.ptr(ws), ws.numel(), _lib.ptr(out_i), _lib.ptr(out_l), cap, None,
                 ctypes.byref(nspk), ctypes.byref(npass), int(bool(profile)), ctypes.byref(sst), sp)
             if rc == _lib.FBP_ERR_CAPACITY:

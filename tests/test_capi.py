@@ -51,7 +51,7 @@ def test_workspace_size_is_host_only(lib):
 
 def test_null_arguments_rejected_before_any_cuda_call(lib):
     n1, n2 = ctypes.c_uint32(0), ctypes.c_uint32(0)
-    rc = lib.fbp_pursuit_chunk(None, 100, 4, None, 8, 31, None, None, 30, 1, 0, 10, None, 0,
+    rc = lib.fbp_pursuit_chunk(None, 100, 4, None, 8, 31, None, None, 30, 1, 0, 0, 10, None, 0,
                                None, None, 0, None, ctypes.byref(n1), ctypes.byref(n2), 0, None, None)
     assert rc == _lib.FBP_ERR_BAD_ARG
     assert b"null pointer" in lib.fbp_last_error()

@@ -107,6 +107,33 @@ def test_binary_pursuit_matches_oracle(lib, cfg):
     assert_same_outputs(got, tuple(np.asarray(x) for x in exp), isinstance(exp[0], list))
 
 
+@pytest.mark.parametrize("overlap", ["fast", "exact"])
+def test_overlap_methods_agree_with_oracle(lib, overlap):
+    rec = synthetic.linear16(duration_s=0.08, seed=111, n_templates=24, L=61)
+    si = rec.sort_info()
+    exp = O.binary_pursuit_oracle(rec.voltage, rec.voltage.dtype, si, rec.fresh_metrics(), n_max_shift_inds=60)
+    got = bpp.binary_pursuit(rec.voltage, rec.voltage.dtype, si, rec.fresh_metrics(), n_max_shift_inds=60,
+                             overlap=overlap)
+    assert_same_outputs(got, tuple(np.asarray(x) for x in exp))
+
+
+def test_fast_overlap_exact_ties_between_duplicate_templates(lib):
+    """Two copies of every template: overlap items of twin templates tie
+    exactly, so the lowest item id must win, as in the reference."""
+    rec = synthetic.tetrode(duration_s=0.5, seed=112, L=41, n_templates=4)
+    m = rec.fresh_metrics()
+    for key in ("templates", "template_SS", "neuron_lower_thresholds"):
+        m[key] = np.concatenate([m[key], m[key]], axis=0)
+    m["template_SS_by_chan"] = np.zeros((8, rec.n_chans))
+    si = rec.sort_info(get_adjusted_clips=True)
+    m2 = {k: v.copy() for k, v in m.items()}
+    exp = O.binary_pursuit_oracle(rec.voltage, rec.voltage.dtype, si, m, n_max_shift_inds=40)
+    stats = []
+    got = bpp.binary_pursuit(rec.voltage, rec.voltage.dtype, si, m2, n_max_shift_inds=40, stats=stats)
+    assert_same_outputs(got, tuple(np.asarray(x) for x in exp))
+    assert stats[0]["candidates"] > 0
+
+
 # ----------------------------------------------------------------- stages
 
 def _rng(seed):
