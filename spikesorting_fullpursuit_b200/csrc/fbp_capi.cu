@@ -68,11 +68,11 @@ struct Workspace {
     // fast overlap recheck (present when `fast`)
     bool fast;
     u32 slots;
-    float *NT, *sNT, *tnorm, *Q, *H, *vn, *res_lb, *res_hi;
+    float *NT, *sNT, *tnorm, *Q, *H, *vn, *res_lb, *res_hi, *cand_lb;
     OvConst *oc;
-    u8 *cskip, *fallback;
-    u32 *k0_count, *k0_cursor, *k0_offset, *k0_active, *n_k0_active, *order, *res_cnt, *res_item;
-    u32 *ref_cnt, *ref_item, *fb_slots, *fb_list, *fb_count;
+    u8 *cskip, *fallback, *need;
+    u32 *k0_count, *k0_cursor, *k0_offset, *k0_active, *n_k0_active, *order;
+    u32 *pool_cnt, *pool_item, *fb_slots, *fb_list, *fb_count;
     size_t bytes;
 };
 
@@ -142,11 +142,11 @@ Workspace layout(char *base, u32 n, u32 K, u32 L, u32 nmax, bool want_fast) {
         w.n_k0_active = (u32 *)take(4);
         w.order = (u32 *)take(sl * 4);
         w.res_lb = (float *)take(sl * K * 4);
-        w.res_cnt = (u32 *)take(sl * K * 4);
-        w.res_item = (u32 *)take(sl * K * kOvOutCap * 4);
-        w.res_hi = (float *)take(sl * K * kOvOutCap * 4);
-        w.ref_cnt = (u32 *)take(sl * 4);
-        w.ref_item = (u32 *)take(sl * kOvRefCap * 4);
+        w.res_hi = (float *)take(sl * K * 4);
+        w.need = (u8 *)take(sl * K);
+        w.cand_lb = (float *)take(sl * 4);
+        w.pool_cnt = (u32 *)take(sl * 4);
+        w.pool_item = (u32 *)take(sl * kOvPoolCap * 4);
         w.fb_slots = (u32 *)take(sl * 4);
         w.fb_list = (u32 *)take(sl * 4);
         w.fb_count = (u32 *)take(4);
@@ -268,8 +268,8 @@ OvArgs ov_args(const Workspace &w, const float *v, u32 n, u32 C, const float *T,
     A.H = w.H; A.vn = w.vn; A.cskip = w.cskip;
     A.k0_count = w.k0_count; A.k0_cursor = w.k0_cursor; A.k0_offset = w.k0_offset;
     A.k0_active = w.k0_active; A.n_k0_active = w.n_k0_active; A.order = w.order;
-    A.res_lb = w.res_lb; A.res_cnt = w.res_cnt; A.res_item = w.res_item; A.res_hi = w.res_hi;
-    A.ref_cnt = w.ref_cnt; A.ref_item = w.ref_item; A.fallback = w.fallback;
+    A.res_lb = w.res_lb; A.res_hi = w.res_hi; A.need = w.need; A.cand_lb = w.cand_lb;
+    A.pool_cnt = w.pool_cnt; A.pool_item = w.pool_item; A.fallback = w.fallback;
     A.items_evaluated = items;
     return A;
 }
@@ -291,6 +291,7 @@ int ov_fast_pass(const Workspace &w, const OvArgs &A, u32 W, cudaStream_t st, in
     const u32 S = A.S;
     FBP_CUDA(cudaMemsetAsync(w.k0_count, 0, (size_t)A.K * 4, st));
     FBP_CUDA(cudaMemsetAsync(w.fallback, 0, align_up((size_t)slots + FBP_WINDOW_PAD, kCompactTile), st));
+    (void)W;
     k_ov_prep<<<grid_for((u64)slots * 32, 256), 256, 0, st>>>(A);
     k_ov_group<<<1, 32, 0, st>>>(A);
     k_ov_scatter<<<grid_for(slots, 256), 256, 0, st>>>(A);
@@ -302,14 +303,13 @@ int ov_fast_pass(const Workspace &w, const OvArgs &A, u32 W, cudaStream_t st, in
         k_ov_tables<<<grid_for((u64)slots * kTabThreads, kTabThreads, 4), kTabThreads, smem, st>>>(A);
         FBP_LAUNCH_CHECK();
     }
-    {
-        const size_t smem = sweep_smem_bytes(S, A.L);
-        if (smem > 48 * 1024)
-            FBP_CUDA(cudaFuncSetAttribute(k_ov_sweep, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-        k_ov_sweep<<<sm_count(), kSweepThreads, smem, st>>>(A);
-        FBP_LAUNCH_CHECK();
-    }
+    const size_t sweep_smem = sweep_smem_bytes(S, A.L);
+    if (sweep_smem > 48 * 1024)
+        FBP_CUDA(cudaFuncSetAttribute(k_ov_sweep, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sweep_smem));
+    k_ov_sweep<<<sm_count(), kSweepThreads, sweep_smem, st>>>(A, 0);
     k_ov_merge<<<grid_for((u64)slots * 32, 256), 256, 0, st>>>(A);
+    k_ov_sweep<<<sm_count(), kSweepThreads, sweep_smem, st>>>(A, 1);
+    k_ov_mark_fallback<<<grid_for(slots, 256), 256, 0, st>>>(A);
     k_ov_refine<<<grid_for((u64)slots * 32, 256), 256, 0, st>>>(A);
     FBP_LAUNCH_CHECK();
     int rc = compact(w.fallback, slots, w.fb_slots, w.fb_count, w.tile_counts, st);
@@ -319,7 +319,7 @@ int ov_fast_pass(const Workspace &w, const OvArgs &A, u32 W, cudaStream_t st, in
     fbp_window_state s{A.best_idx, A.best_lab, A.best_ll, A.ov_idx, A.ov_lab, nullptr, A.ovr};
     rc = launch_overlap(A.v, A.n, A.C, A.T, A.K, A.L, w.fb_list, w.fb_count, slots, s, A.Lk, A.nmax, A.thr,
                         A.items_evaluated, st);
-    *launches = 14;
+    *launches = 16;
     return rc;
 }
 

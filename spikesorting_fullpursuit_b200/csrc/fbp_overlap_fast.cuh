@@ -30,15 +30,13 @@
 
 namespace fbp {
 
-constexpr int kOvListCap = 32;      // per-warp contender list during the sweep
-constexpr int kOvOutCap = 8;        // contenders kept per (candidate, template)
-constexpr int kOvRefCap = 64;       // contenders refined per candidate
-constexpr u32 kOvOverflow = 0xffffffffu;
+constexpr u32 kOvPoolCap = 512;     // contenders refined exactly per candidate
 constexpr float kUnitRoundoff = 5.9604644775390625e-08f;   // 2^-24
 
 // Constants of one chunk (computed on the device once per call).
 struct OvConst {
-    float kappa;          // interval half-width multiplier
+    float kappa_ref;      // bound of the reference's rounding, per unit of sum|terms|
+    float kappa_mine;     // bound of this approximation's rounding
     u32 cnz_max;          // max non-zero channels of a template
 };
 
@@ -57,12 +55,12 @@ struct OvArgs {
     u8 *cskip;                       // [slot]
     u32 *k0_count, *k0_cursor, *k0_offset, *k0_active, *n_k0_active;
     u32 *order;                      // [slot]
-    float *res_lb;                   // [slot][K]
-    u32 *res_cnt;                    // [slot][K]
-    u32 *res_item;                   // [slot][K][kOvOutCap]
-    float *res_hi;                   // [slot][K][kOvOutCap]
-    u32 *ref_cnt;                    // [slot]
-    u32 *ref_item;                   // [slot][kOvRefCap]
+    float *res_lb;                   // [slot][K]  largest lower bound of (candidate, t)
+    float *res_hi;                   // [slot][K]  largest upper bound of (candidate, t)
+    u8 *need;                        // [slot][K]  (candidate, t) can hold a contender
+    float *cand_lb;                  // [slot]     largest lower bound of the candidate
+    u32 *pool_cnt;                   // [slot]
+    u32 *pool_item;                  // [slot][kOvPoolCap]
     u8 *fallback;                    // [slot]
     u64 *items_evaluated;
 };
@@ -118,9 +116,14 @@ __global__ void k_ov_chunk_tables(const float *__restrict__ T, u32 K, u32 C, u32
         __syncthreads();
         if (threadIdx.x == 0) {
             oc->cnz_max = cmax;
-            // twice gamma_n for the reference's sum plus this approximation
-            const double nterms = 2.0 * cmax * L + C + L + 8.0;
-            oc->kappa = (float)(4.0 * nterms * (double)kUnitRoundoff);
+            // gamma_n with n the reference's non-zero terms: products of two
+            // templates' channels, the per-channel subtractions and sums of
+            // squares, each product carrying two roundings
+            const double u = (double)kUnitRoundoff;
+            const double n_ref = 2.0 * cmax * L + C + 2.0 * L + 16.0;
+            const double n_mine = (double)cmax * L + 8.0;
+            oc->kappa_ref = (float)(1.05 * n_ref * u / (1.0 - n_ref * u));
+            oc->kappa_mine = (float)(1.05 * n_mine * u / (1.0 - n_mine * u));
         }
     }
 }
@@ -173,8 +176,7 @@ __global__ void k_ov_prep(OvArgs A) {
         if (lane == 0) {
             A.cskip[g] = skip;
             A.vn[g] = (float)(sqrt(e) * (1.0 + 1e-6));
-            A.fallback[g] = 0;
-            A.ref_cnt[g] = 0;
+            A.pool_cnt[g] = 0;
             if (!skip) atomicAdd(&A.k0_count[lab], 1u);
         }
     }
@@ -282,43 +284,11 @@ k_ov_tables(OvArgs A) {
     }
 }
 
-// Warp-shared contender list during the sweep.
-struct OvList {
-    u32 item[kOvListCap];
-    float hi[kOvListCap];
-};
-
-// Drop entries whose upper bound fell below lb (warp-cooperative).
-__device__ __forceinline__ u32 ov_list_prune(OvList &Ls, u32 cnt, float lb, u32 lane) {
-    u32 it = 0;
-    float hv = -INFINITY;
-    bool keep = false;
-    if (lane < cnt) {
-        it = Ls.item[lane];
-        hv = Ls.hi[lane];
-        keep = hv >= lb;
-    }
-    const u32 m = __ballot_sync(0xffffffffu, keep);
-    __syncwarp();
-    if (keep) {
-        const u32 p = __popc(m & ((1u << lane) - 1u));
-        Ls.item[p] = it;
-        Ls.hi[p] = hv;
-    }
-    __syncwarp();
-    return __popc(m);
-}
-
-// Sweep: one task per (label k0 present this pass, template t).  Q[k0][t]
-// is staged once; each warp walks the candidates of label k0 and enumerates
-// the items that survive the reference's skip rules (.cl:534-576): a with
-// L[k0][afix] not <= 0 (all b within L of a), or (t, b) with L[t][ashift]
-// not <= 0 (all other a within L of b).
 constexpr int kSweepThreads = 512;
 // Per-warp scratch of the sweep: ga_lo, ga_hi, hb_lo, hb_hi (S floats each),
-// the a and b row lists (S u16 each), then the contender list.
+// then the a and b row lists (S u16 each).
 __host__ __device__ inline size_t sweep_warp_bytes(u32 S) {
-    return align_up(align_up((size_t)20 * S, 16) + sizeof(OvList), 16);
+    return align_up((size_t)20 * S, 16);
 }
 __host__ __device__ inline size_t sweep_smem_bytes(u32 S, u32 L) {
     return align_up((size_t)(2 * L - 1) * (L + 1) * 4 + (size_t)4 * S * 4, 16) +
@@ -328,8 +298,19 @@ __host__ __device__ inline size_t tables_smem_bytes(u32 S, u32 K, u32 L) {
     const size_t Lp = (L + 7) & ~7u, Sp = (size_t)(S + 7) / 8 * 8, Kp = (size_t)(K + 7) / 8 * 8;
     return (Sp + Lp + 8 + Lp * Kp) * 4;
 }
+
+// Sweep over the items of one (label k0, template t) task.  Q[k0][t] is
+// staged once; each warp walks the candidates of label k0 and enumerates the
+// items that survive the reference's skip rules (.cl:534-576): rows a with
+// L[k0][afix] not <= 0 (every in-bounds b within L of a), then rows b with
+// L[t][ashift] not <= 0 (every other in-bounds a within L of b).
+//  mode 0: per (candidate, t) the largest lower bound and the largest upper
+//          bound of its items (res_lb, res_hi).
+//  mode 1: for the (candidate, t) pairs flagged by k_ov_merge, append every
+//          item whose upper bound reaches the candidate's best lower bound
+//          and exceeds its current best likelihood to the candidate's pool.
 __global__ void __launch_bounds__(kSweepThreads)
-k_ov_sweep(OvArgs A) {
+k_ov_sweep(OvArgs A, int mode) {
     extern __shared__ float sm[];
     const u32 S = A.S, K = A.K, L = A.L, nmax = A.nmax, n = A.n;
     const u32 R = 2 * L - 1;
@@ -338,11 +319,22 @@ k_ov_sweep(OvArgs A) {
     float *nt0 = q + (size_t)R * (L + 1);           // NT[k0][S], sNT[k0][S], NT[t][S], sNT[t][S]
     float *snt0 = nt0 + S, *ntt = snt0 + S, *sntt = ntt + S;
     char *wbase = (char *)sm + align_up((size_t)R * (L + 1) * 4 + (size_t)4 * S * 4, 16);
-    const size_t per_warp = sweep_warp_bytes(S);
+    float *ga_lo = (float *)(wbase + (size_t)warp * sweep_warp_bytes(S));
+    float *ga_hi = ga_lo + S, *hb_lo = ga_hi + S, *hb_hi = hb_lo + S;
+    u16 *alist = (u16 *)(hb_hi + S);
+    u16 *blist = alist + S;
     const u32 ntasks = *A.n_k0_active * K;
-    const float kappa = A.oc->kappa;
+    const float kr = A.oc->kappa_ref, km = A.oc->kappa_mine;
     for (u32 task = blockIdx.x; task < ntasks; task += gridDim.x) {
         const u32 k0 = A.k0_active[task / K], t = task % K;
+        const u32 gcount = A.k0_count[k0], goff = A.k0_offset[k0];
+        if (mode == 1) {
+            // nothing to collect for this task: skip staging
+            bool any = false;
+            for (u32 ci = threadIdx.x; ci < gcount && !any; ci += blockDim.x)
+                any = A.need[(size_t)A.order[goff + ci] * K + t] != 0;
+            if (!__syncthreads_or(any)) continue;
+        }
         __syncthreads();
         const float *qg = A.Q + ((size_t)k0 * K + t) * R * (L + 1);
         for (u32 e = threadIdx.x; e < R * (L + 1); e += blockDim.x) q[e] = qg[e];
@@ -353,34 +345,32 @@ k_ov_sweep(OvArgs A) {
             sntt[b] = A.sNT[(size_t)t * S + b];
         }
         __syncthreads();
-        // per-warp scratch
-        float *ga_lo = (float *)(wbase + (size_t)warp * per_warp);
-        float *ga_hi = ga_lo + S, *hb_lo = ga_hi + S, *hb_hi = hb_lo + S;
-        u16 *alist = (u16 *)(hb_hi + S);
-        u16 *blist = alist + S;
-        OvList &Ls = *(OvList *)((char *)ga_lo + align_up((size_t)20 * S, 16));
         const float eq = 4.0f * kUnitRoundoff * A.tnorm[k0] * A.tnorm[t];
-        const u32 gcount = A.k0_count[k0], goff = A.k0_offset[k0];
         u32 evaluated = 0;
         for (u32 ci = warp; ci < gcount; ci += nwarps) {
             const u32 g = A.order[goff + ci];
+            const size_t slot = (size_t)g * K + t;
+            if (mode == 1 && !A.need[slot]) continue;
             const u32 id = A.cand[g];
             const u32 bidx = A.best_idx[id];
             const float lbest = A.best_ll[id];
             const float vn = A.vn[g];
+            const float LB = mode == 1 ? A.cand_lb[g] : 0.0f;
             const float *Hg = A.H + (size_t)g * K * S;
-            // rows for a (label k0) and b (template t), and the surviving-item lists
+            // interval rows for a (label k0) and b (template t), and the item rows
             u32 na = 0, nb = 0;
             for (u32 x0 = 0; x0 < S; x0 += 32) {
                 const u32 x = x0 + lane;
                 bool ap = false, bp = false;
                 if (x < S) {
                     const float G = Hg[(size_t)k0 * S + x];
-                    const float ea = kappa * (snt0[x] * vn + nt0[x] + fabsf(G));
+                    const float fa = snt0[x] * vn + nt0[x];
+                    const float ea = (kr + km) * fa + 4.0f * kUnitRoundoff * fabsf(G);
                     ga_lo[x] = G - ea;
                     ga_hi[x] = G + ea;
                     const float Hv = Hg[(size_t)t * S + x];
-                    const float eb = kappa * (sntt[x] * vn + ntt[x] + fabsf(Hv)) + eq;
+                    const float fb = sntt[x] * vn + ntt[x];
+                    const float eb = (kr + km) * fb + 4.0f * kUnitRoundoff * fabsf(Hv) + eq;
                     hb_lo[x] = Hv - eb;
                     hb_hi[x] = Hv + eb;
                     const bool inb = !(x + bidx < nmax || x + bidx >= n - L + nmax);
@@ -397,10 +387,7 @@ k_ov_sweep(OvArgs A) {
                 nb += __popc(mb);
             }
             __syncwarp();
-            float lb = -INFINITY;
-            u32 cnt = 0;
-            bool overflow = false;
-            // enumerate items: phase 0 rows a in alist (all b), phase 1 rows b in blist (a not in alist)
+            float lbmax = -INFINITY, himax = -INFINITY;
             for (int phase = 0; phase < 2; phase++) {
                 const u32 nrows = phase == 0 ? na : nb;
                 for (u32 ri = 0; ri < nrows; ri++) {
@@ -411,18 +398,10 @@ k_ov_sweep(OvArgs A) {
                         const u32 x = x0 + lane;
                         const u32 a = phase == 0 ? fixed : x;
                         const u32 b = phase == 0 ? x : fixed;
-                        bool valid = x <= hi_x;
-                        if (valid) {
-                            // bounds of the moving index (.cl:534-541)
-                            valid = !(x + bidx < nmax || x + bidx >= n - L + nmax);
-                            if (valid && phase == 1) {
-                                // rows a with L[k0][afix] > 0 were enumerated in phase 0
-                                const u32 pos = bidx + a - nmax;
-                                valid = (A.Lk[(size_t)k0 * n + pos] <= 0.0f);
-                            }
-                        }
+                        bool valid = x <= hi_x && !(x + bidx < nmax || x + bidx >= n - L + nmax);
+                        if (valid && phase == 1)     // rows a with L[k0][afix] > 0 came in phase 0
+                            valid = (A.Lk[(size_t)k0 * n + bidx + a - nmax] <= 0.0f);
                         float lo = -INFINITY, hi = -INFINITY;
-                        u32 item = 0;
                         if (valid) {
                             const int r = (int)a - (int)b;
                             float X = 0.0f;
@@ -435,46 +414,41 @@ k_ov_sweep(OvArgs A) {
                                     X = qr[hi_m] - qr[lo_m];
                                 }
                             }
-                            const float ex = 2.0f * kappa * fabsf(X);
+                            const float ex = (2.0f * kr + 4.0f * kUnitRoundoff) * fabsf(X);
                             hi = ga_hi[a] + hb_hi[b] - X + ex;
                             lo = ga_lo[a] + hb_lo[b] - X - ex;
-                            item = t + K * (a + S * b);
                             evaluated++;
                         }
-                        lb = fmaxf(lb, warp_max_f(lo));
-                        const bool keep = valid && hi > lbest && hi >= lb;
-                        const u32 mk = __ballot_sync(0xffffffffu, keep);
-                        if (mk) {
-                            const u32 add = __popc(mk);
-                            if (cnt + add > kOvListCap) cnt = ov_list_prune(Ls, cnt, lb, lane);
-                            if (cnt + add > kOvListCap) {
-                                overflow = true;
-                            } else {
+                        if (mode == 0) {
+                            lbmax = fmaxf(lbmax, lo);
+                            himax = fmaxf(himax, hi);
+                        } else {
+                            const bool keep = valid && hi >= LB && hi > lbest;
+                            const u32 mk = __ballot_sync(0xffffffffu, keep);
+                            if (mk) {
+                                u32 base = 0;
+                                if (lane == 0) base = atomicAdd(&A.pool_cnt[g], (u32)__popc(mk));
+                                base = __shfl_sync(0xffffffffu, base, 0);
                                 if (keep) {
-                                    const u32 p = cnt + __popc(mk & ((1u << lane) - 1u));
-                                    Ls.item[p] = item;
-                                    Ls.hi[p] = hi;
+                                    const u32 p = base + __popc(mk & ((1u << lane) - 1u));
+                                    if (p < kOvPoolCap) A.pool_item[(size_t)g * kOvPoolCap + p] = t + K * (a + S * b);
                                 }
-                                cnt += add;
-                                __syncwarp();
                             }
                         }
                     }
                 }
             }
-            cnt = ov_list_prune(Ls, cnt, lb, lane);
-            const size_t slot = (size_t)g * K + t;
-            if (lane == 0) {
-                A.res_lb[slot] = lb;
-                A.res_cnt[slot] = (overflow || cnt > kOvOutCap) ? kOvOverflow : cnt;
-            }
-            if (!overflow && lane < cnt && lane < kOvOutCap) {
-                A.res_item[slot * kOvOutCap + lane] = Ls.item[lane];
-                A.res_hi[slot * kOvOutCap + lane] = Ls.hi[lane];
+            if (mode == 0) {
+                lbmax = warp_max_f(lbmax);
+                himax = warp_max_f(himax);
+                if (lane == 0) {
+                    A.res_lb[slot] = lbmax;
+                    A.res_hi[slot] = himax;
+                }
             }
             __syncwarp();
         }
-        if (A.items_evaluated) {
+        if (mode == 0 && A.items_evaluated) {
 #pragma unroll
             for (int o = 16; o > 0; o >>= 1) evaluated += __shfl_xor_sync(0xffffffffu, evaluated, o);
             if (lane == 0 && evaluated) atomicAdd(A.items_evaluated, (u64)evaluated);
@@ -482,8 +456,8 @@ k_ov_sweep(OvArgs A) {
     }
 }
 
-// One warp per candidate slot: the best lower bound over all templates and
-// the contenders whose upper bound reaches it.
+// One warp per candidate slot: the best lower bound over all templates, the
+// templates whose items can reach it, and a reset of the contender pool.
 __global__ void k_ov_merge(OvArgs A) {
     const u32 nc = *A.n_cand;
     const u32 lane = threadIdx.x & 31, K = A.K;
@@ -492,40 +466,24 @@ __global__ void k_ov_merge(OvArgs A) {
         if (A.cskip[g]) continue;
         const float lbest = A.best_ll[A.cand[g]];
         float lb = -INFINITY;
-        bool ov = false;
-        for (u32 t = lane; t < K; t += 32) {
-            lb = fmaxf(lb, A.res_lb[(size_t)g * K + t]);
-            ov |= A.res_cnt[(size_t)g * K + t] == kOvOverflow;
-        }
+        for (u32 t = lane; t < K; t += 32) lb = fmaxf(lb, A.res_lb[(size_t)g * K + t]);
         lb = warp_max_f(lb);
-        ov = __any_sync(0xffffffffu, ov);
-        u32 cnt = 0;
-        if (!ov) {
-            for (u32 t0 = 0; t0 < K; t0 += 32) {
-                const u32 t = t0 + lane;
-                const u32 c = t < K ? A.res_cnt[(size_t)g * K + t] : 0;
-                for (u32 e = 0; e < kOvOutCap; e++) {
-                    bool keep = false;
-                    u32 it = 0;
-                    if (e < c) {
-                        const size_t s = ((size_t)g * K + t) * kOvOutCap + e;
-                        keep = A.res_hi[s] >= lb && A.res_hi[s] > lbest;
-                        it = A.res_item[s];
-                    }
-                    const u32 m = __ballot_sync(0xffffffffu, keep);
-                    if (keep) {
-                        const u32 p = cnt + __popc(m & ((1u << lane) - 1u));
-                        if (p < kOvRefCap) A.ref_item[(size_t)g * kOvRefCap + p] = it;
-                    }
-                    cnt += __popc(m);
-                }
-            }
+        for (u32 t = lane; t < K; t += 32) {
+            const float h = A.res_hi[(size_t)g * K + t];
+            A.need[(size_t)g * K + t] = (h >= lb && h > lbest) ? 1 : 0;
         }
         if (lane == 0) {
-            A.ref_cnt[g] = cnt;
-            A.fallback[g] = (ov || cnt > kOvRefCap) ? 1 : 0;
+            A.cand_lb[g] = lb;
+            A.pool_cnt[g] = 0;
         }
     }
+}
+
+// Candidates whose pool overflowed go to the exact kernel.
+__global__ void k_ov_mark_fallback(OvArgs A) {
+    const u32 nc = *A.n_cand;
+    for (u32 g = blockIdx.x * blockDim.x + threadIdx.x; g < nc; g += gridDim.x * blockDim.x)
+        A.fallback[g] = (!A.cskip[g] && A.pool_cnt[g] > kOvPoolCap) ? 1 : 0;
 }
 
 // Exact value of one item (reference order), window read from global memory.
@@ -567,9 +525,9 @@ __global__ void k_ov_refine(OvArgs A) {
         u64 bi = ~0ull;
         if (!A.cskip[g]) {
             const u32 lab = A.best_lab[id], bidx = A.best_idx[id];
-            const u32 cnt = A.ref_cnt[g];
+            const u32 cnt = A.pool_cnt[g];
             for (u32 e = lane; e < cnt; e += 32) {
-                const u32 it = A.ref_item[(size_t)g * kOvRefCap + e];
+                const u32 it = A.pool_item[(size_t)g * kOvPoolCap + e];
                 const u32 t = it % K, a = (it / K) % S, b = it / (K * S);
                 const float ll = overlap_item_exact_global(A, lab, bidx, t, a, b);
                 if (ll > bv || (ll == bv && ll > start && it < bi)) { bv = ll; bi = it; }

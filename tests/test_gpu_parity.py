@@ -126,7 +126,7 @@ def test_fast_overlap_exact_ties_between_duplicate_templates(lib):
         m[key] = np.concatenate([m[key], m[key]], axis=0)
     m["template_SS_by_chan"] = np.zeros((8, rec.n_chans))
     si = rec.sort_info(get_adjusted_clips=True)
-    m2 = {k: v.copy() for k, v in m.items()}
+    m2 = {k: (v.copy() if isinstance(v, np.ndarray) else v) for k, v in m.items()}
     exp = O.binary_pursuit_oracle(rec.voltage, rec.voltage.dtype, si, m, n_max_shift_inds=40)
     stats = []
     got = bpp.binary_pursuit(rec.voltage, rec.voltage.dtype, si, m2, n_max_shift_inds=40, stats=stats)
