@@ -332,6 +332,8 @@ def main():
                                  % (C * n * 4 / 1e9, K * n * 4 / 1e9),
                            "passes": int(stats[-1].passes), "spikes": int(stats[-1].spikes),
                            "overlap_candidates": int(stats[-1].candidates),
+                           "overlap_refined_items": int(stats[-1].refined_items),
+                           "overlap_fallback_candidates": int(stats[-1].fallback_candidates),
                            "parallelism": "segment-parallel x%d" % world},
                 "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": gpu_launches,
                 "clocks": clock_info}

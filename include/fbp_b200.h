@@ -87,6 +87,9 @@ typedef struct fbp_stage_stats {
     uint64_t launches[FBP_N_STAGES];
     uint64_t work[FBP_N_STAGES];
     uint64_t candidates;        /* overlap-recheck candidates over all passes */
+    uint64_t refined_items;     /* overlap items re-evaluated exactly because their
+                                   interval reached the best one (FBP_OVERLAP_FAST) */
+    uint64_t fallback_candidates; /* candidates the fast path handed to the exact kernel */
     uint32_t passes;
     uint32_t spikes;
 } fbp_stage_stats;

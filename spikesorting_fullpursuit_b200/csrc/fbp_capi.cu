@@ -8,6 +8,7 @@
 #include <cstdarg>
 #include <cstdio>
 #include <cstring>
+#include <algorithm>
 #include <mutex>
 #include <string>
 #include <vector>
@@ -72,7 +73,9 @@ struct Workspace {
     OvConst *oc;
     u8 *cskip, *fallback, *need;
     u32 *k0_count, *k0_cursor, *k0_offset, *k0_active, *n_k0_active, *order;
-    u32 *pool_cnt, *pool_item, *fb_slots, *fb_list, *fb_count;
+    u32 *pool_slot, *pool_item, *fb_slots, *fb_list;
+    u64 *best_key;
+    u32 pool_cap;
     size_t bytes;
 };
 
@@ -145,11 +148,12 @@ Workspace layout(char *base, u32 n, u32 K, u32 L, u32 nmax, bool want_fast) {
         w.res_hi = (float *)take(sl * K * 4);
         w.need = (u8 *)take(sl * K);
         w.cand_lb = (float *)take(sl * 4);
-        w.pool_cnt = (u32 *)take(sl * 4);
-        w.pool_item = (u32 *)take(sl * kOvPoolCap * 4);
+        w.best_key = (u64 *)take(sl * 8);
+        w.pool_cap = (u32)std::min<u64>(0x7fffffffull, std::max<u64>(1u << 22, (u64)sl * 128));
+        w.pool_slot = (u32 *)take((size_t)w.pool_cap * 4);
+        w.pool_item = (u32 *)take((size_t)w.pool_cap * 4);
         w.fb_slots = (u32 *)take(sl * 4);
         w.fb_list = (u32 *)take(sl * 4);
-        w.fb_count = (u32 *)take(4);
     }
     w.bytes = off;
     return w;
@@ -257,7 +261,7 @@ int launch_accept(u32 n, u32 C, u32 L, const float *thr, const u32 *win, const u
 
 OvArgs ov_args(const Workspace &w, const float *v, u32 n, u32 C, const float *T, u32 K, u32 L, u32 nmax,
                const float *thr, const fbp_window_state &s, const float *Lk, const u32 *cand,
-               const u32 *n_cand, u64 *items) {
+               const u32 *n_cand, Counters *cnt) {
     OvArgs A{};
     A.n = n; A.C = C; A.K = K; A.L = L; A.nmax = nmax; A.S = 2 * nmax + 1;
     A.v = v; A.T = T; A.Lk = Lk; A.thr = thr;
@@ -269,8 +273,10 @@ OvArgs ov_args(const Workspace &w, const float *v, u32 n, u32 C, const float *T,
     A.k0_count = w.k0_count; A.k0_cursor = w.k0_cursor; A.k0_offset = w.k0_offset;
     A.k0_active = w.k0_active; A.n_k0_active = w.n_k0_active; A.order = w.order;
     A.res_lb = w.res_lb; A.res_hi = w.res_hi; A.need = w.need; A.cand_lb = w.cand_lb;
-    A.pool_cnt = w.pool_cnt; A.pool_item = w.pool_item; A.fallback = w.fallback;
-    A.items_evaluated = items;
+    A.pool_slot = w.pool_slot; A.pool_item = w.pool_item; A.pool_cap = w.pool_cap;
+    A.best_key = w.best_key; A.fallback = w.fallback;
+    A.items_evaluated = &cnt->ov_items;
+    A.pool_total = &cnt->pool_total;
     return A;
 }
 
@@ -286,12 +292,12 @@ int ov_chunk_setup(const Workspace &w, const float *T, u32 K, u32 C, u32 L, u32 
 
 // One pass of the fast overlap recheck over the candidate list (device count
 // n_cand).  Returns the number of kernels launched in *launches.
-int ov_fast_pass(const Workspace &w, const OvArgs &A, u32 W, cudaStream_t st, int *launches) {
+int ov_fast_pass(const Workspace &w, const OvArgs &A, Counters *cnt, cudaStream_t st, int *launches) {
     const u32 slots = w.slots;
     const u32 S = A.S;
     FBP_CUDA(cudaMemsetAsync(w.k0_count, 0, (size_t)A.K * 4, st));
     FBP_CUDA(cudaMemsetAsync(w.fallback, 0, align_up((size_t)slots + FBP_WINDOW_PAD, kCompactTile), st));
-    (void)W;
+    FBP_CUDA(cudaMemsetAsync(&cnt->pool_total, 0, 4, st));
     k_ov_prep<<<grid_for((u64)slots * 32, 256), 256, 0, st>>>(A);
     k_ov_group<<<1, 32, 0, st>>>(A);
     k_ov_scatter<<<grid_for(slots, 256), 256, 0, st>>>(A);
@@ -309,15 +315,15 @@ int ov_fast_pass(const Workspace &w, const OvArgs &A, u32 W, cudaStream_t st, in
     k_ov_sweep<<<sm_count(), kSweepThreads, sweep_smem, st>>>(A, 0);
     k_ov_merge<<<grid_for((u64)slots * 32, 256), 256, 0, st>>>(A);
     k_ov_sweep<<<sm_count(), kSweepThreads, sweep_smem, st>>>(A, 1);
-    k_ov_mark_fallback<<<grid_for(slots, 256), 256, 0, st>>>(A);
-    k_ov_refine<<<grid_for((u64)slots * 32, 256), 256, 0, st>>>(A);
+    k_ov_refine<<<(int)sm_count() * 16, 128, 0, st>>>(A);
+    k_ov_finalize<<<grid_for(slots, 256), 256, 0, st>>>(A);
     FBP_LAUNCH_CHECK();
-    int rc = compact(w.fallback, slots, w.fb_slots, w.fb_count, w.tile_counts, st);
+    int rc = compact(w.fallback, slots, w.fb_slots, &cnt->fb_count, w.tile_counts, st);
     if (rc) return rc;
-    k_ov_fallback_list<<<grid_for(slots, 256), 256, 0, st>>>(A, w.fb_slots, w.fb_count, w.fb_list);
+    k_ov_fallback_list<<<grid_for(slots, 256), 256, 0, st>>>(A, w.fb_slots, &cnt->fb_count, w.fb_list);
     FBP_LAUNCH_CHECK();
     fbp_window_state s{A.best_idx, A.best_lab, A.best_ll, A.ov_idx, A.ov_lab, nullptr, A.ovr};
-    rc = launch_overlap(A.v, A.n, A.C, A.T, A.K, A.L, w.fb_list, w.fb_count, slots, s, A.Lk, A.nmax, A.thr,
+    rc = launch_overlap(A.v, A.n, A.C, A.T, A.K, A.L, w.fb_list, &cnt->fb_count, slots, s, A.Lk, A.nmax, A.thr,
                         A.items_evaluated, st);
     *launches = 16;
     return rc;
@@ -489,8 +495,8 @@ int fbp_pursuit_chunk(float *voltage, uint32_t n, uint32_t C, const float *templ
             if (w.fast) {
                 int nl = 0;
                 OvArgs A = ov_args(w, voltage, n, C, templates, K, L, nmax, thresholds, s, w.Lk, w.cand,
-                                   &w.cnt->n_cand, &w.cnt->ov_items);
-                if ((rc = ov_fast_pass(w, A, W, st, &nl))) break;
+                                   &w.cnt->n_cand, w.cnt);
+                if ((rc = ov_fast_pass(w, A, w.cnt, st, &nl))) break;
                 S.launches[FBP_STAGE_OVERLAP] += nl;
             } else {
                 if ((rc = launch_overlap(voltage, n, C, templates, K, L, w.cand, &w.cnt->n_cand, W, s, w.Lk,
@@ -524,6 +530,10 @@ int fbp_pursuit_chunk(float *voltage, uint32_t n, uint32_t C, const float *templ
         if (do_overlap_recheck) {
             S.work[FBP_STAGE_CHECK] += h_counts[1];
             S.candidates += h_counts[1];
+            if (w.fast) {
+                S.refined_items += std::min(h_counts[6], w.pool_cap);
+                S.fallback_candidates += h_counts[7];
+            }
         }
         if (pass_counts)
             FBP_CUDA(cudaMemcpyAsync(pass_counts + passes - 1, &w.cnt->n_spk, 4, cudaMemcpyDeviceToDevice, st));

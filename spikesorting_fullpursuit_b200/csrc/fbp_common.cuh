@@ -27,7 +27,8 @@ struct Counters {
     u32 total;        // spikes written to the output so far
     u32 overflow;     // set when the output buffer is too small
     u32 scan_total;   // scratch: result of the last compaction
-    u32 pad0[2];
+    u32 pool_total;   // overlap contenders appended this pass (may exceed the pool)
+    u32 fb_count;     // overlap candidates sent to the exact kernel this pass
     u64 ov_items;     // overlap items evaluated (after the skip rules)
     u32 pad[22];
 };

@@ -30,7 +30,8 @@
 
 namespace fbp {
 
-constexpr u32 kOvPoolCap = 512;     // contenders refined exactly per candidate
+// Contenders of all candidates of a pass share one pool of (slot, item)
+// pairs; a candidate whose contenders do not fit goes to the exact kernel.
 constexpr float kUnitRoundoff = 5.9604644775390625e-08f;   // 2^-24
 
 // Constants of one chunk (computed on the device once per call).
@@ -59,8 +60,11 @@ struct OvArgs {
     float *res_hi;                   // [slot][K]  largest upper bound of (candidate, t)
     u8 *need;                        // [slot][K]  (candidate, t) can hold a contender
     float *cand_lb;                  // [slot]     largest lower bound of the candidate
-    u32 *pool_cnt;                   // [slot]
-    u32 *pool_item;                  // [slot][kOvPoolCap]
+    u32 *pool_total;                 // appended entries this pass
+    u32 pool_cap;
+    u32 *pool_slot;                  // [pool_cap]
+    u32 *pool_item;                  // [pool_cap]
+    u64 *best_key;                   // [slot] packed (value, ~item) of the best refined contender
     u8 *fallback;                    // [slot]
     u64 *items_evaluated;
 };
@@ -176,7 +180,7 @@ __global__ void k_ov_prep(OvArgs A) {
         if (lane == 0) {
             A.cskip[g] = skip;
             A.vn[g] = (float)(sqrt(e) * (1.0 + 1e-6));
-            A.pool_cnt[g] = 0;
+            A.best_key[g] = 0ull;
             if (!skip) atomicAdd(&A.k0_count[lab], 1u);
         }
     }
@@ -427,11 +431,16 @@ k_ov_sweep(OvArgs A, int mode) {
                             const u32 mk = __ballot_sync(0xffffffffu, keep);
                             if (mk) {
                                 u32 base = 0;
-                                if (lane == 0) base = atomicAdd(&A.pool_cnt[g], (u32)__popc(mk));
+                                if (lane == 0) base = atomicAdd(A.pool_total, (u32)__popc(mk));
                                 base = __shfl_sync(0xffffffffu, base, 0);
                                 if (keep) {
                                     const u32 p = base + __popc(mk & ((1u << lane) - 1u));
-                                    if (p < kOvPoolCap) A.pool_item[(size_t)g * kOvPoolCap + p] = t + K * (a + S * b);
+                                    if (p < A.pool_cap) {
+                                        A.pool_slot[p] = g;
+                                        A.pool_item[p] = t + K * (a + S * b);
+                                    } else {
+                                        A.fallback[g] = 1;
+                                    }
                                 }
                             }
                         }
@@ -472,18 +481,20 @@ __global__ void k_ov_merge(OvArgs A) {
             const float h = A.res_hi[(size_t)g * K + t];
             A.need[(size_t)g * K + t] = (h >= lb && h > lbest) ? 1 : 0;
         }
-        if (lane == 0) {
-            A.cand_lb[g] = lb;
-            A.pool_cnt[g] = 0;
-        }
+        if (lane == 0) A.cand_lb[g] = lb;
     }
 }
 
-// Candidates whose pool overflowed go to the exact kernel.
-__global__ void k_ov_mark_fallback(OvArgs A) {
-    const u32 nc = *A.n_cand;
-    for (u32 g = blockIdx.x * blockDim.x + threadIdx.x; g < nc; g += gridDim.x * blockDim.x)
-        A.fallback[g] = (!A.cskip[g] && A.pool_cnt[g] > kOvPoolCap) ? 1 : 0;
+// Order-preserving key: larger value first, then lower item id.
+__device__ __forceinline__ u64 ov_pack(float v, u32 item) {
+    u32 u = __float_as_uint(v);
+    u = (u & 0x80000000u) ? ~u : (u | 0x80000000u);
+    return ((u64)u << 32) | (u64)(0xffffffffu - item);
+}
+__device__ __forceinline__ float ov_unpack_value(u64 key) {
+    u32 u = (u32)(key >> 32);
+    u = (u & 0x80000000u) ? (u & 0x7fffffffu) : ~u;
+    return __uint_as_float(u);
 }
 
 // Exact value of one item (reference order), window read from global memory.
@@ -511,37 +522,39 @@ __device__ float overlap_item_exact_global(const OvArgs &A, u32 lab, u32 bidx, u
     return cml;
 }
 
-// One warp per candidate slot: exact values of the contenders, the first
-// (lowest item id) maximum above the current best, and the parse decision.
+// Exact values of all pooled contenders, one thread each, in the reference's
+// order of operations; each candidate keeps the largest value above its
+// current best, lowest item id on ties (the parse kernel's strict-greater
+// scan over single-item groups, .cl:699-706).
 __global__ void k_ov_refine(OvArgs A) {
+    const u32 m = min(*A.pool_total, A.pool_cap);
+    for (u32 e = blockIdx.x * blockDim.x + threadIdx.x; e < m; e += gridDim.x * blockDim.x) {
+        const u32 g = A.pool_slot[e];
+        if (A.fallback[g]) continue;
+        const u32 it = A.pool_item[e];
+        const u32 id = A.cand[g];
+        const u32 t = it % A.K, a = (it / A.K) % A.S, b = it / (A.K * A.S);
+        const float ll = overlap_item_exact_global(A, A.best_lab[id], A.best_idx[id], t, a, b);
+        if (ll > A.best_ll[id]) atomicMax(&A.best_key[g], ov_pack(ll, it));
+    }
+}
+
+// One thread per candidate slot: the parse decision (.cl:707-814) for the
+// winning contender, or "no improvement".
+__global__ void k_ov_finalize(OvArgs A) {
     const u32 nc = *A.n_cand;
-    const u32 lane = threadIdx.x & 31, K = A.K, S = A.S;
-    for (u32 g = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); g < nc;
-         g += gridDim.x * (blockDim.x >> 5)) {
+    for (u32 g = blockIdx.x * blockDim.x + threadIdx.x; g < nc; g += gridDim.x * blockDim.x) {
         if (A.fallback[g]) continue;
         const u32 id = A.cand[g];
-        const float start = A.best_ll[id];
-        float bv = start;
-        u64 bi = ~0ull;
-        if (!A.cskip[g]) {
-            const u32 lab = A.best_lab[id], bidx = A.best_idx[id];
-            const u32 cnt = A.pool_cnt[g];
-            for (u32 e = lane; e < cnt; e += 32) {
-                const u32 it = A.pool_item[(size_t)g * kOvPoolCap + e];
-                const u32 t = it % K, a = (it / K) % S, b = it / (K * S);
-                const float ll = overlap_item_exact_global(A, lab, bidx, t, a, b);
-                if (ll > bv || (ll == bv && ll > start && it < bi)) { bv = ll; bi = it; }
-            }
+        const u64 key = A.best_key[g];
+        float bv = A.best_ll[id];
+        u64 bi = 0;
+        if (key != 0ull) {
+            bv = ov_unpack_value(key);
+            bi = 0xffffffffu - (u32)(key & 0xffffffffu);
         }
-#pragma unroll
-        for (int o = 16; o > 0; o >>= 1) {
-            const float ov = __shfl_xor_sync(0xffffffffu, bv, o);
-            const u64 oi = __shfl_xor_sync(0xffffffffu, bi, o);
-            if (ov > bv || (ov == bv && oi < bi)) { bv = ov; bi = oi; }
-        }
-        if (lane == 0)
-            overlap_parse(id, A.n, K, S, A.nmax, bv, bi == ~0ull ? 0 : bi, A.best_idx, A.best_lab, A.best_ll,
-                          A.ov_idx, A.ov_lab, A.ovr, A.Lk, A.thr);
+        overlap_parse(id, A.n, A.K, A.S, A.nmax, bv, bi, A.best_idx, A.best_lab, A.best_ll, A.ov_idx,
+                      A.ov_lab, A.ovr, A.Lk, A.thr);
     }
 }
 
