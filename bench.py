@@ -334,6 +334,8 @@ def main():
                            "overlap_candidates": int(stats[-1].candidates),
                            "overlap_refined_items": int(stats[-1].refined_items),
                            "overlap_fallback_candidates": int(stats[-1].fallback_candidates),
+                           "likelihood_refined": int(stats[-1].lik_refined),
+                           "likelihood_exact_passes": int(stats[-1].lik_exact_passes),
                            "parallelism": "segment-parallel x%d" % world},
                 "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": gpu_launches,
                 "clocks": clock_info}

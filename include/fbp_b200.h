@@ -43,8 +43,13 @@ typedef enum fbp_status {
 } fbp_status;
 
 /* Arithmetic of the full-pass likelihood (path (a)).  Both modes produce
- * the same spikes; FBP_PREC_FP32 evaluates every likelihood in the
- * reference's order on the FP32 pipes. */
+ * the same spikes.  FBP_PREC_FP32 evaluates every likelihood in the
+ * reference's order on the FP32 pipes.  FBP_PREC_BF16_REFINE runs the
+ * contraction on the tensor cores (tcgen05, BF16 operands, FP32
+ * accumulation), bounds its error, and re-evaluates in the reference's
+ * order every entry that could be positive; the others are provably
+ * negative, which is all the pursuit reads of them.  Shapes whose templates
+ * do not fit in shared memory use the FP32 kernel. */
 typedef enum fbp_precision {
     FBP_PREC_FP32 = 0,
     FBP_PREC_BF16_REFINE = 1
@@ -90,6 +95,10 @@ typedef struct fbp_stage_stats {
     uint64_t refined_items;     /* overlap items re-evaluated exactly because their
                                    interval reached the best one (FBP_OVERLAP_FAST) */
     uint64_t fallback_candidates; /* candidates the fast path handed to the exact kernel */
+    uint64_t lik_refined;       /* likelihood entries whose BF16 interval could exceed 0,
+                                   re-evaluated exactly (FBP_PREC_BF16_REFINE) */
+    uint64_t lik_exact_passes;  /* passes whose refinement list overflowed and were redone
+                                   in FP32 */
     uint32_t passes;
     uint32_t spikes;
 } fbp_stage_stats;

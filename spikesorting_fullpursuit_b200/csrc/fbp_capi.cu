@@ -15,6 +15,7 @@
 
 #include "../../include/fbp_b200.h"
 #include "fbp_overlap_fast.cuh"
+#include "fbp_lik_tc.cuh"
 
 using namespace fbp;
 
@@ -76,6 +77,12 @@ struct Workspace {
     u32 *pool_slot, *pool_item, *fb_slots, *fb_list;
     u64 *best_key;
     u32 pool_cap;
+    // tensor-core likelihood (present when `tc`)
+    bool tc;
+    u32 tc_Cg2, tc_Np, tc_cols, tc_ref_cap;
+    uint4 *Tb;
+    float *tc_tnorm;
+    u32 *tc_ref_t, *tc_ref_s;
     size_t bytes;
 };
 
@@ -91,7 +98,15 @@ bool fast_overlap_fits(u32 K, u32 L, u32 nmax) {
 
 size_t window_bytes_u8(u32 W) { return align_up((size_t)W + FBP_WINDOW_PAD, kCompactTile); }
 
-Workspace layout(char *base, u32 n, u32 K, u32 L, u32 nmax, bool want_fast) {
+// The tensor-core likelihood keeps all templates of a chunk in shared memory.
+bool tc_fits(u32 C, u32 K, u32 L, u32 *Cg2, u32 *Np) {
+    *Cg2 = ((C + 15) / 16) * 2;
+    *Np = ((K + 15) / 16) * 16;
+    if (*Np > 256) return false;
+    return tc_smem_bytes(L, *Cg2, *Np) <= 227 * 1024;
+}
+
+Workspace layout(char *base, u32 n, u32 K, u32 L, u32 nmax, bool want_fast, u32 C = 0, bool want_tc = false) {
     Workspace w{};
     const u32 W = ceil_div(n, L);
     const size_t Wp = (size_t)W + FBP_WINDOW_PAD;
@@ -155,6 +170,16 @@ Workspace layout(char *base, u32 n, u32 K, u32 L, u32 nmax, bool want_fast) {
         w.fb_slots = (u32 *)take(sl * 4);
         w.fb_list = (u32 *)take(sl * 4);
     }
+    w.tc = want_tc && tc_fits(C, K, L, &w.tc_Cg2, &w.tc_Np);
+    if (w.tc) {
+        w.tc_cols = 32;
+        while (w.tc_cols < w.tc_Np) w.tc_cols <<= 1;
+        w.Tb = (uint4 *)take((size_t)L * w.tc_Cg2 * w.tc_Np * 16);
+        w.tc_tnorm = (float *)take((size_t)K * 4);
+        w.tc_ref_cap = (u32)std::min<u64>(0x7fffffffull, std::max<u64>(1u << 20, (u64)n * K / 16));
+        w.tc_ref_t = (u32 *)take((size_t)w.tc_ref_cap * 4);
+        w.tc_ref_s = (u32 *)take((size_t)w.tc_ref_cap * 4);
+    }
     w.bytes = off;
     return w;
 }
@@ -183,7 +208,7 @@ int compact(const u8 *f, u32 W, u32 *list, u32 *count_dev, u32 *tile_counts, cud
 
 int launch_likelihood(const float *v, u32 n, u32 C, const float *T, u32 K, u32 L, const float *tss,
                       const u32 *win, const u32 *n_win_dev, u32 max_windows, float *Lk,
-                      cudaStream_t st) {
+                      cudaStream_t st, const u32 *gate = nullptr) {
     const size_t smem = (size_t)kLikChanChunk * (kLikTile + L) * sizeof(float);
     static size_t configured = 0;
     if (smem > 48 * 1024 && smem > configured) {
@@ -193,7 +218,7 @@ int launch_likelihood(const float *v, u32 n, u32 C, const float *T, u32 K, u32 L
     }
     const u64 items = (u64)max_windows * ceil_div(K, kLikTplPerBlock);
     const int grid = grid_for(items * kLikThreads, kLikThreads, 16);
-    k_likelihood_fp32<<<grid, kLikThreads, smem, st>>>(v, n, C, T, K, L, tss, win, n_win_dev, Lk);
+    k_likelihood_fp32<<<grid, kLikThreads, smem, st>>>(v, n, C, T, K, L, tss, win, n_win_dev, Lk, gate);
     FBP_LAUNCH_CHECK();
     return FBP_OK;
 }
@@ -329,6 +354,63 @@ int ov_fast_pass(const Workspace &w, const OvArgs &A, Counters *cnt, cudaStream_
     return rc;
 }
 
+__global__ void k_tnorm(const float *__restrict__ T, u32 K, u32 CL, float *__restrict__ out) {
+    for (u32 t = blockIdx.x * blockDim.x + threadIdx.x; t < K; t += gridDim.x * blockDim.x) {
+        double ss = 0.0;
+        for (u32 i = 0; i < CL; i++) ss += (double)T[(size_t)t * CL + i] * T[(size_t)t * CL + i];
+        out[t] = (float)(sqrt(ss) * (1.0 + 1e-6));
+    }
+}
+
+__global__ void k_tc_gate(Counters *cnt, u32 cap) { cnt->tc_overflow = cnt->tc_ref > cap ? 1u : 0u; }
+
+int tc_chunk_setup(const Workspace &w, const float *T, u32 K, u32 C, u32 L, cudaStream_t st) {
+    const u64 total = (u64)L * w.tc_Cg2 * w.tc_Np;
+    k_tc_pack_templates<<<grid_for(total, 256), 256, 0, st>>>(T, K, C, L, w.tc_Cg2, w.tc_Np, w.Tb);
+    k_tnorm<<<grid_for(K, 64), 64, 0, st>>>(T, K, C * L, w.tc_tnorm);
+    FBP_LAUNCH_CHECK();
+    return FBP_OK;
+}
+
+// bound on |bf16 tensor-core value - reference value| per unit of ||t||*||window||
+float tc_kappa(u32 C, u32 L, u32 Cg2) {
+    const double u_bf = 1.0 / 256.0, u = 1.0 / 16777216.0;
+    const double prod = 2.0 * u_bf + u_bf * u_bf;                 // both operands rounded to bf16
+    const double n_acc = (double)Cg2 * 8 * L + 1;                 // tensor-core additions
+    const double n_ref = (double)C * L + 2;                       // reference additions
+    const double k = prod + (1.0 + 4 * u_bf) * n_acc * 2.0 * u + 1.01 * n_ref * u;
+    return (float)(k * 1.01);
+}
+
+// One pass of the tensor-core likelihood over the listed windows.
+int tc_likelihood_pass(const Workspace &w, const float *v, u32 n, u32 C, const float *T, u32 K, u32 L,
+                       const float *tss, const u32 *win, const u32 *n_win, u32 max_windows, float *Lk,
+                       Counters *cnt, cudaStream_t st, int *launches) {
+    TcArgs A{};
+    A.n = n; A.C = C; A.K = K; A.L = L;
+    A.Cg2 = w.tc_Cg2; A.Np = w.tc_Np;
+    A.rows_pad = (kTcM + L - 1 + 7) / 8 * 8;
+    A.tmem_cols = w.tc_cols;
+    A.kappa_b = tc_kappa(C, L, w.tc_Cg2);
+    A.v = v; A.T = T; A.tss = tss; A.tnorm = w.tc_tnorm; A.Tb = w.Tb;
+    A.tb_bytes = (u32)((size_t)L * w.tc_Cg2 * w.tc_Np * 16);
+    A.win = win; A.n_win = n_win; A.Lk = Lk;
+    A.ref_t = w.tc_ref_t; A.ref_s = w.tc_ref_s; A.ref_count = &cnt->tc_ref; A.ref_cap = w.tc_ref_cap;
+    A.err = &cnt->tc_err;
+    const size_t smem = tc_smem_bytes(L, w.tc_Cg2, w.tc_Np);
+    FBP_CUDA(cudaMemsetAsync(&cnt->tc_ref, 0, 4, st));
+    FBP_CUDA(cudaFuncSetAttribute(k_lik_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    k_lik_tc<<<sm_count(), kTcThreads, smem, st>>>(A);
+    FBP_LAUNCH_CHECK();
+    k_tc_refine<<<sm_count() * 8, 256, 0, st>>>(v, n, C, T, K, L, tss, w.tc_ref_t, w.tc_ref_s, &cnt->tc_ref,
+                                                 w.tc_ref_cap, Lk);
+    k_tc_gate<<<1, 1, 0, st>>>(cnt, w.tc_ref_cap);
+    FBP_LAUNCH_CHECK();
+    int rc = launch_likelihood(v, n, C, T, K, L, tss, win, n_win, max_windows, Lk, st, &cnt->tc_overflow);
+    *launches = 4;
+    return rc;
+}
+
 // CUDA-event timing of the stages of a pass.  Events come from a pool that
 // is drained after every host synchronisation (collect()).
 class StageTimer {
@@ -403,8 +485,7 @@ int fbp_pursuit_workspace_bytes(uint32_t n, uint32_t C, uint32_t K, uint32_t L, 
                                 int precision, size_t *bytes_out) {
     if (!bytes_out || n == 0 || C == 0 || K == 0 || L == 0)
         return fail(FBP_ERR_BAD_ARG, "workspace size: bad arguments");
-    (void)precision;
-    *bytes_out = layout(nullptr, n, K, L, nmax, true).bytes;
+    *bytes_out = layout(nullptr, n, K, L, nmax, true, C, precision == FBP_PREC_BF16_REFINE).bytes;
     return FBP_OK;
 }
 
@@ -426,7 +507,8 @@ int fbp_pursuit_chunk(float *voltage, uint32_t n, uint32_t C, const float *templ
         return fail(FBP_ERR_BAD_ARG, "fbp_pursuit_chunk: n_max_shift too large");
     if (overlap_method != FBP_OVERLAP_FAST && overlap_method != FBP_OVERLAP_EXACT)
         return fail(FBP_ERR_BAD_ARG, "fbp_pursuit_chunk: unknown overlap method %d", overlap_method);
-    Workspace w = layout((char *)workspace, n, K, L, nmax, overlap_method == FBP_OVERLAP_FAST);
+    Workspace w = layout((char *)workspace, n, K, L, nmax, overlap_method == FBP_OVERLAP_FAST, C,
+                         precision == FBP_PREC_BF16_REFINE);
     if (workspace_bytes < w.bytes)
         return fail(FBP_ERR_BAD_ARG, "fbp_pursuit_chunk: workspace has %zu bytes, needs %zu",
                     workspace_bytes, w.bytes);
@@ -457,6 +539,13 @@ int fbp_pursuit_chunk(float *voltage, uint32_t n, uint32_t C, const float *templ
     FBP_LAUNCH_CHECK();
     S.launches[FBP_STAGE_LISTS] += 1;
     timer.end(FBP_STAGE_LISTS);
+    if (w.tc) {
+        timer.begin(FBP_STAGE_LIKELIHOOD);
+        int rc0 = tc_chunk_setup(w, templates, K, C, L, st);
+        if (rc0) return rc0;
+        S.launches[FBP_STAGE_LIKELIHOOD] += 2;
+        timer.end(FBP_STAGE_LIKELIHOOD);
+    }
     if (w.fast && do_overlap_recheck) {
         timer.begin(FBP_STAGE_OVERLAP);
         int rc0 = ov_chunk_setup(w, templates, K, C, L, nmax, st);
@@ -475,10 +564,18 @@ int fbp_pursuit_chunk(float *voltage, uint32_t n, uint32_t C, const float *templ
         passes++;
         // 1. likelihood over the listed windows (.py:538-549)
         timer.begin(FBP_STAGE_LIKELIHOOD);
-        if ((rc = launch_likelihood(voltage, n, C, templates, K, L, neg_half_ss, w.win, &w.cnt->n_win, W,
-                                    w.Lk, st)))
-            break;
-        S.launches[FBP_STAGE_LIKELIHOOD] += 1;
+        if (w.tc) {
+            int nl = 0;
+            if ((rc = tc_likelihood_pass(w, voltage, n, C, templates, K, L, neg_half_ss, w.win, &w.cnt->n_win, W,
+                                         w.Lk, w.cnt, st, &nl)))
+                break;
+            S.launches[FBP_STAGE_LIKELIHOOD] += nl;
+        } else {
+            if ((rc = launch_likelihood(voltage, n, C, templates, K, L, neg_half_ss, w.win, &w.cnt->n_win, W,
+                                        w.Lk, st)))
+                break;
+            S.launches[FBP_STAGE_LIKELIHOOD] += 1;
+        }
         timer.end(FBP_STAGE_LIKELIHOOD);
         // 2. per-window argmax over all templates (.py:551-562)
         timer.begin(FBP_STAGE_ARGMAX);
@@ -524,6 +621,12 @@ int fbp_pursuit_chunk(float *voltage, uint32_t n, uint32_t C, const float *templ
         timer.collect();
         const u32 added = h_counts[2];
         const u32 nwin = h_counts[0];
+        if (w.tc) {
+            const Counters *hc = (const Counters *)h_counts;
+            if (hc->tc_err) { rc = fail(FBP_ERR_CUDA, "tensor-core likelihood: bounded wait %u gave up", hc->tc_err); break; }
+            S.lik_refined += std::min(hc->tc_ref, w.tc_ref_cap);
+            S.lik_exact_passes += hc->tc_overflow;
+        }
         S.work[FBP_STAGE_LIKELIHOOD] += (u64)nwin * L * K;
         S.work[FBP_STAGE_ARGMAX] += (u64)nwin * 3 * L * K;
         S.work[FBP_STAGE_ACCEPT] += nwin;

@@ -30,7 +30,10 @@ struct Counters {
     u32 pool_total;   // overlap contenders appended this pass (may exceed the pool)
     u32 fb_count;     // overlap candidates sent to the exact kernel this pass
     u64 ov_items;     // overlap items evaluated (after the skip rules)
-    u32 pad[22];
+    u32 tc_ref;       // tensor-core likelihood entries queued for exact refinement this pass
+    u32 tc_err;       // non-zero: a bounded wait in the tensor-core kernel gave up
+    u32 tc_overflow;  // refinement list overflowed: the exact kernel redoes the pass
+    u32 pad[19];
 };
 static_assert(sizeof(Counters) == 128, "Counters is one 128-byte line");
 

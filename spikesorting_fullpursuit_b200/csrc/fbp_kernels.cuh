@@ -99,8 +99,9 @@ constexpr int kLikChanChunk = 8;
 __global__ void __launch_bounds__(kLikThreads)
 k_likelihood_fp32(const float *__restrict__ v, u32 n, u32 C, const float *__restrict__ T, u32 K, u32 L,
                   const float *__restrict__ tss, const u32 *__restrict__ win,
-                  const u32 *__restrict__ n_win_dev, float *__restrict__ Lk) {
+                  const u32 *__restrict__ n_win_dev, float *__restrict__ Lk, const u32 *__restrict__ gate) {
     extern __shared__ float strip[];   // kLikChanChunk x (kLikTile + L)
+    if (gate && *gate == 0) return;    // only run when the gate asks for it
     const u32 n_win = *n_win_dev;
     const u32 kgroups = ceil_div(K, kLikTplPerBlock);
     const u32 stride = kLikTile + L;

@@ -66,13 +66,14 @@ def P(t):
 
 # ----------------------------------------------------------------- whole pursuit
 
+@pytest.mark.parametrize("precision", ["fp32", "bf16"])
 @pytest.mark.parametrize("path", golden_paths(), ids=lambda p: p.split("/")[-1][:-4])
-def test_binary_pursuit_matches_reference_golden(lib, path):
+def test_binary_pursuit_matches_reference_golden(lib, path, precision):
     c = GoldenCase(path)
     m = c.metrics()
     out = bpp.binary_pursuit(c.voltage, c.voltage.dtype, c.sort_info, m,
                              n_max_shift_inds=c.n_max_shift_inds, chunk_samples=c.chunk_samples,
-                             precision="fp32")
+                             precision=precision)
     assert_same_outputs(out, c.expected, c.empty)
     assert np.array_equal(m["n_spikes"], c.n_spikes)
 
@@ -88,8 +89,9 @@ LIVE = [
 ]
 
 
+@pytest.mark.parametrize("precision", ["fp32", "bf16"])
 @pytest.mark.parametrize("cfg", LIVE, ids=lambda c: "%s-%d" % (c["kind"], c["seed"]))
-def test_binary_pursuit_matches_oracle(lib, cfg):
+def test_binary_pursuit_matches_oracle(lib, cfg, precision):
     kw = dict(duration_s=cfg["dur"], seed=cfg["seed"], L=cfg["L"])
     if "K" in cfg:
         kw["n_templates"] = cfg["K"]
@@ -102,9 +104,15 @@ def test_binary_pursuit_matches_oracle(lib, cfg):
     chunk = cfg.get("chunk")
     exp = O.binary_pursuit_oracle(rec.voltage, rec.voltage.dtype, si, rec.fresh_metrics(),
                                   n_max_shift_inds=cfg["nmax"], chunk_samples=chunk)
+    stats = []
     got = bpp.binary_pursuit(rec.voltage, rec.voltage.dtype, si, rec.fresh_metrics(),
-                             n_max_shift_inds=cfg["nmax"], chunk_samples=chunk)
+                             n_max_shift_inds=cfg["nmax"], chunk_samples=chunk, precision=precision,
+                             stats=stats)
     assert_same_outputs(got, tuple(np.asarray(x) for x in exp), isinstance(exp[0], list))
+    if precision == "bf16":
+        # the tensor-core path ran (no shape here is too large for it) and
+        # refined some entries exactly
+        assert stats[0]["launches"]["likelihood"] >= 4 * stats[0]["passes"]
 
 
 @pytest.mark.parametrize("overlap", ["fast", "exact"])
