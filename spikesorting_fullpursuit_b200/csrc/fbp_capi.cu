@@ -82,7 +82,8 @@ struct Workspace {
     u32 tc_Cg2, tc_Np, tc_cols, tc_ref_cap;
     uint4 *Tb;
     float *tc_tnorm;
-    u32 *tc_ref_t, *tc_ref_s;
+    u32 *tc_ref_t, *tc_ref_s, *tc_seg_s0, *tc_seg_base, *tc_seg_cnt, *tc_seg_count;
+    u32 tc_seg_cap;
     size_t bytes;
 };
 
@@ -103,6 +104,7 @@ bool tc_fits(u32 C, u32 K, u32 L, u32 *Cg2, u32 *Np) {
     *Cg2 = ((C + 15) / 16) * 2;
     *Np = ((K + 15) / 16) * 16;
     if (*Np > 256) return false;
+    if (tc_refine_smem_bytes(K, L) > 227 * 1024) return false;
     return tc_smem_bytes(L, *Cg2, *Np) <= 227 * 1024;
 }
 
@@ -176,9 +178,14 @@ Workspace layout(char *base, u32 n, u32 K, u32 L, u32 nmax, bool want_fast, u32 
         while (w.tc_cols < w.tc_Np) w.tc_cols <<= 1;
         w.Tb = (uint4 *)take((size_t)L * w.tc_Cg2 * w.tc_Np * 16);
         w.tc_tnorm = (float *)take((size_t)K * 4);
-        w.tc_ref_cap = (u32)std::min<u64>(0x7fffffffull, std::max<u64>(1u << 20, (u64)n * K / 16));
+        w.tc_ref_cap = (u32)std::min<u64>(0x7fffffffull, std::max<u64>(1u << 20, (u64)n * K / 4));
         w.tc_ref_t = (u32 *)take((size_t)w.tc_ref_cap * 4);
         w.tc_ref_s = (u32 *)take((size_t)w.tc_ref_cap * 4);
+        w.tc_seg_cap = W * ((L + kTcM - 1) / kTcM) + 16;
+        w.tc_seg_s0 = (u32 *)take((size_t)w.tc_seg_cap * 4);
+        w.tc_seg_base = (u32 *)take((size_t)w.tc_seg_cap * 4);
+        w.tc_seg_cnt = (u32 *)take((size_t)w.tc_seg_cap * 4);
+        w.tc_seg_count = (u32 *)take(4);
     }
     w.bytes = off;
     return w;
@@ -362,7 +369,9 @@ __global__ void k_tnorm(const float *__restrict__ T, u32 K, u32 CL, float *__res
     }
 }
 
-__global__ void k_tc_gate(Counters *cnt, u32 cap) { cnt->tc_overflow = cnt->tc_ref > cap ? 1u : 0u; }
+__global__ void k_tc_gate(Counters *cnt, u32 cap, const u32 *seg_count, u32 seg_cap) {
+    cnt->tc_overflow = (cnt->tc_ref > cap || *seg_count > seg_cap) ? 1u : 0u;
+}
 
 int tc_chunk_setup(const Workspace &w, const float *T, u32 K, u32 C, u32 L, cudaStream_t st) {
     const u64 total = (u64)L * w.tc_Cg2 * w.tc_Np;
@@ -396,15 +405,22 @@ int tc_likelihood_pass(const Workspace &w, const float *v, u32 n, u32 C, const f
     A.tb_bytes = (u32)((size_t)L * w.tc_Cg2 * w.tc_Np * 16);
     A.win = win; A.n_win = n_win; A.Lk = Lk;
     A.ref_t = w.tc_ref_t; A.ref_s = w.tc_ref_s; A.ref_count = &cnt->tc_ref; A.ref_cap = w.tc_ref_cap;
+    A.seg_s0 = w.tc_seg_s0; A.seg_base = w.tc_seg_base; A.seg_cnt = w.tc_seg_cnt;
+    A.seg_count = w.tc_seg_count; A.seg_overflow = &cnt->tc_overflow; A.seg_cap = w.tc_seg_cap;
     A.err = &cnt->tc_err;
     const size_t smem = tc_smem_bytes(L, w.tc_Cg2, w.tc_Np);
     FBP_CUDA(cudaMemsetAsync(&cnt->tc_ref, 0, 4, st));
+    FBP_CUDA(cudaMemsetAsync(w.tc_seg_count, 0, 4, st));
     FBP_CUDA(cudaFuncSetAttribute(k_lik_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     k_lik_tc<<<sm_count(), kTcThreads, smem, st>>>(A);
     FBP_LAUNCH_CHECK();
-    k_tc_refine<<<sm_count() * 8, 256, 0, st>>>(v, n, C, T, K, L, tss, w.tc_ref_t, w.tc_ref_s, &cnt->tc_ref,
-                                                 w.tc_ref_cap, Lk);
-    k_tc_gate<<<1, 1, 0, st>>>(cnt, w.tc_ref_cap);
+    const size_t rsmem = tc_refine_smem_bytes(K, L);
+    if (rsmem > 48 * 1024)
+        FBP_CUDA(cudaFuncSetAttribute(k_tc_refine, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)rsmem));
+    k_tc_refine<<<sm_count() * 2, kRefThreads, rsmem, st>>>(v, n, C, T, K, L, tss, w.tc_ref_t, w.tc_ref_s,
+                                                            w.tc_seg_s0, w.tc_seg_base, w.tc_seg_cnt,
+                                                            w.tc_seg_count, w.tc_seg_cap, Lk);
+    k_tc_gate<<<1, 1, 0, st>>>(cnt, w.tc_ref_cap, w.tc_seg_count, w.tc_seg_cap);
     FBP_LAUNCH_CHECK();
     int rc = launch_likelihood(v, n, C, T, K, L, tss, win, n_win, max_windows, Lk, st, &cnt->tc_overflow);
     *launches = 4;

@@ -46,9 +46,12 @@ struct TcArgs {
     const u32 *win;
     const u32 *n_win;
     float *Lk;                       // [K][n]
-    u32 *ref_t, *ref_s;              // refinement list
+    u32 *ref_t, *ref_s;              // refinement list (one contiguous segment per tile)
     u32 *ref_count;
     u32 ref_cap;
+    u32 *seg_s0, *seg_base, *seg_cnt;  // tile segments of the refinement list
+    u32 *seg_count, *seg_overflow;
+    u32 seg_cap;
     u32 *err;                        // non-zero: a bounded wait gave up
 };
 
@@ -57,10 +60,26 @@ __host__ __device__ inline size_t tc_smem_bytes(u32 L, u32 Cg2, u32 Np) {
     return (size_t)L * Cg2 * Np * 16          // templates
            + rows_pad * Cg2 * 16              // voltage strip
            + rows_pad * 4 * 2                 // row energies and their prefix sums
-           + 64;                              // mbarriers + tmem address
+           + 64;                              // mbarriers, tmem address, scan scratch
 }
 
 __device__ __forceinline__ u32 smem_u32(const void *p) { return (u32)__cvta_generic_to_shared(p); }
+
+// Exclusive scan over the 128 threads of the tensor-core kernel.
+__device__ __forceinline__ u32 tc_block_excl_scan(u32 v, u32 *total, u32 *tmp) {
+    const u32 lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    u32 incl = warp_incl_scan(v);
+    if (lane == 31) tmp[warp] = incl;
+    __syncthreads();
+    u32 off = 0, tot = 0;
+    for (u32 w = 0; w < kTcThreads / 32; w++) {
+        if (w < warp) off += tmp[w];
+        tot += tmp[w];
+    }
+    __syncthreads();
+    *total = tot;
+    return off + incl - v;
+}
 
 // K-major, no swizzle: rows 16 B apart, 8-row groups SBO apart, K chunks LBO apart.
 __device__ __forceinline__ u64 umma_desc(u32 saddr, u32 lbo, u32 sbo) {
@@ -101,6 +120,8 @@ k_lik_tc(TcArgs A) {
     float *wpre = rowsq + rows_pad;
     u64 *bars = (u64 *)(wpre + rows_pad);      // [0] templates loaded, [1] MMA done
     u32 *tmem_slot = (u32 *)(bars + 2);
+    u32 *seg_info = tmem_slot + 1;
+    u32 *scan_tmp = seg_info + 1;              // 4 warps + total
     const u32 tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     const u32 bar_b = smem_u32(&bars[0]), bar_mma = smem_u32(&bars[1]);
     const u32 kWaitLimit = 1u << 24;
@@ -226,6 +247,9 @@ k_lik_tc(TcArgs A) {
             const float lo = row ? wpre[row - 1] : 0.0f;
             wn = sqrtf(fmaxf(hi - lo, 0.0f)) * 1.0001f + 1e-30f;
         }
+        // phase 1: store the provably-negative values, mark the others
+        u32 wantbits[8] = {0, 0, 0, 0, 0, 0, 0, 0};      // Np <= 256
+        u32 nwant = 0;
         for (u32 c0 = 0; c0 < Np; c0 += 16) {
             u32 r[16];
             asm volatile(
@@ -236,34 +260,51 @@ k_lik_tc(TcArgs A) {
                   "=r"(r[15])
                 : "r"(tmem + ((warp * 32u) << 16) + c0));
             asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
-            bool want[16];
 #pragma unroll
             for (int q = 0; q < 16; q++) {
                 const u32 t = c0 + q;
-                want[q] = false;
                 if (!in_win || t >= A.K) continue;
-                float* dst = A.Lk + (size_t)t * n + s;
+                float *dst = A.Lk + (size_t)t * n + s;
                 if (s + L >= n) { *dst = 0.0f; continue; }               // .cl:231-234
                 const float tssv = A.tss[t];
                 const float approx = __uint_as_float(r[q]) + tssv;
                 const float E = kappa_b * A.tnorm[t] * wn + 2.384185791015625e-07f * (fabsf(tssv) + fabsf(approx));
-                if (approx + E > 0.0f) want[q] = true;
-                else *dst = approx;
+                if (approx + E > 0.0f) {
+                    wantbits[t >> 5] |= 1u << (t & 31);
+                    nwant++;
+                } else {
+                    *dst = approx;
+                }
             }
-            // append the entries to refine (warp-aggregated)
-#pragma unroll
-            for (int q = 0; q < 16; q++) {
-                const u32 mk = __ballot_sync(0xffffffffu, want[q]);
-                if (!mk) continue;
-                u32 base = 0;
-                if (lane == 0) base = atomicAdd(A.ref_count, (u32)__popc(mk));
-                base = __shfl_sync(0xffffffffu, base, 0);
-                if (want[q]) {
-                    const u32 p = base + __popc(mk & ((1u << lane) - 1u));
-                    if (p < A.ref_cap) {
-                        A.ref_t[p] = c0 + q;
-                        A.ref_s[p] = s;
-                    }
+        }
+        // phase 2: one contiguous segment of (template, sample) entries per tile
+        u32 seg_total;
+        const u32 my_off = tc_block_excl_scan(nwant, &seg_total, scan_tmp);
+        if (tid == 0) {
+            seg_info[0] = seg_total ? atomicAdd(A.ref_count, seg_total) : 0u;
+        }
+        __syncthreads();
+        const u32 seg_base = seg_info[0];
+        if (seg_total && tid == 0 && seg_base + seg_total <= A.ref_cap) {
+            const u32 si = atomicAdd(A.seg_count, 1u);
+            if (si < A.seg_cap) {
+                A.seg_s0[si] = s0;
+                A.seg_base[si] = seg_base;
+                A.seg_cnt[si] = seg_total;
+            } else {
+                atomicExch(A.seg_overflow, 1u);
+            }
+        }
+        if (nwant && seg_base + seg_total <= A.ref_cap) {
+            u32 p = seg_base + my_off;
+            for (u32 wd = 0; wd < 8; wd++) {
+                u32 bits = wantbits[wd];
+                while (bits) {
+                    const u32 b = __ffs(bits) - 1;
+                    bits &= bits - 1;
+                    A.ref_t[p] = wd * 32 + b;
+                    A.ref_s[p] = s;
+                    p++;
                 }
             }
         }
@@ -297,22 +338,63 @@ __global__ void k_tc_pack_templates(const float *__restrict__ T, u32 K, u32 C, u
     }
 }
 
-// Exact reference-order values of the listed (template, sample) entries
-// (compute_maximum_likelihood, binary_pursuit.cl:216-252).
-__global__ void k_tc_refine(const float *__restrict__ v, u32 n, u32 C, const float *__restrict__ T, u32 K, u32 L,
-                            const float *__restrict__ tss, const u32 *__restrict__ ref_t,
-                            const u32 *__restrict__ ref_s, const u32 *__restrict__ ref_count, u32 ref_cap,
-                            float *__restrict__ Lk) {
-    const u32 m = min(*ref_count, ref_cap);
-    for (u32 e = blockIdx.x * blockDim.x + threadIdx.x; e < m; e += gridDim.x * blockDim.x) {
-        const u32 t = ref_t[e], s = ref_s[e];
-        float acc = tss[t];
-        for (u32 c = 0; c < C; c++) {
-            const float *tp = T + ((size_t)t * C + c) * L;
-            const float *vp = v + (size_t)c * n + s;
-            for (u32 i = 0; i < L; i++) acc = __fadd_rn(acc, __fmul_rn(__ldg(tp + i), __ldg(vp + i)));
+// Exact reference-order values of the refinement list, one tile segment per
+// block (compute_maximum_likelihood, binary_pursuit.cl:216-252): channel by
+// channel, the tile's voltage row and all templates' channel row are staged
+// in shared memory, and every entry's chain advances through that channel's
+// lags -- the reference's channel-major, lag-minor order.  Each thread keeps
+// up to kRefIlp independent chains.
+constexpr int kRefThreads = 256;
+constexpr int kRefIlp = 4;
+__host__ __device__ inline size_t tc_refine_smem_bytes(u32 K, u32 L) {
+    return ((size_t)K * L + kTcM + L + 8) * 4;
+}
+__global__ void __launch_bounds__(kRefThreads)
+k_tc_refine(const float *__restrict__ v, u32 n, u32 C, const float *__restrict__ T, u32 K, u32 L,
+            const float *__restrict__ tss, const u32 *__restrict__ ref_t, const u32 *__restrict__ ref_s,
+            const u32 *__restrict__ seg_s0, const u32 *__restrict__ seg_base, const u32 *__restrict__ seg_cnt,
+            const u32 *__restrict__ seg_count, u32 seg_cap, float *__restrict__ Lk) {
+    extern __shared__ float rsm[];
+    float *Ts = rsm;                     // [K][L] channel c of every template
+    float *strip = rsm + (size_t)K * L;  // [kTcM + L] voltage of channel c from s0
+    const u32 nseg = min(*seg_count, seg_cap);
+    for (u32 sg = blockIdx.x; sg < nseg; sg += gridDim.x) {
+        const u32 s0 = seg_s0[sg], base = seg_base[sg], cnt = seg_cnt[sg];
+        for (u32 e0 = 0; e0 < cnt; e0 += blockDim.x * kRefIlp) {
+            u32 tt[kRefIlp], ss[kRefIlp];
+            float acc[kRefIlp];
+            bool act[kRefIlp];
+#pragma unroll
+            for (int q = 0; q < kRefIlp; q++) {
+                const u32 e = e0 + q * blockDim.x + threadIdx.x;
+                act[q] = e < cnt;
+                tt[q] = act[q] ? ref_t[base + e] : 0;
+                ss[q] = act[q] ? ref_s[base + e] - s0 : 0;
+                acc[q] = act[q] ? tss[tt[q]] : 0.0f;
+            }
+            for (u32 c = 0; c < C; c++) {
+                __syncthreads();
+                for (u32 x = threadIdx.x; x < K * L; x += blockDim.x) Ts[x] = T[((size_t)(x / L) * C + c) * L + x % L];
+                for (u32 x = threadIdx.x; x < kTcM + L; x += blockDim.x) {
+                    const u32 pos = s0 + x;
+                    strip[x] = pos < n ? v[(size_t)c * n + pos] : 0.0f;
+                }
+                __syncthreads();
+                const float *tp[kRefIlp], *sp[kRefIlp];
+#pragma unroll
+                for (int q = 0; q < kRefIlp; q++) {
+                    tp[q] = Ts + (size_t)tt[q] * L;
+                    sp[q] = strip + ss[q];
+                }
+                for (u32 i = 0; i < L; i++) {
+#pragma unroll
+                    for (int q = 0; q < kRefIlp; q++) acc[q] = __fadd_rn(acc[q], __fmul_rn(tp[q][i], sp[q][i]));
+                }
+            }
+#pragma unroll
+            for (int q = 0; q < kRefIlp; q++)
+                if (act[q]) Lk[(size_t)tt[q] * n + s0 + ss[q]] = acc[q];
         }
-        Lk[(size_t)t * n + s] = acc;
     }
 }
 
