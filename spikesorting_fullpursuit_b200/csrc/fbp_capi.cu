@@ -81,7 +81,8 @@ struct Workspace {
     bool tc;
     u32 tc_Cg2, tc_Np, tc_cols, tc_ref_cap;
     uint4 *Tb;
-    float *tc_tnorm;
+    float *tc_tnorm, *tc_tabs;
+    int *tc_texp;
     u32 *tc_ref_t, *tc_ref_s, *tc_seg_s0, *tc_seg_base, *tc_seg_cnt, *tc_seg_count;
     u32 tc_seg_cap;
     size_t bytes;
@@ -104,7 +105,7 @@ bool tc_fits(u32 C, u32 K, u32 L, u32 *Cg2, u32 *Np) {
     *Cg2 = ((C + 15) / 16) * 2;
     *Np = ((K + 15) / 16) * 16;
     if (*Np > 256) return false;
-    if (tc_refine_smem_bytes(K, L) > 227 * 1024) return false;
+    if (tc_refine_smem_bytes(C, L) > 227 * 1024) return false;
     return tc_smem_bytes(L, *Cg2, *Np) <= 227 * 1024;
 }
 
@@ -178,6 +179,8 @@ Workspace layout(char *base, u32 n, u32 K, u32 L, u32 nmax, bool want_fast, u32 
         while (w.tc_cols < w.tc_Np) w.tc_cols <<= 1;
         w.Tb = (uint4 *)take((size_t)L * w.tc_Cg2 * w.tc_Np * 16);
         w.tc_tnorm = (float *)take((size_t)K * 4);
+        w.tc_tabs = (float *)take((size_t)K * 4);
+        w.tc_texp = (int *)take((size_t)K * 4);
         w.tc_ref_cap = (u32)std::min<u64>(0x7fffffffull, std::max<u64>(1u << 20, (u64)n * K / 4));
         w.tc_ref_t = (u32 *)take((size_t)w.tc_ref_cap * 4);
         w.tc_ref_s = (u32 *)take((size_t)w.tc_ref_cap * 4);
@@ -361,11 +364,27 @@ int ov_fast_pass(const Workspace &w, const OvArgs &A, Counters *cnt, cudaStream_
     return rc;
 }
 
-__global__ void k_tnorm(const float *__restrict__ T, u32 K, u32 CL, float *__restrict__ out) {
+// Per template: ||t||_2, ||t||_1 (rounded up) and the power-of-two scale that
+// brings its largest magnitude just under 2^14 in fp16.
+__global__ void k_tnorm(const float *__restrict__ T, u32 K, u32 CL, float *__restrict__ out,
+                        float *__restrict__ out1, int *__restrict__ texp) {
     for (u32 t = blockIdx.x * blockDim.x + threadIdx.x; t < K; t += gridDim.x * blockDim.x) {
-        double ss = 0.0;
-        for (u32 i = 0; i < CL; i++) ss += (double)T[(size_t)t * CL + i] * T[(size_t)t * CL + i];
+        double ss = 0.0, s1 = 0.0;
+        float mx = 0.0f;
+        for (u32 i = 0; i < CL; i++) {
+            const float x = T[(size_t)t * CL + i];
+            ss += (double)x * x;
+            s1 += fabs((double)x);
+            mx = fmaxf(mx, fabsf(x));
+        }
         out[t] = (float)(sqrt(ss) * (1.0 + 1e-6));
+        out1[t] = (float)(s1 * (1.0 + 1e-6));
+        int e = 0;
+        if (mx > 0.0f) {
+            frexpf(mx, &e);
+            e = 14 - e;
+        }
+        texp[t] = e;
     }
 }
 
@@ -375,19 +394,22 @@ __global__ void k_tc_gate(Counters *cnt, u32 cap, const u32 *seg_count, u32 seg_
 
 int tc_chunk_setup(const Workspace &w, const float *T, u32 K, u32 C, u32 L, cudaStream_t st) {
     const u64 total = (u64)L * w.tc_Cg2 * w.tc_Np;
-    k_tc_pack_templates<<<grid_for(total, 256), 256, 0, st>>>(T, K, C, L, w.tc_Cg2, w.tc_Np, w.Tb);
-    k_tnorm<<<grid_for(K, 64), 64, 0, st>>>(T, K, C * L, w.tc_tnorm);
+    k_tnorm<<<grid_for(K, 64), 64, 0, st>>>(T, K, C * L, w.tc_tnorm, w.tc_tabs, w.tc_texp);
+    k_tc_pack_templates<<<grid_for(total, 256), 256, 0, st>>>(T, K, C, L, w.tc_Cg2, w.tc_Np, w.tc_texp, w.Tb);
     FBP_LAUNCH_CHECK();
     return FBP_OK;
 }
 
-// bound on |bf16 tensor-core value - reference value| per unit of ||t||*||window||
+// Bound on |tensor-core value - reference value| per unit of
+// ||t|| * ||window||: both operands rounded to fp16 (normal range; the
+// subnormal part is a separate absolute term), FP32 accumulation of every
+// product allowed one ulp of error, and the reference's own recursive sum.
 float tc_kappa(u32 C, u32 L, u32 Cg2) {
-    const double u_bf = 1.0 / 256.0, u = 1.0 / 16777216.0;
-    const double prod = 2.0 * u_bf + u_bf * u_bf;                 // both operands rounded to bf16
-    const double n_acc = (double)Cg2 * 8 * L + 1;                 // tensor-core additions
-    const double n_ref = (double)C * L + 2;                       // reference additions
-    const double k = prod + (1.0 + 4 * u_bf) * n_acc * 2.0 * u + 1.01 * n_ref * u;
+    const double u_h = 1.0 / 2048.0, u = 1.0 / 16777216.0;
+    const double prod = 2.0 * u_h + u_h * u_h;
+    const double n_acc = (double)Cg2 * 8 * L + 1;
+    const double n_ref = (double)C * L + 2;
+    const double k = prod + (1.0 + 4 * u_h) * n_acc * 2.0 * u + 1.01 * n_ref * u;
     return (float)(k * 1.01);
 }
 
@@ -401,7 +423,7 @@ int tc_likelihood_pass(const Workspace &w, const float *v, u32 n, u32 C, const f
     A.rows_pad = (kTcM + L - 1 + 7) / 8 * 8;
     A.tmem_cols = w.tc_cols;
     A.kappa_b = tc_kappa(C, L, w.tc_Cg2);
-    A.v = v; A.T = T; A.tss = tss; A.tnorm = w.tc_tnorm; A.Tb = w.Tb;
+    A.v = v; A.T = T; A.tss = tss; A.tnorm = w.tc_tnorm; A.tabs = w.tc_tabs; A.texp = w.tc_texp; A.Tb = w.Tb;
     A.tb_bytes = (u32)((size_t)L * w.tc_Cg2 * w.tc_Np * 16);
     A.win = win; A.n_win = n_win; A.Lk = Lk;
     A.ref_t = w.tc_ref_t; A.ref_s = w.tc_ref_s; A.ref_count = &cnt->tc_ref; A.ref_cap = w.tc_ref_cap;
@@ -414,7 +436,7 @@ int tc_likelihood_pass(const Workspace &w, const float *v, u32 n, u32 C, const f
     FBP_CUDA(cudaFuncSetAttribute(k_lik_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     k_lik_tc<<<sm_count(), kTcThreads, smem, st>>>(A);
     FBP_LAUNCH_CHECK();
-    const size_t rsmem = tc_refine_smem_bytes(K, L);
+    const size_t rsmem = tc_refine_smem_bytes(C, L);
     if (rsmem > 48 * 1024)
         FBP_CUDA(cudaFuncSetAttribute(k_tc_refine, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)rsmem));
     k_tc_refine<<<sm_count() * 2, kRefThreads, rsmem, st>>>(v, n, C, T, K, L, tss, w.tc_ref_t, w.tc_ref_s,

@@ -1,10 +1,11 @@
-// Path (a) on the tensor cores: BF16 tcgen05 likelihood with exact refinement.
+// Path (a) on the tensor cores: tcgen05 likelihood (16-bit operands, FP32
+// accumulation) with exact refinement.
 //
 // likelihood[t][s] = -0.5*SS_t + sum_c sum_m T[t][c][m] * v[c][s+m]
 // (compute_full_likelihood, binary_pursuit.cl:216-300) is the product of a
 // Toeplitz voltage operand (rows = samples, K = (channel, lag)) and the
 // template matrix.  The voltage strip of a tile lives in shared memory as
-// rows of 8 channels (16 bytes, bf16): that is the K-major, no-swizzle
+// rows of 8 channels (16 bytes, fp16): that is the K-major, no-swizzle
 // canonical UMMA layout, and the operand for lag m is the same strip started
 // m rows later -- so the contraction is L accumulating
 // tcgen05.mma (M = 128 samples, N = templates, K = 16 channels) per channel
@@ -12,17 +13,24 @@
 // copied into shared memory once per CTA with one bulk asynchronous copy.
 // Accumulators are FP32 in tensor memory.
 //
+// Operands are IEEE fp16 after exact power-of-two scaling (per tile for the
+// voltage, per template for the templates), undone exactly in the epilogue;
+// fp16's 11 significant bits give a 2^-10 product bound where bf16 would give
+// 2^-7, with the same shared-memory footprint.
+//
 // Exactness: every value is either re-evaluated in the reference's order
 // (IEEE binary32, .cl:239-249) or provably <= 0.  With
-//   E(t,s) = kappa_b * ||t|| * ||window(s)|| + 2^-22 (|SS_t/2| + |approx|)
-// bounding |approx - reference| (bf16 rounding of both operands, FP32
-// accumulation in any order, and the reference's own rounding), entries
+//   E(t,s) = kappa * ||t|| * ||window(s)|| + 2^-25 (||t||_1 / s_v + |window|_1 / s_t)
+//            + 2^-22 (|SS_t/2| + |approx|)
+// bounding |approx - reference| (fp16 rounding of both operands including
+// subnormals, FP32 accumulation in any order, and the reference's own
+// rounding), entries
 // with approx + E > 0 go to the refinement list; the rest are stored as
 // approx, which is < 0 like the reference value.  Every later decision reads
 // such an entry only through "> 0" / "<= 0" tests (window argmax, check flag,
 // overlap skip rules and parse), so the pursuit is unchanged.
 #pragma once
-#include <cuda_bf16.h>
+#include <cuda_fp16.h>
 #include "fbp_kernels.cuh"
 
 namespace fbp {
@@ -40,8 +48,10 @@ struct TcArgs {
     const float *v;                  // [C][n]
     const float *T;                  // [K][C][L] (exact refinement)
     const float *tss;                // [K]
-    const float *tnorm;              // [K]
-    const uint4 *Tb;                 // [L][Cg2][Np] x 8 bf16
+    const float *tnorm;              // [K] ||t||_2
+    const float *tabs;               // [K] ||t||_1
+    const int *texp;                 // [K] power-of-two scale of template t's fp16 copy
+    const uint4 *Tb;                 // [L][Cg2][Np] x 8 fp16 (scaled)
     u32 tb_bytes;
     const u32 *win;
     const u32 *n_win;
@@ -59,8 +69,9 @@ __host__ __device__ inline size_t tc_smem_bytes(u32 L, u32 Cg2, u32 Np) {
     const size_t rows_pad = (kTcM + L - 1 + 7) / 8 * 8;
     return (size_t)L * Cg2 * Np * 16          // templates
            + rows_pad * Cg2 * 16              // voltage strip
-           + rows_pad * 4 * 2                 // row energies and their prefix sums
-           + 64;                              // mbarriers, tmem address, scan scratch
+           + rows_pad * 4 * 2                 // row energies / absolute sums, their prefix sums
+           + 64                               // mbarriers, tmem address, scan scratch
+           + (size_t)Np * 4;                  // per-template counters
 }
 
 __device__ __forceinline__ u32 smem_u32(const void *p) { return (u32)__cvta_generic_to_shared(p); }
@@ -116,12 +127,14 @@ k_lik_tc(TcArgs A) {
     const u32 L = A.L, Cg2 = A.Cg2, Np = A.Np, rows_pad = A.rows_pad, n = A.n;
     unsigned char *Bs = tsm;
     unsigned char *As = Bs + (size_t)L * Cg2 * Np * 16;
-    float *rowsq = (float *)(As + (size_t)rows_pad * Cg2 * 16);
-    float *wpre = rowsq + rows_pad;
-    u64 *bars = (u64 *)(wpre + rows_pad);      // [0] templates loaded, [1] MMA done
+    float *rowsq = (float *)(As + (size_t)rows_pad * Cg2 * 16);   // prefix of sum_c v^2 after the scan
+    float *rowab = rowsq + rows_pad;                              // prefix of sum_c |v|
+    u64 *bars = (u64 *)(rowab + rows_pad);     // [0] templates loaded, [1] MMA done
     u32 *tmem_slot = (u32 *)(bars + 2);
     u32 *seg_info = tmem_slot + 1;
     u32 *scan_tmp = seg_info + 1;              // 4 warps + total
+    int *tile_exp = (int *)(scan_tmp + 5);     // power-of-two scale of this tile's voltage
+    u32 *tcnt = (u32 *)(tile_exp + 3);         // [Np] per-template counters of the tile
     const u32 tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     const u32 bar_b = smem_u32(&bars[0]), bar_mma = smem_u32(&bars[1]);
     const u32 kWaitLimit = 1u << 24;
@@ -154,8 +167,8 @@ k_lik_tc(TcArgs A) {
         mbar_wait_bounded(bar_b, 0, kWaitLimit);  // let the copy land before leaving
     }
 
-    // instruction descriptor: D f32, A/B bf16, both K-major, M = 128, N = Np
-    const u32 idesc = (1u << 4) | (1u << 7) | (1u << 10) | ((Np >> 3) << 17) | ((u32)(kTcM >> 4) << 24);
+    // instruction descriptor: D f32, A/B f16, both K-major, M = 128, N = Np
+    const u32 idesc = (1u << 4) | ((Np >> 3) << 17) | ((u32)(kTcM >> 4) << 24);
     const u32 lbo_a = rows_pad * 16, lbo_b = Np * 16;
     const u32 a_base = smem_u32(As), b_base = smem_u32(Bs);
     const float kappa_b = A.kappa_b;
@@ -167,32 +180,53 @@ k_lik_tc(TcArgs A) {
         const u32 w = A.win[item / sub];
         const u32 s0 = w * L + (u32)(item % sub) * kTcM;
         const u32 ew = min((w + 1) * L, n);
-        // ---- stage the strip: rows x -> samples s0 + x, bf16 channels, row energies
-        for (u32 e = tid; e < rows_pad * Cg2; e += blockDim.x) {
-            const u32 x = e % rows_pad, g = e / rows_pad;
-            const u32 pos = s0 + x;
-            float f[8];
-#pragma unroll
-            for (int j = 0; j < 8; j++) {
-                const u32 c = g * 8 + j;
-                f[j] = (c < A.C && pos < n) ? A.v[(size_t)c * n + pos] : 0.0f;
-            }
-            uint4 q;
-            q.x = ((u32)__bfloat16_as_ushort(__float2bfloat16_rn(f[1])) << 16) | __bfloat16_as_ushort(__float2bfloat16_rn(f[0]));
-            q.y = ((u32)__bfloat16_as_ushort(__float2bfloat16_rn(f[3])) << 16) | __bfloat16_as_ushort(__float2bfloat16_rn(f[2]));
-            q.z = ((u32)__bfloat16_as_ushort(__float2bfloat16_rn(f[5])) << 16) | __bfloat16_as_ushort(__float2bfloat16_rn(f[4]));
-            q.w = ((u32)__bfloat16_as_ushort(__float2bfloat16_rn(f[7])) << 16) | __bfloat16_as_ushort(__float2bfloat16_rn(f[6]));
-            *reinterpret_cast<uint4 *>(As + ((size_t)g * rows_pad + x) * 16) = q;
-        }
+        // ---- row sums (energy, absolute) and the tile's largest magnitude
+        float mx = 0.0f;
         for (u32 x = tid; x < rows_pad; x += blockDim.x) {
             const u32 pos = s0 + x;
-            float e2 = 0.0f;
+            float e2 = 0.0f, ab = 0.0f;
             if (pos < n)
                 for (u32 c = 0; c < A.C; c++) {
                     const float f = A.v[(size_t)c * n + pos];
                     e2 = fmaf(f, f, e2);
+                    ab += fabsf(f);
+                    mx = fmaxf(mx, fabsf(f));
                 }
             rowsq[x] = e2;
+            rowab[x] = ab;
+        }
+        mx = warp_max_f(mx);
+        if (lane == 0) scan_tmp[warp] = __float_as_uint(mx);
+        __syncthreads();
+        if (tid == 0) {
+            float m = 0.0f;
+            for (int q = 0; q < kTcThreads / 32; q++) m = fmaxf(m, __uint_as_float(scan_tmp[q]));
+            int e = 0;
+            if (m > 0.0f) {
+                frexpf(m, &e);                       // m < 2^e
+                e = 14 - e;                          // scaled magnitudes < 2^14
+            }
+            *tile_exp = e;
+        }
+        __syncthreads();
+        const int kexp = *tile_exp;
+        // ---- stage the strip: rows x -> samples s0 + x, 8 fp16 channels per row
+        for (u32 e = tid; e < rows_pad * Cg2; e += blockDim.x) {
+            const u32 x = e % rows_pad, g = e / rows_pad;
+            const u32 pos = s0 + x;
+            u16 h[8];
+#pragma unroll
+            for (int j = 0; j < 8; j++) {
+                const u32 c = g * 8 + j;
+                const float f = (c < A.C && pos < n) ? A.v[(size_t)c * n + pos] : 0.0f;
+                h[j] = __half_as_ushort(__float2half_rn(ldexpf(f, kexp)));
+            }
+            uint4 q;
+            q.x = ((u32)h[1] << 16) | h[0];
+            q.y = ((u32)h[3] << 16) | h[2];
+            q.z = ((u32)h[5] << 16) | h[4];
+            q.w = ((u32)h[7] << 16) | h[6];
+            *reinterpret_cast<uint4 *>(As + ((size_t)g * rows_pad + x) * 16) = q;
         }
         asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
         __syncthreads();
@@ -214,17 +248,19 @@ k_lik_tc(TcArgs A) {
             asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];"
                          ::"r"(bar_mma) : "memory");
         }
-        // ---- meanwhile: window energies ||v[s .. s+L)||^2 by prefix sums (warp 1)
-        if (warp == 1) {
+        // ---- meanwhile: prefix sums of the row sums (warp 1: energies, warp 2: absolute)
+        if (warp == 1 || warp == 2) {
+            float *arr = warp == 1 ? rowsq : rowab;
             float carry = 0.0f;
             for (u32 x0 = 0; x0 < rows_pad; x0 += 32) {
-                float val = (x0 + lane < rows_pad) ? rowsq[x0 + lane] : 0.0f;
+                float val = (x0 + lane < rows_pad) ? arr[x0 + lane] : 0.0f;
 #pragma unroll
                 for (int o = 1; o < 32; o <<= 1) {
                     const float y = __shfl_up_sync(0xffffffffu, val, o);
                     if (lane >= (u32)o) val += y;
                 }
-                if (x0 + lane < rows_pad) wpre[x0 + lane] = carry + val;
+                __syncwarp();
+                if (x0 + lane < rows_pad) arr[x0 + lane] = carry + val;
                 carry += __shfl_sync(0xffffffffu, val, 31);
             }
         }
@@ -241,11 +277,11 @@ k_lik_tc(TcArgs A) {
         const u32 row = warp * 32 + lane;
         const u32 s = s0 + row;
         const bool in_win = s < ew && row < kTcM;
-        float wn = 0.0f;
+        float wn = 0.0f, wa = 0.0f;
         if (in_win) {
-            const float hi = wpre[min(row + L, rows_pad) - 1];
-            const float lo = row ? wpre[row - 1] : 0.0f;
-            wn = sqrtf(fmaxf(hi - lo, 0.0f)) * 1.0001f + 1e-30f;
+            const u32 hi_i = min(row + L, rows_pad) - 1;
+            wn = sqrtf(fmaxf(rowsq[hi_i] - (row ? rowsq[row - 1] : 0.0f), 0.0f)) * 1.0001f + 1e-30f;
+            wa = fmaxf(rowab[hi_i] - (row ? rowab[row - 1] : 0.0f), 0.0f) * 1.0001f + 1e-30f;
         }
         // phase 1: store the provably-negative values, mark the others
         u32 wantbits[8] = {0, 0, 0, 0, 0, 0, 0, 0};      // Np <= 256
@@ -267,8 +303,12 @@ k_lik_tc(TcArgs A) {
                 float *dst = A.Lk + (size_t)t * n + s;
                 if (s + L >= n) { *dst = 0.0f; continue; }               // .cl:231-234
                 const float tssv = A.tss[t];
-                const float approx = __uint_as_float(r[q]) + tssv;
-                const float E = kappa_b * A.tnorm[t] * wn + 2.384185791015625e-07f * (fabsf(tssv) + fabsf(approx));
+                const int je = A.texp[t];
+                const float approx = ldexpf(__uint_as_float(r[q]), -(kexp + je)) + tssv;
+                const float sub = 2.98023223876953125e-08f *          // 2^-25: fp16 subnormal spacing / 2
+                                  (ldexpf(A.tabs[t], -kexp) + ldexpf(wa, -je)) * 1.001f;
+                const float E = kappa_b * A.tnorm[t] * wn + sub +
+                                2.384185791015625e-07f * (fabsf(tssv) + fabsf(approx));
                 if (approx + E > 0.0f) {
                     wantbits[t >> 5] |= 1u << (t & 31);
                     nwant++;
@@ -277,11 +317,28 @@ k_lik_tc(TcArgs A) {
                 }
             }
         }
-        // phase 2: one contiguous segment of (template, sample) entries per tile
+        // phase 2: one contiguous segment of (template, sample) entries per
+        // tile, ordered by template so the refinement shares template rows
+        for (u32 t = tid; t < Np; t += blockDim.x) tcnt[t] = 0;
+        __syncthreads();
+        for (u32 wd = 0; wd < 8; wd++) {
+            u32 bits = wantbits[wd];
+            while (bits) {
+                const u32 b = __ffs(bits) - 1;
+                bits &= bits - 1;
+                atomicAdd(&tcnt[wd * 32 + b], 1u);
+            }
+        }
         u32 seg_total;
-        const u32 my_off = tc_block_excl_scan(nwant, &seg_total, scan_tmp);
+        (void)tc_block_excl_scan(nwant, &seg_total, scan_tmp);
         if (tid == 0) {
             seg_info[0] = seg_total ? atomicAdd(A.ref_count, seg_total) : 0u;
+            u32 off = 0;                            // template offsets inside the segment
+            for (u32 t = 0; t < Np; t++) {
+                const u32 c = tcnt[t];
+                tcnt[t] = off;
+                off += c;
+            }
         }
         __syncthreads();
         const u32 seg_base = seg_info[0];
@@ -296,15 +353,15 @@ k_lik_tc(TcArgs A) {
             }
         }
         if (nwant && seg_base + seg_total <= A.ref_cap) {
-            u32 p = seg_base + my_off;
             for (u32 wd = 0; wd < 8; wd++) {
                 u32 bits = wantbits[wd];
                 while (bits) {
                     const u32 b = __ffs(bits) - 1;
                     bits &= bits - 1;
-                    A.ref_t[p] = wd * 32 + b;
+                    const u32 t = wd * 32 + b;
+                    const u32 p = seg_base + atomicAdd(&tcnt[t], 1u);
+                    A.ref_t[p] = t;
                     A.ref_s[p] = s;
-                    p++;
                 }
             }
         }
@@ -315,10 +372,11 @@ k_lik_tc(TcArgs A) {
     if (warp == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(A.tmem_cols));
 }
 
-// Templates in the UMMA B layout: Tb[m][g][t] = 8 bf16 channels 8g..8g+7 of
-// template t at lag m (zero padding for channels >= C and t >= K).
+// Templates in the UMMA B layout: Tb[m][g][t] = 8 fp16 channels 8g..8g+7 of
+// template t at lag m, scaled by 2^texp[t] (zero padding for channels >= C
+// and t >= K).
 __global__ void k_tc_pack_templates(const float *__restrict__ T, u32 K, u32 C, u32 L, u32 Cg2, u32 Np,
-                                    uint4 *__restrict__ Tb) {
+                                    const int *__restrict__ texp, uint4 *__restrict__ Tb) {
     const u64 total = (u64)L * Cg2 * Np;
     for (u64 e = (u64)blockIdx.x * blockDim.x + threadIdx.x; e < total; e += (u64)gridDim.x * blockDim.x) {
         const u32 t = (u32)(e % Np), g = (u32)((e / Np) % Cg2), m = (u32)(e / ((u64)Np * Cg2));
@@ -326,8 +384,8 @@ __global__ void k_tc_pack_templates(const float *__restrict__ T, u32 K, u32 C, u
 #pragma unroll
         for (int j = 0; j < 8; j++) {
             const u32 c = g * 8 + j;
-            const float f = (t < K && c < C) ? T[((size_t)t * C + c) * L + m] : 0.0f;
-            h[j] = __bfloat16_as_ushort(__float2bfloat16_rn(f));
+            const float f = (t < K && c < C) ? ldexpf(T[((size_t)t * C + c) * L + m], texp[t]) : 0.0f;
+            h[j] = __half_as_ushort(__float2half_rn(f));
         }
         uint4 q;
         q.x = ((u32)h[1] << 16) | h[0];
@@ -338,16 +396,16 @@ __global__ void k_tc_pack_templates(const float *__restrict__ T, u32 K, u32 C, u
     }
 }
 
-// Exact reference-order values of the refinement list, one tile segment per
-// block (compute_maximum_likelihood, binary_pursuit.cl:216-252): channel by
-// channel, the tile's voltage row and all templates' channel row are staged
-// in shared memory, and every entry's chain advances through that channel's
-// lags -- the reference's channel-major, lag-minor order.  Each thread keeps
-// up to kRefIlp independent chains.
+// Exact reference-order values of the refinement list
+// (compute_maximum_likelihood, binary_pursuit.cl:216-252).  One tile
+// segment per block; its entries are ordered by template.  The tile's
+// voltage (all channels) is staged once; each warp takes 32 consecutive
+// entries -- mostly one template, so the template reads are broadcasts --
+// and every lane advances its own entry's chain in the reference's
+// channel-major, lag-minor order.
 constexpr int kRefThreads = 256;
-constexpr int kRefIlp = 4;
-__host__ __device__ inline size_t tc_refine_smem_bytes(u32 K, u32 L) {
-    return ((size_t)K * L + kTcM + L + 8) * 4;
+__host__ __device__ inline size_t tc_refine_smem_bytes(u32 C, u32 L) {
+    return ((size_t)C * (kTcM + L) + 8) * 4;
 }
 __global__ void __launch_bounds__(kRefThreads)
 k_tc_refine(const float *__restrict__ v, u32 n, u32 C, const float *__restrict__ T, u32 K, u32 L,
@@ -355,45 +413,25 @@ k_tc_refine(const float *__restrict__ v, u32 n, u32 C, const float *__restrict__
             const u32 *__restrict__ seg_s0, const u32 *__restrict__ seg_base, const u32 *__restrict__ seg_cnt,
             const u32 *__restrict__ seg_count, u32 seg_cap, float *__restrict__ Lk) {
     extern __shared__ float rsm[];
-    float *Ts = rsm;                     // [K][L] channel c of every template
-    float *strip = rsm + (size_t)K * L;  // [kTcM + L] voltage of channel c from s0
+    const u32 rl = kTcM + L;               // strip row length
     const u32 nseg = min(*seg_count, seg_cap);
     for (u32 sg = blockIdx.x; sg < nseg; sg += gridDim.x) {
         const u32 s0 = seg_s0[sg], base = seg_base[sg], cnt = seg_cnt[sg];
-        for (u32 e0 = 0; e0 < cnt; e0 += blockDim.x * kRefIlp) {
-            u32 tt[kRefIlp], ss[kRefIlp];
-            float acc[kRefIlp];
-            bool act[kRefIlp];
-#pragma unroll
-            for (int q = 0; q < kRefIlp; q++) {
-                const u32 e = e0 + q * blockDim.x + threadIdx.x;
-                act[q] = e < cnt;
-                tt[q] = act[q] ? ref_t[base + e] : 0;
-                ss[q] = act[q] ? ref_s[base + e] - s0 : 0;
-                acc[q] = act[q] ? tss[tt[q]] : 0.0f;
-            }
+        __syncthreads();
+        for (u32 x = threadIdx.x; x < C * rl; x += blockDim.x) {
+            const u32 c = x / rl, i = x % rl, pos = s0 + i;
+            rsm[x] = pos < n ? v[(size_t)c * n + pos] : 0.0f;
+        }
+        __syncthreads();
+        for (u32 e = threadIdx.x; e < cnt; e += blockDim.x) {
+            const u32 t = ref_t[base + e], so = ref_s[base + e] - s0;
+            float acc = tss[t];
             for (u32 c = 0; c < C; c++) {
-                __syncthreads();
-                for (u32 x = threadIdx.x; x < K * L; x += blockDim.x) Ts[x] = T[((size_t)(x / L) * C + c) * L + x % L];
-                for (u32 x = threadIdx.x; x < kTcM + L; x += blockDim.x) {
-                    const u32 pos = s0 + x;
-                    strip[x] = pos < n ? v[(size_t)c * n + pos] : 0.0f;
-                }
-                __syncthreads();
-                const float *tp[kRefIlp], *sp[kRefIlp];
-#pragma unroll
-                for (int q = 0; q < kRefIlp; q++) {
-                    tp[q] = Ts + (size_t)tt[q] * L;
-                    sp[q] = strip + ss[q];
-                }
-                for (u32 i = 0; i < L; i++) {
-#pragma unroll
-                    for (int q = 0; q < kRefIlp; q++) acc[q] = __fadd_rn(acc[q], __fmul_rn(tp[q][i], sp[q][i]));
-                }
+                const float *tp = T + ((size_t)t * C + c) * L;
+                const float *sp = rsm + (size_t)c * rl + so;
+                for (u32 i = 0; i < L; i++) acc = __fadd_rn(acc, __fmul_rn(__ldg(tp + i), sp[i]));
             }
-#pragma unroll
-            for (int q = 0; q < kRefIlp; q++)
-                if (act[q]) Lk[(size_t)tt[q] * n + s0 + ss[q]] = acc[q];
+            Lk[(size_t)t * n + s0 + so] = acc;
         }
     }
 }
