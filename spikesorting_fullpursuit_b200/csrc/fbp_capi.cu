@@ -93,7 +93,7 @@ struct Workspace {
 bool fast_overlap_fits(u32 K, u32 L, u32 nmax) {
     const u64 S = 2 * (u64)nmax + 1;
     if (S > 4 * (u64)L + 1 || S > 65535) return false;
-    if (sweep_smem_bytes((u32)S, L) > 227 * 1024) return false;
+    if (sweep_smem_bytes((u32)S, L, 256) > 227 * 1024) return false;
     if (tables_smem_bytes((u32)S, K, L) > 227 * 1024) return false;
     return true;
 }
@@ -344,12 +344,16 @@ int ov_fast_pass(const Workspace &w, const OvArgs &A, Counters *cnt, cudaStream_
         k_ov_tables<<<grid_for((u64)slots * kTabThreads, kTabThreads, 4), kTabThreads, smem, st>>>(A);
         FBP_LAUNCH_CHECK();
     }
-    const size_t sweep_smem = sweep_smem_bytes(S, A.L);
+    // as many warps per block as the shared memory allows (the task's
+    // prefix table is shared by all of them)
+    u32 sweep_threads = kSweepMaxThreads;
+    while (sweep_threads > 256 && sweep_smem_bytes(S, A.L, sweep_threads) > 227 * 1024) sweep_threads /= 2;
+    const size_t sweep_smem = sweep_smem_bytes(S, A.L, sweep_threads);
     if (sweep_smem > 48 * 1024)
         FBP_CUDA(cudaFuncSetAttribute(k_ov_sweep, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sweep_smem));
-    k_ov_sweep<<<sm_count(), kSweepThreads, sweep_smem, st>>>(A, 0);
+    k_ov_sweep<<<sm_count(), sweep_threads, sweep_smem, st>>>(A, 0);
     k_ov_merge<<<grid_for((u64)slots * 32, 256), 256, 0, st>>>(A);
-    k_ov_sweep<<<sm_count(), kSweepThreads, sweep_smem, st>>>(A, 1);
+    k_ov_sweep<<<sm_count(), sweep_threads, sweep_smem, st>>>(A, 1);
     k_ov_refine<<<(int)sm_count() * 16, 128, 0, st>>>(A);
     k_ov_finalize<<<grid_for(slots, 256), 256, 0, st>>>(A);
     FBP_LAUNCH_CHECK();

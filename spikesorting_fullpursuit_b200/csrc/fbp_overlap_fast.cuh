@@ -288,52 +288,77 @@ k_ov_tables(OvArgs A) {
     }
 }
 
-constexpr int kSweepThreads = 512;
+constexpr int kSweepMaxThreads = 1024;
 // Per-warp scratch of the sweep: ga_lo, ga_hi, hb_lo, hb_hi (S floats each),
-// then the a and b row lists (S u16 each).
+// the a and b row lists (S u16 each), and the bitmask of rows a with
+// L[k0][afix] not <= 0 (S bits).
 __host__ __device__ inline size_t sweep_warp_bytes(u32 S) {
-    return align_up((size_t)20 * S, 16);
+    return align_up((size_t)20 * S + (size_t)(S + 31) / 32 * 4, 16);
 }
-__host__ __device__ inline size_t sweep_smem_bytes(u32 S, u32 L) {
-    return align_up((size_t)(2 * L - 1) * (L + 1) * 4 + (size_t)4 * S * 4, 16) +
-           (size_t)(kSweepThreads / 32) * sweep_warp_bytes(S);
+__host__ __device__ inline size_t sweep_head_bytes(u32 S, u32 L) {
+    return align_up((size_t)(2 * L - 1) * (L + 1) * 4 + (size_t)4 * S * 4 + 16, 16);
+}
+__host__ __device__ inline size_t sweep_smem_bytes(u32 S, u32 L, u32 threads) {
+    return sweep_head_bytes(S, L) + (size_t)(threads / 32) * sweep_warp_bytes(S);
 }
 __host__ __device__ inline size_t tables_smem_bytes(u32 S, u32 K, u32 L) {
     const size_t Lp = (L + 7) & ~7u, Sp = (size_t)(S + 7) / 8 * 8, Kp = (size_t)(K + 7) / 8 * 8;
     return (Sp + Lp + 8 + Lp * Kp) * 4;
 }
 
+// Interval of one item from its row-invariant and moving parts.
+__device__ __forceinline__ void ov_item_bounds(const float *__restrict__ q, u32 L, int a_minus_nmax, int r,
+                                               float loA, float hiA, float loB, float hiB, float kx,
+                                               float &lo, float &hi) {
+    float X = 0.0f;
+    if (r > -(int)L && r < (int)L) {
+        const int lo_m = max(max(0, -r), -a_minus_nmax);
+        const int hi_m = min(min((int)L, (int)L - r), (int)L - a_minus_nmax);
+        if (lo_m < hi_m) {
+            const float *qr = q + (size_t)(r + (int)L - 1) * (L + 1);
+            X = qr[hi_m] - qr[lo_m];
+        }
+    }
+    const float ex = kx * fabsf(X);
+    hi = hiA + hiB - X + ex;
+    lo = loA + loB - X - ex;
+}
+
 // Sweep over the items of one (label k0, template t) task.  Q[k0][t] is
-// staged once; each warp walks the candidates of label k0 and enumerates the
-// items that survive the reference's skip rules (.cl:534-576): rows a with
-// L[k0][afix] not <= 0 (every in-bounds b within L of a), then rows b with
-// L[t][ashift] not <= 0 (every other in-bounds a within L of b).
+// staged once; warps take the candidates of label k0 one at a time from a
+// shared counter and enumerate the items that survive the reference's skip
+// rules (.cl:534-576): rows a with L[k0][afix] not <= 0 (every in-bounds b
+// within L of a), then rows b with L[t][ashift] not <= 0 (every other
+// in-bounds a within L of b).
 //  mode 0: per (candidate, t) the largest lower bound and the largest upper
 //          bound of its items (res_lb, res_hi).
 //  mode 1: for the (candidate, t) pairs flagged by k_ov_merge, append every
 //          item whose upper bound reaches the candidate's best lower bound
-//          and exceeds its current best likelihood to the candidate's pool.
-__global__ void __launch_bounds__(kSweepThreads)
+//          and exceeds its current best likelihood to the pool.
+__global__ void __launch_bounds__(kSweepMaxThreads)
 k_ov_sweep(OvArgs A, int mode) {
     extern __shared__ float sm[];
     const u32 S = A.S, K = A.K, L = A.L, nmax = A.nmax, n = A.n;
     const u32 R = 2 * L - 1;
-    const u32 nwarps = blockDim.x >> 5, warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const u32 warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     float *q = sm;                                  // [R][L+1]
     float *nt0 = q + (size_t)R * (L + 1);           // NT[k0][S], sNT[k0][S], NT[t][S], sNT[t][S]
     float *snt0 = nt0 + S, *ntt = snt0 + S, *sntt = ntt + S;
-    char *wbase = (char *)sm + align_up((size_t)R * (L + 1) * 4 + (size_t)4 * S * 4, 16);
+    u32 *next = (u32 *)(sntt + S);                  // candidate counter of the task
+    char *wbase = (char *)sm + sweep_head_bytes(S, L);
     float *ga_lo = (float *)(wbase + (size_t)warp * sweep_warp_bytes(S));
     float *ga_hi = ga_lo + S, *hb_lo = ga_hi + S, *hb_hi = hb_lo + S;
     u16 *alist = (u16 *)(hb_hi + S);
     u16 *blist = alist + S;
+    u32 *abits = (u32 *)((char *)ga_lo + (size_t)20 * S);
     const u32 ntasks = *A.n_k0_active * K;
     const float kr = A.oc->kappa_ref, km = A.oc->kappa_mine;
+    const float kx = 2.0f * kr + 4.0f * kUnitRoundoff;
+    // in-bounds shifts x: x + bidx >= nmax and x + bidx < n - L + nmax
     for (u32 task = blockIdx.x; task < ntasks; task += gridDim.x) {
         const u32 k0 = A.k0_active[task / K], t = task % K;
         const u32 gcount = A.k0_count[k0], goff = A.k0_offset[k0];
         if (mode == 1) {
-            // nothing to collect for this task: skip staging
             bool any = false;
             for (u32 ci = threadIdx.x; ci < gcount && !any; ci += blockDim.x)
                 any = A.need[(size_t)A.order[goff + ci] * K + t] != 0;
@@ -348,10 +373,15 @@ k_ov_sweep(OvArgs A, int mode) {
             ntt[b] = A.NT[(size_t)t * S + b];
             sntt[b] = A.sNT[(size_t)t * S + b];
         }
+        if (threadIdx.x == 0) *next = 0;
         __syncthreads();
         const float eq = 4.0f * kUnitRoundoff * A.tnorm[k0] * A.tnorm[t];
         u32 evaluated = 0;
-        for (u32 ci = warp; ci < gcount; ci += nwarps) {
+        for (;;) {
+            u32 ci = 0;
+            if (lane == 0) ci = atomicAdd(next, 1u);
+            ci = __shfl_sync(0xffffffffu, ci, 0);
+            if (ci >= gcount) break;
             const u32 g = A.order[goff + ci];
             const size_t slot = (size_t)g * K + t;
             if (mode == 1 && !A.need[slot]) continue;
@@ -361,24 +391,24 @@ k_ov_sweep(OvArgs A, int mode) {
             const float vn = A.vn[g];
             const float LB = mode == 1 ? A.cand_lb[g] : 0.0f;
             const float *Hg = A.H + (size_t)g * K * S;
-            // interval rows for a (label k0) and b (template t), and the item rows
+            // in-bounds shift range [xlo, xhi] (.cl:534-541)
+            const u32 xlo = bidx >= nmax ? 0u : nmax - bidx;
+            const u32 xhi_ex = n - L + nmax - bidx;       // first out-of-bounds shift
+            // interval rows and item rows
             u32 na = 0, nb = 0;
             for (u32 x0 = 0; x0 < S; x0 += 32) {
                 const u32 x = x0 + lane;
                 bool ap = false, bp = false;
                 if (x < S) {
                     const float G = Hg[(size_t)k0 * S + x];
-                    const float fa = snt0[x] * vn + nt0[x];
-                    const float ea = (kr + km) * fa + 4.0f * kUnitRoundoff * fabsf(G);
+                    const float ea = (kr + km) * (snt0[x] * vn + nt0[x]) + 4.0f * kUnitRoundoff * fabsf(G);
                     ga_lo[x] = G - ea;
                     ga_hi[x] = G + ea;
                     const float Hv = Hg[(size_t)t * S + x];
-                    const float fb = sntt[x] * vn + ntt[x];
-                    const float eb = (kr + km) * fb + 4.0f * kUnitRoundoff * fabsf(Hv) + eq;
+                    const float eb = (kr + km) * (sntt[x] * vn + ntt[x]) + 4.0f * kUnitRoundoff * fabsf(Hv) + eq;
                     hb_lo[x] = Hv - eb;
                     hb_hi[x] = Hv + eb;
-                    const bool inb = !(x + bidx < nmax || x + bidx >= n - L + nmax);
-                    if (inb) {
+                    if (x >= xlo && x < xhi_ex) {
                         const u32 pos = bidx + x - nmax;
                         ap = !(A.Lk[(size_t)k0 * n + pos] <= 0.0f);
                         bp = !(A.Lk[(size_t)t * n + pos] <= 0.0f);
@@ -387,60 +417,82 @@ k_ov_sweep(OvArgs A, int mode) {
                 const u32 ma = __ballot_sync(0xffffffffu, ap), mb = __ballot_sync(0xffffffffu, bp);
                 if (ap) alist[na + __popc(ma & ((1u << lane) - 1u))] = (u16)x;
                 if (bp) blist[nb + __popc(mb & ((1u << lane) - 1u))] = (u16)x;
+                if (lane == 0 && x0 / 32 < (S + 31) / 32) abits[x0 / 32] = ma;
                 na += __popc(ma);
                 nb += __popc(mb);
             }
             __syncwarp();
             float lbmax = -INFINITY, himax = -INFINITY;
-            for (int phase = 0; phase < 2; phase++) {
-                const u32 nrows = phase == 0 ? na : nb;
-                for (u32 ri = 0; ri < nrows; ri++) {
-                    const u32 fixed = phase == 0 ? alist[ri] : blist[ri];
-                    const u32 lo_x = fixed > L ? fixed - L : 0;
-                    const u32 hi_x = min(S - 1, fixed + L);
-                    for (u32 x0 = lo_x; x0 <= hi_x; x0 += 32) {
-                        const u32 x = x0 + lane;
-                        const u32 a = phase == 0 ? fixed : x;
-                        const u32 b = phase == 0 ? x : fixed;
-                        bool valid = x <= hi_x && !(x + bidx < nmax || x + bidx >= n - L + nmax);
-                        if (valid && phase == 1)     // rows a with L[k0][afix] > 0 came in phase 0
-                            valid = (A.Lk[(size_t)k0 * n + bidx + a - nmax] <= 0.0f);
-                        float lo = -INFINITY, hi = -INFINITY;
-                        if (valid) {
-                            const int r = (int)a - (int)b;
-                            float X = 0.0f;
-                            if (r > -(int)L && r < (int)L) {
-                                const int da = (int)a - (int)nmax;
-                                const int lo_m = max(max(0, -r), -da);
-                                const int hi_m = min(min((int)L, (int)L - r), (int)L - da);
-                                if (lo_m < hi_m) {
-                                    const float *qr = q + (size_t)(r + (int)L - 1) * (L + 1);
-                                    X = qr[hi_m] - qr[lo_m];
+            // phase 0: rows a in alist, b moves
+            for (u32 ri = 0; ri < na; ri++) {
+                const u32 a = alist[ri];
+                const float loA = ga_lo[a], hiA = ga_hi[a];
+                const int am = (int)a - (int)nmax;
+                const u32 b_lo = max(a > L ? a - L : 0u, xlo);
+                const u32 b_hi = min(min(S - 1, a + L), xhi_ex - 1);
+                for (u32 b0 = b_lo; b0 <= b_hi; b0 += 32) {
+                    const u32 b = b0 + lane;
+                    const bool valid = b <= b_hi;
+                    float lo = -INFINITY, hi = -INFINITY;
+                    if (valid) {
+                        ov_item_bounds(q, L, am, (int)a - (int)b, loA, hiA, hb_lo[b], hb_hi[b], kx, lo, hi);
+                        evaluated++;
+                    }
+                    if (mode == 0) {
+                        lbmax = fmaxf(lbmax, lo);
+                        himax = fmaxf(himax, hi);
+                    } else {
+                        const bool keep = valid && hi >= LB && hi > lbest;
+                        const u32 mk = __ballot_sync(0xffffffffu, keep);
+                        if (mk) {
+                            u32 base = 0;
+                            if (lane == 0) base = atomicAdd(A.pool_total, (u32)__popc(mk));
+                            base = __shfl_sync(0xffffffffu, base, 0);
+                            if (keep) {
+                                const u32 p = base + __popc(mk & ((1u << lane) - 1u));
+                                if (p < A.pool_cap) {
+                                    A.pool_slot[p] = g;
+                                    A.pool_item[p] = t + K * (a + S * b);
+                                } else {
+                                    A.fallback[g] = 1;
                                 }
                             }
-                            const float ex = (2.0f * kr + 4.0f * kUnitRoundoff) * fabsf(X);
-                            hi = ga_hi[a] + hb_hi[b] - X + ex;
-                            lo = ga_lo[a] + hb_lo[b] - X - ex;
-                            evaluated++;
                         }
-                        if (mode == 0) {
-                            lbmax = fmaxf(lbmax, lo);
-                            himax = fmaxf(himax, hi);
-                        } else {
-                            const bool keep = valid && hi >= LB && hi > lbest;
-                            const u32 mk = __ballot_sync(0xffffffffu, keep);
-                            if (mk) {
-                                u32 base = 0;
-                                if (lane == 0) base = atomicAdd(A.pool_total, (u32)__popc(mk));
-                                base = __shfl_sync(0xffffffffu, base, 0);
-                                if (keep) {
-                                    const u32 p = base + __popc(mk & ((1u << lane) - 1u));
-                                    if (p < A.pool_cap) {
-                                        A.pool_slot[p] = g;
-                                        A.pool_item[p] = t + K * (a + S * b);
-                                    } else {
-                                        A.fallback[g] = 1;
-                                    }
+                    }
+                }
+            }
+            // phase 1: rows b in blist, a moves (rows a of phase 0 excluded)
+            for (u32 ri = 0; ri < nb; ri++) {
+                const u32 b = blist[ri];
+                const float loB = hb_lo[b], hiB = hb_hi[b];
+                const u32 a_lo = max(b > L ? b - L : 0u, xlo);
+                const u32 a_hi = min(min(S - 1, b + L), xhi_ex - 1);
+                for (u32 a0 = a_lo; a0 <= a_hi; a0 += 32) {
+                    const u32 a = a0 + lane;
+                    const bool valid = a <= a_hi && !((abits[a >> 5] >> (a & 31)) & 1u);
+                    float lo = -INFINITY, hi = -INFINITY;
+                    if (valid) {
+                        ov_item_bounds(q, L, (int)a - (int)nmax, (int)a - (int)b, ga_lo[a], ga_hi[a], loB, hiB, kx,
+                                       lo, hi);
+                        evaluated++;
+                    }
+                    if (mode == 0) {
+                        lbmax = fmaxf(lbmax, lo);
+                        himax = fmaxf(himax, hi);
+                    } else {
+                        const bool keep = valid && hi >= LB && hi > lbest;
+                        const u32 mk = __ballot_sync(0xffffffffu, keep);
+                        if (mk) {
+                            u32 base = 0;
+                            if (lane == 0) base = atomicAdd(A.pool_total, (u32)__popc(mk));
+                            base = __shfl_sync(0xffffffffu, base, 0);
+                            if (keep) {
+                                const u32 p = base + __popc(mk & ((1u << lane) - 1u));
+                                if (p < A.pool_cap) {
+                                    A.pool_slot[p] = g;
+                                    A.pool_item[p] = t + K * (a + S * b);
+                                } else {
+                                    A.fallback[g] = 1;
                                 }
                             }
                         }
