@@ -77,6 +77,9 @@ struct Workspace {
     u32 *pool_slot, *pool_item, *fb_slots, *fb_list;
     u64 *best_key;
     u32 pool_cap;
+    float *ua;
+    int *kexp_tile;
+    u32 stiles;
     // tensor-core likelihood (present when `tc`)
     bool tc;
     u32 tc_Cg2, tc_Np, tc_cols, tc_ref_cap;
@@ -172,6 +175,9 @@ Workspace layout(char *base, u32 n, u32 K, u32 L, u32 nmax, bool want_fast, u32 
         w.pool_item = (u32 *)take((size_t)w.pool_cap * 4);
         w.fb_slots = (u32 *)take(sl * 4);
         w.fb_list = (u32 *)take(sl * 4);
+        w.ua = (float *)take(sl * 4);
+        w.stiles = (S + kTcM - 1) / kTcM;
+        w.kexp_tile = (int *)take(sl * w.stiles * 4);
     }
     w.tc = want_tc && tc_fits(C, K, L, &w.tc_Cg2, &w.tc_Np);
     if (w.tc) {
@@ -294,6 +300,8 @@ int launch_accept(u32 n, u32 C, u32 L, const float *thr, const u32 *win, const u
     return FBP_OK;
 }
 
+float tc_kappa(u32 C, u32 L, u32 Cg2);
+
 OvArgs ov_args(const Workspace &w, const float *v, u32 n, u32 C, const float *T, u32 K, u32 L, u32 nmax,
                const float *thr, const fbp_window_state &s, const float *Lk, const u32 *cand,
                const u32 *n_cand, Counters *cnt) {
@@ -312,6 +320,14 @@ OvArgs ov_args(const Workspace &w, const float *v, u32 n, u32 C, const float *T,
     A.best_key = w.best_key; A.fallback = w.fallback;
     A.items_evaluated = &cnt->ov_items;
     A.pool_total = &cnt->pool_total;
+    A.ua = w.ua;
+    if (w.tc) {                      // H from the tensor cores
+        A.km_override = tc_kappa(C, L, w.tc_Cg2);
+        A.tabs = w.tc_tabs;
+        A.texp = w.tc_texp;
+        A.kexp_tile = w.kexp_tile;
+        A.stiles = w.stiles;
+    }
     return A;
 }
 
@@ -337,7 +353,23 @@ int ov_fast_pass(const Workspace &w, const OvArgs &A, Counters *cnt, cudaStream_
     k_ov_group<<<1, 32, 0, st>>>(A);
     k_ov_scatter<<<grid_for(slots, 256), 256, 0, st>>>(A);
     FBP_LAUNCH_CHECK();
-    {
+    if (w.tc) {
+        TcArgs T{};
+        T.n = A.n; T.C = A.C; T.K = A.K; T.L = A.L;
+        T.Cg2 = w.tc_Cg2; T.Np = w.tc_Np;
+        T.rows_pad = (kTcM + A.L - 1 + 7) / 8 * 8;
+        T.tmem_cols = w.tc_cols;
+        T.v = A.v; T.T = A.T; T.texp = w.tc_texp; T.Tb = w.Tb;
+        T.tb_bytes = (u32)((size_t)A.L * w.tc_Cg2 * w.tc_Np * 16);
+        T.err = &cnt->tc_err;
+        T.S = S; T.nmax = A.nmax; T.stiles = w.stiles;
+        T.cand = A.cand; T.n_cand = A.n_cand; T.best_idx = A.best_idx; T.cskip = A.cskip;
+        T.NT = A.NT; T.H = A.H; T.kexp_tile = w.kexp_tile;
+        const size_t smem = tc_smem_bytes(A.L, w.tc_Cg2, w.tc_Np);
+        FBP_CUDA(cudaFuncSetAttribute(k_lik_tc<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        k_lik_tc<1><<<sm_count(), kTcThreads, smem, st>>>(T);
+        FBP_LAUNCH_CHECK();
+    } else {
         const size_t smem = tables_smem_bytes(S, A.K, A.L);
         if (smem > 48 * 1024)
             FBP_CUDA(cudaFuncSetAttribute(k_ov_tables, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
@@ -437,13 +469,13 @@ int tc_likelihood_pass(const Workspace &w, const float *v, u32 n, u32 C, const f
     const size_t smem = tc_smem_bytes(L, w.tc_Cg2, w.tc_Np);
     FBP_CUDA(cudaMemsetAsync(&cnt->tc_ref, 0, 4, st));
     FBP_CUDA(cudaMemsetAsync(w.tc_seg_count, 0, 4, st));
-    FBP_CUDA(cudaFuncSetAttribute(k_lik_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    k_lik_tc<<<sm_count(), kTcThreads, smem, st>>>(A);
+    FBP_CUDA(cudaFuncSetAttribute(k_lik_tc<0>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    k_lik_tc<0><<<sm_count(), kTcThreads, smem, st>>>(A);
     FBP_LAUNCH_CHECK();
     const size_t rsmem = tc_refine_smem_bytes(C, L);
     if (rsmem > 48 * 1024)
         FBP_CUDA(cudaFuncSetAttribute(k_tc_refine, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)rsmem));
-    k_tc_refine<<<sm_count() * 2, kRefThreads, rsmem, st>>>(v, n, C, T, K, L, tss, w.tc_ref_t, w.tc_ref_s,
+    k_tc_refine<<<sm_count() * 8, kRefThreads, rsmem, st>>>(v, n, C, T, K, L, tss, w.tc_ref_t, w.tc_ref_s,
                                                             w.tc_seg_s0, w.tc_seg_base, w.tc_seg_cnt,
                                                             w.tc_seg_count, w.tc_seg_cap, Lk);
     k_tc_gate<<<1, 1, 0, st>>>(cnt, w.tc_ref_cap, w.tc_seg_count, w.tc_seg_cap);

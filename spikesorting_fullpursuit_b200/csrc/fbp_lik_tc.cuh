@@ -63,6 +63,13 @@ struct TcArgs {
     u32 *seg_count, *seg_overflow;
     u32 seg_cap;
     u32 *err;                        // non-zero: a bounded wait gave up
+    // overlap-table tiles (MODE 1): rows are the shifts b of a candidate window
+    u32 S, nmax, stiles;
+    const u32 *cand, *n_cand, *best_idx;
+    const u8 *cskip;
+    const float *NT;                 // [K][S]
+    float *H;                        // [slot][K][S]
+    int *kexp_tile;                  // [slot][stiles] voltage scale of each tile
 };
 
 __host__ __device__ inline size_t tc_smem_bytes(u32 L, u32 Cg2, u32 Np) {
@@ -121,6 +128,13 @@ __device__ __forceinline__ bool mbar_wait_bounded(u32 bar, u32 parity, u32 limit
     return false;
 }
 
+// MODE 0: likelihood tiles (128 samples of a listed window).
+// MODE 1: overlap tables -- tile = (candidate, 128 shifts b); the strip is the
+//         candidate window [i0, i0+L) with zeros around it, so row b of the
+//         product is the correlation of every template shifted by b - n_max
+//         with the window (H of the fast overlap recheck, without refinement:
+//         its error bound goes into the overlap intervals).
+template <int MODE>
 __global__ void __launch_bounds__(kTcThreads, 1)
 k_lik_tc(TcArgs A) {
     extern __shared__ __align__(128) unsigned char tsm[];
@@ -172,20 +186,33 @@ k_lik_tc(TcArgs A) {
     const u32 lbo_a = rows_pad * 16, lbo_b = Np * 16;
     const u32 a_base = smem_u32(As), b_base = smem_u32(Bs);
     const float kappa_b = A.kappa_b;
-    const u32 n_win = *A.n_win;
-    const u32 sub = (L + kTcM - 1) / kTcM;       // 128-sample tiles per window
+    const u32 sub = MODE == 0 ? (L + kTcM - 1) / kTcM : A.stiles;   // tiles per window / candidate
+    const u64 nitems = (u64)(MODE == 0 ? *A.n_win : *A.n_cand) * sub;
     u32 phase = 0;
 
-    for (u64 item = blockIdx.x; ok && item < (u64)n_win * sub; item += gridDim.x) {
-        const u32 w = A.win[item / sub];
-        const u32 s0 = w * L + (u32)(item % sub) * kTcM;
-        const u32 ew = min((w + 1) * L, n);
+    for (u64 item = blockIdx.x; ok && item < nitems; item += gridDim.x) {
+        // strip row x holds sample s0 + x (MODE 1: signed, masked to [m_lo, m_hi))
+        long long s0;
+        u32 ew = 0, g = 0;
+        long long m_lo = 0, m_hi = n;
+        if (MODE == 0) {
+            const u32 w = A.win[item / sub];
+            s0 = (long long)w * L + (u32)(item % sub) * kTcM;
+            ew = min((w + 1) * L, n);
+        } else {
+            g = (u32)(item / sub);
+            if (A.cskip[g]) continue;
+            const u32 i0 = A.best_idx[A.cand[g]];
+            s0 = (long long)i0 - (long long)A.nmax + (long long)(item % sub) * kTcM;
+            m_lo = i0;
+            m_hi = (long long)i0 + L;
+        }
         // ---- row sums (energy, absolute) and the tile's largest magnitude
         float mx = 0.0f;
         for (u32 x = tid; x < rows_pad; x += blockDim.x) {
-            const u32 pos = s0 + x;
+            const long long pos = s0 + x;
             float e2 = 0.0f, ab = 0.0f;
-            if (pos < n)
+            if (pos >= m_lo && pos < m_hi && pos < n)
                 for (u32 c = 0; c < A.C; c++) {
                     const float f = A.v[(size_t)c * n + pos];
                     e2 = fmaf(f, f, e2);
@@ -207,18 +234,20 @@ k_lik_tc(TcArgs A) {
                 e = 14 - e;                          // scaled magnitudes < 2^14
             }
             *tile_exp = e;
+            if (MODE == 1) A.kexp_tile[(size_t)g * sub + (u32)(item % sub)] = e;
         }
         __syncthreads();
         const int kexp = *tile_exp;
         // ---- stage the strip: rows x -> samples s0 + x, 8 fp16 channels per row
         for (u32 e = tid; e < rows_pad * Cg2; e += blockDim.x) {
-            const u32 x = e % rows_pad, g = e / rows_pad;
-            const u32 pos = s0 + x;
+            const u32 x = e % rows_pad, cg = e / rows_pad;
+            const long long pos = s0 + x;
+            const bool inside = pos >= m_lo && pos < m_hi && pos < n;
             u16 h[8];
 #pragma unroll
             for (int j = 0; j < 8; j++) {
-                const u32 c = g * 8 + j;
-                const float f = (c < A.C && pos < n) ? A.v[(size_t)c * n + pos] : 0.0f;
+                const u32 c = cg * 8 + j;
+                const float f = (c < A.C && inside) ? A.v[(size_t)c * n + pos] : 0.0f;
                 h[j] = __half_as_ushort(__float2half_rn(ldexpf(f, kexp)));
             }
             uint4 q;
@@ -226,7 +255,7 @@ k_lik_tc(TcArgs A) {
             q.y = ((u32)h[3] << 16) | h[2];
             q.z = ((u32)h[5] << 16) | h[4];
             q.w = ((u32)h[7] << 16) | h[6];
-            *reinterpret_cast<uint4 *>(As + ((size_t)g * rows_pad + x) * 16) = q;
+            *reinterpret_cast<uint4 *>(As + ((size_t)cg * rows_pad + x) * 16) = q;
         }
         asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
         __syncthreads();
@@ -249,7 +278,7 @@ k_lik_tc(TcArgs A) {
                          ::"r"(bar_mma) : "memory");
         }
         // ---- meanwhile: prefix sums of the row sums (warp 1: energies, warp 2: absolute)
-        if (warp == 1 || warp == 2) {
+        if (MODE == 0 && (warp == 1 || warp == 2)) {
             float *arr = warp == 1 ? rowsq : rowab;
             float carry = 0.0f;
             for (u32 x0 = 0; x0 < rows_pad; x0 += 32) {
@@ -273,9 +302,37 @@ k_lik_tc(TcArgs A) {
         }
         phase ^= 1u;
         asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+        if (MODE == 1) {
+            // H[g][t][b] = correlation - 0.5 * clipped energy, b = shift row
+            const u32 row = warp * 32 + lane;
+            const u32 b = (u32)(item % sub) * kTcM + row;
+            for (u32 c0 = 0; c0 < Np; c0 += 16) {
+                u32 r[16];
+                asm volatile(
+                    "tcgen05.ld.sync.aligned.32x32b.x16.b32 "
+                    "{%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, %15}, [%16];"
+                    : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]),
+                      "=r"(r[7]), "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]),
+                      "=r"(r[14]), "=r"(r[15])
+                    : "r"(tmem + ((warp * 32u) << 16) + c0));
+                asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+                if (b < A.S) {
+#pragma unroll
+                    for (int q = 0; q < 16; q++) {
+                        const u32 t = c0 + q;
+                        if (t >= A.K) continue;
+                        A.H[((size_t)g * A.K + t) * A.S + b] =
+                            ldexpf(__uint_as_float(r[q]), -(kexp + A.texp[t])) - 0.5f * A.NT[(size_t)t * A.S + b];
+                    }
+                }
+            }
+            asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+            __syncthreads();
+            continue;
+        }
         // ---- epilogue: warp w reads rows 32w..32w+31 (one sample per thread)
         const u32 row = warp * 32 + lane;
-        const u32 s = s0 + row;
+        const u32 s = (u32)s0 + row;
         const bool in_win = s < ew && row < kTcM;
         float wn = 0.0f, wa = 0.0f;
         if (in_win) {
@@ -345,7 +402,7 @@ k_lik_tc(TcArgs A) {
         if (seg_total && tid == 0 && seg_base + seg_total <= A.ref_cap) {
             const u32 si = atomicAdd(A.seg_count, 1u);
             if (si < A.seg_cap) {
-                A.seg_s0[si] = s0;
+                A.seg_s0[si] = (u32)s0;
                 A.seg_base[si] = seg_base;
                 A.seg_cnt[si] = seg_total;
             } else {

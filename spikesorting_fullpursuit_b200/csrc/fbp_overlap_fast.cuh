@@ -67,6 +67,14 @@ struct OvArgs {
     u64 *best_key;                   // [slot] packed (value, ~item) of the best refined contender
     u8 *fallback;                    // [slot]
     u64 *items_evaluated;
+    // H from the tensor cores: its rounding bound replaces kappa_mine, plus
+    // the fp16 subnormal terms (see fbp_lik_tc.cuh)
+    float km_override;               // > 0: bound of the tensor-core tables
+    const float *tabs;               // [K] ||t||_1
+    const int *texp;                 // [K] template scale exponents
+    const int *kexp_tile;            // [slot][stiles] window scale exponents
+    u32 stiles;
+    float *ua;                       // [slot] ||window||_1
 };
 
 __device__ __forceinline__ float warp_max_f(float x) {
@@ -169,17 +177,22 @@ __global__ void k_ov_prep(OvArgs A) {
         const u32 lab = A.best_lab[id], bidx = A.best_idx[id];
         const float bll = A.Lk[(size_t)lab * A.n + bidx];
         const bool skip = (bll < A.thr[lab]) || (bidx >= A.n - A.L);
-        double e = 0.0;
+        double e = 0.0, e1 = 0.0;
         if (!skip)
             for (u32 q = lane; q < A.C * A.L; q += 32) {
                 const double x = A.v[(size_t)(q / A.L) * A.n + bidx + q % A.L];
                 e += x * x;
+                e1 += fabs(x);
             }
 #pragma unroll
-        for (int o = 16; o > 0; o >>= 1) e += __shfl_xor_sync(0xffffffffu, e, o);
+        for (int o = 16; o > 0; o >>= 1) {
+            e += __shfl_xor_sync(0xffffffffu, e, o);
+            e1 += __shfl_xor_sync(0xffffffffu, e1, o);
+        }
         if (lane == 0) {
             A.cskip[g] = skip;
             A.vn[g] = (float)(sqrt(e) * (1.0 + 1e-6));
+            if (A.ua) A.ua[g] = (float)(e1 * (1.0 + 1e-6));
             A.best_key[g] = 0ull;
             if (!skip) atomicAdd(&A.k0_count[lab], 1u);
         }
@@ -352,8 +365,9 @@ k_ov_sweep(OvArgs A, int mode) {
     u16 *blist = alist + S;
     u32 *abits = (u32 *)((char *)ga_lo + (size_t)20 * S);
     const u32 ntasks = *A.n_k0_active * K;
-    const float kr = A.oc->kappa_ref, km = A.oc->kappa_mine;
+    const float kr = A.oc->kappa_ref, km = A.km_override > 0.0f ? A.km_override : A.oc->kappa_mine;
     const float kx = 2.0f * kr + 4.0f * kUnitRoundoff;
+    const bool tc_tables = A.kexp_tile != nullptr;
     // in-bounds shifts x: x + bidx >= nmax and x + bidx < n - L + nmax
     for (u32 task = blockIdx.x; task < ntasks; task += gridDim.x) {
         const u32 k0 = A.k0_active[task / K], t = task % K;
@@ -391,6 +405,15 @@ k_ov_sweep(OvArgs A, int mode) {
             const float vn = A.vn[g];
             const float LB = mode == 1 ? A.cand_lb[g] : 0.0f;
             const float *Hg = A.H + (size_t)g * K * S;
+            // fp16 subnormal terms of tensor-core tables: 2^-25 (|t|_1 / s_window + |window|_1 / s_t)
+            float subA0 = 0.0f, subA1 = 0.0f, subB1 = 0.0f, subB0 = 0.0f;
+            if (tc_tables) {
+                const float ua = A.ua[g];
+                subA1 = 2.98023224e-08f * 1.001f * ldexpf(ua, -A.texp[k0]);
+                subB1 = 2.98023224e-08f * 1.001f * ldexpf(ua, -A.texp[t]);
+                subA0 = 2.98023224e-08f * 1.001f * A.tabs[k0];
+                subB0 = 2.98023224e-08f * 1.001f * A.tabs[t];
+            }
             // in-bounds shift range [xlo, xhi] (.cl:534-541)
             const u32 xlo = bidx >= nmax ? 0u : nmax - bidx;
             const u32 xhi_ex = n - L + nmax - bidx;       // first out-of-bounds shift
@@ -400,12 +423,18 @@ k_ov_sweep(OvArgs A, int mode) {
                 const u32 x = x0 + lane;
                 bool ap = false, bp = false;
                 if (x < S) {
+                    float sa = 0.0f, sb = 0.0f;
+                    if (tc_tables) {
+                        const float w2 = ldexpf(1.0f, -A.kexp_tile[(size_t)g * A.stiles + x / 128]);
+                        sa = subA0 * w2 + subA1;
+                        sb = subB0 * w2 + subB1;
+                    }
                     const float G = Hg[(size_t)k0 * S + x];
-                    const float ea = (kr + km) * (snt0[x] * vn + nt0[x]) + 4.0f * kUnitRoundoff * fabsf(G);
+                    const float ea = (kr + km) * (snt0[x] * vn + nt0[x]) + 4.0f * kUnitRoundoff * fabsf(G) + sa;
                     ga_lo[x] = G - ea;
                     ga_hi[x] = G + ea;
                     const float Hv = Hg[(size_t)t * S + x];
-                    const float eb = (kr + km) * (sntt[x] * vn + ntt[x]) + 4.0f * kUnitRoundoff * fabsf(Hv) + eq;
+                    const float eb = (kr + km) * (sntt[x] * vn + ntt[x]) + 4.0f * kUnitRoundoff * fabsf(Hv) + eq + sb;
                     hb_lo[x] = Hv - eb;
                     hb_hi[x] = Hv + eb;
                     if (x >= xlo && x < xhi_ex) {
