@@ -86,6 +86,9 @@ struct Workspace {
     uint4 *Tb;
     float *tc_tnorm, *tc_tabs;
     int *tc_texp;
+    u8 *apx;
+    float *wn_s, *wa_s;
+    signed char *kx_s;
     u32 *tc_ref_t, *tc_ref_s, *tc_seg_s0, *tc_seg_base, *tc_seg_cnt, *tc_seg_count;
     u32 tc_seg_cap;
     size_t bytes;
@@ -184,6 +187,10 @@ Workspace layout(char *base, u32 n, u32 K, u32 L, u32 nmax, bool want_fast, u32 
         w.tc_cols = 32;
         while (w.tc_cols < w.tc_Np) w.tc_cols <<= 1;
         w.Tb = (uint4 *)take((size_t)L * w.tc_Cg2 * w.tc_Np * 16);
+        w.apx = (u8 *)take((size_t)K * n);
+        w.wn_s = (float *)take((size_t)n * 4);
+        w.wa_s = (float *)take((size_t)n * 4);
+        w.kx_s = (signed char *)take((size_t)n);
         w.tc_tnorm = (float *)take((size_t)K * 4);
         w.tc_tabs = (float *)take((size_t)K * 4);
         w.tc_texp = (int *)take((size_t)K * 4);
@@ -224,7 +231,7 @@ int compact(const u8 *f, u32 W, u32 *list, u32 *count_dev, u32 *tile_counts, cud
 
 int launch_likelihood(const float *v, u32 n, u32 C, const float *T, u32 K, u32 L, const float *tss,
                       const u32 *win, const u32 *n_win_dev, u32 max_windows, float *Lk,
-                      cudaStream_t st, const u32 *gate = nullptr) {
+                      cudaStream_t st, const u32 *gate = nullptr, u8 *apx = nullptr) {
     const size_t smem = (size_t)kLikChanChunk * (kLikTile + L) * sizeof(float);
     static size_t configured = 0;
     if (smem > 48 * 1024 && smem > configured) {
@@ -234,24 +241,29 @@ int launch_likelihood(const float *v, u32 n, u32 C, const float *T, u32 K, u32 L
     }
     const u64 items = (u64)max_windows * ceil_div(K, kLikTplPerBlock);
     const int grid = grid_for(items * kLikThreads, kLikThreads, 16);
-    k_likelihood_fp32<<<grid, kLikThreads, smem, st>>>(v, n, C, T, K, L, tss, win, n_win_dev, Lk, gate);
+    k_likelihood_fp32<<<grid, kLikThreads, smem, st>>>(v, n, C, T, K, L, tss, win, n_win_dev, Lk, gate, apx);
     FBP_LAUNCH_CHECK();
     return FBP_OK;
 }
 
 int launch_argmax(u32 n, u32 L, u32 K, const u32 *win, const u32 *n_win_dev, u32 max_windows,
-                  const fbp_window_state &s, const float *Lk, cudaStream_t st) {
+                  const fbp_window_state &s, float *Lk, cudaStream_t st, const LazyLk &z = LazyLk{}) {
     const int threads = 256;
     const int grid = grid_for((u64)max_windows * 32, threads, 8);
+    if (z.apx) {
+        k_lazy_refine<<<grid, threads, 0, st>>>(n, L, K, win, n_win_dev, Lk, z);
+        FBP_LAUNCH_CHECK();
+    }
     k_window_argmax<<<grid, threads, 0, st>>>(n, L, K, win, n_win_dev, s.best_idx, s.best_lab, s.best_ll,
-                                              s.flags, s.overlap_recheck, s.ov_idx, s.ov_lab, Lk);
+                                              s.flags, s.overlap_recheck, s.ov_idx, s.ov_lab, Lk, z.apx);
     FBP_LAUNCH_CHECK();
     return FBP_OK;
 }
 
 int launch_overlap(const float *v, u32 n, u32 C, const float *T, u32 K, u32 L, const u32 *cand,
-                   const u32 *n_cand_dev, u32 max_cand, const fbp_window_state &s, const float *Lk,
-                   u32 nmax, const float *thr, u64 *items_evaluated, cudaStream_t st) {
+                   const u32 *n_cand_dev, u32 max_cand, const fbp_window_state &s, float *Lk,
+                   u32 nmax, const float *thr, u64 *items_evaluated, cudaStream_t st,
+                   const LazyLk &z = LazyLk{}) {
     const size_t smem = (size_t)2 * C * L * sizeof(float);
     if (smem > 227 * 1024)
         return fail(FBP_ERR_BAD_ARG, "overlap recheck: C*L = %u too large for shared memory", C * L);
@@ -264,7 +276,7 @@ int launch_overlap(const float *v, u32 n, u32 C, const float *T, u32 K, u32 L, c
     const int grid = grid_for((u64)max_cand * kOvThreads, kOvThreads, 4);
     k_overlap_exact<<<grid, kOvThreads, smem, st>>>(v, n, C, T, K, L, cand, n_cand_dev, s.best_idx,
                                                     s.best_lab, s.best_ll, s.ov_idx, s.ov_lab,
-                                                    s.overlap_recheck, Lk, nmax, thr, items_evaluated);
+                                                    s.overlap_recheck, Lk, nmax, thr, items_evaluated, z);
     FBP_LAUNCH_CHECK();
     return FBP_OK;
 }
@@ -302,9 +314,20 @@ int launch_accept(u32 n, u32 C, u32 L, const float *thr, const u32 *win, const u
 
 float tc_kappa(u32 C, u32 L, u32 Cg2);
 
+// Context for likelihood entries the tensor-core path left approximate.
+LazyLk lazy_ctx(const Workspace &w, const float *v, const float *T, const float *tss, u32 C, u32 L) {
+    LazyLk z{};
+    if (!w.tc) return z;
+    z.apx = w.apx; z.wn = w.wn_s; z.wa = w.wa_s; z.kx = w.kx_s;
+    z.tnorm = w.tc_tnorm; z.tabs = w.tc_tabs; z.tss = tss; z.texp = w.tc_texp;
+    z.v = v; z.T = T; z.C = C; z.L = L;
+    z.kappa_b = tc_kappa(C, L, w.tc_Cg2);
+    return z;
+}
+
 OvArgs ov_args(const Workspace &w, const float *v, u32 n, u32 C, const float *T, u32 K, u32 L, u32 nmax,
-               const float *thr, const fbp_window_state &s, const float *Lk, const u32 *cand,
-               const u32 *n_cand, Counters *cnt) {
+               const float *thr, const fbp_window_state &s, float *Lk, const u32 *cand,
+               const u32 *n_cand, Counters *cnt, const float *tss) {
     OvArgs A{};
     A.n = n; A.C = C; A.K = K; A.L = L; A.nmax = nmax; A.S = 2 * nmax + 1;
     A.v = v; A.T = T; A.Lk = Lk; A.thr = thr;
@@ -321,6 +344,7 @@ OvArgs ov_args(const Workspace &w, const float *v, u32 n, u32 C, const float *T,
     A.items_evaluated = &cnt->ov_items;
     A.pool_total = &cnt->pool_total;
     A.ua = w.ua;
+    A.lazy = lazy_ctx(w, v, T, tss, C, L);
     if (w.tc) {                      // H from the tensor cores
         A.km_override = tc_kappa(C, L, w.tc_Cg2);
         A.tabs = w.tc_tabs;
@@ -395,7 +419,7 @@ int ov_fast_pass(const Workspace &w, const OvArgs &A, Counters *cnt, cudaStream_
     FBP_LAUNCH_CHECK();
     fbp_window_state s{A.best_idx, A.best_lab, A.best_ll, A.ov_idx, A.ov_lab, nullptr, A.ovr};
     rc = launch_overlap(A.v, A.n, A.C, A.T, A.K, A.L, w.fb_list, &cnt->fb_count, slots, s, A.Lk, A.nmax, A.thr,
-                        A.items_evaluated, st);
+                        A.items_evaluated, st, A.lazy);
     *launches = 16;
     return rc;
 }
@@ -466,6 +490,7 @@ int tc_likelihood_pass(const Workspace &w, const float *v, u32 n, u32 C, const f
     A.seg_s0 = w.tc_seg_s0; A.seg_base = w.tc_seg_base; A.seg_cnt = w.tc_seg_cnt;
     A.seg_count = w.tc_seg_count; A.seg_overflow = &cnt->tc_overflow; A.seg_cap = w.tc_seg_cap;
     A.err = &cnt->tc_err;
+    A.apx = w.apx; A.wn_s = w.wn_s; A.wa_s = w.wa_s; A.kx_s = w.kx_s;
     const size_t smem = tc_smem_bytes(L, w.tc_Cg2, w.tc_Np);
     FBP_CUDA(cudaMemsetAsync(&cnt->tc_ref, 0, 4, st));
     FBP_CUDA(cudaMemsetAsync(w.tc_seg_count, 0, 4, st));
@@ -480,7 +505,7 @@ int tc_likelihood_pass(const Workspace &w, const float *v, u32 n, u32 C, const f
                                                             w.tc_seg_count, w.tc_seg_cap, Lk);
     k_tc_gate<<<1, 1, 0, st>>>(cnt, w.tc_ref_cap, w.tc_seg_count, w.tc_seg_cap);
     FBP_LAUNCH_CHECK();
-    int rc = launch_likelihood(v, n, C, T, K, L, tss, win, n_win, max_windows, Lk, st, &cnt->tc_overflow);
+    int rc = launch_likelihood(v, n, C, T, K, L, tss, win, n_win, max_windows, Lk, st, &cnt->tc_overflow, w.apx);
     *launches = 4;
     return rc;
 }
@@ -615,6 +640,7 @@ int fbp_pursuit_chunk(float *voltage, uint32_t n, uint32_t C, const float *templ
     timer.end(FBP_STAGE_LISTS);
     if (w.tc) {
         timer.begin(FBP_STAGE_LIKELIHOOD);
+        FBP_CUDA(cudaMemsetAsync(w.apx, 0, (size_t)K * n, st));
         int rc0 = tc_chunk_setup(w, templates, K, C, L, st);
         if (rc0) return rc0;
         S.launches[FBP_STAGE_LIKELIHOOD] += 2;
@@ -653,8 +679,9 @@ int fbp_pursuit_chunk(float *voltage, uint32_t n, uint32_t C, const float *templ
         timer.end(FBP_STAGE_LIKELIHOOD);
         // 2. per-window argmax over all templates (.py:551-562)
         timer.begin(FBP_STAGE_ARGMAX);
-        if ((rc = launch_argmax(n, L, K, w.win, &w.cnt->n_win, W, s, w.Lk, st))) break;
-        S.launches[FBP_STAGE_ARGMAX] += 1;
+        const LazyLk lz = lazy_ctx(w, voltage, templates, neg_half_ss, C, L);
+        if ((rc = launch_argmax(n, L, K, w.win, &w.cnt->n_win, W, s, w.Lk, st, lz))) break;
+        S.launches[FBP_STAGE_ARGMAX] += lz.apx ? 2 : 1;
         timer.end(FBP_STAGE_ARGMAX);
         // 3. candidates = nonzero(overlap_recheck) (.py:565-569), 4. recheck (.py:570-661)
         if (do_overlap_recheck) {
@@ -666,12 +693,12 @@ int fbp_pursuit_chunk(float *voltage, uint32_t n, uint32_t C, const float *templ
             if (w.fast) {
                 int nl = 0;
                 OvArgs A = ov_args(w, voltage, n, C, templates, K, L, nmax, thresholds, s, w.Lk, w.cand,
-                                   &w.cnt->n_cand, w.cnt);
+                                   &w.cnt->n_cand, w.cnt, neg_half_ss);
                 if ((rc = ov_fast_pass(w, A, w.cnt, st, &nl))) break;
                 S.launches[FBP_STAGE_OVERLAP] += nl;
             } else {
                 if ((rc = launch_overlap(voltage, n, C, templates, K, L, w.cand, &w.cnt->n_cand, W, s, w.Lk,
-                                         nmax, thresholds, &w.cnt->ov_items, st)))
+                                         nmax, thresholds, &w.cnt->ov_items, st, lz)))
                     break;
                 S.launches[FBP_STAGE_OVERLAP] += 1;
             }
@@ -730,6 +757,12 @@ int fbp_pursuit_chunk(float *voltage, uint32_t n, uint32_t C, const float *templ
         timer.end(FBP_STAGE_LISTS);
         // 9. subtract them (.py:712-731)
         timer.begin(FBP_STAGE_RESIDUAL);
+        if (lz.apx) {
+            k_lazy_freeze<<<grid_for((u64)added * 32, 256, 8), 256, 0, st>>>(n, L, K, w.spk_idx, w.spk_lab, added,
+                                                                           w.active, W, w.Lk, lz);
+            FBP_LAUNCH_CHECK();
+            S.launches[FBP_STAGE_RESIDUAL] += 1;
+        }
         k_residual<<<grid_for((u64)added * 256, 256, 16), 256, 0, st>>>(
             voltage, n, C, templates, K, L, w.spk_idx, w.spk_lab, nullptr, added, R);
         FBP_LAUNCH_CHECK();
@@ -801,7 +834,7 @@ int fbp_window_argmax(uint32_t n, uint32_t L, uint32_t K, const uint32_t *window
     if (!st || !window_list || !n_windows_dev || !likelihood)
         return fail(FBP_ERR_BAD_ARG, "fbp_window_argmax: null pointer argument");
     if (max_windows == 0) return FBP_OK;
-    return launch_argmax(n, L, K, window_list, n_windows_dev, max_windows, *st, likelihood,
+    return launch_argmax(n, L, K, window_list, n_windows_dev, max_windows, *st, const_cast<float *>(likelihood),
                          (cudaStream_t)stream);
 }
 
@@ -813,8 +846,8 @@ int fbp_overlap_recheck(const float *voltage, uint32_t n, uint32_t C, const floa
     if (!voltage || !templates || !cand_list || !n_cand_dev || !st || !likelihood || !thresholds)
         return fail(FBP_ERR_BAD_ARG, "fbp_overlap_recheck: null pointer argument");
     if (max_cand == 0) return FBP_OK;
-    return launch_overlap(voltage, n, C, templates, K, L, cand_list, n_cand_dev, max_cand, *st, likelihood,
-                          nmax, thresholds, nullptr, (cudaStream_t)stream);
+    return launch_overlap(voltage, n, C, templates, K, L, cand_list, n_cand_dev, max_cand, *st,
+                          const_cast<float *>(likelihood), nmax, thresholds, nullptr, (cudaStream_t)stream);
 }
 
 int fbp_check_overlap_reassignments(uint32_t n, uint32_t L, const uint32_t *cand_list,

@@ -99,7 +99,8 @@ constexpr int kLikChanChunk = 8;
 __global__ void __launch_bounds__(kLikThreads)
 k_likelihood_fp32(const float *__restrict__ v, u32 n, u32 C, const float *__restrict__ T, u32 K, u32 L,
                   const float *__restrict__ tss, const u32 *__restrict__ win,
-                  const u32 *__restrict__ n_win_dev, float *__restrict__ Lk, const u32 *__restrict__ gate) {
+                  const u32 *__restrict__ n_win_dev, float *__restrict__ Lk, const u32 *__restrict__ gate,
+                  u8 *__restrict__ apx) {
     extern __shared__ float strip[];   // kLikChanChunk x (kLikTile + L)
     if (gate && *gate == 0) return;    // only run when the gate asks for it
     const u32 n_win = *n_win_dev;
@@ -154,9 +155,133 @@ k_likelihood_fp32(const float *__restrict__ v, u32 n, u32 C, const float *__rest
 #pragma unroll
                 for (int r = 0; r < kLikR; r++) {
                     const u32 s = s0 + lane + 32 * r;
-                    if (s < ew && s < s0 + kLikTile)
+                    if (s < ew && s < s0 + kLikTile) {
                         Lk[(size_t)(t0 + q) * n + s] = (s + L >= n) ? 0.0f : acc[q][r];
+                        if (apx) apx[(size_t)(t0 + q) * n + s] = 0;
+                    }
                 }
+            }
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Likelihood entries left approximate by the tensor-core path.  Certainly
+// positive entries keep an approximate value and a flag; their interval is
+// rebuilt from per-sample data (window norms and the tile's fp16 scale) and
+// per-template data, and they are re-evaluated in the reference's order when
+// a decision needs their value (exact values are written back).
+// ---------------------------------------------------------------------------
+// Likelihood entries the tensor-core path stored approximately.  apx[t][s]:
+//   0  the stored value is the reference value, or an approximation that is
+//      certainly <= 0 (only its sign is ever read);
+//   1  approximate and certainly > 0; the interval is approx +- lazy_bound;
+//   2  was 1, the reference value has since been stored.
+// A flag only moves 1 -> 2 inside a kernel (value first), so a reader that
+// sees 1 or 2 may use either version of the value with the interval.
+struct LazyLk {
+    u8 *apx;                          // [K][n]; NULL: every entry is exact
+    const float *wn, *wa;             // [n] window L2 / L1 norms at computation time
+    const signed char *kx;            // [n] fp16 scale exponent of the tile
+    const float *tnorm, *tabs, *tss;  // [K]
+    const int *texp;                  // [K]
+    const float *v, *T;               // voltage (residual) and templates
+    u32 C, L;
+    float kappa_b;
+};
+
+// The bound the tensor-core epilogue used for entry (t, s) (same formula).
+__device__ __forceinline__ float lazy_bound(const LazyLk &z, u32 t, u32 s, float approx) {
+    const float sub = 2.98023223876953125e-08f * (ldexpf(z.tabs[t], -(int)z.kx[s]) + ldexpf(z.wa[s], -z.texp[t])) * 1.001f;
+    return z.kappa_b * z.tnorm[t] * z.wn[s] + sub + 2.384185791015625e-07f * (fabsf(z.tss[t]) + fabsf(approx));
+}
+
+// compute_maximum_likelihood (binary_pursuit.cl:216-252), reference order.
+__device__ __forceinline__ float exact_likelihood(const LazyLk &z, u32 n, u32 t, u32 s) {
+    float acc = z.tss[t];
+    for (u32 c = 0; c < z.C; c++) {
+        const float *tp = z.T + ((size_t)t * z.C + c) * z.L;
+        const float *vp = z.v + (size_t)c * n + s;
+        for (u32 i = 0; i < z.L; i++) acc = __fadd_rn(acc, __fmul_rn(__ldg(tp + i), vp[i]));
+    }
+    return acc;
+}
+
+// The reference value of likelihood[t][pos] for a decision; not written back.
+__device__ __forceinline__ float lk_exact(const LazyLk &z, const float *Lk, u32 n, u32 t, u32 pos) {
+    const size_t e = (size_t)t * n + pos;
+    if (z.apx && z.apx[e] == 1) return exact_likelihood(z, n, t, pos);
+    return Lk[e];
+}
+
+// Before the window argmax: for each listed window, the largest lower bound
+// over its range [sw-L, ew+L) and the reference value of every approximate
+// entry whose upper bound reaches it.  Afterwards every entry of the range
+// that can hold the maximum is exact, and every other one is certainly below
+// it -- so the argmax reads the reference's maxima.
+__global__ void k_lazy_refine(u32 n, u32 L, u32 K, const u32 *__restrict__ win, const u32 *__restrict__ n_win_dev,
+                              float *__restrict__ Lk, LazyLk z) {
+    const u32 n_win = *n_win_dev;
+    const u32 lane = threadIdx.x & 31;
+    const u32 warps_per_block = blockDim.x >> 5;
+    for (u32 g = blockIdx.x * warps_per_block + (threadIdx.x >> 5); g < n_win;
+         g += gridDim.x * warps_per_block) {
+        const u32 id = win[g];
+        const u32 sw = id * L, ew = (id + 1) * L;
+        const u32 start = (L > sw) ? 0 : sw - L;
+        const u32 stop = (ew + L) > n ? n : ew + L;
+        if (ew >= n - L) continue;                       // the argmax skips it (.cl:380-383)
+        float lb = 0.0f;
+        bool any = false;
+        for (u32 t = 0; t < K; t++)
+            for (u32 s = start + lane; s < stop; s += 32) {
+                const size_t e = (size_t)t * n + s;
+                const float cur = Lk[e];
+                const u8 f = z.apx[e];
+                any |= f != 0;
+                lb = fmaxf(lb, f ? cur - lazy_bound(z, t, s, cur) : cur);
+            }
+        if (!__any_sync(0xffffffffu, any)) continue;
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) lb = fmaxf(lb, __shfl_xor_sync(0xffffffffu, lb, o));
+        for (u32 t = 0; t < K; t++)
+            for (u32 s = start + lane; s < stop; s += 32) {
+                const size_t e = (size_t)t * n + s;
+                if (z.apx[e] != 1) continue;
+                const float cur = Lk[e];
+                if (cur + lazy_bound(z, t, s, cur) >= lb) {
+                    Lk[e] = exact_likelihood(z, n, t, s);
+                    __threadfence();
+                    z.apx[e] = 2;
+                }
+            }
+    }
+}
+
+// Before the residual subtracts this pass's spikes: an approximate entry
+// that reads a changing sample and whose window is not recomputed next pass
+// keeps, in the reference, the value it was computed with; store that value
+// now, from the voltage it was computed from.
+__global__ void k_lazy_freeze(u32 n, u32 L, u32 K, const u32 *__restrict__ idx, const u32 *__restrict__ lab,
+                              u32 m, const u8 *__restrict__ next_active, u32 W, float *__restrict__ Lk,
+                              LazyLk z) {
+    const u32 lane = threadIdx.x & 31;
+    const u32 warps_per_block = blockDim.x >> 5;
+    for (u32 g = blockIdx.x * warps_per_block + (threadIdx.x >> 5); g < m;
+         g += gridDim.x * warps_per_block) {
+        if (lab[g] >= K) continue;
+        const u32 p = idx[g];
+        const u32 lo = p + 1 > L ? p + 1 - L : 0;
+        const u32 hi = min(n, p + L);
+        for (u32 s = lo + lane; s < hi; s += 32) {
+            const u32 wd = s / L;
+            if (wd < W && next_active[wd]) continue;     // recomputed next pass
+            for (u32 t = 0; t < K; t++) {
+                const size_t e = (size_t)t * n + s;
+                if (z.apx[e] != 1) continue;
+                Lk[e] = exact_likelihood(z, n, t, s);
+                __threadfence();
+                z.apx[e] = 2;
             }
         }
     }
@@ -175,7 +300,7 @@ __global__ void k_window_argmax(u32 n, u32 L, u32 K, const u32 *__restrict__ win
                                 u32 *__restrict__ best_lab, float *__restrict__ best_ll,
                                 u8 *__restrict__ flags, u8 *__restrict__ ovr,
                                 u32 *__restrict__ ov_idx, u32 *__restrict__ ov_lab,
-                                const float *__restrict__ Lk) {
+                                const float *__restrict__ Lk, const u8 *__restrict__ apx) {
     const u32 n_win = *n_win_dev;
     const u32 lane = threadIdx.x & 31;
     const u32 warps_per_block = blockDim.x >> 5;
@@ -196,7 +321,8 @@ __global__ void k_window_argmax(u32 n, u32 L, u32 K, const u32 *__restrict__ win
             for (u32 s = start + lane; s < stop; s += 32) {
                 const float cur = row[s];
                 if (cur > lv) { lv = cur; li = s; }
-                check |= (cur > 0.0f) && s >= sw && s < ew;
+                // a flagged entry is certainly positive
+                check |= (cur > 0.0f || (apx && apx[(size_t)t * n + s])) && s >= sw && s < ew;
             }
 #pragma unroll
             for (int o = 16; o > 0; o >>= 1) {
@@ -255,15 +381,15 @@ __device__ __forceinline__ float overlap_pair_exact(const float *__restrict__ vw
 __device__ __forceinline__ void overlap_parse(u32 id, u32 n, u32 K, u32 S, u32 nmax, float best_group,
                                               u64 best_item, u32 *best_idx, u32 *best_lab,
                                               float *best_ll, u32 *ov_idx, u32 *ov_lab, u8 *ovr,
-                                              const float *Lk, const float *thr) {
+                                              const float *Lk, const float *thr, const LazyLk &z) {
     if (best_group <= best_ll[id] || best_group <= 0.0f) { ovr[id] = 0; return; }
     const u32 lab = best_lab[id], bidx = best_idx[id];
     const u32 t = (u32)(best_item % K);
     const u32 a = (u32)((best_item / K) % S);
     const u32 b = (u32)((best_item / ((u64)S * K)) % S);
     const u32 afix = bidx + a - nmax, ashift = bidx + b - nmax;
-    const float lf = Lk[(size_t)lab * n + afix];
-    const float ls = Lk[(size_t)t * n + ashift];
+    const float lf = lk_exact(z, Lk, n, lab, afix);
+    const float ls = lk_exact(z, Lk, n, t, ashift);
     if (best_group < lf || best_group < ls) { ovr[id] = 0; return; }
     if (lf <= 0.0f || ls <= 0.0f) { ovr[id] = 0; return; }
     if (lf >= ls && lf > thr[lab]) {
@@ -285,7 +411,7 @@ k_overlap_exact(const float *__restrict__ v, u32 n, u32 C, const float *__restri
                 u32 *__restrict__ best_idx, u32 *__restrict__ best_lab, float *__restrict__ best_ll,
                 u32 *__restrict__ ov_idx, u32 *__restrict__ ov_lab, u8 *__restrict__ ovr,
                 const float *__restrict__ Lk, u32 nmax, const float *__restrict__ thr,
-                u64 *__restrict__ items_evaluated) {
+                u64 *__restrict__ items_evaluated, LazyLk z) {
     extern __shared__ float sm[];          // vwin [C*L], tk0 [C*L]
     __shared__ float red_v[kOvThreads / 32];
     __shared__ u64 red_i[kOvThreads / 32];
@@ -348,7 +474,7 @@ k_overlap_exact(const float *__restrict__ v, u32 n, u32 C, const float *__restri
             for (u32 w = 1; w < blockDim.x / 32; w++)
                 if (red_v[w] > bv || (red_v[w] == bv && red_i[w] < bi)) { bv = red_v[w]; bi = red_i[w]; }
             overlap_parse(id, n, K, S, nmax, bv, bi == ~0ull ? 0 : bi, best_idx, best_lab, best_ll,
-                          ov_idx, ov_lab, ovr, Lk, thr);
+                          ov_idx, ov_lab, ovr, Lk, thr, z);
         }
     }
 }

@@ -63,6 +63,9 @@ struct TcArgs {
     u32 *seg_count, *seg_overflow;
     u32 seg_cap;
     u32 *err;                        // non-zero: a bounded wait gave up
+    u8 *apx;                         // [K][n] approximate-entry flags
+    float *wn_s, *wa_s;              // [n] per-sample window norms
+    signed char *kx_s;               // [n] per-sample fp16 scale exponent
     // overlap-table tiles (MODE 1): rows are the shifts b of a candidate window
     u32 S, nmax, stiles;
     const u32 *cand, *n_cand, *best_idx;
@@ -232,6 +235,7 @@ k_lik_tc(TcArgs A) {
             if (m > 0.0f) {
                 frexpf(m, &e);                       // m < 2^e
                 e = 14 - e;                          // scaled magnitudes < 2^14
+                e = max(-127, min(127, e));          // stored as int8 with the entries
             }
             *tile_exp = e;
             if (MODE == 1) A.kexp_tile[(size_t)g * sub + (u32)(item % sub)] = e;
@@ -340,9 +344,14 @@ k_lik_tc(TcArgs A) {
             wn = sqrtf(fmaxf(rowsq[hi_i] - (row ? rowsq[row - 1] : 0.0f), 0.0f)) * 1.0001f + 1e-30f;
             wa = fmaxf(rowab[hi_i] - (row ? rowab[row - 1] : 0.0f), 0.0f) * 1.0001f + 1e-30f;
         }
-        // phase 1: store the provably-negative values, mark the others
+        // phase 1: store the values whose sign is certain, mark the others
         u32 wantbits[8] = {0, 0, 0, 0, 0, 0, 0, 0};      // Np <= 256
         u32 nwant = 0;
+        if (in_win) {                                    // interval data of this sample
+            A.wn_s[s] = wn;
+            A.wa_s[s] = wa;
+            A.kx_s[s] = (signed char)kexp;
+        }
         for (u32 c0 = 0; c0 < Np; c0 += 16) {
             u32 r[16];
             asm volatile(
@@ -358,7 +367,8 @@ k_lik_tc(TcArgs A) {
                 const u32 t = c0 + q;
                 if (!in_win || t >= A.K) continue;
                 float *dst = A.Lk + (size_t)t * n + s;
-                if (s + L >= n) { *dst = 0.0f; continue; }               // .cl:231-234
+                u8 *fl = A.apx + (size_t)t * n + s;
+                if (s + L >= n) { *dst = 0.0f; *fl = 0; continue; }     // .cl:231-234
                 const float tssv = A.tss[t];
                 const int je = A.texp[t];
                 const float approx = ldexpf(__uint_as_float(r[q]), -(kexp + je)) + tssv;
@@ -366,11 +376,16 @@ k_lik_tc(TcArgs A) {
                                   (ldexpf(A.tabs[t], -kexp) + ldexpf(wa, -je)) * 1.001f;
                 const float E = kappa_b * A.tnorm[t] * wn + sub +
                                 2.384185791015625e-07f * (fabsf(tssv) + fabsf(approx));
-                if (approx + E > 0.0f) {
+                if (approx + E <= 0.0f) {            // certainly <= 0: only its sign is read
+                    *dst = approx;
+                    *fl = 0;
+                } else if (approx - E > 0.0f) {      // certainly > 0: refined when a decision needs it
+                    *dst = approx;
+                    *fl = 1;
+                } else {                             // sign uncertain: refined now
                     wantbits[t >> 5] |= 1u << (t & 31);
                     nwant++;
-                } else {
-                    *dst = approx;
+                    *fl = 0;
                 }
             }
         }

@@ -43,7 +43,8 @@ struct OvConst {
 
 struct OvArgs {
     u32 n, C, K, L, nmax, S;
-    const float *v, *T, *Lk, *thr;
+    const float *v, *T, *thr;
+    float *Lk;
     const float *NT, *sNT, *tnorm;   // [K][S], [K][S], [K]
     const float *Q;                  // [K][K][2L-1][L+1]
     const OvConst *oc;
@@ -75,6 +76,7 @@ struct OvArgs {
     const int *kexp_tile;            // [slot][stiles] window scale exponents
     u32 stiles;
     float *ua;                       // [slot] ||window||_1
+    LazyLk lazy;                     // approximate likelihood entries (tensor-core path)
 };
 
 __device__ __forceinline__ float warp_max_f(float x) {
@@ -635,7 +637,7 @@ __global__ void k_ov_finalize(OvArgs A) {
             bi = 0xffffffffu - (u32)(key & 0xffffffffu);
         }
         overlap_parse(id, A.n, A.K, A.S, A.nmax, bv, bi, A.best_idx, A.best_lab, A.best_ll, A.ov_idx,
-                      A.ov_lab, A.ovr, A.Lk, A.thr);
+                      A.ov_lab, A.ovr, A.Lk, A.thr, A.lazy);
     }
 }
 
