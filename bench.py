@@ -335,6 +335,7 @@ def main():
                            "overlap_refined_items": int(stats[-1].refined_items),
                            "overlap_fallback_candidates": int(stats[-1].fallback_candidates),
                            "likelihood_refined": int(stats[-1].lik_refined),
+                           "likelihood_lazy_refined": int(stats[-1].lik_lazy_refined),
                            "likelihood_exact_passes": int(stats[-1].lik_exact_passes),
                            "parallelism": "segment-parallel x%d" % world},
                 "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": gpu_launches,

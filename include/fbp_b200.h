@@ -101,6 +101,9 @@ typedef struct fbp_stage_stats {
                                    in FP32 */
     uint32_t passes;
     uint32_t spikes;
+    uint64_t lik_lazy_refined;  /* likelihood entries left approximate (certainly > 0) and
+                                   re-evaluated exactly when a decision needed them
+                                   (FBP_PREC_BF16_REFINE) */
 } fbp_stage_stats;
 
 /* Library version (major*10000 + minor*100 + patch). */

@@ -322,6 +322,7 @@ LazyLk lazy_ctx(const Workspace &w, const float *v, const float *T, const float 
     z.tnorm = w.tc_tnorm; z.tabs = w.tc_tabs; z.tss = tss; z.texp = w.tc_texp;
     z.v = v; z.T = T; z.C = C; z.L = L;
     z.kappa_b = tc_kappa(C, L, w.tc_Cg2);
+    z.refined = &w.cnt->lazy_ref;
     return z;
 }
 
@@ -779,6 +780,7 @@ int fbp_pursuit_chunk(float *voltage, uint32_t n, uint32_t C, const float *templ
             *n_spikes_host = h_counts[3];
             S.spikes = h_counts[3];
             S.work[FBP_STAGE_OVERLAP] = *(const u64 *)(h_counts + 8);
+            S.lik_lazy_refined = ((const Counters *)h_counts)->lazy_ref;
             if (h_counts[4]) rc = fail(FBP_ERR_CAPACITY, "spike output holds %u spikes; more were found", spike_cap);
         }
     }

@@ -33,7 +33,9 @@ struct Counters {
     u32 tc_ref;       // tensor-core likelihood entries queued for exact refinement this pass
     u32 tc_err;       // non-zero: a bounded wait in the tensor-core kernel gave up
     u32 tc_overflow;  // refinement list overflowed: the exact kernel redoes the pass
-    u32 pad[19];
+    u32 pad0;
+    u64 lazy_ref;     // approximate likelihood entries refined on demand (whole chunk)
+    u32 pad[16];
 };
 static_assert(sizeof(Counters) == 128, "Counters is one 128-byte line");
 

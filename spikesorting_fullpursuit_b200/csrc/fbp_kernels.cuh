@@ -188,6 +188,7 @@ struct LazyLk {
     const float *v, *T;               // voltage (residual) and templates
     u32 C, L;
     float kappa_b;
+    u64 *refined;                     // count of entries refined on demand (may be NULL)
 };
 
 // The bound the tensor-core epilogue used for entry (t, s) (same formula).
@@ -244,6 +245,7 @@ __global__ void k_lazy_refine(u32 n, u32 L, u32 K, const u32 *__restrict__ win, 
         if (!__any_sync(0xffffffffu, any)) continue;
 #pragma unroll
         for (int o = 16; o > 0; o >>= 1) lb = fmaxf(lb, __shfl_xor_sync(0xffffffffu, lb, o));
+        u32 nref = 0;
         for (u32 t = 0; t < K; t++)
             for (u32 s = start + lane; s < stop; s += 32) {
                 const size_t e = (size_t)t * n + s;
@@ -253,8 +255,10 @@ __global__ void k_lazy_refine(u32 n, u32 L, u32 K, const u32 *__restrict__ win, 
                     Lk[e] = exact_likelihood(z, n, t, s);
                     __threadfence();
                     z.apx[e] = 2;
+                    nref++;
                 }
             }
+        if (z.refined && nref) atomicAdd(z.refined, (u64)nref);
     }
 }
 
@@ -273,6 +277,7 @@ __global__ void k_lazy_freeze(u32 n, u32 L, u32 K, const u32 *__restrict__ idx, 
         const u32 p = idx[g];
         const u32 lo = p + 1 > L ? p + 1 - L : 0;
         const u32 hi = min(n, p + L);
+        u32 nref = 0;
         for (u32 s = lo + lane; s < hi; s += 32) {
             const u32 wd = s / L;
             if (wd < W && next_active[wd]) continue;     // recomputed next pass
@@ -282,8 +287,10 @@ __global__ void k_lazy_freeze(u32 n, u32 L, u32 K, const u32 *__restrict__ idx, 
                 Lk[e] = exact_likelihood(z, n, t, s);
                 __threadfence();
                 z.apx[e] = 2;
+                nref++;
             }
         }
+        if (z.refined && nref) atomicAdd(z.refined, (u64)nref);
     }
 }
 
