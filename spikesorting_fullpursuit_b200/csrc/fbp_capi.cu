@@ -87,7 +87,7 @@ struct Workspace {
     float *tc_tnorm, *tc_tabs;
     int *tc_texp;
     u8 *apx;
-    float *wn_s, *wa_s;
+    float *wn_s, *wa_s, *bm_s, *wlb;
     signed char *kx_s;
     u32 *tc_ref_t, *tc_ref_s, *tc_seg_s0, *tc_seg_base, *tc_seg_cnt, *tc_seg_count;
     u32 tc_seg_cap;
@@ -189,6 +189,8 @@ Workspace layout(char *base, u32 n, u32 K, u32 L, u32 nmax, bool want_fast, u32 
         w.Tb = (uint4 *)take((size_t)L * w.tc_Cg2 * w.tc_Np * 16);
         w.apx = (u8 *)take((size_t)K * n);
         w.wn_s = (float *)take((size_t)n * 4);
+        w.bm_s = (float *)take((size_t)n * 4);
+        w.wlb = (float *)take((size_t)ceil_div(n, L) * 4);
         w.wa_s = (float *)take((size_t)n * 4);
         w.kx_s = (signed char *)take((size_t)n);
         w.tc_tnorm = (float *)take((size_t)K * 4);
@@ -250,12 +252,8 @@ int launch_argmax(u32 n, u32 L, u32 K, const u32 *win, const u32 *n_win_dev, u32
                   const fbp_window_state &s, float *Lk, cudaStream_t st, const LazyLk &z = LazyLk{}) {
     const int threads = 256;
     const int grid = grid_for((u64)max_windows * 32, threads, 8);
-    if (z.apx) {
-        k_lazy_refine<<<grid, threads, 0, st>>>(n, L, K, win, n_win_dev, Lk, z);
-        FBP_LAUNCH_CHECK();
-    }
     k_window_argmax<<<grid, threads, 0, st>>>(n, L, K, win, n_win_dev, s.best_idx, s.best_lab, s.best_ll,
-                                              s.flags, s.overlap_recheck, s.ov_idx, s.ov_lab, Lk, z.apx);
+                                              s.flags, s.overlap_recheck, s.ov_idx, s.ov_lab, Lk, z);
     FBP_LAUNCH_CHECK();
     return FBP_OK;
 }
@@ -315,7 +313,7 @@ int launch_accept(u32 n, u32 C, u32 L, const float *thr, const u32 *win, const u
 float tc_kappa(u32 C, u32 L, u32 Cg2);
 
 // Context for likelihood entries the tensor-core path left approximate.
-LazyLk lazy_ctx(const Workspace &w, const float *v, const float *T, const float *tss, u32 C, u32 L) {
+LazyLk lazy_ctx(const Workspace &w, const float *v, const float *T, const float *tss, u32 C, u32 L, u32 pass) {
     LazyLk z{};
     if (!w.tc) return z;
     z.apx = w.apx; z.wn = w.wn_s; z.wa = w.wa_s; z.kx = w.kx_s;
@@ -323,6 +321,8 @@ LazyLk lazy_ctx(const Workspace &w, const float *v, const float *T, const float 
     z.v = v; z.T = T; z.C = C; z.L = L;
     z.kappa_b = tc_kappa(C, L, w.tc_Cg2);
     z.refined = &w.cnt->lazy_ref;
+    z.wlb = w.wlb; z.bm = w.bm_s;
+    z.tag = 2u + (pass & 1u);
     return z;
 }
 
@@ -345,7 +345,7 @@ OvArgs ov_args(const Workspace &w, const float *v, u32 n, u32 C, const float *T,
     A.items_evaluated = &cnt->ov_items;
     A.pool_total = &cnt->pool_total;
     A.ua = w.ua;
-    A.lazy = lazy_ctx(w, v, T, tss, C, L);
+    A.lazy = lazy_ctx(w, v, T, tss, C, L, 0);   // read only: the tag is not used
     if (w.tc) {                      // H from the tensor cores
         A.km_override = tc_kappa(C, L, w.tc_Cg2);
         A.tabs = w.tc_tabs;
@@ -491,7 +491,7 @@ int tc_likelihood_pass(const Workspace &w, const float *v, u32 n, u32 C, const f
     A.seg_s0 = w.tc_seg_s0; A.seg_base = w.tc_seg_base; A.seg_cnt = w.tc_seg_cnt;
     A.seg_count = w.tc_seg_count; A.seg_overflow = &cnt->tc_overflow; A.seg_cap = w.tc_seg_cap;
     A.err = &cnt->tc_err;
-    A.apx = w.apx; A.wn_s = w.wn_s; A.wa_s = w.wa_s; A.kx_s = w.kx_s;
+    A.apx = w.apx; A.wn_s = w.wn_s; A.wa_s = w.wa_s; A.kx_s = w.kx_s; A.bm_s = w.bm_s; A.wlb = w.wlb;
     const size_t smem = tc_smem_bytes(L, w.tc_Cg2, w.tc_Np);
     FBP_CUDA(cudaMemsetAsync(&cnt->tc_ref, 0, 4, st));
     FBP_CUDA(cudaMemsetAsync(w.tc_seg_count, 0, 4, st));
@@ -642,6 +642,7 @@ int fbp_pursuit_chunk(float *voltage, uint32_t n, uint32_t C, const float *templ
     if (w.tc) {
         timer.begin(FBP_STAGE_LIKELIHOOD);
         FBP_CUDA(cudaMemsetAsync(w.apx, 0, (size_t)K * n, st));
+        FBP_CUDA(cudaMemsetAsync(w.wlb, 0, (size_t)W * 4, st));
         int rc0 = tc_chunk_setup(w, templates, K, C, L, st);
         if (rc0) return rc0;
         S.launches[FBP_STAGE_LIKELIHOOD] += 2;
@@ -680,9 +681,9 @@ int fbp_pursuit_chunk(float *voltage, uint32_t n, uint32_t C, const float *templ
         timer.end(FBP_STAGE_LIKELIHOOD);
         // 2. per-window argmax over all templates (.py:551-562)
         timer.begin(FBP_STAGE_ARGMAX);
-        const LazyLk lz = lazy_ctx(w, voltage, templates, neg_half_ss, C, L);
+        const LazyLk lz = lazy_ctx(w, voltage, templates, neg_half_ss, C, L, passes);
         if ((rc = launch_argmax(n, L, K, w.win, &w.cnt->n_win, W, s, w.Lk, st, lz))) break;
-        S.launches[FBP_STAGE_ARGMAX] += lz.apx ? 2 : 1;
+        S.launches[FBP_STAGE_ARGMAX] += 1;
         timer.end(FBP_STAGE_ARGMAX);
         // 3. candidates = nonzero(overlap_recheck) (.py:565-569), 4. recheck (.py:570-661)
         if (do_overlap_recheck) {
@@ -747,7 +748,7 @@ int fbp_pursuit_chunk(float *voltage, uint32_t n, uint32_t C, const float *templ
         timer.begin(FBP_STAGE_LISTS);
         FBP_CUDA(cudaMemsetAsync(w.ovr, 0, wb, st));
         if ((rc = compact(w.flags_out, W, w.win, &w.cnt->n_win, w.tile_counts, st))) break;
-        k_mark_active<<<grid_for(W, 256), 256, 0, st>>>(w.flags_out, w.active, W);
+        k_mark_active<<<grid_for(W, 256), 256, 0, st>>>(w.flags_out, w.active, W, w.tc ? w.wlb : nullptr);
         FBP_CUDA(cudaMemsetAsync(w.flags, 0, wb, st));
         // 8. keep the spikes (.py:702-710)
         k_append_spikes<<<grid_for(added, 256), 256, 0, st>>>(w.spk_idx, w.spk_lab, w.cnt, spike_idx,

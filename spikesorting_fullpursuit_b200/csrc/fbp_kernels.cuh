@@ -73,9 +73,14 @@ __global__ void k_iota_windows(u32 *__restrict__ win, u8 *__restrict__ active, u
 }
 
 // active[j] = (flags[j] != 0) for the next pass.
-__global__ void k_mark_active(const u8 *__restrict__ flags, u8 *__restrict__ active, u32 W) {
-    for (u32 i = blockIdx.x * blockDim.x + threadIdx.x; i < W; i += gridDim.x * blockDim.x)
+// active = flags != 0; windows about to be recomputed also drop their
+// lower bound (wlb, tensor-core path; may be NULL).
+__global__ void k_mark_active(const u8 *__restrict__ flags, u8 *__restrict__ active, u32 W,
+                              float *__restrict__ wlb) {
+    for (u32 i = blockIdx.x * blockDim.x + threadIdx.x; i < W; i += gridDim.x * blockDim.x) {
         active[i] = flags[i] != 0;
+        if (wlb && flags[i]) wlb[i] = 0.0f;
+    }
 }
 
 // ---------------------------------------------------------------------------
@@ -173,12 +178,15 @@ k_likelihood_fp32(const float *__restrict__ v, u32 n, u32 C, const float *__rest
 // a decision needs their value (exact values are written back).
 // ---------------------------------------------------------------------------
 // Likelihood entries the tensor-core path stored approximately.  apx[t][s]:
-//   0  the stored value is the reference value, or an approximation that is
-//      certainly <= 0 (only its sign is ever read);
-//   1  approximate and certainly > 0; the interval is approx +- lazy_bound;
-//   2  was 1, the reference value has since been stored.
-// A flag only moves 1 -> 2 inside a kernel (value first), so a reader that
-// sees 1 or 2 may use either version of the value with the interval.
+//   0     the stored value is the reference value, or an approximation that
+//         is certainly <= 0 (only its sign is ever read);
+//   1     approximate and certainly > 0; the interval is approx +- lazy_bound;
+//   2, 3  was 1; the reference value was stored by a kernel of the pass with
+//         that parity (tag = 2 + pass % 2).
+// A kernel stores the value before the tag, so a reader in the SAME kernel
+// that sees its own pass's tag may still read the old approximation: it
+// treats the entry like a 1 (the interval holds both values).  A tag of the
+// other parity was written by an earlier launch and is exact.
 struct LazyLk {
     u8 *apx;                          // [K][n]; NULL: every entry is exact
     const float *wn, *wa;             // [n] window L2 / L1 norms at computation time
@@ -189,6 +197,9 @@ struct LazyLk {
     u32 C, L;
     float kappa_b;
     u64 *refined;                     // count of entries refined on demand (may be NULL)
+    const float *wlb;                 // [W] largest lower bound over each window's entries
+    const float *bm;                  // [n] largest bound of a flagged entry of each sample
+    u32 tag;                          // 2 + pass % 2
 };
 
 // The bound the tensor-core epilogue used for entry (t, s) (same formula).
@@ -215,53 +226,6 @@ __device__ __forceinline__ float lk_exact(const LazyLk &z, const float *Lk, u32 
     return Lk[e];
 }
 
-// Before the window argmax: for each listed window, the largest lower bound
-// over its range [sw-L, ew+L) and the reference value of every approximate
-// entry whose upper bound reaches it.  Afterwards every entry of the range
-// that can hold the maximum is exact, and every other one is certainly below
-// it -- so the argmax reads the reference's maxima.
-__global__ void k_lazy_refine(u32 n, u32 L, u32 K, const u32 *__restrict__ win, const u32 *__restrict__ n_win_dev,
-                              float *__restrict__ Lk, LazyLk z) {
-    const u32 n_win = *n_win_dev;
-    const u32 lane = threadIdx.x & 31;
-    const u32 warps_per_block = blockDim.x >> 5;
-    for (u32 g = blockIdx.x * warps_per_block + (threadIdx.x >> 5); g < n_win;
-         g += gridDim.x * warps_per_block) {
-        const u32 id = win[g];
-        const u32 sw = id * L, ew = (id + 1) * L;
-        const u32 start = (L > sw) ? 0 : sw - L;
-        const u32 stop = (ew + L) > n ? n : ew + L;
-        if (ew >= n - L) continue;                       // the argmax skips it (.cl:380-383)
-        float lb = 0.0f;
-        bool any = false;
-        for (u32 t = 0; t < K; t++)
-            for (u32 s = start + lane; s < stop; s += 32) {
-                const size_t e = (size_t)t * n + s;
-                const float cur = Lk[e];
-                const u8 f = z.apx[e];
-                any |= f != 0;
-                lb = fmaxf(lb, f ? cur - lazy_bound(z, t, s, cur) : cur);
-            }
-        if (!__any_sync(0xffffffffu, any)) continue;
-#pragma unroll
-        for (int o = 16; o > 0; o >>= 1) lb = fmaxf(lb, __shfl_xor_sync(0xffffffffu, lb, o));
-        u32 nref = 0;
-        for (u32 t = 0; t < K; t++)
-            for (u32 s = start + lane; s < stop; s += 32) {
-                const size_t e = (size_t)t * n + s;
-                if (z.apx[e] != 1) continue;
-                const float cur = Lk[e];
-                if (cur + lazy_bound(z, t, s, cur) >= lb) {
-                    Lk[e] = exact_likelihood(z, n, t, s);
-                    __threadfence();
-                    z.apx[e] = 2;
-                    nref++;
-                }
-            }
-        if (z.refined && nref) atomicAdd(z.refined, (u64)nref);
-    }
-}
-
 // Before the residual subtracts this pass's spikes: an approximate entry
 // that reads a changing sample and whose window is not recomputed next pass
 // keeps, in the reference, the value it was computed with; store that value
@@ -286,7 +250,7 @@ __global__ void k_lazy_freeze(u32 n, u32 L, u32 K, const u32 *__restrict__ idx, 
                 if (z.apx[e] != 1) continue;
                 Lk[e] = exact_likelihood(z, n, t, s);
                 __threadfence();
-                z.apx[e] = 2;
+                z.apx[e] = (u8)z.tag;
                 nref++;
             }
         }
@@ -307,10 +271,11 @@ __global__ void k_window_argmax(u32 n, u32 L, u32 K, const u32 *__restrict__ win
                                 u32 *__restrict__ best_lab, float *__restrict__ best_ll,
                                 u8 *__restrict__ flags, u8 *__restrict__ ovr,
                                 u32 *__restrict__ ov_idx, u32 *__restrict__ ov_lab,
-                                const float *__restrict__ Lk, const u8 *__restrict__ apx) {
+                                float *__restrict__ Lk, LazyLk z) {
     const u32 n_win = *n_win_dev;
     const u32 lane = threadIdx.x & 31;
     const u32 warps_per_block = blockDim.x >> 5;
+    const u32 W = (n + L - 1) / L;
     for (u32 g = blockIdx.x * warps_per_block + (threadIdx.x >> 5); g < n_win;
          g += gridDim.x * warps_per_block) {
         const u32 id = win[g];
@@ -318,18 +283,40 @@ __global__ void k_window_argmax(u32 n, u32 L, u32 K, const u32 *__restrict__ win
         const u32 start = (L > sw) ? 0 : sw - L;
         const u32 stop = (ew + L) > n ? n : ew + L;
         if (ew >= n - L) continue;                       // .cl:380-383
+        // Approximate entries (tensor-core path): lb = the largest lower
+        // bound over windows id-1..id+1, which is the range [start, stop).
+        // The maximum is >= lb, and an entry whose upper bound is below lb
+        // cannot hold it, so only entries that reach lb need their
+        // reference value; every other one is read as stored (< lb).
+        float lb = 0.0f;
+        if (z.apx) {
+            lb = z.wlb[id];
+            if (id > 0) lb = fmaxf(lb, z.wlb[id - 1]);
+            if (id + 1 < W) lb = fmaxf(lb, z.wlb[id + 1]);
+        }
+        u32 nref = 0;
         float bl = 0.0f;                                 // .cl:389-393 (template 0 resets)
         u32 blab = best_lab[id], bidx = best_idx[id];
         bool check = false;
         for (u32 t = 0; t < K; t++) {
-            const float *row = Lk + (size_t)t * n;
+            float *row = Lk + (size_t)t * n;
             float lv = -INFINITY;
             u32 li = 0xffffffffu;
             for (u32 s = start + lane; s < stop; s += 32) {
-                const float cur = row[s];
+                float cur = row[s];
+                check |= cur > 0.0f && s >= sw && s < ew;    // a flagged entry is > 0 either way
+                if (z.apx && cur + z.bm[s] >= lb) {
+                    const size_t e = (size_t)t * n + s;
+                    const u32 f = z.apx[e];
+                    if ((f == 1 || f == z.tag) && cur + lazy_bound(z, t, s, cur) >= lb) {
+                        cur = exact_likelihood(z, n, t, s);
+                        row[s] = cur;
+                        __threadfence();
+                        z.apx[e] = (u8)z.tag;
+                        nref++;
+                    }
+                }
                 if (cur > lv) { lv = cur; li = s; }
-                // a flagged entry is certainly positive
-                check |= (cur > 0.0f || (apx && apx[(size_t)t * n + s])) && s >= sw && s < ew;
             }
 #pragma unroll
             for (int o = 16; o > 0; o >>= 1) {
@@ -340,6 +327,11 @@ __global__ void k_window_argmax(u32 n, u32 L, u32 K, const u32 *__restrict__ win
             if (lv > bl) { bl = lv; blab = t; bidx = li; }
         }
         check = __any_sync(0xffffffffu, check);
+        if (z.refined) {
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) nref += __shfl_xor_sync(0xffffffffu, nref, o);
+            if (lane == 0 && nref) atomicAdd(z.refined, (u64)nref);
+        }
         if (lane == 0) {
             if (check) flags[id] = 1;                    // .cl:419-422
             ovr[id] = (bl > 0.0f && bidx >= sw && bidx < ew) ? 1 : 0;   // .cl:423-433

@@ -65,6 +65,8 @@ struct TcArgs {
     u32 *err;                        // non-zero: a bounded wait gave up
     u8 *apx;                         // [K][n] approximate-entry flags
     float *wn_s, *wa_s;              // [n] per-sample window norms
+    float *bm_s;                     // [n] largest bound of a flagged entry of the sample
+    float *wlb;                      // [W] largest lower bound over a window's entries
     signed char *kx_s;               // [n] per-sample fp16 scale exponent
     // overlap-table tiles (MODE 1): rows are the shifts b of a candidate window
     u32 S, nmax, stiles;
@@ -347,6 +349,7 @@ k_lik_tc(TcArgs A) {
         // phase 1: store the values whose sign is certain, mark the others
         u32 wantbits[8] = {0, 0, 0, 0, 0, 0, 0, 0};      // Np <= 256
         u32 nwant = 0;
+        float lomax = 0.0f, bmax = 0.0f;                 // this sample's lower bounds / flagged bounds
         if (in_win) {                                    // interval data of this sample
             A.wn_s[s] = wn;
             A.wa_s[s] = wa;
@@ -376,18 +379,24 @@ k_lik_tc(TcArgs A) {
                                   (ldexpf(A.tabs[t], -kexp) + ldexpf(wa, -je)) * 1.001f;
                 const float E = kappa_b * A.tnorm[t] * wn + sub +
                                 2.384185791015625e-07f * (fabsf(tssv) + fabsf(approx));
+                lomax = fmaxf(lomax, approx - E);
                 if (approx + E <= 0.0f) {            // certainly <= 0: only its sign is read
                     *dst = approx;
                     *fl = 0;
                 } else if (approx - E > 0.0f) {      // certainly > 0: refined when a decision needs it
                     *dst = approx;
                     *fl = 1;
+                    bmax = fmaxf(bmax, E);
                 } else {                             // sign uncertain: refined now
                     wantbits[t >> 5] |= 1u << (t & 31);
                     nwant++;
                     *fl = 0;
                 }
             }
+        }
+        if (in_win) {
+            A.bm_s[s] = bmax;
+            if (lomax > 0.0f) atomicMax(reinterpret_cast<int *>(A.wlb) + s / L, __float_as_int(lomax));
         }
         // phase 2: one contiguous segment of (template, sample) entries per
         // tile, ordered by template so the refinement shares template rows
