@@ -70,7 +70,7 @@ struct Workspace {
     // fast overlap recheck (present when `fast`)
     bool fast;
     u32 slots;
-    float *NT, *sNT, *tnorm, *Q, *H, *vn, *res_lb, *res_hi, *cand_lb;
+    float *NT, *sNT, *tnorm, *Q, *XMr, *XM, *H, *vn, *res_hi, *cand_lb;
     OvConst *oc;
     u8 *cskip, *fallback, *need;
     u32 *k0_count, *k0_cursor, *k0_offset, *k0_active, *n_k0_active, *order;
@@ -158,6 +158,8 @@ Workspace layout(char *base, u32 n, u32 K, u32 L, u32 nmax, bool want_fast, u32 
         w.sNT = (float *)take((size_t)K * S * 4);
         w.tnorm = (float *)take((size_t)K * 4);
         w.Q = (float *)take((size_t)K * K * (2 * L - 1) * (L + 1) * 4);
+        w.XMr = (float *)take((size_t)K * K * (2 * L + 1) * 4);
+        w.XM = (float *)take((size_t)K * K * 4);
         w.H = (float *)take(sl * K * S * 4);
         w.vn = (float *)take(sl * 4);
         w.cskip = (u8 *)take(sl);
@@ -168,7 +170,6 @@ Workspace layout(char *base, u32 n, u32 K, u32 L, u32 nmax, bool want_fast, u32 
         w.k0_active = (u32 *)take((size_t)K * 4);
         w.n_k0_active = (u32 *)take(4);
         w.order = (u32 *)take(sl * 4);
-        w.res_lb = (float *)take(sl * K * 4);
         w.res_hi = (float *)take(sl * K * 4);
         w.need = (u8 *)take(sl * K);
         w.cand_lb = (float *)take(sl * 4);
@@ -332,14 +333,14 @@ OvArgs ov_args(const Workspace &w, const float *v, u32 n, u32 C, const float *T,
     OvArgs A{};
     A.n = n; A.C = C; A.K = K; A.L = L; A.nmax = nmax; A.S = 2 * nmax + 1;
     A.v = v; A.T = T; A.Lk = Lk; A.thr = thr;
-    A.NT = w.NT; A.sNT = w.sNT; A.tnorm = w.tnorm; A.Q = w.Q; A.oc = w.oc;
+    A.NT = w.NT; A.sNT = w.sNT; A.tnorm = w.tnorm; A.Q = w.Q; A.XMr = w.XMr; A.XM = w.XM; A.oc = w.oc;
     A.cand = cand; A.n_cand = n_cand;
     A.best_idx = s.best_idx; A.best_lab = s.best_lab; A.ov_idx = s.ov_idx; A.ov_lab = s.ov_lab;
     A.best_ll = s.best_ll; A.ovr = s.overlap_recheck;
     A.H = w.H; A.vn = w.vn; A.cskip = w.cskip;
     A.k0_count = w.k0_count; A.k0_cursor = w.k0_cursor; A.k0_offset = w.k0_offset;
     A.k0_active = w.k0_active; A.n_k0_active = w.n_k0_active; A.order = w.order;
-    A.res_lb = w.res_lb; A.res_hi = w.res_hi; A.need = w.need; A.cand_lb = w.cand_lb;
+    A.res_hi = w.res_hi; A.need = w.need; A.cand_lb = w.cand_lb;
     A.pool_slot = w.pool_slot; A.pool_item = w.pool_item; A.pool_cap = w.pool_cap;
     A.best_key = w.best_key; A.fallback = w.fallback;
     A.items_evaluated = &cnt->ov_items;
@@ -362,6 +363,7 @@ int ov_chunk_setup(const Workspace &w, const float *T, u32 K, u32 C, u32 L, u32 
     k_ov_chunk_tables<<<grid_for((u64)K * S, 256), 256, 0, st>>>(T, K, C, L, nmax, w.NT, w.sNT, w.tnorm, w.oc);
     const u64 rows = (u64)K * K * (2 * L - 1);
     k_ov_q_table<<<grid_for(rows, 128, 16), 128, 0, st>>>(T, K, C, L, w.Q);
+    k_ov_xm<<<(int)std::min<u64>((u64)K * K, (u64)sm_count() * 16), 256, 0, st>>>(w.Q, K, L, nmax, w.oc, w.XMr, w.XM);
     FBP_LAUNCH_CHECK();
     return FBP_OK;
 }
@@ -408,6 +410,10 @@ int ov_fast_pass(const Workspace &w, const OvArgs &A, Counters *cnt, cudaStream_
     const size_t sweep_smem = sweep_smem_bytes(S, A.L, sweep_threads);
     if (sweep_smem > 48 * 1024)
         FBP_CUDA(cudaFuncSetAttribute(k_ov_sweep, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sweep_smem));
+    const size_t seed_smem = seed_smem_bytes(S);
+    if (seed_smem > 48 * 1024)
+        FBP_CUDA(cudaFuncSetAttribute(k_ov_seed, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)seed_smem));
+    k_ov_seed<<<grid_for((u64)slots * 32, kSeedThreads), kSeedThreads, seed_smem, st>>>(A);
     k_ov_sweep<<<sm_count(), sweep_threads, sweep_smem, st>>>(A, 0);
     k_ov_merge<<<grid_for((u64)slots * 32, 256), 256, 0, st>>>(A);
     k_ov_sweep<<<sm_count(), sweep_threads, sweep_smem, st>>>(A, 1);
@@ -421,7 +427,7 @@ int ov_fast_pass(const Workspace &w, const OvArgs &A, Counters *cnt, cudaStream_
     fbp_window_state s{A.best_idx, A.best_lab, A.best_ll, A.ov_idx, A.ov_lab, nullptr, A.ovr};
     rc = launch_overlap(A.v, A.n, A.C, A.T, A.K, A.L, w.fb_list, &cnt->fb_count, slots, s, A.Lk, A.nmax, A.thr,
                         A.items_evaluated, st, A.lazy);
-    *launches = 16;
+    *launches = 17;
     return rc;
 }
 
@@ -652,7 +658,7 @@ int fbp_pursuit_chunk(float *voltage, uint32_t n, uint32_t C, const float *templ
         timer.begin(FBP_STAGE_OVERLAP);
         int rc0 = ov_chunk_setup(w, templates, K, C, L, nmax, st);
         if (rc0) return rc0;
-        S.launches[FBP_STAGE_OVERLAP] += 2;
+        S.launches[FBP_STAGE_OVERLAP] += 3;
         timer.end(FBP_STAGE_OVERLAP);
     }
 

@@ -47,6 +47,8 @@ struct OvArgs {
     float *Lk;
     const float *NT, *sNT, *tnorm;   // [K][S], [K][S], [K]
     const float *Q;                  // [K][K][2L-1][L+1]
+    const float *XMr;                // [K][K][2L+1] upper bound of -X + kx|X| per lag r = a - b
+    const float *XM;                 // [K][K]       its largest value over the lags
     const OvConst *oc;
     const u32 *cand, *n_cand;
     u32 *best_idx, *best_lab, *ov_idx, *ov_lab;
@@ -57,10 +59,9 @@ struct OvArgs {
     u8 *cskip;                       // [slot]
     u32 *k0_count, *k0_cursor, *k0_offset, *k0_active, *n_k0_active;
     u32 *order;                      // [slot]
-    float *res_lb;                   // [slot][K]  largest lower bound of (candidate, t)
-    float *res_hi;                   // [slot][K]  largest upper bound of (candidate, t)
+    float *res_hi;                   // [slot][K]  largest upper bound of the items (candidate, t) enumerated
     u8 *need;                        // [slot][K]  (candidate, t) can hold a contender
-    float *cand_lb;                  // [slot]     largest lower bound of the candidate
+    float *cand_lb;                  // [slot]     largest lower bound of an item (atomic max, >= 0)
     u32 *pool_total;                 // appended entries this pass
     u32 pool_cap;
     u32 *pool_slot;                  // [pool_cap]
@@ -196,6 +197,7 @@ __global__ void k_ov_prep(OvArgs A) {
             A.vn[g] = (float)(sqrt(e) * (1.0 + 1e-6));
             if (A.ua) A.ua[g] = (float)(e1 * (1.0 + 1e-6));
             A.best_key[g] = 0ull;
+            A.cand_lb[g] = 0.0f;
             if (!skip) atomicAdd(&A.k0_count[lab], 1u);
         }
     }
@@ -305,13 +307,13 @@ k_ov_tables(OvArgs A) {
 
 constexpr int kSweepMaxThreads = 1024;
 // Per-warp scratch of the sweep: ga_lo, ga_hi, hb_lo, hb_hi (S floats each),
-// the a and b row lists (S u16 each), and the bitmask of rows a with
-// L[k0][afix] not <= 0 (S bits).
+// the a and b row lists (S u16 each), and the bitmasks of rows a with
+// L[k0][afix] not <= 0 and rows b with L[t][ashift] not <= 0 (S bits each).
 __host__ __device__ inline size_t sweep_warp_bytes(u32 S) {
-    return align_up((size_t)20 * S + (size_t)(S + 31) / 32 * 4, 16);
+    return align_up((size_t)20 * S + (size_t)(S + 31) / 32 * 8, 16);
 }
 __host__ __device__ inline size_t sweep_head_bytes(u32 S, u32 L) {
-    return align_up((size_t)(2 * L - 1) * (L + 1) * 4 + (size_t)4 * S * 4 + 16, 16);
+    return align_up((size_t)(2 * L - 1) * (L + 1) * 4 + (size_t)(2 * L + 1) * 4 + (size_t)4 * S * 4 + 16, 16);
 }
 __host__ __device__ inline size_t sweep_smem_bytes(u32 S, u32 L, u32 threads) {
     return sweep_head_bytes(S, L) + (size_t)(threads / 32) * sweep_warp_bytes(S);
@@ -320,11 +322,13 @@ __host__ __device__ inline size_t tables_smem_bytes(u32 S, u32 K, u32 L) {
     const size_t Lp = (L + 7) & ~7u, Sp = (size_t)(S + 7) / 8 * 8, Kp = (size_t)(K + 7) / 8 * 8;
     return (Sp + Lp + 8 + Lp * Kp) * 4;
 }
+constexpr int kSeedThreads = 256;
+__host__ __device__ inline size_t seed_smem_bytes(u32 S) {
+    return (size_t)(kSeedThreads / 32) * align_up((size_t)4 * S + (size_t)(S + 31) / 32 * 4, 16);
+}
 
 // Interval of one item from its row-invariant and moving parts.
-__device__ __forceinline__ void ov_item_bounds(const float *__restrict__ q, u32 L, int a_minus_nmax, int r,
-                                               float loA, float hiA, float loB, float hiB, float kx,
-                                               float &lo, float &hi) {
+__device__ __forceinline__ float ov_x(const float *__restrict__ q, u32 L, int a_minus_nmax, int r) {
     float X = 0.0f;
     if (r > -(int)L && r < (int)L) {
         const int lo_m = max(max(0, -r), -a_minus_nmax);
@@ -334,19 +338,208 @@ __device__ __forceinline__ void ov_item_bounds(const float *__restrict__ q, u32 
             X = qr[hi_m] - qr[lo_m];
         }
     }
+    return X;
+}
+__device__ __forceinline__ void ov_item_bounds(const float *__restrict__ q, u32 L, int a_minus_nmax, int r,
+                                               float loA, float hiA, float loB, float hiB, float kx,
+                                               float &lo, float &hi) {
+    const float X = ov_x(q, L, a_minus_nmax, r);
     const float ex = kx * fabsf(X);
     hi = hiA + hiB - X + ex;
     lo = loA + loB - X - ex;
 }
 
-// Sweep over the items of one (label k0, template t) task.  Q[k0][t] is
-// staged once; warps take the candidates of label k0 one at a time from a
-// shared counter and enumerate the items that survive the reference's skip
-// rules (.cl:534-576): rows a with L[k0][afix] not <= 0 (every in-bounds b
-// within L of a), then rows b with L[t][ashift] not <= 0 (every other
-// in-bounds a within L of b).
-//  mode 0: per (candidate, t) the largest lower bound and the largest upper
-//          bound of its items (res_lb, res_hi).
+// Interval of a row term: G(a) = H[k0][a] (extra = 0) or H[t][b] (extra =
+// the cross term's own rounding), with the fp16 subnormal terms of
+// tensor-core tables (sub0 / sub1 scaled by the tile's voltage exponent).
+__device__ __forceinline__ void ov_row_interval(const OvArgs &A, u32 g, u32 x, float Hv, float nt, float snt,
+                                                float vn, float krm, float extra, float sub0, float sub1,
+                                                float &lo, float &hi) {
+    float sx = 0.0f;
+    if (A.kexp_tile) sx = sub0 * ldexpf(1.0f, -A.kexp_tile[(size_t)g * A.stiles + x / 128]) + sub1;
+    const float e = krm * (snt * vn + nt) + 4.0f * kUnitRoundoff * fabsf(Hv) + extra + sx;
+    lo = Hv - e;
+    hi = Hv + e;
+}
+
+// Per-candidate constants of the row intervals.
+struct OvCand {
+    u32 id, k0, bidx, xlo, xhi_ex;
+    float lbest, vn, subA0, subA1;
+};
+__device__ __forceinline__ OvCand ov_cand(const OvArgs &A, u32 g) {
+    OvCand c;
+    c.id = A.cand[g];
+    c.k0 = A.best_lab[c.id];
+    c.bidx = A.best_idx[c.id];
+    c.lbest = A.best_ll[c.id];
+    c.vn = A.vn[g];
+    c.xlo = c.bidx >= A.nmax ? 0u : A.nmax - c.bidx;          // in-bounds shifts (.cl:534-541)
+    c.xhi_ex = A.n - A.L + A.nmax - c.bidx;                    // first out-of-bounds shift
+    c.subA0 = c.subA1 = 0.0f;
+    if (A.kexp_tile) {
+        c.subA1 = 2.98023224e-08f * 1.001f * ldexpf(A.ua[g], -A.texp[c.k0]);
+        c.subA0 = 2.98023224e-08f * 1.001f * A.tabs[c.k0];
+    }
+    return c;
+}
+__device__ __forceinline__ void ov_sub_b(const OvArgs &A, u32 g, u32 t, float &subB0, float &subB1) {
+    subB0 = subB1 = 0.0f;
+    if (A.kexp_tile) {
+        subB1 = 2.98023224e-08f * 1.001f * ldexpf(A.ua[g], -A.texp[t]);
+        subB0 = 2.98023224e-08f * 1.001f * A.tabs[t];
+    }
+}
+__device__ __forceinline__ float ov_kx(const OvArgs &A) { return 2.0f * A.oc->kappa_ref + 4.0f * kUnitRoundoff; }
+__device__ __forceinline__ float ov_krm(const OvArgs &A) {
+    return A.oc->kappa_ref + (A.km_override > 0.0f ? A.km_override : A.oc->kappa_mine);
+}
+// Slack for the float roundings of the pruning sums (2^-18 relative).
+constexpr float kPruneSlack = 3.814697265625e-06f;
+
+// Per chunk: XMr[k0][t][r + L] = an upper bound of -X + kx|X| over every
+// shift a of an item with lag r = a - b (X = 0 where the clipped templates
+// do not overlap), and XM[k0][t] = its maximum over r.  Then
+//     hi(a, b) <= hiA(a) + hiB(b) + XMr[a - b]
+// bounds every item's interval without its cross term.
+__global__ void __launch_bounds__(256)
+k_ov_xm(const float *__restrict__ Q, u32 K, u32 L, u32 nmax, const OvConst *__restrict__ oc,
+        float *__restrict__ XMr, float *__restrict__ XM) {
+    const u32 R = 2 * L - 1, S = 2 * nmax + 1, NR = 2 * L + 1;
+    const float kx = 2.0f * oc->kappa_ref + 4.0f * kUnitRoundoff;
+    __shared__ float red[8];
+    for (u32 pair = blockIdx.x; pair < K * K; pair += gridDim.x) {
+        const float *q = Q + (size_t)pair * R * (L + 1);
+        float pm = -INFINITY;
+        for (u32 ri = threadIdx.x; ri < NR; ri += blockDim.x) {
+            const int r = (int)ri - (int)L;
+            float m = -INFINITY;
+            for (u32 a = 0; a < S; a++) {
+                const float X = ov_x(q, L, (int)a - (int)nmax, r);
+                m = fmaxf(m, -X + kx * fabsf(X));
+            }
+            m += kPruneSlack * fabsf(m);
+            XMr[(size_t)pair * NR + ri] = m;
+            pm = fmaxf(pm, m);
+        }
+        pm = warp_max_f(pm);
+        if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = pm;
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            float v = red[0];
+            for (u32 w = 1; w < blockDim.x / 32; w++) v = fmaxf(v, red[w]);
+            XM[pair] = v;
+        }
+        __syncthreads();
+    }
+}
+
+// Warp argmax: larger value, then lower index.
+__device__ __forceinline__ void warp_argmax(float &v, u32 &i) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        const float ov = __shfl_xor_sync(0xffffffffu, v, o);
+        const u32 oi = __shfl_xor_sync(0xffffffffu, i, o);
+        if (ov > v || (ov == v && oi < i)) { v = ov; i = oi; }
+    }
+}
+
+// Seed of each candidate's best lower bound: per template t, the items
+// (a1, b1), (a1, b2), (a3, b1) with a1 / b1 the rows of largest lower bound,
+// b2 the best row b within L of a1 and a3 the best row a within L of b1.
+// Any item's lower bound is a valid lower bound of the best item, and these
+// are close to the largest one, so the sweeps can prune against it from the
+// start.  One warp per candidate.
+__global__ void __launch_bounds__(kSeedThreads)
+k_ov_seed(OvArgs A) {
+    extern __shared__ float seed_sm[];
+    const u32 nc = *A.n_cand;
+    const u32 lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const u32 S = A.S, K = A.K, L = A.L, nmax = A.nmax, n = A.n, R = 2 * L - 1;
+    float *la = (float *)((char *)seed_sm + (size_t)warp * align_up((size_t)4 * S + (size_t)(S + 31) / 32 * 4, 16));
+    u32 *fbits = (u32 *)(la + S);
+    const float krm = ov_krm(A), kx = ov_kx(A);
+    for (u32 g = blockIdx.x * (kSeedThreads / 32) + warp; g < nc; g += gridDim.x * (kSeedThreads / 32)) {
+        if (A.cskip[g]) continue;
+        const OvCand c = ov_cand(A, g);
+        const float *Hg = A.H + (size_t)g * K * S;
+        // rows a: lower bounds (in-bounds only) and the L[k0][afix] > 0 bits
+        float va = -INFINITY;
+        u32 a1 = 0;
+        for (u32 x0 = 0; x0 < S; x0 += 32) {
+            const u32 x = x0 + lane;
+            bool ap = false;
+            if (x < S) {
+                float lo = -INFINITY, hi;
+                if (x >= c.xlo && x < c.xhi_ex) {
+                    ov_row_interval(A, g, x, Hg[(size_t)c.k0 * S + x], A.NT[(size_t)c.k0 * S + x],
+                                    A.sNT[(size_t)c.k0 * S + x], c.vn, krm, 0.0f, c.subA0, c.subA1, lo, hi);
+                    ap = !(A.Lk[(size_t)c.k0 * n + c.bidx + x - nmax] <= 0.0f);
+                    if (lo > va) { va = lo; a1 = x; }
+                }
+                la[x] = lo;
+            }
+            const u32 m = __ballot_sync(0xffffffffu, ap);
+            if (lane == 0) fbits[x0 / 32] = m;
+        }
+        warp_argmax(va, a1);
+        __syncwarp();
+        if (va == -INFINITY) continue;                  // no in-bounds row
+        const float eq = 4.0f * kUnitRoundoff * A.tnorm[c.k0];
+        float seed = 0.0f;
+        for (u32 t = 0; t < K; t++) {
+            float subB0, subB1;
+            ov_sub_b(A, g, t, subB0, subB1);
+            const float eqt = eq * A.tnorm[t];
+            float v1 = -INFINITY, v2 = -INFINITY;
+            u32 b1 = 0, b2 = 0;
+            for (u32 x = c.xlo + lane; x < min(S, c.xhi_ex); x += 32) {
+                float lo, hi;
+                ov_row_interval(A, g, x, Hg[(size_t)t * S + x], A.NT[(size_t)t * S + x], A.sNT[(size_t)t * S + x],
+                                c.vn, krm, eqt, subB0, subB1, lo, hi);
+                if (lo > v1) { v1 = lo; b1 = x; }
+                if ((x > a1 ? x - a1 : a1 - x) <= L && lo > v2) { v2 = lo; b2 = x; }
+            }
+            warp_argmax(v1, b1);
+            warp_argmax(v2, b2);
+            float v3 = -INFINITY;
+            u32 a3 = 0;
+            for (u32 x = c.xlo + lane; x < min(S, c.xhi_ex); x += 32)
+                if ((x > b1 ? x - b1 : b1 - x) <= L && la[x] > v3) { v3 = la[x]; a3 = x; }
+            warp_argmax(v3, a3);
+            if (lane < 3) {
+                const u32 a = lane == 2 ? a3 : a1, b = lane == 0 ? b1 : (lane == 1 ? b2 : b1);
+                const float lb_b = lane == 1 ? v2 : v1;
+                const float lb_a = lane == 2 ? v3 : va;
+                const bool geo = (a > b ? a - b : b - a) <= L && lb_a > -INFINITY && lb_b > -INFINITY;
+                if (geo) {
+                    const bool fp = (fbits[a >> 5] >> (a & 31)) & 1u;
+                    const bool sp = !(A.Lk[(size_t)t * n + c.bidx + b - nmax] <= 0.0f);
+                    if (fp || sp) {                      // .cl:572-576
+                        const float *q = A.Q + ((size_t)c.k0 * K + t) * R * (L + 1);
+                        const float X = ov_x(q, L, (int)a - (int)nmax, (int)a - (int)b);
+                        seed = fmaxf(seed, lb_a + lb_b - X - kx * fabsf(X));
+                    }
+                }
+            }
+        }
+        seed = warp_max_f(seed);
+        if (lane == 0 && seed > 0.0f) atomicMax(reinterpret_cast<int *>(A.cand_lb) + g, __float_as_int(seed));
+    }
+}
+
+// Sweep over the items of one (label k0, template t) task.  Q[k0][t] and the
+// lag bounds XMr[k0][t] are staged once; warps take the candidates of label
+// k0 one at a time from a shared counter.  Per candidate, with
+// TH = max(best lower bound so far, current best likelihood):
+//   - the whole (candidate, t) is skipped when max hiA + max hiB + XM < TH;
+//   - rows a / b whose bound with the other side's maximum is below TH drop;
+//   - of the remaining pairs, those that pass the reference's skip rules
+//     (.cl:534-576) and hiA + hiB + XMr[a-b] >= TH get their exact interval.
+// An item that is never enumerated has hi < TH, so it can neither be the
+// best item (whose value is >= every lower bound) nor beat the current best.
+//  mode 0: raise the candidate's best lower bound; record the largest upper
+//          bound of the enumerated items (res_hi).
 //  mode 1: for the (candidate, t) pairs flagged by k_ov_merge, append every
 //          item whose upper bound reaches the candidate's best lower bound
 //          and exceeds its current best likelihood to the pool.
@@ -354,10 +547,11 @@ __global__ void __launch_bounds__(kSweepMaxThreads)
 k_ov_sweep(OvArgs A, int mode) {
     extern __shared__ float sm[];
     const u32 S = A.S, K = A.K, L = A.L, nmax = A.nmax, n = A.n;
-    const u32 R = 2 * L - 1;
+    const u32 R = 2 * L - 1, NR = 2 * L + 1;
     const u32 warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     float *q = sm;                                  // [R][L+1]
-    float *nt0 = q + (size_t)R * (L + 1);           // NT[k0][S], sNT[k0][S], NT[t][S], sNT[t][S]
+    float *xmr = q + (size_t)R * (L + 1);           // [2L+1]
+    float *nt0 = xmr + NR;                          // NT[k0][S], sNT[k0][S], NT[t][S], sNT[t][S]
     float *snt0 = nt0 + S, *ntt = snt0 + S, *sntt = ntt + S;
     u32 *next = (u32 *)(sntt + S);                  // candidate counter of the task
     char *wbase = (char *)sm + sweep_head_bytes(S, L);
@@ -366,11 +560,9 @@ k_ov_sweep(OvArgs A, int mode) {
     u16 *alist = (u16 *)(hb_hi + S);
     u16 *blist = alist + S;
     u32 *abits = (u32 *)((char *)ga_lo + (size_t)20 * S);
+    u32 *bbits = abits + (S + 31) / 32;
     const u32 ntasks = *A.n_k0_active * K;
-    const float kr = A.oc->kappa_ref, km = A.km_override > 0.0f ? A.km_override : A.oc->kappa_mine;
-    const float kx = 2.0f * kr + 4.0f * kUnitRoundoff;
-    const bool tc_tables = A.kexp_tile != nullptr;
-    // in-bounds shifts x: x + bidx >= nmax and x + bidx < n - L + nmax
+    const float krm = ov_krm(A), kx = ov_kx(A);
     for (u32 task = blockIdx.x; task < ntasks; task += gridDim.x) {
         const u32 k0 = A.k0_active[task / K], t = task % K;
         const u32 gcount = A.k0_count[k0], goff = A.k0_offset[k0];
@@ -381,8 +573,10 @@ k_ov_sweep(OvArgs A, int mode) {
             if (!__syncthreads_or(any)) continue;
         }
         __syncthreads();
-        const float *qg = A.Q + ((size_t)k0 * K + t) * R * (L + 1);
+        const size_t pair = (size_t)k0 * K + t;
+        const float *qg = A.Q + pair * R * (L + 1);
         for (u32 e = threadIdx.x; e < R * (L + 1); e += blockDim.x) q[e] = qg[e];
+        for (u32 e = threadIdx.x; e < NR; e += blockDim.x) xmr[e] = A.XMr[pair * NR + e];
         for (u32 b = threadIdx.x; b < S; b += blockDim.x) {
             nt0[b] = A.NT[(size_t)k0 * S + b];
             snt0[b] = A.sNT[(size_t)k0 * S + b];
@@ -391,7 +585,8 @@ k_ov_sweep(OvArgs A, int mode) {
         }
         if (threadIdx.x == 0) *next = 0;
         __syncthreads();
-        const float eq = 4.0f * kUnitRoundoff * A.tnorm[k0] * A.tnorm[t];
+        const float XM = A.XM[pair];
+        const float eqt = 4.0f * kUnitRoundoff * A.tnorm[k0] * A.tnorm[t];
         u32 evaluated = 0;
         for (;;) {
             u32 ci = 0;
@@ -401,127 +596,100 @@ k_ov_sweep(OvArgs A, int mode) {
             const u32 g = A.order[goff + ci];
             const size_t slot = (size_t)g * K + t;
             if (mode == 1 && !A.need[slot]) continue;
-            const u32 id = A.cand[g];
-            const u32 bidx = A.best_idx[id];
-            const float lbest = A.best_ll[id];
-            const float vn = A.vn[g];
-            const float LB = mode == 1 ? A.cand_lb[g] : 0.0f;
+            const OvCand c = ov_cand(A, g);
+            const float LB = *(volatile const float *)(A.cand_lb + g);   // final in mode 1
+            const float TH = fmaxf(LB, c.lbest);
             const float *Hg = A.H + (size_t)g * K * S;
-            // fp16 subnormal terms of tensor-core tables: 2^-25 (|t|_1 / s_window + |window|_1 / s_t)
-            float subA0 = 0.0f, subA1 = 0.0f, subB1 = 0.0f, subB0 = 0.0f;
-            if (tc_tables) {
-                const float ua = A.ua[g];
-                subA1 = 2.98023224e-08f * 1.001f * ldexpf(ua, -A.texp[k0]);
-                subB1 = 2.98023224e-08f * 1.001f * ldexpf(ua, -A.texp[t]);
-                subA0 = 2.98023224e-08f * 1.001f * A.tabs[k0];
-                subB0 = 2.98023224e-08f * 1.001f * A.tabs[t];
-            }
-            // in-bounds shift range [xlo, xhi] (.cl:534-541)
-            const u32 xlo = bidx >= nmax ? 0u : nmax - bidx;
-            const u32 xhi_ex = n - L + nmax - bidx;       // first out-of-bounds shift
-            // interval rows and item rows
-            u32 na = 0, nb = 0;
+            float subB0, subB1;
+            ov_sub_b(A, g, t, subB0, subB1);
+            // row intervals, the skip-rule bits, and the largest upper bounds
+            float mA = -INFINITY, mB = -INFINITY, mabs = 0.0f;
             for (u32 x0 = 0; x0 < S; x0 += 32) {
                 const u32 x = x0 + lane;
                 bool ap = false, bp = false;
                 if (x < S) {
-                    float sa = 0.0f, sb = 0.0f;
-                    if (tc_tables) {
-                        const float w2 = ldexpf(1.0f, -A.kexp_tile[(size_t)g * A.stiles + x / 128]);
-                        sa = subA0 * w2 + subA1;
-                        sb = subB0 * w2 + subB1;
-                    }
-                    const float G = Hg[(size_t)k0 * S + x];
-                    const float ea = (kr + km) * (snt0[x] * vn + nt0[x]) + 4.0f * kUnitRoundoff * fabsf(G) + sa;
-                    ga_lo[x] = G - ea;
-                    ga_hi[x] = G + ea;
-                    const float Hv = Hg[(size_t)t * S + x];
-                    const float eb = (kr + km) * (sntt[x] * vn + ntt[x]) + 4.0f * kUnitRoundoff * fabsf(Hv) + eq + sb;
-                    hb_lo[x] = Hv - eb;
-                    hb_hi[x] = Hv + eb;
-                    if (x >= xlo && x < xhi_ex) {
-                        const u32 pos = bidx + x - nmax;
+                    float lo, hi;
+                    ov_row_interval(A, g, x, Hg[(size_t)k0 * S + x], nt0[x], snt0[x], c.vn, krm, 0.0f, c.subA0,
+                                    c.subA1, lo, hi);
+                    ga_lo[x] = lo;
+                    ga_hi[x] = hi;
+                    float lo2, hi2;
+                    ov_row_interval(A, g, x, Hg[(size_t)t * S + x], ntt[x], sntt[x], c.vn, krm, eqt, subB0, subB1,
+                                    lo2, hi2);
+                    hb_lo[x] = lo2;
+                    hb_hi[x] = hi2;
+                    if (x >= c.xlo && x < c.xhi_ex) {
+                        const u32 pos = c.bidx + x - nmax;
                         ap = !(A.Lk[(size_t)k0 * n + pos] <= 0.0f);
                         bp = !(A.Lk[(size_t)t * n + pos] <= 0.0f);
+                        mA = fmaxf(mA, hi);
+                        mB = fmaxf(mB, hi2);
+                        mabs = fmaxf(mabs, fmaxf(fabsf(hi), fabsf(hi2)));
                     }
                 }
                 const u32 ma = __ballot_sync(0xffffffffu, ap), mb = __ballot_sync(0xffffffffu, bp);
-                if (ap) alist[na + __popc(ma & ((1u << lane) - 1u))] = (u16)x;
-                if (bp) blist[nb + __popc(mb & ((1u << lane) - 1u))] = (u16)x;
-                if (lane == 0 && x0 / 32 < (S + 31) / 32) abits[x0 / 32] = ma;
-                na += __popc(ma);
-                nb += __popc(mb);
-            }
-            __syncwarp();
-            float lbmax = -INFINITY, himax = -INFINITY;
-            // phase 0: rows a in alist, b moves
-            for (u32 ri = 0; ri < na; ri++) {
-                const u32 a = alist[ri];
-                const float loA = ga_lo[a], hiA = ga_hi[a];
-                const int am = (int)a - (int)nmax;
-                const u32 b_lo = max(a > L ? a - L : 0u, xlo);
-                const u32 b_hi = min(min(S - 1, a + L), xhi_ex - 1);
-                for (u32 b0 = b_lo; b0 <= b_hi; b0 += 32) {
-                    const u32 b = b0 + lane;
-                    const bool valid = b <= b_hi;
-                    float lo = -INFINITY, hi = -INFINITY;
-                    if (valid) {
-                        ov_item_bounds(q, L, am, (int)a - (int)b, loA, hiA, hb_lo[b], hb_hi[b], kx, lo, hi);
-                        evaluated++;
-                    }
-                    if (mode == 0) {
-                        lbmax = fmaxf(lbmax, lo);
-                        himax = fmaxf(himax, hi);
-                    } else {
-                        const bool keep = valid && hi >= LB && hi > lbest;
-                        const u32 mk = __ballot_sync(0xffffffffu, keep);
-                        if (mk) {
-                            u32 base = 0;
-                            if (lane == 0) base = atomicAdd(A.pool_total, (u32)__popc(mk));
-                            base = __shfl_sync(0xffffffffu, base, 0);
-                            if (keep) {
-                                const u32 p = base + __popc(mk & ((1u << lane) - 1u));
-                                if (p < A.pool_cap) {
-                                    A.pool_slot[p] = g;
-                                    A.pool_item[p] = t + K * (a + S * b);
-                                } else {
-                                    A.fallback[g] = 1;
-                                }
-                            }
-                        }
-                    }
+                if (lane == 0) {
+                    abits[x0 / 32] = ma;
+                    bbits[x0 / 32] = mb;
                 }
             }
-            // phase 1: rows b in blist, a moves (rows a of phase 0 excluded)
-            for (u32 ri = 0; ri < nb; ri++) {
-                const u32 b = blist[ri];
-                const float loB = hb_lo[b], hiB = hb_hi[b];
-                const u32 a_lo = max(b > L ? b - L : 0u, xlo);
-                const u32 a_hi = min(min(S - 1, b + L), xhi_ex - 1);
-                for (u32 a0 = a_lo; a0 <= a_hi; a0 += 32) {
-                    const u32 a = a0 + lane;
-                    const bool valid = a <= a_hi && !((abits[a >> 5] >> (a & 31)) & 1u);
+            mA = warp_max_f(mA);
+            mB = warp_max_f(mB);
+            mabs = warp_max_f(mabs);
+            const float slack = kPruneSlack * (2.0f * mabs + fabsf(TH) + fabsf(XM));
+            float lbmax = -INFINITY, himax = -INFINITY;
+            if (mA + mB + XM + slack >= TH) {
+                // rows that can reach TH with the other side's best
+                u32 na = 0, nb = 0;
+                for (u32 x0 = 0; x0 < S; x0 += 32) {
+                    const u32 x = x0 + lane;
+                    const bool inb = x < S && x >= c.xlo && x < c.xhi_ex;
+                    const bool ka = inb && ga_hi[x] + mB + XM + slack >= TH;
+                    const bool kb = inb && hb_hi[x] + mA + XM + slack >= TH;
+                    const u32 ma = __ballot_sync(0xffffffffu, ka), mb = __ballot_sync(0xffffffffu, kb);
+                    if (ka) alist[na + __popc(ma & ((1u << lane) - 1u))] = (u16)x;
+                    if (kb) blist[nb + __popc(mb & ((1u << lane) - 1u))] = (u16)x;
+                    na += __popc(ma);
+                    nb += __popc(mb);
+                }
+                __syncwarp();
+                const u32 P = na * nb;
+                for (u32 p0 = 0; p0 < P; p0 += 32) {
+                    const u32 p = p0 + lane;
+                    bool valid = false;
+                    u32 a = 0, b = 0;
+                    if (p < P) {
+                        const u32 ai = p / nb;
+                        a = alist[ai];
+                        b = blist[p - ai * nb];
+                        valid = (a > b ? a - b : b - a) <= L &&                                    // .cl:543-556
+                                (((abits[a >> 5] >> (a & 31)) | (bbits[b >> 5] >> (b & 31))) & 1u);  // .cl:572-576
+                        if (valid) {
+                            const float xr = xmr[(int)a - (int)b + (int)L];
+                            valid = ga_hi[a] + hb_hi[b] + xr + slack + kPruneSlack * fabsf(xr) >= TH;
+                        }
+                    }
                     float lo = -INFINITY, hi = -INFINITY;
                     if (valid) {
-                        ov_item_bounds(q, L, (int)a - (int)nmax, (int)a - (int)b, ga_lo[a], ga_hi[a], loB, hiB, kx,
-                                       lo, hi);
+                        ov_item_bounds(q, L, (int)a - (int)nmax, (int)a - (int)b, ga_lo[a], ga_hi[a], hb_lo[b],
+                                       hb_hi[b], kx, lo, hi);
                         evaluated++;
                     }
                     if (mode == 0) {
                         lbmax = fmaxf(lbmax, lo);
                         himax = fmaxf(himax, hi);
                     } else {
-                        const bool keep = valid && hi >= LB && hi > lbest;
+                        const bool keep = valid && hi >= LB && hi > c.lbest;
                         const u32 mk = __ballot_sync(0xffffffffu, keep);
                         if (mk) {
                             u32 base = 0;
                             if (lane == 0) base = atomicAdd(A.pool_total, (u32)__popc(mk));
                             base = __shfl_sync(0xffffffffu, base, 0);
                             if (keep) {
-                                const u32 p = base + __popc(mk & ((1u << lane) - 1u));
-                                if (p < A.pool_cap) {
-                                    A.pool_slot[p] = g;
-                                    A.pool_item[p] = t + K * (a + S * b);
+                                const u32 pp = base + __popc(mk & ((1u << lane) - 1u));
+                                if (pp < A.pool_cap) {
+                                    A.pool_slot[pp] = g;
+                                    A.pool_item[pp] = t + K * (a + S * b);
                                 } else {
                                     A.fallback[g] = 1;
                                 }
@@ -534,8 +702,8 @@ k_ov_sweep(OvArgs A, int mode) {
                 lbmax = warp_max_f(lbmax);
                 himax = warp_max_f(himax);
                 if (lane == 0) {
-                    A.res_lb[slot] = lbmax;
                     A.res_hi[slot] = himax;
+                    if (lbmax > 0.0f) atomicMax(reinterpret_cast<int *>(A.cand_lb) + g, __float_as_int(lbmax));
                 }
             }
             __syncwarp();
@@ -548,8 +716,8 @@ k_ov_sweep(OvArgs A, int mode) {
     }
 }
 
-// One warp per candidate slot: the best lower bound over all templates, the
-// templates whose items can reach it, and a reset of the contender pool.
+// One warp per candidate slot: the templates whose enumerated items can
+// reach the candidate's best lower bound, and a reset of the contender pool.
 __global__ void k_ov_merge(OvArgs A) {
     const u32 nc = *A.n_cand;
     const u32 lane = threadIdx.x & 31, K = A.K;
@@ -557,14 +725,11 @@ __global__ void k_ov_merge(OvArgs A) {
          g += gridDim.x * (blockDim.x >> 5)) {
         if (A.cskip[g]) continue;
         const float lbest = A.best_ll[A.cand[g]];
-        float lb = -INFINITY;
-        for (u32 t = lane; t < K; t += 32) lb = fmaxf(lb, A.res_lb[(size_t)g * K + t]);
-        lb = warp_max_f(lb);
+        const float lb = A.cand_lb[g];
         for (u32 t = lane; t < K; t += 32) {
             const float h = A.res_hi[(size_t)g * K + t];
             A.need[(size_t)g * K + t] = (h >= lb && h > lbest) ? 1 : 0;
         }
-        if (lane == 0) A.cand_lb[g] = lb;
     }
 }
 
