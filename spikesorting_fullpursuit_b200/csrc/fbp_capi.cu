@@ -363,7 +363,11 @@ int ov_chunk_setup(const Workspace &w, const float *T, u32 K, u32 C, u32 L, u32 
     k_ov_chunk_tables<<<grid_for((u64)K * S, 256), 256, 0, st>>>(T, K, C, L, nmax, w.NT, w.sNT, w.tnorm, w.oc);
     const u64 rows = (u64)K * K * (2 * L - 1);
     k_ov_q_table<<<grid_for(rows, 128, 16), 128, 0, st>>>(T, K, C, L, w.Q);
-    k_ov_xm<<<(int)std::min<u64>((u64)K * K, (u64)sm_count() * 16), 256, 0, st>>>(w.Q, K, L, nmax, w.oc, w.XMr, w.XM);
+    const size_t xm_smem = (size_t)(2 * L - 1) * (L + 1) * 4;
+    if (xm_smem > 48 * 1024)
+        FBP_CUDA(cudaFuncSetAttribute(k_ov_xm, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)xm_smem));
+    k_ov_xm<<<(int)std::min<u64>((u64)K * K, (u64)sm_count() * 2), 256, xm_smem, st>>>(w.Q, K, L, nmax, w.oc, w.XMr,
+                                                                                        w.XM);
     FBP_LAUNCH_CHECK();
     return FBP_OK;
 }

@@ -405,17 +405,21 @@ constexpr float kPruneSlack = 3.814697265625e-06f;
 __global__ void __launch_bounds__(256)
 k_ov_xm(const float *__restrict__ Q, u32 K, u32 L, u32 nmax, const OvConst *__restrict__ oc,
         float *__restrict__ XMr, float *__restrict__ XM) {
+    extern __shared__ float xm_sm[];                 // Q[k0][t]: [2L-1][L+1]
     const u32 R = 2 * L - 1, S = 2 * nmax + 1, NR = 2 * L + 1;
     const float kx = 2.0f * oc->kappa_ref + 4.0f * kUnitRoundoff;
     __shared__ float red[8];
     for (u32 pair = blockIdx.x; pair < K * K; pair += gridDim.x) {
-        const float *q = Q + (size_t)pair * R * (L + 1);
+        const float *qg = Q + (size_t)pair * R * (L + 1);
+        __syncthreads();
+        for (u32 e = threadIdx.x; e < R * (L + 1); e += blockDim.x) xm_sm[e] = qg[e];
+        __syncthreads();
         float pm = -INFINITY;
         for (u32 ri = threadIdx.x; ri < NR; ri += blockDim.x) {
             const int r = (int)ri - (int)L;
             float m = -INFINITY;
             for (u32 a = 0; a < S; a++) {
-                const float X = ov_x(q, L, (int)a - (int)nmax, r);
+                const float X = ov_x(xm_sm, L, (int)a - (int)nmax, r);
                 m = fmaxf(m, -X + kx * fabsf(X));
             }
             m += kPruneSlack * fabsf(m);
@@ -430,7 +434,6 @@ k_ov_xm(const float *__restrict__ Q, u32 K, u32 L, u32 nmax, const OvConst *__re
             for (u32 w = 1; w < blockDim.x / 32; w++) v = fmaxf(v, red[w]);
             XM[pair] = v;
         }
-        __syncthreads();
     }
 }
 
