@@ -70,10 +70,10 @@ struct Workspace {
     // fast overlap recheck (present when `fast`)
     bool fast;
     u32 slots;
-    float *NT, *sNT, *tnorm, *Q, *XMr, *XM, *H, *vn, *res_hi, *cand_lb;
+    float *NT, *sNT, *tnorm, *Q, *XMr, *XM, *H, *vn, *cand_lb, *ga_lo, *ga_hi, *ga_max, *ga_abs, *pool_hi;
+    u32 *ga_bits;
     OvConst *oc;
     u8 *cskip, *fallback, *need;
-    u32 *k0_count, *k0_cursor, *k0_offset, *k0_active, *n_k0_active, *order;
     u32 *pool_slot, *pool_item, *fb_slots, *fb_list;
     u64 *best_key;
     u32 pool_cap;
@@ -99,7 +99,7 @@ struct Workspace {
 bool fast_overlap_fits(u32 K, u32 L, u32 nmax) {
     const u64 S = 2 * (u64)nmax + 1;
     if (S > 4 * (u64)L + 1 || S > 65535) return false;
-    if (sweep_smem_bytes((u32)S, L, 256) > 227 * 1024) return false;
+    if (xm_smem_bytes(L) > 227 * 1024 || scan_smem_bytes((u32)S) > 227 * 1024) return false;
     if (tables_smem_bytes((u32)S, K, L) > 227 * 1024) return false;
     return true;
 }
@@ -164,19 +164,17 @@ Workspace layout(char *base, u32 n, u32 K, u32 L, u32 nmax, bool want_fast, u32 
         w.vn = (float *)take(sl * 4);
         w.cskip = (u8 *)take(sl);
         w.fallback = (u8 *)take(align_up(sl + FBP_WINDOW_PAD, kCompactTile));
-        w.k0_count = (u32 *)take((size_t)K * 4);
-        w.k0_cursor = (u32 *)take((size_t)K * 4);
-        w.k0_offset = (u32 *)take((size_t)K * 4);
-        w.k0_active = (u32 *)take((size_t)K * 4);
-        w.n_k0_active = (u32 *)take(4);
-        w.order = (u32 *)take(sl * 4);
-        w.res_hi = (float *)take(sl * K * 4);
-        w.need = (u8 *)take(sl * K);
+        w.ga_lo = (float *)take(sl * S * 4);
+        w.ga_hi = (float *)take(sl * S * 4);
+        w.ga_bits = (u32 *)take(sl * ((S + 31) / 32) * 4);
+        w.ga_max = (float *)take(sl * 4);
+        w.ga_abs = (float *)take(sl * 4);
         w.cand_lb = (float *)take(sl * 4);
         w.best_key = (u64 *)take(sl * 8);
         w.pool_cap = (u32)std::min<u64>(0x7fffffffull, std::max<u64>(1u << 22, (u64)sl * 128));
         w.pool_slot = (u32 *)take((size_t)w.pool_cap * 4);
         w.pool_item = (u32 *)take((size_t)w.pool_cap * 4);
+        w.pool_hi = (float *)take((size_t)w.pool_cap * 4);
         w.fb_slots = (u32 *)take(sl * 4);
         w.fb_list = (u32 *)take(sl * 4);
         w.ua = (float *)take(sl * 4);
@@ -338,10 +336,10 @@ OvArgs ov_args(const Workspace &w, const float *v, u32 n, u32 C, const float *T,
     A.best_idx = s.best_idx; A.best_lab = s.best_lab; A.ov_idx = s.ov_idx; A.ov_lab = s.ov_lab;
     A.best_ll = s.best_ll; A.ovr = s.overlap_recheck;
     A.H = w.H; A.vn = w.vn; A.cskip = w.cskip;
-    A.k0_count = w.k0_count; A.k0_cursor = w.k0_cursor; A.k0_offset = w.k0_offset;
-    A.k0_active = w.k0_active; A.n_k0_active = w.n_k0_active; A.order = w.order;
-    A.res_hi = w.res_hi; A.need = w.need; A.cand_lb = w.cand_lb;
-    A.pool_slot = w.pool_slot; A.pool_item = w.pool_item; A.pool_cap = w.pool_cap;
+    A.cand_lb = w.cand_lb;
+    A.ga_lo = w.ga_lo; A.ga_hi = w.ga_hi; A.ga_bits = w.ga_bits; A.ga_max = w.ga_max; A.ga_abs = w.ga_abs;
+    A.pool_slot = w.pool_slot; A.pool_item = w.pool_item; A.pool_hi = w.pool_hi; A.pool_cap = w.pool_cap;
+    A.refined = &cnt->ov_ref;
     A.best_key = w.best_key; A.fallback = w.fallback;
     A.items_evaluated = &cnt->ov_items;
     A.pool_total = &cnt->pool_total;
@@ -377,12 +375,10 @@ int ov_chunk_setup(const Workspace &w, const float *T, u32 K, u32 C, u32 L, u32 
 int ov_fast_pass(const Workspace &w, const OvArgs &A, Counters *cnt, cudaStream_t st, int *launches) {
     const u32 slots = w.slots;
     const u32 S = A.S;
-    FBP_CUDA(cudaMemsetAsync(w.k0_count, 0, (size_t)A.K * 4, st));
     FBP_CUDA(cudaMemsetAsync(w.fallback, 0, align_up((size_t)slots + FBP_WINDOW_PAD, kCompactTile), st));
     FBP_CUDA(cudaMemsetAsync(&cnt->pool_total, 0, 4, st));
+    FBP_CUDA(cudaMemsetAsync(&cnt->ov_ref, 0, 4, st));
     k_ov_prep<<<grid_for((u64)slots * 32, 256), 256, 0, st>>>(A);
-    k_ov_group<<<1, 32, 0, st>>>(A);
-    k_ov_scatter<<<grid_for(slots, 256), 256, 0, st>>>(A);
     FBP_LAUNCH_CHECK();
     if (w.tc) {
         TcArgs T{};
@@ -407,20 +403,14 @@ int ov_fast_pass(const Workspace &w, const OvArgs &A, Counters *cnt, cudaStream_
         k_ov_tables<<<grid_for((u64)slots * kTabThreads, kTabThreads, 4), kTabThreads, smem, st>>>(A);
         FBP_LAUNCH_CHECK();
     }
-    // as many warps per block as the shared memory allows (the task's
-    // prefix table is shared by all of them)
-    u32 sweep_threads = kSweepMaxThreads;
-    while (sweep_threads > 256 && sweep_smem_bytes(S, A.L, sweep_threads) > 227 * 1024) sweep_threads /= 2;
-    const size_t sweep_smem = sweep_smem_bytes(S, A.L, sweep_threads);
-    if (sweep_smem > 48 * 1024)
-        FBP_CUDA(cudaFuncSetAttribute(k_ov_sweep, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sweep_smem));
     const size_t seed_smem = seed_smem_bytes(S);
     if (seed_smem > 48 * 1024)
         FBP_CUDA(cudaFuncSetAttribute(k_ov_seed, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)seed_smem));
     k_ov_seed<<<grid_for((u64)slots * 32, kSeedThreads), kSeedThreads, seed_smem, st>>>(A);
-    k_ov_sweep<<<sm_count(), sweep_threads, sweep_smem, st>>>(A, 0);
-    k_ov_merge<<<grid_for((u64)slots * 32, 256), 256, 0, st>>>(A);
-    k_ov_sweep<<<sm_count(), sweep_threads, sweep_smem, st>>>(A, 1);
+    const size_t scan_smem = scan_smem_bytes(S);
+    if (scan_smem > 48 * 1024)
+        FBP_CUDA(cudaFuncSetAttribute(k_ov_scan, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)scan_smem));
+    k_ov_scan<<<grid_for((u64)slots * A.K * 32, kScanThreads, 8), kScanThreads, scan_smem, st>>>(A);
     k_ov_refine<<<(int)sm_count() * 16, 128, 0, st>>>(A);
     k_ov_finalize<<<grid_for(slots, 256), 256, 0, st>>>(A);
     FBP_LAUNCH_CHECK();
@@ -431,7 +421,7 @@ int ov_fast_pass(const Workspace &w, const OvArgs &A, Counters *cnt, cudaStream_
     fbp_window_state s{A.best_idx, A.best_lab, A.best_ll, A.ov_idx, A.ov_lab, nullptr, A.ovr};
     rc = launch_overlap(A.v, A.n, A.C, A.T, A.K, A.L, w.fb_list, &cnt->fb_count, slots, s, A.Lk, A.nmax, A.thr,
                         A.items_evaluated, st, A.lazy);
-    *launches = 17;
+    *launches = 14;
     return rc;
 }
 
@@ -747,7 +737,7 @@ int fbp_pursuit_chunk(float *voltage, uint32_t n, uint32_t C, const float *templ
             S.work[FBP_STAGE_CHECK] += h_counts[1];
             S.candidates += h_counts[1];
             if (w.fast) {
-                S.refined_items += std::min(h_counts[6], w.pool_cap);
+                S.refined_items += ((const Counters *)h_counts)->ov_ref;
                 S.fallback_candidates += h_counts[7];
             }
         }

@@ -35,7 +35,8 @@ struct Counters {
     u32 tc_overflow;  // refinement list overflowed: the exact kernel redoes the pass
     u32 pad0;
     u64 lazy_ref;     // approximate likelihood entries refined on demand (whole chunk)
-    u32 pad[16];
+    u32 ov_ref;       // overlap contenders evaluated exactly this pass
+    u32 pad[15];
 };
 static_assert(sizeof(Counters) == 128, "Counters is one 128-byte line");
 

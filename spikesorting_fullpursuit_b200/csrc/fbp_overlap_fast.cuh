@@ -57,15 +57,16 @@ struct OvArgs {
     float *H;                        // [slot][K][S]
     float *vn;                       // [slot]
     u8 *cskip;                       // [slot]
-    u32 *k0_count, *k0_cursor, *k0_offset, *k0_active, *n_k0_active;
-    u32 *order;                      // [slot]
-    float *res_hi;                   // [slot][K]  largest upper bound of the items (candidate, t) enumerated
-    u8 *need;                        // [slot][K]  (candidate, t) can hold a contender
     float *cand_lb;                  // [slot]     largest lower bound of an item (atomic max, >= 0)
+    float *ga_lo, *ga_hi;            // [slot][S]  interval of G(a) = H[k0][a]
+    u32 *ga_bits;                    // [slot][ceil(S/32)] rows a with L[k0][afix] not <= 0
+    float *ga_max, *ga_abs;          // [slot]     largest in-bounds hi(a), largest |hi(a)|
     u32 *pool_total;                 // appended entries this pass
     u32 pool_cap;
     u32 *pool_slot;                  // [pool_cap]
     u32 *pool_item;                  // [pool_cap]
+    float *pool_hi;                  // [pool_cap] upper bound of the contender
+    u32 *refined;                    // contenders evaluated exactly this pass
     u64 *best_key;                   // [slot] packed (value, ~item) of the best refined contender
     u8 *fallback;                    // [slot]
     u64 *items_evaluated;
@@ -198,31 +199,7 @@ __global__ void k_ov_prep(OvArgs A) {
             if (A.ua) A.ua[g] = (float)(e1 * (1.0 + 1e-6));
             A.best_key[g] = 0ull;
             A.cand_lb[g] = 0.0f;
-            if (!skip) atomicAdd(&A.k0_count[lab], 1u);
         }
-    }
-}
-
-// One block: offsets of the label groups and the list of labels present.
-__global__ void k_ov_group(OvArgs A) {
-    if (threadIdx.x == 0) {
-        u32 off = 0, na = 0;
-        for (u32 k = 0; k < A.K; k++) {
-            A.k0_offset[k] = off;
-            A.k0_cursor[k] = 0;
-            off += A.k0_count[k];
-            if (A.k0_count[k]) A.k0_active[na++] = k;
-        }
-        *A.n_k0_active = na;
-    }
-}
-
-__global__ void k_ov_scatter(OvArgs A) {
-    const u32 nc = *A.n_cand;
-    for (u32 g = blockIdx.x * blockDim.x + threadIdx.x; g < nc; g += gridDim.x * blockDim.x) {
-        if (A.cskip[g]) continue;
-        const u32 lab = A.best_lab[A.cand[g]];
-        A.order[A.k0_offset[lab] + atomicAdd(&A.k0_cursor[lab], 1u)] = g;
     }
 }
 
@@ -305,19 +282,18 @@ k_ov_tables(OvArgs A) {
     }
 }
 
-constexpr int kSweepMaxThreads = 1024;
-// Per-warp scratch of the sweep: ga_lo, ga_hi, hb_lo, hb_hi (S floats each),
+constexpr int kScanThreads = 256;
+// Per-warp scratch of the scan: ga_lo, ga_hi, hb_lo, hb_hi (S floats each),
 // the a and b row lists (S u16 each), and the bitmasks of rows a with
 // L[k0][afix] not <= 0 and rows b with L[t][ashift] not <= 0 (S bits each).
 __host__ __device__ inline size_t sweep_warp_bytes(u32 S) {
     return align_up((size_t)20 * S + (size_t)(S + 31) / 32 * 8, 16);
 }
-__host__ __device__ inline size_t sweep_head_bytes(u32 S, u32 L) {
-    return align_up((size_t)(2 * L - 1) * (L + 1) * 4 + (size_t)(2 * L + 1) * 4 + (size_t)4 * S * 4 + 16, 16);
+__host__ __device__ inline size_t scan_smem_bytes(u32 S) {
+    return (size_t)(kScanThreads / 32) * sweep_warp_bytes(S);
 }
-__host__ __device__ inline size_t sweep_smem_bytes(u32 S, u32 L, u32 threads) {
-    return sweep_head_bytes(S, L) + (size_t)(threads / 32) * sweep_warp_bytes(S);
-}
+// k_ov_xm stages one template pair's prefix table.
+__host__ __device__ inline size_t xm_smem_bytes(u32 L) { return (size_t)(2 * L - 1) * (L + 1) * 4; }
 __host__ __device__ inline size_t tables_smem_bytes(u32 S, u32 K, u32 L) {
     const size_t Lp = (L + 7) & ~7u, Sp = (size_t)(S + 7) / 8 * 8, Kp = (size_t)(K + 7) / 8 * 8;
     return (Sp + Lp + 8 + Lp * Kp) * 4;
@@ -466,26 +442,42 @@ k_ov_seed(OvArgs A) {
         if (A.cskip[g]) continue;
         const OvCand c = ov_cand(A, g);
         const float *Hg = A.H + (size_t)g * K * S;
-        // rows a: lower bounds (in-bounds only) and the L[k0][afix] > 0 bits
-        float va = -INFINITY;
+        // rows a: intervals (kept for the sweep), the L[k0][afix] > 0 bits,
+        // the row of largest lower bound
+        float va = -INFINITY, mA = -INFINITY, mabs = 0.0f;
         u32 a1 = 0;
         for (u32 x0 = 0; x0 < S; x0 += 32) {
             const u32 x = x0 + lane;
             bool ap = false;
             if (x < S) {
-                float lo = -INFINITY, hi;
+                float lo, hi;
+                ov_row_interval(A, g, x, Hg[(size_t)c.k0 * S + x], A.NT[(size_t)c.k0 * S + x],
+                                A.sNT[(size_t)c.k0 * S + x], c.vn, krm, 0.0f, c.subA0, c.subA1, lo, hi);
+                A.ga_lo[(size_t)g * S + x] = lo;
+                A.ga_hi[(size_t)g * S + x] = hi;
                 if (x >= c.xlo && x < c.xhi_ex) {
-                    ov_row_interval(A, g, x, Hg[(size_t)c.k0 * S + x], A.NT[(size_t)c.k0 * S + x],
-                                    A.sNT[(size_t)c.k0 * S + x], c.vn, krm, 0.0f, c.subA0, c.subA1, lo, hi);
                     ap = !(A.Lk[(size_t)c.k0 * n + c.bidx + x - nmax] <= 0.0f);
                     if (lo > va) { va = lo; a1 = x; }
+                    mA = fmaxf(mA, hi);
+                    mabs = fmaxf(mabs, fabsf(hi));
+                } else {
+                    lo = -INFINITY;
                 }
                 la[x] = lo;
             }
             const u32 m = __ballot_sync(0xffffffffu, ap);
-            if (lane == 0) fbits[x0 / 32] = m;
+            if (lane == 0) {
+                fbits[x0 / 32] = m;
+                A.ga_bits[(size_t)g * ((S + 31) / 32) + x0 / 32] = m;
+            }
         }
         warp_argmax(va, a1);
+        mA = warp_max_f(mA);
+        mabs = warp_max_f(mabs);
+        if (lane == 0) {
+            A.ga_max[g] = mA;
+            A.ga_abs[g] = mabs;
+        }
         __syncwarp();
         if (va == -INFINITY) continue;                  // no in-bounds row
         const float eq = 4.0f * kUnitRoundoff * A.tnorm[c.k0];
@@ -531,208 +523,143 @@ k_ov_seed(OvArgs A) {
     }
 }
 
-// Sweep over the items of one (label k0, template t) task.  Q[k0][t] and the
-// lag bounds XMr[k0][t] are staged once; warps take the candidates of label
-// k0 one at a time from a shared counter.  Per candidate, with
-// TH = max(best lower bound so far, current best likelihood):
-//   - the whole (candidate, t) is skipped when max hiA + max hiB + XM < TH;
+// One warp per (candidate, template t): every item (a, b, t) the reference
+// evaluates (.cl:534-576) either gets its interval here or is shown to have
+// hi < TH, TH = max(best lower bound so far, current best likelihood):
+//   - the whole pair is skipped when max hiA + max hiB + XM < TH;
 //   - rows a / b whose bound with the other side's maximum is below TH drop;
-//   - of the remaining pairs, those that pass the reference's skip rules
-//     (.cl:534-576) and hiA + hiB + XMr[a-b] >= TH get their exact interval.
-// An item that is never enumerated has hi < TH, so it can neither be the
-// best item (whose value is >= every lower bound) nor beat the current best.
-//  mode 0: raise the candidate's best lower bound; record the largest upper
-//          bound of the enumerated items (res_hi).
-//  mode 1: for the (candidate, t) pairs flagged by k_ov_merge, append every
-//          item whose upper bound reaches the candidate's best lower bound
-//          and exceeds its current best likelihood to the pool.
-__global__ void __launch_bounds__(kSweepMaxThreads)
-k_ov_sweep(OvArgs A, int mode) {
+//   - of the remaining pairs, those that pass the skip rules and
+//     hiA + hiB + XMr[a-b] >= TH get their interval from the prefix table.
+// An item that is never enumerated can neither be the best item (whose value
+// is >= every lower bound) nor beat the current best.  Items with
+// hi >= TH and hi > current best go to the contender pool with their hi;
+// their lower bounds raise the candidate's best lower bound.
+__global__ void __launch_bounds__(kScanThreads)
+k_ov_scan(OvArgs A) {
     extern __shared__ float sm[];
     const u32 S = A.S, K = A.K, L = A.L, nmax = A.nmax, n = A.n;
-    const u32 R = 2 * L - 1, NR = 2 * L + 1;
+    const u32 R = 2 * L - 1, NR = 2 * L + 1, NB = (S + 31) / 32;
     const u32 warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    float *q = sm;                                  // [R][L+1]
-    float *xmr = q + (size_t)R * (L + 1);           // [2L+1]
-    float *nt0 = xmr + NR;                          // NT[k0][S], sNT[k0][S], NT[t][S], sNT[t][S]
-    float *snt0 = nt0 + S, *ntt = snt0 + S, *sntt = ntt + S;
-    u32 *next = (u32 *)(sntt + S);                  // candidate counter of the task
-    char *wbase = (char *)sm + sweep_head_bytes(S, L);
-    float *ga_lo = (float *)(wbase + (size_t)warp * sweep_warp_bytes(S));
+    float *ga_lo = (float *)((char *)sm + (size_t)warp * sweep_warp_bytes(S));
     float *ga_hi = ga_lo + S, *hb_lo = ga_hi + S, *hb_hi = hb_lo + S;
     u16 *alist = (u16 *)(hb_hi + S);
     u16 *blist = alist + S;
     u32 *abits = (u32 *)((char *)ga_lo + (size_t)20 * S);
-    u32 *bbits = abits + (S + 31) / 32;
-    const u32 ntasks = *A.n_k0_active * K;
-    const float krm = ov_krm(A), kx = ov_kx(A);
-    for (u32 task = blockIdx.x; task < ntasks; task += gridDim.x) {
-        const u32 k0 = A.k0_active[task / K], t = task % K;
-        const u32 gcount = A.k0_count[k0], goff = A.k0_offset[k0];
-        if (mode == 1) {
-            bool any = false;
-            for (u32 ci = threadIdx.x; ci < gcount && !any; ci += blockDim.x)
-                any = A.need[(size_t)A.order[goff + ci] * K + t] != 0;
-            if (!__syncthreads_or(any)) continue;
-        }
-        __syncthreads();
-        const size_t pair = (size_t)k0 * K + t;
-        const float *qg = A.Q + pair * R * (L + 1);
-        for (u32 e = threadIdx.x; e < R * (L + 1); e += blockDim.x) q[e] = qg[e];
-        for (u32 e = threadIdx.x; e < NR; e += blockDim.x) xmr[e] = A.XMr[pair * NR + e];
-        for (u32 b = threadIdx.x; b < S; b += blockDim.x) {
-            nt0[b] = A.NT[(size_t)k0 * S + b];
-            snt0[b] = A.sNT[(size_t)k0 * S + b];
-            ntt[b] = A.NT[(size_t)t * S + b];
-            sntt[b] = A.sNT[(size_t)t * S + b];
-        }
-        if (threadIdx.x == 0) *next = 0;
-        __syncthreads();
-        const float XM = A.XM[pair];
-        const float eqt = 4.0f * kUnitRoundoff * A.tnorm[k0] * A.tnorm[t];
-        u32 evaluated = 0;
-        for (;;) {
-            u32 ci = 0;
-            if (lane == 0) ci = atomicAdd(next, 1u);
-            ci = __shfl_sync(0xffffffffu, ci, 0);
-            if (ci >= gcount) break;
-            const u32 g = A.order[goff + ci];
-            const size_t slot = (size_t)g * K + t;
-            if (mode == 1 && !A.need[slot]) continue;
-            const OvCand c = ov_cand(A, g);
-            const float LB = *(volatile const float *)(A.cand_lb + g);   // final in mode 1
-            const float TH = fmaxf(LB, c.lbest);
-            const float *Hg = A.H + (size_t)g * K * S;
-            float subB0, subB1;
-            ov_sub_b(A, g, t, subB0, subB1);
-            // row intervals, the skip-rule bits, and the largest upper bounds
-            float mA = -INFINITY, mB = -INFINITY, mabs = 0.0f;
-            for (u32 x0 = 0; x0 < S; x0 += 32) {
-                const u32 x = x0 + lane;
-                bool ap = false, bp = false;
-                if (x < S) {
-                    float lo, hi;
-                    ov_row_interval(A, g, x, Hg[(size_t)k0 * S + x], nt0[x], snt0[x], c.vn, krm, 0.0f, c.subA0,
-                                    c.subA1, lo, hi);
-                    ga_lo[x] = lo;
-                    ga_hi[x] = hi;
-                    float lo2, hi2;
-                    ov_row_interval(A, g, x, Hg[(size_t)t * S + x], ntt[x], sntt[x], c.vn, krm, eqt, subB0, subB1,
-                                    lo2, hi2);
-                    hb_lo[x] = lo2;
-                    hb_hi[x] = hi2;
-                    if (x >= c.xlo && x < c.xhi_ex) {
-                        const u32 pos = c.bidx + x - nmax;
-                        ap = !(A.Lk[(size_t)k0 * n + pos] <= 0.0f);
-                        bp = !(A.Lk[(size_t)t * n + pos] <= 0.0f);
-                        mA = fmaxf(mA, hi);
-                        mB = fmaxf(mB, hi2);
-                        mabs = fmaxf(mabs, fmaxf(fabsf(hi), fabsf(hi2)));
-                    }
-                }
-                const u32 ma = __ballot_sync(0xffffffffu, ap), mb = __ballot_sync(0xffffffffu, bp);
-                if (lane == 0) {
-                    abits[x0 / 32] = ma;
-                    bbits[x0 / 32] = mb;
-                }
-            }
-            mA = warp_max_f(mA);
-            mB = warp_max_f(mB);
-            mabs = warp_max_f(mabs);
-            const float slack = kPruneSlack * (2.0f * mabs + fabsf(TH) + fabsf(XM));
-            float lbmax = -INFINITY, himax = -INFINITY;
-            if (mA + mB + XM + slack >= TH) {
-                // rows that can reach TH with the other side's best
-                u32 na = 0, nb = 0;
-                for (u32 x0 = 0; x0 < S; x0 += 32) {
-                    const u32 x = x0 + lane;
-                    const bool inb = x < S && x >= c.xlo && x < c.xhi_ex;
-                    const bool ka = inb && ga_hi[x] + mB + XM + slack >= TH;
-                    const bool kb = inb && hb_hi[x] + mA + XM + slack >= TH;
-                    const u32 ma = __ballot_sync(0xffffffffu, ka), mb = __ballot_sync(0xffffffffu, kb);
-                    if (ka) alist[na + __popc(ma & ((1u << lane) - 1u))] = (u16)x;
-                    if (kb) blist[nb + __popc(mb & ((1u << lane) - 1u))] = (u16)x;
-                    na += __popc(ma);
-                    nb += __popc(mb);
-                }
-                __syncwarp();
-                const u32 P = na * nb;
-                for (u32 p0 = 0; p0 < P; p0 += 32) {
-                    const u32 p = p0 + lane;
-                    bool valid = false;
-                    u32 a = 0, b = 0;
-                    if (p < P) {
-                        const u32 ai = p / nb;
-                        a = alist[ai];
-                        b = blist[p - ai * nb];
-                        valid = (a > b ? a - b : b - a) <= L &&                                    // .cl:543-556
-                                (((abits[a >> 5] >> (a & 31)) | (bbits[b >> 5] >> (b & 31))) & 1u);  // .cl:572-576
-                        if (valid) {
-                            const float xr = xmr[(int)a - (int)b + (int)L];
-                            valid = ga_hi[a] + hb_hi[b] + xr + slack + kPruneSlack * fabsf(xr) >= TH;
-                        }
-                    }
-                    float lo = -INFINITY, hi = -INFINITY;
-                    if (valid) {
-                        ov_item_bounds(q, L, (int)a - (int)nmax, (int)a - (int)b, ga_lo[a], ga_hi[a], hb_lo[b],
-                                       hb_hi[b], kx, lo, hi);
-                        evaluated++;
-                    }
-                    if (mode == 0) {
-                        lbmax = fmaxf(lbmax, lo);
-                        himax = fmaxf(himax, hi);
-                    } else {
-                        const bool keep = valid && hi >= LB && hi > c.lbest;
-                        const u32 mk = __ballot_sync(0xffffffffu, keep);
-                        if (mk) {
-                            u32 base = 0;
-                            if (lane == 0) base = atomicAdd(A.pool_total, (u32)__popc(mk));
-                            base = __shfl_sync(0xffffffffu, base, 0);
-                            if (keep) {
-                                const u32 pp = base + __popc(mk & ((1u << lane) - 1u));
-                                if (pp < A.pool_cap) {
-                                    A.pool_slot[pp] = g;
-                                    A.pool_item[pp] = t + K * (a + S * b);
-                                } else {
-                                    A.fallback[g] = 1;
-                                }
-                            }
-                        }
-                    }
-                }
-            }
-            if (mode == 0) {
-                lbmax = warp_max_f(lbmax);
-                himax = warp_max_f(himax);
-                if (lane == 0) {
-                    A.res_hi[slot] = himax;
-                    if (lbmax > 0.0f) atomicMax(reinterpret_cast<int *>(A.cand_lb) + g, __float_as_int(lbmax));
-                }
-            }
-            __syncwarp();
-        }
-        if (mode == 0 && A.items_evaluated) {
-#pragma unroll
-            for (int o = 16; o > 0; o >>= 1) evaluated += __shfl_xor_sync(0xffffffffu, evaluated, o);
-            if (lane == 0 && evaluated) atomicAdd(A.items_evaluated, (u64)evaluated);
-        }
-    }
-}
-
-// One warp per candidate slot: the templates whose enumerated items can
-// reach the candidate's best lower bound, and a reset of the contender pool.
-__global__ void k_ov_merge(OvArgs A) {
+    u32 *bbits = abits + NB;
     const u32 nc = *A.n_cand;
-    const u32 lane = threadIdx.x & 31, K = A.K;
-    for (u32 g = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); g < nc;
-         g += gridDim.x * (blockDim.x >> 5)) {
+    const u64 total = (u64)nc * K;
+    const u64 nwarps = (u64)gridDim.x * (blockDim.x >> 5);
+    const float krm = ov_krm(A), kx = ov_kx(A);
+    u32 evaluated = 0;
+    for (u64 e = (u64)blockIdx.x * (blockDim.x >> 5) + warp; e < total; e += nwarps) {
+        const u32 g = (u32)(e / K), t = (u32)(e % K);
         if (A.cskip[g]) continue;
-        const float lbest = A.best_ll[A.cand[g]];
-        const float lb = A.cand_lb[g];
-        for (u32 t = lane; t < K; t += 32) {
-            const float h = A.res_hi[(size_t)g * K + t];
-            A.need[(size_t)g * K + t] = (h >= lb && h > lbest) ? 1 : 0;
+        const float mA = A.ga_max[g];
+        if (mA == -INFINITY) continue;                  // no in-bounds row
+        const OvCand c = ov_cand(A, g);
+        const float LB = *(volatile const float *)(A.cand_lb + g);
+        const float TH = fmaxf(LB, c.lbest);
+        const size_t pair = (size_t)c.k0 * K + t;
+        const float XM = A.XM[pair];
+        const float *Hg = A.H + ((size_t)g * K + t) * S;
+        float subB0, subB1;
+        ov_sub_b(A, g, t, subB0, subB1);
+        const float eqt = 4.0f * kUnitRoundoff * A.tnorm[c.k0] * A.tnorm[t];
+        // rows b: intervals and the L[t][ashift] > 0 bits; rows a: copied
+        float mB = -INFINITY, mabs = A.ga_abs[g];
+        for (u32 x0 = 0; x0 < S; x0 += 32) {
+            const u32 x = x0 + lane;
+            bool bp = false;
+            if (x < S) {
+                ga_lo[x] = A.ga_lo[(size_t)g * S + x];
+                ga_hi[x] = A.ga_hi[(size_t)g * S + x];
+                float lo, hi;
+                ov_row_interval(A, g, x, Hg[x], A.NT[(size_t)t * S + x], A.sNT[(size_t)t * S + x], c.vn, krm, eqt,
+                                subB0, subB1, lo, hi);
+                hb_lo[x] = lo;
+                hb_hi[x] = hi;
+                if (x >= c.xlo && x < c.xhi_ex) {
+                    bp = !(A.Lk[(size_t)t * n + c.bidx + x - nmax] <= 0.0f);
+                    mB = fmaxf(mB, hi);
+                    mabs = fmaxf(mabs, fabsf(hi));
+                }
+            }
+            const u32 mb = __ballot_sync(0xffffffffu, bp);
+            if (lane == 0) {
+                bbits[x0 / 32] = mb;
+                abits[x0 / 32] = A.ga_bits[(size_t)g * NB + x0 / 32];
+            }
         }
+        mB = warp_max_f(mB);
+        mabs = warp_max_f(mabs);
+        const float slack = kPruneSlack * (2.0f * mabs + fabsf(TH) + fabsf(XM));
+        if (!(mA + mB + XM + slack >= TH)) continue;
+        // rows that can reach TH with the other side's best
+        u32 na = 0, nb = 0;
+        for (u32 x0 = 0; x0 < S; x0 += 32) {
+            const u32 x = x0 + lane;
+            const bool inb = x < S && x >= c.xlo && x < c.xhi_ex;
+            const bool ka = inb && ga_hi[x] + mB + XM + slack >= TH;
+            const bool kb = inb && hb_hi[x] + mA + XM + slack >= TH;
+            const u32 ma = __ballot_sync(0xffffffffu, ka), mb = __ballot_sync(0xffffffffu, kb);
+            if (ka) alist[na + __popc(ma & ((1u << lane) - 1u))] = (u16)x;
+            if (kb) blist[nb + __popc(mb & ((1u << lane) - 1u))] = (u16)x;
+            na += __popc(ma);
+            nb += __popc(mb);
+        }
+        __syncwarp();
+        const float *xmr = A.XMr + pair * NR;
+        const float *q = A.Q + pair * R * (L + 1);
+        const u32 P = na * nb;
+        float lbmax = -INFINITY;
+        for (u32 p0 = 0; p0 < P; p0 += 32) {
+            const u32 p = p0 + lane;
+            bool valid = false;
+            u32 a = 0, b = 0;
+            if (p < P) {
+                const u32 ai = p / nb;
+                a = alist[ai];
+                b = blist[p - ai * nb];
+                valid = (a > b ? a - b : b - a) <= L &&                                    // .cl:543-556
+                        (((abits[a >> 5] >> (a & 31)) | (bbits[b >> 5] >> (b & 31))) & 1u);  // .cl:572-576
+                if (valid) {
+                    const float xr = __ldg(xmr + (int)a - (int)b + (int)L);
+                    valid = ga_hi[a] + hb_hi[b] + xr + slack + kPruneSlack * fabsf(xr) >= TH;
+                }
+            }
+            float lo = -INFINITY, hi = -INFINITY;
+            if (valid) {
+                ov_item_bounds(q, L, (int)a - (int)nmax, (int)a - (int)b, ga_lo[a], ga_hi[a], hb_lo[b], hb_hi[b],
+                               kx, lo, hi);
+                evaluated++;
+            }
+            lbmax = fmaxf(lbmax, lo);
+            const bool keep = valid && hi >= TH && hi > c.lbest;
+            const u32 mk = __ballot_sync(0xffffffffu, keep);
+            if (mk) {
+                u32 base = 0;
+                if (lane == 0) base = atomicAdd(A.pool_total, (u32)__popc(mk));
+                base = __shfl_sync(0xffffffffu, base, 0);
+                if (keep) {
+                    const u32 pp = base + __popc(mk & ((1u << lane) - 1u));
+                    if (pp < A.pool_cap) {
+                        A.pool_slot[pp] = g;
+                        A.pool_item[pp] = t + K * (a + S * b);
+                        A.pool_hi[pp] = hi;
+                    } else {
+                        A.fallback[g] = 1;
+                    }
+                }
+            }
+        }
+        lbmax = warp_max_f(lbmax);
+        if (lane == 0 && lbmax > 0.0f) atomicMax(reinterpret_cast<int *>(A.cand_lb) + g, __float_as_int(lbmax));
+        __syncwarp();
+    }
+    if (A.items_evaluated) {
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) evaluated += __shfl_xor_sync(0xffffffffu, evaluated, o);
+        if (lane == 0 && evaluated) atomicAdd(A.items_evaluated, (u64)evaluated);
     }
 }
 
@@ -782,6 +709,8 @@ __global__ void k_ov_refine(OvArgs A) {
     for (u32 e = blockIdx.x * blockDim.x + threadIdx.x; e < m; e += gridDim.x * blockDim.x) {
         const u32 g = A.pool_slot[e];
         if (A.fallback[g]) continue;
+        if (A.pool_hi[e] < A.cand_lb[g]) continue;      // below another item's lower bound
+        atomicAdd(A.refined, 1u);
         const u32 it = A.pool_item[e];
         const u32 id = A.cand[g];
         const u32 t = it % A.K, a = (it / A.K) % A.S, b = it / (A.K * A.S);
