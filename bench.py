@@ -42,7 +42,9 @@ def parse():
     ap.add_argument("--workload", choices=["linear16", "tetrode", "hd384"], default="linear16")
     ap.add_argument("--duration", type=float, default=None,
                     help="override the segment length in seconds (development only)")
-    ap.add_argument("--precision", choices=["fp32", "bf16"], default="fp32")
+    ap.add_argument("--precision", choices=["fp32", "bf16"], default="bf16",
+                    help="bf16: 16-bit tensor-core likelihood and overlap tables with exact fp32 refinement "
+                         "(results identical to fp32); fp32: exact fp32 pipes only")
     ap.add_argument("--overlap", choices=["fast", "exact"], default="fast")
     ap.add_argument("--cpu-sample-s", type=float, default=0.05,
                     help="seconds of recording timed on the CPU baseline")
@@ -323,7 +325,8 @@ def main():
     if rank == 0:
         line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
                 "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True,
-                "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+                "scaling": "weak", "vs_baseline": None,
+                "dtype": "f32" if args.precision == "fp32" else "f16-tc+f32",
                 "data": "synthetic (seeded; one independent segment per rank)",
                 "config": {"workload": rec.name, "n_chans": C, "n_samples": n, "n_templates": K,
                            "template_len": L, "n_max_shift": nmax, "precision": args.precision,

@@ -71,7 +71,7 @@ struct Workspace {
     bool fast;
     u32 slots;
     float *NT, *sNT, *tnorm, *Q, *XMr, *XM, *H, *vn, *cand_lb, *ga_lo, *ga_hi, *ga_max, *ga_abs, *pool_hi;
-    u32 *ga_bits;
+    u32 *ga_bits, *seed_a1;
     OvConst *oc;
     u8 *cskip, *fallback, *need;
     u32 *pool_slot, *pool_item, *fb_slots, *fb_list;
@@ -169,6 +169,7 @@ Workspace layout(char *base, u32 n, u32 K, u32 L, u32 nmax, bool want_fast, u32 
         w.ga_bits = (u32 *)take(sl * ((S + 31) / 32) * 4);
         w.ga_max = (float *)take(sl * 4);
         w.ga_abs = (float *)take(sl * 4);
+        w.seed_a1 = (u32 *)take(sl * 4);
         w.cand_lb = (float *)take(sl * 4);
         w.best_key = (u64 *)take(sl * 8);
         w.pool_cap = (u32)std::min<u64>(0x7fffffffull, std::max<u64>(1u << 22, (u64)sl * 128));
@@ -249,7 +250,7 @@ int launch_likelihood(const float *v, u32 n, u32 C, const float *T, u32 K, u32 L
 
 int launch_argmax(u32 n, u32 L, u32 K, const u32 *win, const u32 *n_win_dev, u32 max_windows,
                   const fbp_window_state &s, float *Lk, cudaStream_t st, const LazyLk &z = LazyLk{}) {
-    const int threads = 256;
+    const int threads = kArgmaxThreads;
     const int grid = grid_for((u64)max_windows * 32, threads, 8);
     k_window_argmax<<<grid, threads, 0, st>>>(n, L, K, win, n_win_dev, s.best_idx, s.best_lab, s.best_ll,
                                               s.flags, s.overlap_recheck, s.ov_idx, s.ov_lab, Lk, z);
@@ -338,6 +339,7 @@ OvArgs ov_args(const Workspace &w, const float *v, u32 n, u32 C, const float *T,
     A.H = w.H; A.vn = w.vn; A.cskip = w.cskip;
     A.cand_lb = w.cand_lb;
     A.ga_lo = w.ga_lo; A.ga_hi = w.ga_hi; A.ga_bits = w.ga_bits; A.ga_max = w.ga_max; A.ga_abs = w.ga_abs;
+    A.seed_a1 = w.seed_a1;
     A.pool_slot = w.pool_slot; A.pool_item = w.pool_item; A.pool_hi = w.pool_hi; A.pool_cap = w.pool_cap;
     A.refined = &cnt->ov_ref;
     A.best_key = w.best_key; A.fallback = w.fallback;
@@ -403,16 +405,14 @@ int ov_fast_pass(const Workspace &w, const OvArgs &A, Counters *cnt, cudaStream_
         k_ov_tables<<<grid_for((u64)slots * kTabThreads, kTabThreads, 4), kTabThreads, smem, st>>>(A);
         FBP_LAUNCH_CHECK();
     }
-    const size_t seed_smem = seed_smem_bytes(S);
-    if (seed_smem > 48 * 1024)
-        FBP_CUDA(cudaFuncSetAttribute(k_ov_seed, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)seed_smem));
-    k_ov_seed<<<grid_for((u64)slots * 32, kSeedThreads), kSeedThreads, seed_smem, st>>>(A);
+    k_ov_rows<<<grid_for((u64)slots * 32, kSeedThreads, 8), kSeedThreads, 0, st>>>(A);
+    k_ov_seed<<<grid_for((u64)slots * A.K * 32, kSeedThreads, 8), kSeedThreads, 0, st>>>(A);
     const size_t scan_smem = scan_smem_bytes(S);
     if (scan_smem > 48 * 1024)
         FBP_CUDA(cudaFuncSetAttribute(k_ov_scan, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)scan_smem));
     k_ov_scan<<<grid_for((u64)slots * A.K * 32, kScanThreads, 8), kScanThreads, scan_smem, st>>>(A);
-    k_ov_refine<<<(int)sm_count() * 16, 128, 0, st>>>(A);
-    k_ov_finalize<<<grid_for(slots, 256), 256, 0, st>>>(A);
+    k_ov_refine<<<(int)sm_count() * 8, kRefineThreads, 0, st>>>(A);
+    k_ov_finalize<<<grid_for((u64)slots * 32, kRefineThreads, 8), kRefineThreads, 0, st>>>(A);
     FBP_LAUNCH_CHECK();
     int rc = compact(w.fallback, slots, w.fb_slots, &cnt->fb_count, w.tile_counts, st);
     if (rc) return rc;
@@ -421,7 +421,7 @@ int ov_fast_pass(const Workspace &w, const OvArgs &A, Counters *cnt, cudaStream_
     fbp_window_state s{A.best_idx, A.best_lab, A.best_ll, A.ov_idx, A.ov_lab, nullptr, A.ovr};
     rc = launch_overlap(A.v, A.n, A.C, A.T, A.K, A.L, w.fb_list, &cnt->fb_count, slots, s, A.Lk, A.nmax, A.thr,
                         A.items_evaluated, st, A.lazy);
-    *launches = 14;
+    *launches = 15;
     return rc;
 }
 

@@ -226,15 +226,60 @@ __device__ __forceinline__ float lk_exact(const LazyLk &z, const float *Lk, u32 
     return Lk[e];
 }
 
+// Warp-cooperative reference-order sums.  The products of a sum are
+// independent, so the lanes form them (each rounded as in the reference)
+// into a per-warp buffer; lane 0 then adds them in the reference's order --
+// float addition is not associative, so the chain itself stays sequential,
+// but its loads no longer wait on global memory one by one.
+constexpr u32 kWarpChunk = 256;
+
+__device__ __forceinline__ float warp_chain(float acc, const float *buf, u32 m) {
+    u32 k = 0;
+    for (; k + 8 <= m; k += 8) {
+#pragma unroll
+        for (int j = 0; j < 8; j++) acc = __fadd_rn(acc, buf[k + j]);
+    }
+    for (; k < m; k++) acc = __fadd_rn(acc, buf[k]);
+    return acc;
+}
+
+// exact_likelihood(z, n, t, s) computed by the whole warp; every lane gets it.
+__device__ float warp_exact_likelihood(const LazyLk &z, u32 n, u32 t, u32 s, float *buf) {
+    const u32 lane = threadIdx.x & 31;
+    const u32 CL = z.C * z.L;
+    const float *tp = z.T + (size_t)t * CL;
+    float acc = z.tss[t];
+    for (u32 q0 = 0; q0 < CL; q0 += kWarpChunk) {
+        const u32 m = min(kWarpChunk, CL - q0);
+        for (u32 k = lane; k < m; k += 32) {
+            const u32 q = q0 + k, c = q / z.L, i = q - c * z.L;
+            buf[k] = __fmul_rn(__ldg(tp + q), z.v[(size_t)c * n + s + i]);
+        }
+        __syncwarp();
+        if (lane == 0) acc = warp_chain(acc, buf, m);
+        __syncwarp();
+    }
+    return __shfl_sync(0xffffffffu, acc, 0);
+}
+
+// lk_exact for a whole warp (all lanes pass the same entry).
+__device__ __forceinline__ float warp_lk_exact(const LazyLk &z, const float *Lk, u32 n, u32 t, u32 pos, float *buf) {
+    const size_t e = (size_t)t * n + pos;
+    if (z.apx && z.apx[e] == 1) return warp_exact_likelihood(z, n, t, pos, buf);
+    return Lk[e];
+}
+
 // Before the residual subtracts this pass's spikes: an approximate entry
 // that reads a changing sample and whose window is not recomputed next pass
 // keeps, in the reference, the value it was computed with; store that value
 // now, from the voltage it was computed from.
-__global__ void k_lazy_freeze(u32 n, u32 L, u32 K, const u32 *__restrict__ idx, const u32 *__restrict__ lab,
-                              u32 m, const u8 *__restrict__ next_active, u32 W, float *__restrict__ Lk,
-                              LazyLk z) {
+__global__ void __launch_bounds__(256)
+k_lazy_freeze(u32 n, u32 L, u32 K, const u32 *__restrict__ idx, const u32 *__restrict__ lab,
+              u32 m, const u8 *__restrict__ next_active, u32 W, float *__restrict__ Lk, LazyLk z) {
+    __shared__ float fbuf[8][kWarpChunk];
     const u32 lane = threadIdx.x & 31;
     const u32 warps_per_block = blockDim.x >> 5;
+    float *wbuf = fbuf[threadIdx.x >> 5];
     for (u32 g = blockIdx.x * warps_per_block + (threadIdx.x >> 5); g < m;
          g += gridDim.x * warps_per_block) {
         if (lab[g] >= K) continue;
@@ -242,16 +287,24 @@ __global__ void k_lazy_freeze(u32 n, u32 L, u32 K, const u32 *__restrict__ idx, 
         const u32 lo = p + 1 > L ? p + 1 - L : 0;
         const u32 hi = min(n, p + L);
         u32 nref = 0;
-        for (u32 s = lo + lane; s < hi; s += 32) {
+        for (u32 s0 = lo; s0 < hi; s0 += 32) {
+            const u32 s = s0 + lane;
             const u32 wd = s / L;
-            if (wd < W && next_active[wd]) continue;     // recomputed next pass
+            const bool cand = s < hi && !(wd < W && next_active[wd]);   // not recomputed next pass
             for (u32 t = 0; t < K; t++) {
                 const size_t e = (size_t)t * n + s;
-                if (z.apx[e] != 1) continue;
-                Lk[e] = exact_likelihood(z, n, t, s);
-                __threadfence();
-                z.apx[e] = (u8)z.tag;
-                nref++;
+                u32 nm = __ballot_sync(0xffffffffu, cand && z.apx[e] == 1);
+                while (nm) {
+                    const u32 src = __ffs(nm) - 1;
+                    nm &= nm - 1;
+                    const float x = warp_exact_likelihood(z, n, t, __shfl_sync(0xffffffffu, s, src), wbuf);
+                    if (lane == src) {
+                        Lk[e] = x;
+                        __threadfence();
+                        z.apx[e] = (u8)z.tag;
+                        nref++;
+                    }
+                }
             }
         }
         if (z.refined && nref) atomicAdd(z.refined, (u64)nref);
@@ -266,15 +319,19 @@ __global__ void k_lazy_freeze(u32 n, u32 L, u32 K, const u32 *__restrict__ idx, 
 // template's maximum, and the running best is replaced only on a strictly
 // larger value -- the sequential scan's result.
 // ---------------------------------------------------------------------------
-__global__ void k_window_argmax(u32 n, u32 L, u32 K, const u32 *__restrict__ win,
+constexpr int kArgmaxThreads = 256;
+__global__ void __launch_bounds__(kArgmaxThreads)
+k_window_argmax(u32 n, u32 L, u32 K, const u32 *__restrict__ win,
                                 const u32 *__restrict__ n_win_dev, u32 *__restrict__ best_idx,
                                 u32 *__restrict__ best_lab, float *__restrict__ best_ll,
                                 u8 *__restrict__ flags, u8 *__restrict__ ovr,
                                 u32 *__restrict__ ov_idx, u32 *__restrict__ ov_lab,
                                 float *__restrict__ Lk, LazyLk z) {
+    __shared__ float abuf[kArgmaxThreads / 32][kWarpChunk];
     const u32 n_win = *n_win_dev;
     const u32 lane = threadIdx.x & 31;
     const u32 warps_per_block = blockDim.x >> 5;
+    float *wbuf = abuf[threadIdx.x >> 5];
     const u32 W = (n + L - 1) / L;
     for (u32 g = blockIdx.x * warps_per_block + (threadIdx.x >> 5); g < n_win;
          g += gridDim.x * warps_per_block) {
@@ -302,21 +359,30 @@ __global__ void k_window_argmax(u32 n, u32 L, u32 K, const u32 *__restrict__ win
             float *row = Lk + (size_t)t * n;
             float lv = -INFINITY;
             u32 li = 0xffffffffu;
-            for (u32 s = start + lane; s < stop; s += 32) {
-                float cur = row[s];
-                check |= cur > 0.0f && s >= sw && s < ew;    // a flagged entry is > 0 either way
-                if (z.apx && cur + z.bm[s] >= lb) {
-                    const size_t e = (size_t)t * n + s;
-                    const u32 f = z.apx[e];
-                    if ((f == 1 || f == z.tag) && cur + lazy_bound(z, t, s, cur) >= lb) {
-                        cur = exact_likelihood(z, n, t, s);
-                        row[s] = cur;
+            for (u32 s0 = start; s0 < stop; s0 += 32) {
+                const u32 s = s0 + lane;
+                const bool in = s < stop;
+                float cur = in ? row[s] : -INFINITY;
+                check |= in && cur > 0.0f && s >= sw && s < ew;   // a flagged entry is > 0 either way
+                bool need = false;
+                if (z.apx && in && cur + z.bm[s] >= lb) {
+                    const u32 f = z.apx[(size_t)t * n + s];
+                    need = (f == 1 || f == z.tag) && cur + lazy_bound(z, t, s, cur) >= lb;
+                }
+                u32 nm = __ballot_sync(0xffffffffu, need);
+                while (nm) {                             // the warp refines them one by one
+                    const u32 src = __ffs(nm) - 1;
+                    nm &= nm - 1;
+                    const float x = warp_exact_likelihood(z, n, t, __shfl_sync(0xffffffffu, s, src), wbuf);
+                    if (lane == src) {
+                        cur = x;
+                        row[s] = x;
                         __threadfence();
-                        z.apx[e] = (u8)z.tag;
+                        z.apx[(size_t)t * n + s] = (u8)z.tag;
                         nref++;
                     }
                 }
-                if (cur > lv) { lv = cur; li = s; }
+                if (in && cur > lv) { lv = cur; li = s; }
             }
 #pragma unroll
             for (int o = 16; o > 0; o >>= 1) {
@@ -376,7 +442,25 @@ __device__ __forceinline__ float overlap_pair_exact(const float *__restrict__ vw
 }
 
 // parse_overlap_recheck_indices' decision, binary_pursuit.cl:707-814, given
-// the winning item (best_group > best_ll[id] already established or not).
+// the winning item and the reference values lf = L[lab][afix], ls = L[t][ashift].
+__device__ __forceinline__ void overlap_parse_tail(u32 id, float best_group, u32 lab, u32 t, u32 afix, u32 ashift,
+                                                   float lf, float ls, u32 *best_idx, u32 *best_lab,
+                                                   float *best_ll, u32 *ov_idx, u32 *ov_lab, u8 *ovr,
+                                                   const float *thr) {
+    if (best_group < lf || best_group < ls) { ovr[id] = 0; return; }
+    if (lf <= 0.0f || ls <= 0.0f) { ovr[id] = 0; return; }
+    if (lf >= ls && lf > thr[lab]) {
+        best_ll[id] = lf; ov_lab[id] = lab; ov_idx[id] = afix;
+    } else if (ls > lf && ls > thr[t]) {
+        best_ll[id] = ls; ov_lab[id] = t; ov_idx[id] = ashift;
+    } else if (lf > thr[lab]) {
+        best_ll[id] = lf; ov_lab[id] = lab; ov_idx[id] = afix;
+    } else {
+        ov_idx[id] = best_idx[id]; ov_lab[id] = best_lab[id]; ovr[id] = 0;
+    }
+}
+
+// The same decision (best_group > best_ll[id] already established or not).
 __device__ __forceinline__ void overlap_parse(u32 id, u32 n, u32 K, u32 S, u32 nmax, float best_group,
                                               u64 best_item, u32 *best_idx, u32 *best_lab,
                                               float *best_ll, u32 *ov_idx, u32 *ov_lab, u8 *ovr,
@@ -389,17 +473,8 @@ __device__ __forceinline__ void overlap_parse(u32 id, u32 n, u32 K, u32 S, u32 n
     const u32 afix = bidx + a - nmax, ashift = bidx + b - nmax;
     const float lf = lk_exact(z, Lk, n, lab, afix);
     const float ls = lk_exact(z, Lk, n, t, ashift);
-    if (best_group < lf || best_group < ls) { ovr[id] = 0; return; }
-    if (lf <= 0.0f || ls <= 0.0f) { ovr[id] = 0; return; }
-    if (lf >= ls && lf > thr[lab]) {
-        best_ll[id] = lf; ov_lab[id] = lab; ov_idx[id] = afix;
-    } else if (ls > lf && ls > thr[t]) {
-        best_ll[id] = ls; ov_lab[id] = t; ov_idx[id] = ashift;
-    } else if (lf > thr[lab]) {
-        best_ll[id] = lf; ov_lab[id] = lab; ov_idx[id] = afix;
-    } else {
-        ov_idx[id] = best_idx[id]; ov_lab[id] = best_lab[id]; ovr[id] = 0;
-    }
+    overlap_parse_tail(id, best_group, lab, t, afix, ashift, lf, ls, best_idx, best_lab, best_ll, ov_idx, ov_lab,
+                       ovr, thr);
 }
 
 constexpr int kOvThreads = 256;

@@ -61,6 +61,7 @@ struct OvArgs {
     float *ga_lo, *ga_hi;            // [slot][S]  interval of G(a) = H[k0][a]
     u32 *ga_bits;                    // [slot][ceil(S/32)] rows a with L[k0][afix] not <= 0
     float *ga_max, *ga_abs;          // [slot]     largest in-bounds hi(a), largest |hi(a)|
+    u32 *seed_a1;                    // [slot]     in-bounds row a of largest lower bound
     u32 *pool_total;                 // appended entries this pass
     u32 pool_cap;
     u32 *pool_slot;                  // [pool_cap]
@@ -299,9 +300,6 @@ __host__ __device__ inline size_t tables_smem_bytes(u32 S, u32 K, u32 L) {
     return (Sp + Lp + 8 + Lp * Kp) * 4;
 }
 constexpr int kSeedThreads = 256;
-__host__ __device__ inline size_t seed_smem_bytes(u32 S) {
-    return (size_t)(kSeedThreads / 32) * align_up((size_t)4 * S + (size_t)(S + 31) / 32 * 4, 16);
-}
 
 // Interval of one item from its row-invariant and moving parts.
 __device__ __forceinline__ float ov_x(const float *__restrict__ q, u32 L, int a_minus_nmax, int r) {
@@ -423,27 +421,20 @@ __device__ __forceinline__ void warp_argmax(float &v, u32 &i) {
     }
 }
 
-// Seed of each candidate's best lower bound: per template t, the items
-// (a1, b1), (a1, b2), (a3, b1) with a1 / b1 the rows of largest lower bound,
-// b2 the best row b within L of a1 and a3 the best row a within L of b1.
-// Any item's lower bound is a valid lower bound of the best item, and these
-// are close to the largest one, so the sweeps can prune against it from the
-// start.  One warp per candidate.
+// Rows a of each candidate (one warp per candidate): the intervals of
+// G(a) = H[k0][a], the L[k0][afix] > 0 bits, the largest in-bounds upper
+// bound and |upper bound|, and the row of largest lower bound (a1), for the
+// seed and the scan.
 __global__ void __launch_bounds__(kSeedThreads)
-k_ov_seed(OvArgs A) {
-    extern __shared__ float seed_sm[];
+k_ov_rows(OvArgs A) {
     const u32 nc = *A.n_cand;
     const u32 lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    const u32 S = A.S, K = A.K, L = A.L, nmax = A.nmax, n = A.n, R = 2 * L - 1;
-    float *la = (float *)((char *)seed_sm + (size_t)warp * align_up((size_t)4 * S + (size_t)(S + 31) / 32 * 4, 16));
-    u32 *fbits = (u32 *)(la + S);
-    const float krm = ov_krm(A), kx = ov_kx(A);
+    const u32 S = A.S, n = A.n, nmax = A.nmax, NB = (S + 31) / 32;
+    const float krm = ov_krm(A);
     for (u32 g = blockIdx.x * (kSeedThreads / 32) + warp; g < nc; g += gridDim.x * (kSeedThreads / 32)) {
         if (A.cskip[g]) continue;
         const OvCand c = ov_cand(A, g);
-        const float *Hg = A.H + (size_t)g * K * S;
-        // rows a: intervals (kept for the sweep), the L[k0][afix] > 0 bits,
-        // the row of largest lower bound
+        const float *Hg = A.H + ((size_t)g * A.K + c.k0) * S;
         float va = -INFINITY, mA = -INFINITY, mabs = 0.0f;
         u32 a1 = 0;
         for (u32 x0 = 0; x0 < S; x0 += 32) {
@@ -451,8 +442,8 @@ k_ov_seed(OvArgs A) {
             bool ap = false;
             if (x < S) {
                 float lo, hi;
-                ov_row_interval(A, g, x, Hg[(size_t)c.k0 * S + x], A.NT[(size_t)c.k0 * S + x],
-                                A.sNT[(size_t)c.k0 * S + x], c.vn, krm, 0.0f, c.subA0, c.subA1, lo, hi);
+                ov_row_interval(A, g, x, Hg[x], A.NT[(size_t)c.k0 * S + x], A.sNT[(size_t)c.k0 * S + x], c.vn,
+                                krm, 0.0f, c.subA0, c.subA1, lo, hi);
                 A.ga_lo[(size_t)g * S + x] = lo;
                 A.ga_hi[(size_t)g * S + x] = hi;
                 if (x >= c.xlo && x < c.xhi_ex) {
@@ -460,16 +451,10 @@ k_ov_seed(OvArgs A) {
                     if (lo > va) { va = lo; a1 = x; }
                     mA = fmaxf(mA, hi);
                     mabs = fmaxf(mabs, fabsf(hi));
-                } else {
-                    lo = -INFINITY;
                 }
-                la[x] = lo;
             }
             const u32 m = __ballot_sync(0xffffffffu, ap);
-            if (lane == 0) {
-                fbits[x0 / 32] = m;
-                A.ga_bits[(size_t)g * ((S + 31) / 32) + x0 / 32] = m;
-            }
+            if (lane == 0) A.ga_bits[(size_t)g * NB + x0 / 32] = m;
         }
         warp_argmax(va, a1);
         mA = warp_max_f(mA);
@@ -477,44 +462,65 @@ k_ov_seed(OvArgs A) {
         if (lane == 0) {
             A.ga_max[g] = mA;
             A.ga_abs[g] = mabs;
+            A.seed_a1[g] = a1;
         }
-        __syncwarp();
-        if (va == -INFINITY) continue;                  // no in-bounds row
-        const float eq = 4.0f * kUnitRoundoff * A.tnorm[c.k0];
+    }
+}
+
+// Seed of each candidate's best lower bound, one warp per (candidate,
+// template t): the items (a1, b1), (a1, b2), (a3, b1) with b1 the row b of
+// largest lower bound, b2 the best row b within L of a1 and a3 the best row a
+// within L of b1.  Any item's lower bound is a valid lower bound of the best
+// item, and these are close to the largest one, so the scan can prune
+// against it from the start.
+__global__ void __launch_bounds__(kSeedThreads)
+k_ov_seed(OvArgs A) {
+    const u32 nc = *A.n_cand;
+    const u32 lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const u32 S = A.S, K = A.K, L = A.L, nmax = A.nmax, n = A.n, R = 2 * L - 1, NB = (S + 31) / 32;
+    const float krm = ov_krm(A), kx = ov_kx(A);
+    const u64 total = (u64)nc * K;
+    const u64 nwarps = (u64)gridDim.x * (kSeedThreads / 32);
+    for (u64 e = (u64)blockIdx.x * (kSeedThreads / 32) + warp; e < total; e += nwarps) {
+        const u32 g = (u32)(e / K), t = (u32)(e % K);
+        if (A.cskip[g] || A.ga_max[g] == -INFINITY) continue;   // skipped, or no in-bounds row
+        const OvCand c = ov_cand(A, g);
+        const u32 a1 = A.seed_a1[g];
+        const float *ga_lo = A.ga_lo + (size_t)g * S;
+        const float va = ga_lo[a1];
+        const float *Hg = A.H + ((size_t)g * K + t) * S;
+        float subB0, subB1;
+        ov_sub_b(A, g, t, subB0, subB1);
+        const float eqt = 4.0f * kUnitRoundoff * A.tnorm[c.k0] * A.tnorm[t];
+        const u32 xend = min(S, c.xhi_ex);
+        float v1 = -INFINITY, v2 = -INFINITY;
+        u32 b1 = 0, b2 = 0;
+        for (u32 x = c.xlo + lane; x < xend; x += 32) {
+            float lo, hi;
+            ov_row_interval(A, g, x, Hg[x], A.NT[(size_t)t * S + x], A.sNT[(size_t)t * S + x], c.vn, krm, eqt,
+                            subB0, subB1, lo, hi);
+            if (lo > v1) { v1 = lo; b1 = x; }
+            if ((x > a1 ? x - a1 : a1 - x) <= L && lo > v2) { v2 = lo; b2 = x; }
+        }
+        warp_argmax(v1, b1);
+        warp_argmax(v2, b2);
+        float v3 = -INFINITY;
+        u32 a3 = 0;
+        for (u32 x = c.xlo + lane; x < xend; x += 32)
+            if ((x > b1 ? x - b1 : b1 - x) <= L && ga_lo[x] > v3) { v3 = ga_lo[x]; a3 = x; }
+        warp_argmax(v3, a3);
         float seed = 0.0f;
-        for (u32 t = 0; t < K; t++) {
-            float subB0, subB1;
-            ov_sub_b(A, g, t, subB0, subB1);
-            const float eqt = eq * A.tnorm[t];
-            float v1 = -INFINITY, v2 = -INFINITY;
-            u32 b1 = 0, b2 = 0;
-            for (u32 x = c.xlo + lane; x < min(S, c.xhi_ex); x += 32) {
-                float lo, hi;
-                ov_row_interval(A, g, x, Hg[(size_t)t * S + x], A.NT[(size_t)t * S + x], A.sNT[(size_t)t * S + x],
-                                c.vn, krm, eqt, subB0, subB1, lo, hi);
-                if (lo > v1) { v1 = lo; b1 = x; }
-                if ((x > a1 ? x - a1 : a1 - x) <= L && lo > v2) { v2 = lo; b2 = x; }
-            }
-            warp_argmax(v1, b1);
-            warp_argmax(v2, b2);
-            float v3 = -INFINITY;
-            u32 a3 = 0;
-            for (u32 x = c.xlo + lane; x < min(S, c.xhi_ex); x += 32)
-                if ((x > b1 ? x - b1 : b1 - x) <= L && la[x] > v3) { v3 = la[x]; a3 = x; }
-            warp_argmax(v3, a3);
-            if (lane < 3) {
-                const u32 a = lane == 2 ? a3 : a1, b = lane == 0 ? b1 : (lane == 1 ? b2 : b1);
-                const float lb_b = lane == 1 ? v2 : v1;
-                const float lb_a = lane == 2 ? v3 : va;
-                const bool geo = (a > b ? a - b : b - a) <= L && lb_a > -INFINITY && lb_b > -INFINITY;
-                if (geo) {
-                    const bool fp = (fbits[a >> 5] >> (a & 31)) & 1u;
-                    const bool sp = !(A.Lk[(size_t)t * n + c.bidx + b - nmax] <= 0.0f);
-                    if (fp || sp) {                      // .cl:572-576
-                        const float *q = A.Q + ((size_t)c.k0 * K + t) * R * (L + 1);
-                        const float X = ov_x(q, L, (int)a - (int)nmax, (int)a - (int)b);
-                        seed = fmaxf(seed, lb_a + lb_b - X - kx * fabsf(X));
-                    }
+        if (lane < 3) {
+            const u32 a = lane == 2 ? a3 : a1, b = lane == 1 ? b2 : b1;
+            const float lb_b = lane == 1 ? v2 : v1;
+            const float lb_a = lane == 2 ? v3 : va;
+            if ((a > b ? a - b : b - a) <= L && lb_a > -INFINITY && lb_b > -INFINITY) {
+                const bool fp = (A.ga_bits[(size_t)g * NB + (a >> 5)] >> (a & 31)) & 1u;
+                const bool sp = !(A.Lk[(size_t)t * n + c.bidx + b - nmax] <= 0.0f);
+                if (fp || sp) {                          // .cl:572-576
+                    const float *q = A.Q + ((size_t)c.k0 * K + t) * R * (L + 1);
+                    const float X = ov_x(q, L, (int)a - (int)nmax, (int)a - (int)b);
+                    seed = lb_a + lb_b - X - kx * fabsf(X);
                 }
             }
         }
@@ -675,55 +681,95 @@ __device__ __forceinline__ float ov_unpack_value(u64 key) {
     return __uint_as_float(u);
 }
 
-// Exact value of one item (reference order), window read from global memory.
-__device__ float overlap_item_exact_global(const OvArgs &A, u32 lab, u32 bidx, u32 t, u32 a, u32 b) {
-    const u32 L = A.L, C = A.C;
+// Exact value of one item (overlap_recheck_indices, .cl:583-646, reference
+// order of operations) computed by a whole warp: per channel the lanes form
+// the clipped sums, their squares and their products with the window; lane 0
+// adds them in the reference's order (two independent chains).
+__device__ float warp_overlap_item_exact(const OvArgs &A, u32 lab, u32 bidx, u32 t, u32 a, u32 b, float *buf) {
+    const u32 L = A.L, C = A.C, lane = threadIdx.x & 31;
     const u32 afix = bidx + a - A.nmax, ashift = bidx + b - A.nmax;
     const int fa = (int)bidx - (int)afix, sa = (int)bidx - (int)ashift;
     const u32 ffj = fa < 0 ? (u32)(-fa) : 0u, sfj = sa < 0 ? (u32)(-sa) : 0u;
+    float *sq = buf, *pr = buf + kWarpChunk;
     float cml = 0.0f;
     for (u32 c = 0; c < C; c++) {
         const float *f = A.T + ((size_t)lab * C + c) * L;
-        const float *s = A.T + ((size_t)t * C + c) * L;
+        const float *sp = A.T + ((size_t)t * C + c) * L;
         const float *vv = A.v + (size_t)c * A.n + bidx;
         float ss = 0.0f;
-        for (u32 j = 0; j < L; j++) {
-            float fv = 0.0f, sv = 0.0f;
-            if (j >= ffj && (u32)(fa + (int)j) < L) fv = __ldg(f + fa + (int)j);
-            if (j >= sfj && (u32)(sa + (int)j) < L) sv = __ldg(s + sa + (int)j);
-            const float sum = __fadd_rn(fv, sv);
-            ss = __fadd_rn(ss, __fmul_rn(sum, sum));
-            cml = __fadd_rn(cml, __fmul_rn(sum, __ldg(vv + j)));
+        for (u32 j0 = 0; j0 < L; j0 += kWarpChunk) {
+            const u32 m = min(kWarpChunk, L - j0);
+            for (u32 k = lane; k < m; k += 32) {
+                const u32 j = j0 + k;
+                float fv = 0.0f, sv = 0.0f;
+                if (j >= ffj && (u32)(fa + (int)j) < L) fv = __ldg(f + fa + (int)j);
+                if (j >= sfj && (u32)(sa + (int)j) < L) sv = __ldg(sp + sa + (int)j);
+                const float sum = __fadd_rn(fv, sv);
+                sq[k] = __fmul_rn(sum, sum);
+                pr[k] = __fmul_rn(sum, __ldg(vv + j));
+            }
+            __syncwarp();
+            if (lane == 0) {
+                u32 k = 0;
+                for (; k + 4 <= m; k += 4) {
+#pragma unroll
+                    for (int q = 0; q < 4; q++) {
+                        ss = __fadd_rn(ss, sq[k + q]);
+                        cml = __fadd_rn(cml, pr[k + q]);
+                    }
+                }
+                for (; k < m; k++) {
+                    ss = __fadd_rn(ss, sq[k]);
+                    cml = __fadd_rn(cml, pr[k]);
+                }
+            }
+            __syncwarp();
         }
-        if ((double)ss > 0.0) cml = __double2float_rn(__dsub_rn((double)cml, __dmul_rn(0.5, (double)ss)));
+        if (lane == 0 && (double)ss > 0.0)                             // .cl:627-630
+            cml = __double2float_rn(__dsub_rn((double)cml, __dmul_rn(0.5, (double)ss)));
     }
-    return cml;
+    return __shfl_sync(0xffffffffu, cml, 0);
 }
 
-// Exact values of all pooled contenders, one thread each, in the reference's
-// order of operations; each candidate keeps the largest value above its
-// current best, lowest item id on ties (the parse kernel's strict-greater
-// scan over single-item groups, .cl:699-706).
-__global__ void k_ov_refine(OvArgs A) {
+constexpr int kRefineThreads = 256;
+
+// Exact values of the pooled contenders whose upper bound reaches their
+// candidate's final lower bound, one warp each, in the reference's order of
+// operations; each candidate keeps the largest value above its current best,
+// lowest item id on ties (the parse kernel's strict-greater scan over
+// single-item groups, .cl:699-706).
+__global__ void __launch_bounds__(kRefineThreads)
+k_ov_refine(OvArgs A) {
+    __shared__ float rbuf[kRefineThreads / 32][2 * kWarpChunk];
+    const u32 lane = threadIdx.x & 31;
+    float *buf = rbuf[threadIdx.x >> 5];
     const u32 m = min(*A.pool_total, A.pool_cap);
-    for (u32 e = blockIdx.x * blockDim.x + threadIdx.x; e < m; e += gridDim.x * blockDim.x) {
+    const u32 nwarps = gridDim.x * (blockDim.x >> 5);
+    for (u32 e = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); e < m; e += nwarps) {
         const u32 g = A.pool_slot[e];
         if (A.fallback[g]) continue;
         if (A.pool_hi[e] < A.cand_lb[g]) continue;      // below another item's lower bound
-        atomicAdd(A.refined, 1u);
         const u32 it = A.pool_item[e];
         const u32 id = A.cand[g];
         const u32 t = it % A.K, a = (it / A.K) % A.S, b = it / (A.K * A.S);
-        const float ll = overlap_item_exact_global(A, A.best_lab[id], A.best_idx[id], t, a, b);
-        if (ll > A.best_ll[id]) atomicMax(&A.best_key[g], ov_pack(ll, it));
+        const float ll = warp_overlap_item_exact(A, A.best_lab[id], A.best_idx[id], t, a, b, buf);
+        if (lane == 0) {
+            atomicAdd(A.refined, 1u);
+            if (ll > A.best_ll[id]) atomicMax(&A.best_key[g], ov_pack(ll, it));
+        }
     }
 }
 
-// One thread per candidate slot: the parse decision (.cl:707-814) for the
+// One warp per candidate slot: the parse decision (.cl:707-814) for the
 // winning contender, or "no improvement".
-__global__ void k_ov_finalize(OvArgs A) {
+__global__ void __launch_bounds__(kRefineThreads)
+k_ov_finalize(OvArgs A) {
+    __shared__ float fbuf[kRefineThreads / 32][kWarpChunk];
+    const u32 lane = threadIdx.x & 31;
+    float *buf = fbuf[threadIdx.x >> 5];
     const u32 nc = *A.n_cand;
-    for (u32 g = blockIdx.x * blockDim.x + threadIdx.x; g < nc; g += gridDim.x * blockDim.x) {
+    const u32 nwarps = gridDim.x * (blockDim.x >> 5);
+    for (u32 g = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); g < nc; g += nwarps) {
         if (A.fallback[g]) continue;
         const u32 id = A.cand[g];
         const u64 key = A.best_key[g];
@@ -733,8 +779,20 @@ __global__ void k_ov_finalize(OvArgs A) {
             bv = ov_unpack_value(key);
             bi = 0xffffffffu - (u32)(key & 0xffffffffu);
         }
-        overlap_parse(id, A.n, A.K, A.S, A.nmax, bv, bi, A.best_idx, A.best_lab, A.best_ll, A.ov_idx,
-                      A.ov_lab, A.ovr, A.Lk, A.thr, A.lazy);
+        if (bv <= A.best_ll[id] || bv <= 0.0f) {
+            if (lane == 0) A.ovr[id] = 0;
+            continue;
+        }
+        const u32 lab = A.best_lab[id], bidx = A.best_idx[id];
+        const u32 t = (u32)(bi % A.K);
+        const u32 a = (u32)((bi / A.K) % A.S);
+        const u32 b = (u32)((bi / ((u64)A.S * A.K)) % A.S);
+        const u32 afix = bidx + a - A.nmax, ashift = bidx + b - A.nmax;
+        const float lf = warp_lk_exact(A.lazy, A.Lk, A.n, lab, afix, buf);
+        const float ls = warp_lk_exact(A.lazy, A.Lk, A.n, t, ashift, buf);
+        if (lane == 0)
+            overlap_parse_tail(id, bv, lab, t, afix, ashift, lf, ls, A.best_idx, A.best_lab, A.best_ll, A.ov_idx,
+                               A.ov_lab, A.ovr, A.thr);
     }
 }
 
