@@ -82,7 +82,7 @@ struct Workspace {
     u32 stiles;
     // tensor-core likelihood (present when `tc`)
     bool tc;
-    u32 tc_Cg2, tc_Np, tc_cols, tc_ref_cap;
+    u32 tc_Cg2, tc_Np, tc_cols, tc_ref_cap, tc_nbuf;
     uint4 *Tb;
     float *tc_tnorm, *tc_tabs;
     int *tc_texp;
@@ -107,12 +107,15 @@ bool fast_overlap_fits(u32 K, u32 L, u32 nmax) {
 size_t window_bytes_u8(u32 W) { return align_up((size_t)W + FBP_WINDOW_PAD, kCompactTile); }
 
 // The tensor-core likelihood keeps all templates of a chunk in shared memory.
-bool tc_fits(u32 C, u32 K, u32 L, u32 *Cg2, u32 *Np) {
+// Two strip / accumulator buffers when they fit (staging overlaps the
+// epilogue), else one.
+bool tc_fits(u32 C, u32 K, u32 L, u32 *Cg2, u32 *Np, u32 *nbuf) {
     *Cg2 = ((C + 15) / 16) * 2;
     *Np = ((K + 15) / 16) * 16;
     if (*Np > 256) return false;
     if (tc_refine_smem_bytes(C, L) > 227 * 1024) return false;
-    return tc_smem_bytes(L, *Cg2, *Np) <= 227 * 1024;
+    *nbuf = tc_smem_bytes(L, *Cg2, *Np, 2) <= 227 * 1024 ? 2 : 1;
+    return tc_smem_bytes(L, *Cg2, *Np, *nbuf) <= 227 * 1024;
 }
 
 Workspace layout(char *base, u32 n, u32 K, u32 L, u32 nmax, bool want_fast, u32 C = 0, bool want_tc = false) {
@@ -182,10 +185,10 @@ Workspace layout(char *base, u32 n, u32 K, u32 L, u32 nmax, bool want_fast, u32 
         w.stiles = (S + kTcM - 1) / kTcM;
         w.kexp_tile = (int *)take(sl * w.stiles * 4);
     }
-    w.tc = want_tc && tc_fits(C, K, L, &w.tc_Cg2, &w.tc_Np);
+    w.tc = want_tc && tc_fits(C, K, L, &w.tc_Cg2, &w.tc_Np, &w.tc_nbuf);
     if (w.tc) {
         w.tc_cols = 32;
-        while (w.tc_cols < w.tc_Np) w.tc_cols <<= 1;
+        while (w.tc_cols < w.tc_nbuf * w.tc_Np) w.tc_cols <<= 1;
         w.Tb = (uint4 *)take((size_t)L * w.tc_Cg2 * w.tc_Np * 16);
         w.apx = (u8 *)take((size_t)K * n);
         w.wn_s = (float *)take((size_t)n * 4);
@@ -388,13 +391,14 @@ int ov_fast_pass(const Workspace &w, const OvArgs &A, Counters *cnt, cudaStream_
         T.Cg2 = w.tc_Cg2; T.Np = w.tc_Np;
         T.rows_pad = (kTcM + A.L - 1 + 7) / 8 * 8;
         T.tmem_cols = w.tc_cols;
+        T.nbuf = w.tc_nbuf;
         T.v = A.v; T.T = A.T; T.texp = w.tc_texp; T.Tb = w.Tb;
         T.tb_bytes = (u32)((size_t)A.L * w.tc_Cg2 * w.tc_Np * 16);
         T.err = &cnt->tc_err;
         T.S = S; T.nmax = A.nmax; T.stiles = w.stiles;
         T.cand = A.cand; T.n_cand = A.n_cand; T.best_idx = A.best_idx; T.cskip = A.cskip;
         T.NT = A.NT; T.H = A.H; T.kexp_tile = w.kexp_tile;
-        const size_t smem = tc_smem_bytes(A.L, w.tc_Cg2, w.tc_Np);
+        const size_t smem = tc_smem_bytes(A.L, w.tc_Cg2, w.tc_Np, w.tc_nbuf);
         FBP_CUDA(cudaFuncSetAttribute(k_lik_tc<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
         k_lik_tc<1><<<sm_count(), kTcThreads, smem, st>>>(T);
         FBP_LAUNCH_CHECK();
@@ -411,7 +415,7 @@ int ov_fast_pass(const Workspace &w, const OvArgs &A, Counters *cnt, cudaStream_
     if (scan_smem > 48 * 1024)
         FBP_CUDA(cudaFuncSetAttribute(k_ov_scan, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)scan_smem));
     k_ov_scan<<<grid_for((u64)slots * A.K * 32, kScanThreads, 8), kScanThreads, scan_smem, st>>>(A);
-    k_ov_refine<<<(int)sm_count() * 8, kRefineThreads, 0, st>>>(A);
+    k_ov_refine<<<(int)sm_count() * 16, kRefineThreads, 0, st>>>(A);
     k_ov_finalize<<<grid_for((u64)slots * 32, kRefineThreads, 8), kRefineThreads, 0, st>>>(A);
     FBP_LAUNCH_CHECK();
     int rc = compact(w.fallback, slots, w.fb_slots, &cnt->fb_count, w.tile_counts, st);
@@ -483,6 +487,7 @@ int tc_likelihood_pass(const Workspace &w, const float *v, u32 n, u32 C, const f
     A.Cg2 = w.tc_Cg2; A.Np = w.tc_Np;
     A.rows_pad = (kTcM + L - 1 + 7) / 8 * 8;
     A.tmem_cols = w.tc_cols;
+    A.nbuf = w.tc_nbuf;
     A.kappa_b = tc_kappa(C, L, w.tc_Cg2);
     A.v = v; A.T = T; A.tss = tss; A.tnorm = w.tc_tnorm; A.tabs = w.tc_tabs; A.texp = w.tc_texp; A.Tb = w.Tb;
     A.tb_bytes = (u32)((size_t)L * w.tc_Cg2 * w.tc_Np * 16);
@@ -492,7 +497,7 @@ int tc_likelihood_pass(const Workspace &w, const float *v, u32 n, u32 C, const f
     A.seg_count = w.tc_seg_count; A.seg_overflow = &cnt->tc_overflow; A.seg_cap = w.tc_seg_cap;
     A.err = &cnt->tc_err;
     A.apx = w.apx; A.wn_s = w.wn_s; A.wa_s = w.wa_s; A.kx_s = w.kx_s; A.bm_s = w.bm_s; A.wlb = w.wlb;
-    const size_t smem = tc_smem_bytes(L, w.tc_Cg2, w.tc_Np);
+    const size_t smem = tc_smem_bytes(L, w.tc_Cg2, w.tc_Np, w.tc_nbuf);
     FBP_CUDA(cudaMemsetAsync(&cnt->tc_ref, 0, 4, st));
     FBP_CUDA(cudaMemsetAsync(w.tc_seg_count, 0, 4, st));
     FBP_CUDA(cudaFuncSetAttribute(k_lik_tc<0>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));

@@ -244,17 +244,30 @@ __device__ __forceinline__ float warp_chain(float acc, const float *buf, u32 m) 
 }
 
 // exact_likelihood(z, n, t, s) computed by the whole warp; every lane gets it.
+// Each lane forms up to eight products of a chunk with its loads in flight
+// together.
 __device__ float warp_exact_likelihood(const LazyLk &z, u32 n, u32 t, u32 s, float *buf) {
+    static_assert(kWarpChunk == 256, "eight products per lane");
     const u32 lane = threadIdx.x & 31;
     const u32 CL = z.C * z.L;
     const float *tp = z.T + (size_t)t * CL;
     float acc = z.tss[t];
     for (u32 q0 = 0; q0 < CL; q0 += kWarpChunk) {
         const u32 m = min(kWarpChunk, CL - q0);
-        for (u32 k = lane; k < m; k += 32) {
-            const u32 q = q0 + k, c = q / z.L, i = q - c * z.L;
-            buf[k] = __fmul_rn(__ldg(tp + q), z.v[(size_t)c * n + s + i]);
+        float tv[8], vv[8];
+#pragma unroll
+        for (int i = 0; i < 8; i++) {
+            const u32 k = lane + 32u * i;
+            tv[i] = vv[i] = 0.0f;
+            if (k < m) {
+                const u32 q = q0 + k, c = q / z.L, j = q - c * z.L;
+                tv[i] = __ldg(tp + q);
+                vv[i] = z.v[(size_t)c * n + s + j];
+            }
         }
+#pragma unroll
+        for (int i = 0; i < 8; i++)
+            if (lane + 32u * i < m) buf[lane + 32u * i] = __fmul_rn(tv[i], vv[i]);
         __syncwarp();
         if (lane == 0) acc = warp_chain(acc, buf, m);
         __syncwarp();

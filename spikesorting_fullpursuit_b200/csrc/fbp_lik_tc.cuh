@@ -35,7 +35,15 @@
 
 namespace fbp {
 
-constexpr int kTcThreads = 128;      // 4 warps: warp w owns TMEM lanes [32w, 32w+32)
+// Warp roles of the tensor-core kernel: warps 0-3 produce tiles (stage the
+// fp16 strip, issue the MMAs), warps 4-11 drain accumulators (epilogue).
+// Epilogue warp w reads TMEM lanes [32(w%4), 32(w%4)+32) -- the lanes a warp
+// may access -- and every other 16-column chunk starting at 16 * ((w-4)/4).
+constexpr int kTcProdWarps = 4;
+constexpr int kTcEpiWarps = 8;
+constexpr int kTcThreads = 32 * (kTcProdWarps + kTcEpiWarps);
+constexpr int kTcProdThreads = 32 * kTcProdWarps;
+constexpr int kTcEpiThreads = 32 * kTcEpiWarps;
 constexpr int kTcM = 128;            // samples per tile
 
 struct TcArgs {
@@ -43,6 +51,7 @@ struct TcArgs {
     u32 Cg2;                         // channel groups of 8, padded to even
     u32 Np;                          // templates padded to a multiple of 16
     u32 rows_pad;                    // strip rows (128 + L - 1) padded to 8
+    u32 nbuf;                        // strip / accumulator buffers (2: staging overlaps the epilogue)
     u32 tmem_cols;
     float kappa_b;
     const float *v;                  // [C][n]
@@ -77,32 +86,38 @@ struct TcArgs {
     int *kexp_tile;                  // [slot][stiles] voltage scale of each tile
 };
 
-__host__ __device__ inline size_t tc_smem_bytes(u32 L, u32 Cg2, u32 Np) {
+// Shared memory of the tensor-core kernel (nbuf strip buffers).
+struct TcSmem {
+    size_t Bs, As, rowsq, rowab, tsc, tsa, ctk, ctb, ctss, cta, tinfo, bars, misc, tcnt, bmh, total;
+};
+__host__ __device__ inline TcSmem tc_smem_layout(u32 L, u32 Cg2, u32 Np, u32 nbuf) {
     const size_t rows_pad = (kTcM + L - 1 + 7) / 8 * 8;
-    return (size_t)L * Cg2 * Np * 16          // templates
-           + rows_pad * Cg2 * 16              // voltage strip
-           + rows_pad * 4 * 2                 // row energies / absolute sums, their prefix sums
-           + 64                               // mbarriers, tmem address, scan scratch
-           + (size_t)Np * 4;                  // per-template counters
+    TcSmem m;
+    size_t o = 0;
+    m.Bs = o;    o += (size_t)L * Cg2 * Np * 16;            // templates
+    m.As = o;    o += (size_t)nbuf * rows_pad * Cg2 * 16;   // voltage strips
+    m.rowsq = o; o += (size_t)nbuf * rows_pad * 4;          // row energies -> prefix sums
+    m.rowab = o; o += (size_t)nbuf * rows_pad * 4;          // row absolute sums -> prefix sums
+    m.tsc = o;   o += (size_t)nbuf * Np * 4;                // per tile: 2^-(kexp + texp[t]) (0: use ldexpf)
+    m.tsa = o;   o += (size_t)nbuf * Np * 4;                // per tile: 2^-25 * 1.001 * |t|_1 * 2^-kexp
+    m.ctk = o;   o += (size_t)Np * 4;                       // kappa * ||t||
+    m.ctb = o;   o += (size_t)Np * 4;                       // 2^-25 * 1.001 * 2^-texp[t]
+    m.ctss = o;  o += (size_t)Np * 4;                       // -SS_t / 2
+    m.cta = o;   o += (size_t)Np * 4;                       // 2^-22 * |SS_t / 2|
+    m.tinfo = o; o += (size_t)nbuf * 32;                    // per buffer: s0, ew, g, kexp
+    o = (o + 7) / 8 * 8;
+    m.bars = o;  o += 8 * 8;                                // full[2], empty[2], templates
+    m.misc = o;  o += 64;                                   // tmem slot, segment info, reductions, abort
+    m.tcnt = o;  o += (size_t)Np * 4;                       // per-template counters of the tile
+    m.bmh = o;   o += (size_t)kTcM * 4;                     // second half's largest flagged bound per row
+    m.total = o;
+    return m;
+}
+__host__ __device__ inline size_t tc_smem_bytes(u32 L, u32 Cg2, u32 Np, u32 nbuf = 1) {
+    return tc_smem_layout(L, Cg2, Np, nbuf).total;
 }
 
 __device__ __forceinline__ u32 smem_u32(const void *p) { return (u32)__cvta_generic_to_shared(p); }
-
-// Exclusive scan over the 128 threads of the tensor-core kernel.
-__device__ __forceinline__ u32 tc_block_excl_scan(u32 v, u32 *total, u32 *tmp) {
-    const u32 lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    u32 incl = warp_incl_scan(v);
-    if (lane == 31) tmp[warp] = incl;
-    __syncthreads();
-    u32 off = 0, tot = 0;
-    for (u32 w = 0; w < kTcThreads / 32; w++) {
-        if (w < warp) off += tmp[w];
-        tot += tmp[w];
-    }
-    __syncthreads();
-    *total = tot;
-    return off + incl - v;
-}
 
 // K-major, no swizzle: rows 16 B apart, 8-row groups SBO apart, K chunks LBO apart.
 __device__ __forceinline__ u64 umma_desc(u32 saddr, u32 lbo, u32 sbo) {
@@ -126,6 +141,24 @@ __device__ __forceinline__ bool mbar_try_wait(u32 bar, u32 parity) {
         : "=r"(ok) : "r"(bar), "r"(parity) : "memory");
     return ok != 0;
 }
+__device__ __forceinline__ void named_bar(u32 id, u32 count) {
+    asm volatile("bar.sync %0, %1;" ::"r"(id), "r"(count) : "memory");
+}
+// Named barrier that also returns the OR of a predicate over its threads
+// (the same value in every thread, so a loop can leave it uniformly).
+__device__ __forceinline__ bool named_bar_or(u32 id, u32 count, bool v) {
+    u32 r;
+    asm volatile(
+        "{\n\t.reg .pred p, q;\n\t"
+        "setp.ne.u32 p, %1, 0;\n\t"
+        "bar.red.or.pred q, %2, %3, p;\n\t"
+        "selp.u32 %0, 1, 0, q;\n\t}"
+        : "=r"(r) : "r"((u32)v), "r"(id), "r"(count) : "memory");
+    return r != 0;
+}
+__device__ __forceinline__ void mbar_arrive(u32 bar) {
+    asm volatile("mbarrier.arrive.release.cta.shared::cta.b64 _, [%0];" ::"r"(bar) : "memory");
+}
 // Bounded wait: gives up after `limit` polls (each poll may itself suspend).
 __device__ __forceinline__ bool mbar_wait_bounded(u32 bar, u32 parity, u32 limit) {
     for (u32 i = 0; i < limit; i++)
@@ -139,28 +172,44 @@ __device__ __forceinline__ bool mbar_wait_bounded(u32 bar, u32 parity, u32 limit
 //         product is the correlation of every template shifted by b - n_max
 //         with the window (H of the fast overlap recheck, without refinement:
 //         its error bound goes into the overlap intervals).
+//
+// Persistent, one CTA per SM.  Producer warps stage tile i into strip buffer
+// i % nbuf and issue its MMAs into accumulator i % nbuf while the epilogue
+// warps drain tile i-1.  full[b] completes when the producer has published
+// the tile's data (one arrive) and its MMAs are done (tcgen05.commit);
+// empty[b] completes when all epilogue warps have read accumulator b and the
+// buffer's row sums.  Every wait is bounded; a wait that gives up sets err
+// and the abort flag, and both roles leave their loops.
 template <int MODE>
 __global__ void __launch_bounds__(kTcThreads, 1)
 k_lik_tc(TcArgs A) {
     extern __shared__ __align__(128) unsigned char tsm[];
-    const u32 L = A.L, Cg2 = A.Cg2, Np = A.Np, rows_pad = A.rows_pad, n = A.n;
-    unsigned char *Bs = tsm;
-    unsigned char *As = Bs + (size_t)L * Cg2 * Np * 16;
-    float *rowsq = (float *)(As + (size_t)rows_pad * Cg2 * 16);   // prefix of sum_c v^2 after the scan
-    float *rowab = rowsq + rows_pad;                              // prefix of sum_c |v|
-    u64 *bars = (u64 *)(rowab + rows_pad);     // [0] templates loaded, [1] MMA done
-    u32 *tmem_slot = (u32 *)(bars + 2);
-    u32 *seg_info = tmem_slot + 1;
-    u32 *scan_tmp = seg_info + 1;              // 4 warps + total
-    int *tile_exp = (int *)(scan_tmp + 5);     // power-of-two scale of this tile's voltage
-    u32 *tcnt = (u32 *)(tile_exp + 3);         // [Np] per-template counters of the tile
+    const u32 L = A.L, Cg2 = A.Cg2, Np = A.Np, rows_pad = A.rows_pad, n = A.n, nbuf = A.nbuf;
+    const TcSmem lay = tc_smem_layout(L, Cg2, Np, nbuf);
+    unsigned char *Bs = tsm + lay.Bs;
+    float *rowsq_all = (float *)(tsm + lay.rowsq), *rowab_all = (float *)(tsm + lay.rowab);
+    float *tsc_all = (float *)(tsm + lay.tsc), *tsa_all = (float *)(tsm + lay.tsa);
+    float *ctk = (float *)(tsm + lay.ctk), *ctb = (float *)(tsm + lay.ctb);
+    float *ctss = (float *)(tsm + lay.ctss), *cta = (float *)(tsm + lay.cta);
+    int *tinfo = (int *)(tsm + lay.tinfo);                 // [nbuf][8]: s0 lo, s0 hi, ew, g, kexp
+    u64 *bars = (u64 *)(tsm + lay.bars);
+    u32 *misc = (u32 *)(tsm + lay.misc);
+    u32 *tmem_slot = misc, *seg_info = misc + 1, *pred = misc + 4, *abort_flag = misc + 8;
+    u32 *tcnt = (u32 *)(tsm + lay.tcnt);
+    float *bmh = (float *)(tsm + lay.bmh);
     const u32 tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-    const u32 bar_b = smem_u32(&bars[0]), bar_mma = smem_u32(&bars[1]);
     const u32 kWaitLimit = 1u << 24;
+    auto bar_full = [&](u32 b) { return smem_u32(&bars[b]); };
+    auto bar_empty = [&](u32 b) { return smem_u32(&bars[2 + b]); };
+    const u32 bar_tb = smem_u32(&bars[4]);
 
     if (tid == 0) {
-        mbar_init(bar_b, 1);
-        mbar_init(bar_mma, 1);
+        for (u32 b = 0; b < 2; b++) {
+            mbar_init(bar_full(b), 2);                // producer arrive + MMA commit
+            mbar_init(bar_empty(b), kTcEpiWarps);     // one arrive per epilogue warp
+        }
+        mbar_init(bar_tb, 1);
+        *abort_flag = 0;
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
     if (warp == 0) {
@@ -168,151 +217,262 @@ k_lik_tc(TcArgs A) {
                      ::"r"(smem_u32(tmem_slot)), "r"(A.tmem_cols));
         asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
     }
+    // per-chunk template constants (epilogue)
+    for (u32 t = tid; t < Np; t += blockDim.x) {
+        const bool real = t < A.K;
+        if (MODE == 0) {
+            ctk[t] = real ? A.kappa_b * A.tnorm[t] : 0.0f;
+            ctb[t] = real ? 2.98023223876953125e-08f * 1.001f * ldexpf(1.0f, -A.texp[t]) : 0.0f;
+            ctss[t] = real ? A.tss[t] : 0.0f;
+            cta[t] = real ? 2.384185791015625e-07f * fabsf(A.tss[t]) : 0.0f;
+        }
+    }
     __syncthreads();
     asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
     const u32 tmem = *tmem_slot;
 
     // templates: one bulk asynchronous copy global -> shared
     if (tid == 0) {
-        asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar_b), "r"(A.tb_bytes)
+        asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar_tb), "r"(A.tb_bytes)
                      : "memory");
         asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];"
-                     ::"r"(smem_u32(Bs)), "l"(A.Tb), "r"(A.tb_bytes), "r"(bar_b) : "memory");
-    }
-    bool ok = mbar_wait_bounded(bar_b, 0, kWaitLimit);
-    ok = __syncthreads_and(ok);                  // block-uniform from here on
-    if (!ok) {
-        if (tid == 0) atomicExch(A.err, 1u);
-        mbar_wait_bounded(bar_b, 0, kWaitLimit);  // let the copy land before leaving
+                     ::"r"(smem_u32(Bs)), "l"(A.Tb), "r"(A.tb_bytes), "r"(bar_tb) : "memory");
     }
 
-    // instruction descriptor: D f32, A/B f16, both K-major, M = 128, N = Np
-    const u32 idesc = (1u << 4) | ((Np >> 3) << 17) | ((u32)(kTcM >> 4) << 24);
-    const u32 lbo_a = rows_pad * 16, lbo_b = Np * 16;
-    const u32 a_base = smem_u32(As), b_base = smem_u32(Bs);
-    const float kappa_b = A.kappa_b;
     const u32 sub = MODE == 0 ? (L + kTcM - 1) / kTcM : A.stiles;   // tiles per window / candidate
     const u64 nitems = (u64)(MODE == 0 ? *A.n_win : *A.n_cand) * sub;
-    u32 phase = 0;
+    u32 last_full_parity[2] = {2u, 2u};              // producer thread 0: outstanding commits
+    bool tb_ready = false;                           // thread 0: the template copy has landed
 
-    for (u64 item = blockIdx.x; ok && item < nitems; item += gridDim.x) {
-        // strip row x holds sample s0 + x (MODE 1: signed, masked to [m_lo, m_hi))
-        long long s0;
-        u32 ew = 0, g = 0;
-        long long m_lo = 0, m_hi = n;
-        if (MODE == 0) {
-            const u32 w = A.win[item / sub];
-            s0 = (long long)w * L + (u32)(item % sub) * kTcM;
-            ew = min((w + 1) * L, n);
-        } else {
-            g = (u32)(item / sub);
-            if (A.cskip[g]) continue;
-            const u32 i0 = A.best_idx[A.cand[g]];
-            s0 = (long long)i0 - (long long)A.nmax + (long long)(item % sub) * kTcM;
-            m_lo = i0;
-            m_hi = (long long)i0 + L;
-        }
-        // ---- row sums (energy, absolute) and the tile's largest magnitude
-        float mx = 0.0f;
-        for (u32 x = tid; x < rows_pad; x += blockDim.x) {
-            const long long pos = s0 + x;
-            float e2 = 0.0f, ab = 0.0f;
-            if (pos >= m_lo && pos < m_hi && pos < n)
-                for (u32 c = 0; c < A.C; c++) {
-                    const float f = A.v[(size_t)c * n + pos];
-                    e2 = fmaf(f, f, e2);
-                    ab += fabsf(f);
-                    mx = fmaxf(mx, fabsf(f));
+    if (warp < kTcProdWarps) {
+        // =========================== producer ===========================
+        const u32 pt = tid;                          // 0..127
+        u32 use[2] = {0u, 0u};
+        u32 it = 0;
+        for (u64 item = blockIdx.x; item < nitems; item += gridDim.x) {
+            long long s0;
+            u32 ew = 0, g = 0;
+            long long m_lo = 0, m_hi = n;
+            if (MODE == 0) {
+                const u32 w = A.win[item / sub];
+                s0 = (long long)w * L + (u32)(item % sub) * kTcM;
+                ew = min((w + 1) * L, n);
+            } else {
+                g = (u32)(item / sub);
+                if (A.cskip[g]) continue;
+                const u32 i0 = A.best_idx[A.cand[g]];
+                s0 = (long long)i0 - (long long)A.nmax + (long long)(item % sub) * kTcM;
+                m_lo = i0;
+                m_hi = (long long)i0 + L;
+            }
+            const u32 b = nbuf == 2 ? (it & 1u) : 0u;
+            it++;
+            if (use[b] > 0) {
+                bool ok = mbar_wait_bounded(bar_empty(b), (use[b] - 1) & 1u, kWaitLimit);
+                if (!ok) { atomicExch(A.err, 3u); atomicExch(abort_flag, 1u); }
+            }
+            if (named_bar_or(1, kTcProdThreads, *(volatile u32 *)abort_flag != 0)) break;
+            float *rowsq = rowsq_all + (size_t)b * rows_pad, *rowab = rowab_all + (size_t)b * rows_pad;
+            unsigned char *As = tsm + lay.As + (size_t)b * rows_pad * Cg2 * 16;
+            // ---- row sums (energy, absolute) and the tile's largest magnitude
+            float mx = 0.0f;
+            for (u32 x = pt; x < rows_pad; x += kTcProdThreads) {
+                const long long pos = s0 + x;
+                float e2 = 0.0f, ab = 0.0f;
+                if (pos >= m_lo && pos < m_hi && pos < n)
+                    for (u32 c = 0; c < A.C; c++) {
+                        const float f = A.v[(size_t)c * n + pos];
+                        e2 = fmaf(f, f, e2);
+                        ab += fabsf(f);
+                        mx = fmaxf(mx, fabsf(f));
+                    }
+                rowsq[x] = e2;
+                rowab[x] = ab;
+            }
+            mx = warp_max_f(mx);
+            if (lane == 0) pred[warp] = __float_as_uint(mx);
+            named_bar(1, kTcProdThreads);
+            int kexp = 0;
+            {
+                float m = 0.0f;
+                for (int q = 0; q < kTcProdWarps; q++) m = fmaxf(m, __uint_as_float(pred[q]));
+                if (m > 0.0f) {
+                    int e;
+                    frexpf(m, &e);                   // m < 2^e
+                    kexp = max(-126, min(126, 14 - e));   // scaled magnitudes < 2^14
                 }
-            rowsq[x] = e2;
-            rowab[x] = ab;
-        }
-        mx = warp_max_f(mx);
-        if (lane == 0) scan_tmp[warp] = __float_as_uint(mx);
-        __syncthreads();
-        if (tid == 0) {
-            float m = 0.0f;
-            for (int q = 0; q < kTcThreads / 32; q++) m = fmaxf(m, __uint_as_float(scan_tmp[q]));
-            int e = 0;
-            if (m > 0.0f) {
-                frexpf(m, &e);                       // m < 2^e
-                e = 14 - e;                          // scaled magnitudes < 2^14
-                e = max(-127, min(127, e));          // stored as int8 with the entries
             }
-            *tile_exp = e;
-            if (MODE == 1) A.kexp_tile[(size_t)g * sub + (u32)(item % sub)] = e;
-        }
-        __syncthreads();
-        const int kexp = *tile_exp;
-        // ---- stage the strip: rows x -> samples s0 + x, 8 fp16 channels per row
-        for (u32 e = tid; e < rows_pad * Cg2; e += blockDim.x) {
-            const u32 x = e % rows_pad, cg = e / rows_pad;
-            const long long pos = s0 + x;
-            const bool inside = pos >= m_lo && pos < m_hi && pos < n;
-            u16 h[8];
+            if (MODE == 1 && pt == 0) A.kexp_tile[(size_t)g * sub + (u32)(item % sub)] = kexp;
+            // ---- the strip: rows x -> samples s0 + x, 8 fp16 channels per row
+            for (u32 e = pt; e < rows_pad * Cg2; e += kTcProdThreads) {
+                const u32 x = e % rows_pad, cg = e / rows_pad;
+                const long long pos = s0 + x;
+                const bool inside = pos >= m_lo && pos < m_hi && pos < n;
+                u16 h[8];
 #pragma unroll
-            for (int j = 0; j < 8; j++) {
-                const u32 c = cg * 8 + j;
-                const float f = (c < A.C && inside) ? A.v[(size_t)c * n + pos] : 0.0f;
-                h[j] = __half_as_ushort(__float2half_rn(ldexpf(f, kexp)));
+                for (int j = 0; j < 8; j++) {
+                    const u32 c = cg * 8 + j;
+                    const float f = (c < A.C && inside) ? A.v[(size_t)c * n + pos] : 0.0f;
+                    h[j] = __half_as_ushort(__float2half_rn(ldexpf(f, kexp)));
+                }
+                uint4 q;
+                q.x = ((u32)h[1] << 16) | h[0];
+                q.y = ((u32)h[3] << 16) | h[2];
+                q.z = ((u32)h[5] << 16) | h[4];
+                q.w = ((u32)h[7] << 16) | h[6];
+                *reinterpret_cast<uint4 *>(As + ((size_t)cg * rows_pad + x) * 16) = q;
             }
-            uint4 q;
-            q.x = ((u32)h[1] << 16) | h[0];
-            q.y = ((u32)h[3] << 16) | h[2];
-            q.z = ((u32)h[5] << 16) | h[4];
-            q.w = ((u32)h[7] << 16) | h[6];
-            *reinterpret_cast<uint4 *>(As + ((size_t)cg * rows_pad + x) * 16) = q;
+            // ---- per-tile template factors; prefix sums of the row sums
+            for (u32 t = pt; t < Np; t += kTcProdThreads) {
+                float sc = 0.0f;
+                if (t < A.K) {
+                    const int ex = -(kexp + A.texp[t]);
+                    if (ex >= -149 && ex <= 127) sc = ldexpf(1.0f, ex);   // exact power of two
+                    if (MODE == 0) tsa_all[(size_t)b * Np + t] =
+                                       2.98023223876953125e-08f * 1.001f * ldexpf(A.tabs[t], -kexp);
+                }
+                tsc_all[(size_t)b * Np + t] = sc;
+            }
+            if (MODE == 0 && (warp == 1 || warp == 2)) {
+                float *arr = warp == 1 ? rowsq : rowab;
+                float carry = 0.0f;
+                for (u32 x0 = 0; x0 < rows_pad; x0 += 32) {
+                    float val = (x0 + lane < rows_pad) ? arr[x0 + lane] : 0.0f;
+#pragma unroll
+                    for (int o = 1; o < 32; o <<= 1) {
+                        const float y = __shfl_up_sync(0xffffffffu, val, o);
+                        if (lane >= (u32)o) val += y;
+                    }
+                    __syncwarp();
+                    if (x0 + lane < rows_pad) arr[x0 + lane] = carry + val;
+                    carry += __shfl_sync(0xffffffffu, val, 31);
+                }
+            }
+            if (pt == 0) {
+                int *ti = tinfo + b * 8;
+                ti[0] = (int)(s0 & 0xffffffffll);
+                ti[1] = (int)(s0 >> 32);
+                ti[2] = (int)ew;
+                ti[3] = (int)g;
+                ti[4] = kexp;
+                ti[5] = (int)(item % sub);
+            }
+            asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+            named_bar(1, kTcProdThreads);
+            // ---- issue the MMAs: for each lag m, each channel pair j
+            if (pt == 0) {
+                if (!tb_ready) {
+                    tb_ready = mbar_wait_bounded(bar_tb, 0, kWaitLimit);
+                    if (!tb_ready) { atomicExch(A.err, 1u); atomicExch(abort_flag, 1u); }
+                }
+                if (tb_ready) {
+                    // instruction descriptor: D f32, A/B f16, both K-major, M = 128, N = Np
+                    const u32 idesc = (1u << 4) | ((Np >> 3) << 17) | ((u32)(kTcM >> 4) << 24);
+                    const u32 lbo_a = rows_pad * 16, lbo_b = Np * 16;
+                    const u32 a_base = smem_u32(As), b_base = smem_u32(Bs);
+                    const u32 dst = tmem + b * Np;
+                    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+                    for (u32 m = 0; m < L; m++) {
+                        for (u32 j = 0; j < Cg2 / 2; j++) {
+                            const u64 da = umma_desc(a_base + 2 * j * lbo_a + m * 16, lbo_a, 128);
+                            const u64 db = umma_desc(b_base + (m * Cg2 + 2 * j) * lbo_b, lbo_b, 128);
+                            const u32 acc = (m | j) ? 1u : 0u;
+                            asm volatile(
+                                "{\n\t.reg .pred p;\n\t"
+                                "setp.ne.b32 p, %4, 0;\n\t"
+                                "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}"
+                                ::"r"(dst), "l"(da), "l"(db), "r"(idesc), "r"(acc) : "memory");
+                        }
+                    }
+                    mbar_arrive(bar_full(b));
+                    asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];"
+                                 ::"r"(bar_full(b)) : "memory");
+                    last_full_parity[b] = use[b] & 1u;
+                } else {
+                    mbar_arrive(bar_full(b));        // let a waiting epilogue see the abort
+                }
+            }
+            use[b]++;
         }
-        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-        __syncthreads();
-        // ---- issue the MMAs: for each lag m, each channel pair j
-        if (tid == 0) {
+    } else {
+        // =========================== epilogue ===========================
+        const u32 et = tid - kTcProdThreads;         // 0..255
+        const u32 ew_ = warp - kTcProdWarps;         // 0..7
+        const u32 quad = warp & 3u;                  // TMEM lanes [32 quad, 32 quad + 32)
+        const u32 half = ew_ >> 2;                   // column chunks 16 * (half + 2k)
+        const u32 row = quad * 32 + lane;
+        u32 use[2] = {0u, 0u};
+        u32 it = 0;
+        for (u64 item = blockIdx.x; item < nitems; item += gridDim.x) {
+            if (MODE == 1) {
+                const u32 gg = (u32)(item / sub);
+                if (A.cskip[gg]) continue;
+            }
+            const u32 b = nbuf == 2 ? (it & 1u) : 0u;
+            it++;
+            const bool ok = mbar_wait_bounded(bar_full(b), use[b] & 1u, kWaitLimit);
+            use[b]++;
+            if (!ok) { atomicExch(A.err, 2u); atomicExch(abort_flag, 1u); }
+            if (named_bar_or(2, kTcEpiThreads, *(volatile u32 *)abort_flag != 0)) break;
             asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-            for (u32 m = 0; m < L; m++) {
-                for (u32 j = 0; j < Cg2 / 2; j++) {
-                    const u64 da = umma_desc(a_base + 2 * j * lbo_a + m * 16, lbo_a, 128);
-                    const u64 db = umma_desc(b_base + (m * Cg2 + 2 * j) * lbo_b, lbo_b, 128);
-                    const u32 acc = (m | j) ? 1u : 0u;
+            const int *ti = tinfo + b * 8;
+            const long long s0 = (long long)(((unsigned long long)(u32)ti[1] << 32) | (u32)ti[0]);
+            const u32 ewin = (u32)ti[2], g = (u32)ti[3];
+            const int kexp = ti[4];
+            const u32 subi = (u32)ti[5];
+            const float *tsc = tsc_all + (size_t)b * Np;
+            const u32 acc0 = tmem + ((quad * 32u) << 16) + b * Np;
+            if (MODE == 1) {
+                // H[g][t][b] = correlation - 0.5 * clipped energy, b = shift row
+                const u32 brow = subi * kTcM + row;
+                for (u32 c0 = 16 * half; c0 < Np; c0 += 32) {
+                    u32 r[16];
                     asm volatile(
-                        "{\n\t.reg .pred p;\n\t"
-                        "setp.ne.b32 p, %4, 0;\n\t"
-                        "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}"
-                        ::"r"(tmem), "l"(da), "l"(db), "r"(idesc), "r"(acc) : "memory");
-                }
-            }
-            asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];"
-                         ::"r"(bar_mma) : "memory");
-        }
-        // ---- meanwhile: prefix sums of the row sums (warp 1: energies, warp 2: absolute)
-        if (MODE == 0 && (warp == 1 || warp == 2)) {
-            float *arr = warp == 1 ? rowsq : rowab;
-            float carry = 0.0f;
-            for (u32 x0 = 0; x0 < rows_pad; x0 += 32) {
-                float val = (x0 + lane < rows_pad) ? arr[x0 + lane] : 0.0f;
+                        "tcgen05.ld.sync.aligned.32x32b.x16.b32 "
+                        "{%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, %15}, [%16];"
+                        : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]),
+                          "=r"(r[7]), "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]),
+                          "=r"(r[14]), "=r"(r[15])
+                        : "r"(acc0 + c0));
+                    asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+                    if (brow < A.S) {
 #pragma unroll
-                for (int o = 1; o < 32; o <<= 1) {
-                    const float y = __shfl_up_sync(0xffffffffu, val, o);
-                    if (lane >= (u32)o) val += y;
+                        for (int q = 0; q < 16; q++) {
+                            const u32 t = c0 + q;
+                            if (t >= A.K) continue;
+                            const float a = __uint_as_float(r[q]);
+                            const float sc = tsc[t];
+                            const float x = sc != 0.0f ? __fmul_rn(a, sc) : ldexpf(a, -(kexp + A.texp[t]));
+                            A.H[((size_t)g * A.K + t) * A.S + brow] = x - 0.5f * A.NT[(size_t)t * A.S + brow];
+                        }
+                    }
                 }
+                asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
                 __syncwarp();
-                if (x0 + lane < rows_pad) arr[x0 + lane] = carry + val;
-                carry += __shfl_sync(0xffffffffu, val, 31);
+                if (lane == 0) mbar_arrive(bar_empty(b));
+                continue;
             }
-        }
-        const bool done = __syncthreads_and(mbar_wait_bounded(bar_mma, phase, kWaitLimit));
-        if (!done) {
-            if (tid == 0) atomicExch(A.err, 2u);
-            mbar_wait_bounded(bar_mma, phase, kWaitLimit);   // MMAs must finish before TMEM is freed
-            ok = false;
-            break;
-        }
-        phase ^= 1u;
-        asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-        if (MODE == 1) {
-            // H[g][t][b] = correlation - 0.5 * clipped energy, b = shift row
-            const u32 row = warp * 32 + lane;
-            const u32 b = (u32)(item % sub) * kTcM + row;
-            for (u32 c0 = 0; c0 < Np; c0 += 16) {
+            // ---- MODE 0 epilogue: one sample per TMEM lane
+            const float *rowsq = rowsq_all + (size_t)b * rows_pad, *rowab = rowab_all + (size_t)b * rows_pad;
+            const float *tsa = tsa_all + (size_t)b * Np;
+            const u32 s = (u32)s0 + row;
+            const bool in_win = s < ewin && row < kTcM;
+            float wn = 0.0f, wa = 0.0f;
+            if (in_win) {
+                const u32 hi_i = min(row + L, rows_pad) - 1;
+                wn = sqrtf(fmaxf(rowsq[hi_i] - (row ? rowsq[row - 1] : 0.0f), 0.0f)) * 1.0001f + 1e-30f;
+                wa = fmaxf(rowab[hi_i] - (row ? rowab[row - 1] : 0.0f), 0.0f) * 1.0001f + 1e-30f;
+            }
+            if (in_win && half == 0) {                   // interval data of this sample
+                A.wn_s[s] = wn;
+                A.wa_s[s] = wa;
+                A.kx_s[s] = (signed char)kexp;
+            }
+            // phase 1: store the values whose sign is certain, mark the others
+            u32 wantbits[8] = {0, 0, 0, 0, 0, 0, 0, 0};  // Np <= 256
+            float lomax = 0.0f, bmax = 0.0f;
+            const bool tail = s + L >= n;                // .cl:231-234
+            for (u32 c0 = 16 * half; c0 < Np; c0 += 32) {
                 u32 r[16];
                 asm volatile(
                     "tcgen05.ld.sync.aligned.32x32b.x16.b32 "
@@ -320,134 +480,104 @@ k_lik_tc(TcArgs A) {
                     : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]),
                       "=r"(r[7]), "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]),
                       "=r"(r[14]), "=r"(r[15])
-                    : "r"(tmem + ((warp * 32u) << 16) + c0));
+                    : "r"(acc0 + c0));
                 asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
-                if (b < A.S) {
+                if (!in_win) continue;
 #pragma unroll
-                    for (int q = 0; q < 16; q++) {
-                        const u32 t = c0 + q;
-                        if (t >= A.K) continue;
-                        A.H[((size_t)g * A.K + t) * A.S + b] =
-                            ldexpf(__uint_as_float(r[q]), -(kexp + A.texp[t])) - 0.5f * A.NT[(size_t)t * A.S + b];
+                for (int q = 0; q < 16; q++) {
+                    const u32 t = c0 + q;
+                    if (t >= A.K) continue;
+                    float *dst = A.Lk + (size_t)t * n + s;
+                    u8 *fl = A.apx + (size_t)t * n + s;
+                    if (tail) { *dst = 0.0f; *fl = 0; continue; }
+                    const float a = __uint_as_float(r[q]);
+                    const float sc = tsc[t];
+                    const float approx = __fadd_rn(sc != 0.0f ? __fmul_rn(a, sc) : ldexpf(a, -(kexp + A.texp[t])),
+                                                   ctss[t]);
+                    // E = kappa ||t|| ||w|| + 2^-25 (|t|_1 / s_v + |w|_1 / s_t) * 1.001 + 2^-22 (|SS/2| + |approx|)
+                    const float E = fmaf(ctk[t], wn, fmaf(ctb[t], wa, tsa[t]) + cta[t] +
+                                                         2.384185791015625e-07f * fabsf(approx));
+                    lomax = fmaxf(lomax, approx - E);
+                    if (approx + E <= 0.0f) {            // certainly <= 0: only its sign is read
+                        *dst = approx;
+                        *fl = 0;
+                    } else if (approx - E > 0.0f) {      // certainly > 0: refined when a decision needs it
+                        *dst = approx;
+                        *fl = 1;
+                        bmax = fmaxf(bmax, E);
+                    } else {                             // sign uncertain: refined now
+                        wantbits[t >> 5] |= 1u << (t & 31);
+                        *fl = 0;
                     }
                 }
             }
+            // accumulator b and the row sums are no longer needed
             asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
-            __syncthreads();
-            continue;
-        }
-        // ---- epilogue: warp w reads rows 32w..32w+31 (one sample per thread)
-        const u32 row = warp * 32 + lane;
-        const u32 s = (u32)s0 + row;
-        const bool in_win = s < ew && row < kTcM;
-        float wn = 0.0f, wa = 0.0f;
-        if (in_win) {
-            const u32 hi_i = min(row + L, rows_pad) - 1;
-            wn = sqrtf(fmaxf(rowsq[hi_i] - (row ? rowsq[row - 1] : 0.0f), 0.0f)) * 1.0001f + 1e-30f;
-            wa = fmaxf(rowab[hi_i] - (row ? rowab[row - 1] : 0.0f), 0.0f) * 1.0001f + 1e-30f;
-        }
-        // phase 1: store the values whose sign is certain, mark the others
-        u32 wantbits[8] = {0, 0, 0, 0, 0, 0, 0, 0};      // Np <= 256
-        u32 nwant = 0;
-        float lomax = 0.0f, bmax = 0.0f;                 // this sample's lower bounds / flagged bounds
-        if (in_win) {                                    // interval data of this sample
-            A.wn_s[s] = wn;
-            A.wa_s[s] = wa;
-            A.kx_s[s] = (signed char)kexp;
-        }
-        for (u32 c0 = 0; c0 < Np; c0 += 16) {
-            u32 r[16];
-            asm volatile(
-                "tcgen05.ld.sync.aligned.32x32b.x16.b32 "
-                "{%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, %15}, [%16];"
-                : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
-                  "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]),
-                  "=r"(r[15])
-                : "r"(tmem + ((warp * 32u) << 16) + c0));
-            asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
-#pragma unroll
-            for (int q = 0; q < 16; q++) {
-                const u32 t = c0 + q;
-                if (!in_win || t >= A.K) continue;
-                float *dst = A.Lk + (size_t)t * n + s;
-                u8 *fl = A.apx + (size_t)t * n + s;
-                if (s + L >= n) { *dst = 0.0f; *fl = 0; continue; }     // .cl:231-234
-                const float tssv = A.tss[t];
-                const int je = A.texp[t];
-                const float approx = ldexpf(__uint_as_float(r[q]), -(kexp + je)) + tssv;
-                const float sub = 2.98023223876953125e-08f *          // 2^-25: fp16 subnormal spacing / 2
-                                  (ldexpf(A.tabs[t], -kexp) + ldexpf(wa, -je)) * 1.001f;
-                const float E = kappa_b * A.tnorm[t] * wn + sub +
-                                2.384185791015625e-07f * (fabsf(tssv) + fabsf(approx));
-                lomax = fmaxf(lomax, approx - E);
-                if (approx + E <= 0.0f) {            // certainly <= 0: only its sign is read
-                    *dst = approx;
-                    *fl = 0;
-                } else if (approx - E > 0.0f) {      // certainly > 0: refined when a decision needs it
-                    *dst = approx;
-                    *fl = 1;
-                    bmax = fmaxf(bmax, E);
-                } else {                             // sign uncertain: refined now
-                    wantbits[t >> 5] |= 1u << (t & 31);
-                    nwant++;
-                    *fl = 0;
-                }
-            }
-        }
-        if (in_win) {
-            A.bm_s[s] = bmax;
-            if (lomax > 0.0f) atomicMax(reinterpret_cast<int *>(A.wlb) + s / L, __float_as_int(lomax));
-        }
-        // phase 2: one contiguous segment of (template, sample) entries per
-        // tile, ordered by template so the refinement shares template rows
-        for (u32 t = tid; t < Np; t += blockDim.x) tcnt[t] = 0;
-        __syncthreads();
-        for (u32 wd = 0; wd < 8; wd++) {
-            u32 bits = wantbits[wd];
-            while (bits) {
-                const u32 b = __ffs(bits) - 1;
-                bits &= bits - 1;
-                atomicAdd(&tcnt[wd * 32 + b], 1u);
-            }
-        }
-        u32 seg_total;
-        (void)tc_block_excl_scan(nwant, &seg_total, scan_tmp);
-        if (tid == 0) {
-            seg_info[0] = seg_total ? atomicAdd(A.ref_count, seg_total) : 0u;
-            u32 off = 0;                            // template offsets inside the segment
-            for (u32 t = 0; t < Np; t++) {
-                const u32 c = tcnt[t];
-                tcnt[t] = off;
-                off += c;
-            }
-        }
-        __syncthreads();
-        const u32 seg_base = seg_info[0];
-        if (seg_total && tid == 0 && seg_base + seg_total <= A.ref_cap) {
-            const u32 si = atomicAdd(A.seg_count, 1u);
-            if (si < A.seg_cap) {
-                A.seg_s0[si] = (u32)s0;
-                A.seg_base[si] = seg_base;
-                A.seg_cnt[si] = seg_total;
-            } else {
-                atomicExch(A.seg_overflow, 1u);
-            }
-        }
-        if (nwant && seg_base + seg_total <= A.ref_cap) {
+            __syncwarp();
+            if (lane == 0) mbar_arrive(bar_empty(b));
+            if (in_win && lomax > 0.0f) atomicMax(reinterpret_cast<int *>(A.wlb) + s / L, __float_as_int(lomax));
+            if (half == 1) bmh[row] = bmax;
+            // phase 2: one contiguous segment of (template, sample) entries per
+            // tile, ordered by template so the refinement shares template rows
+            for (u32 t = et; t < Np; t += kTcEpiThreads) tcnt[t] = 0;
+            named_bar(2, kTcEpiThreads);
+            if (half == 0 && in_win) A.bm_s[s] = fmaxf(bmax, bmh[row]);
             for (u32 wd = 0; wd < 8; wd++) {
                 u32 bits = wantbits[wd];
                 while (bits) {
-                    const u32 b = __ffs(bits) - 1;
+                    const u32 bb = __ffs(bits) - 1;
                     bits &= bits - 1;
-                    const u32 t = wd * 32 + b;
-                    const u32 p = seg_base + atomicAdd(&tcnt[t], 1u);
-                    A.ref_t[p] = t;
-                    A.ref_s[p] = s;
+                    atomicAdd(&tcnt[wd * 32 + bb], 1u);
                 }
             }
+            named_bar(2, kTcEpiThreads);
+            if (et == 0) {
+                u32 off = 0;                             // template offsets inside the segment
+                for (u32 t = 0; t < Np; t++) {
+                    const u32 c = tcnt[t];
+                    tcnt[t] = off;
+                    off += c;
+                }
+                const u32 base = off ? atomicAdd(A.ref_count, off) : 0u;
+                seg_info[0] = base;
+                seg_info[1] = off;
+                if (off && base + off <= A.ref_cap) {
+                    const u32 si = atomicAdd(A.seg_count, 1u);
+                    if (si < A.seg_cap) {
+                        A.seg_s0[si] = (u32)s0;
+                        A.seg_base[si] = base;
+                        A.seg_cnt[si] = off;
+                    } else {
+                        atomicExch(A.seg_overflow, 1u);
+                    }
+                }
+            }
+            named_bar(2, kTcEpiThreads);
+            const u32 seg_base = seg_info[0], seg_total = seg_info[1];
+            if (seg_total && seg_base + seg_total <= A.ref_cap) {
+                for (u32 wd = 0; wd < 8; wd++) {
+                    u32 bits = wantbits[wd];
+                    while (bits) {
+                        const u32 bb = __ffs(bits) - 1;
+                        bits &= bits - 1;
+                        const u32 t = wd * 32 + bb;
+                        const u32 p = seg_base + atomicAdd(&tcnt[t], 1u);
+                        A.ref_t[p] = t;
+                        A.ref_s[p] = s;
+                    }
+                }
+            }
+            named_bar(2, kTcEpiThreads);             // tcnt / seg_info are reused by the next tile
         }
-        asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
-        __syncthreads();
+    }
+    __syncthreads();
+    if (tid == 0) {
+        // the template copy must land before this CTA's shared memory is released
+        if (!tb_ready) mbar_wait_bounded(bar_tb, 0, kWaitLimit);
+        // MMAs must finish before their TMEM is freed
+        if (*(volatile u32 *)abort_flag)
+            for (u32 b = 0; b < 2; b++)
+                if (last_full_parity[b] < 2u) mbar_wait_bounded(bar_full(b), last_full_parity[b], kWaitLimit);
     }
     __syncthreads();
     if (warp == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(A.tmem_cols));

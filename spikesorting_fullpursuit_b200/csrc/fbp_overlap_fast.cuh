@@ -681,82 +681,63 @@ __device__ __forceinline__ float ov_unpack_value(u64 key) {
     return __uint_as_float(u);
 }
 
-// Exact value of one item (overlap_recheck_indices, .cl:583-646, reference
-// order of operations) computed by a whole warp: per channel the lanes form
-// the clipped sums, their squares and their products with the window; lane 0
-// adds them in the reference's order (two independent chains).
-__device__ float warp_overlap_item_exact(const OvArgs &A, u32 lab, u32 bidx, u32 t, u32 a, u32 b, float *buf) {
-    const u32 L = A.L, C = A.C, lane = threadIdx.x & 31;
+// Exact value of one item (overlap_recheck_indices, .cl:583-646), in the
+// reference's order of operations; loads are issued eight lags at a time so
+// the two sequential sums do not wait on each one.
+__device__ float overlap_item_exact_global(const OvArgs &A, u32 lab, u32 bidx, u32 t, u32 a, u32 b) {
+    const u32 L = A.L, C = A.C;
     const u32 afix = bidx + a - A.nmax, ashift = bidx + b - A.nmax;
     const int fa = (int)bidx - (int)afix, sa = (int)bidx - (int)ashift;
-    const u32 ffj = fa < 0 ? (u32)(-fa) : 0u, sfj = sa < 0 ? (u32)(-sa) : 0u;
-    float *sq = buf, *pr = buf + kWarpChunk;
     float cml = 0.0f;
     for (u32 c = 0; c < C; c++) {
         const float *f = A.T + ((size_t)lab * C + c) * L;
         const float *sp = A.T + ((size_t)t * C + c) * L;
         const float *vv = A.v + (size_t)c * A.n + bidx;
         float ss = 0.0f;
-        for (u32 j0 = 0; j0 < L; j0 += kWarpChunk) {
-            const u32 m = min(kWarpChunk, L - j0);
-            for (u32 k = lane; k < m; k += 32) {
-                const u32 j = j0 + k;
-                float fv = 0.0f, sv = 0.0f;
-                if (j >= ffj && (u32)(fa + (int)j) < L) fv = __ldg(f + fa + (int)j);
-                if (j >= sfj && (u32)(sa + (int)j) < L) sv = __ldg(sp + sa + (int)j);
-                const float sum = __fadd_rn(fv, sv);
-                sq[k] = __fmul_rn(sum, sum);
-                pr[k] = __fmul_rn(sum, __ldg(vv + j));
-            }
-            __syncwarp();
-            if (lane == 0) {
-                u32 k = 0;
-                for (; k + 4 <= m; k += 4) {
+        for (u32 j0 = 0; j0 < L; j0 += 8) {
+            float fv[8], sv[8], wv[8];
 #pragma unroll
-                    for (int q = 0; q < 4; q++) {
-                        ss = __fadd_rn(ss, sq[k + q]);
-                        cml = __fadd_rn(cml, pr[k + q]);
-                    }
-                }
-                for (; k < m; k++) {
-                    ss = __fadd_rn(ss, sq[k]);
-                    cml = __fadd_rn(cml, pr[k]);
+            for (int i = 0; i < 8; i++) {
+                const int j = (int)j0 + i;
+                const int jf = fa + j, js = sa + j;
+                fv[i] = (j < (int)L && jf >= 0 && jf < (int)L) ? __ldg(f + jf) : 0.0f;
+                sv[i] = (j < (int)L && js >= 0 && js < (int)L) ? __ldg(sp + js) : 0.0f;
+                wv[i] = j < (int)L ? __ldg(vv + j) : 0.0f;
+            }
+#pragma unroll
+            for (int i = 0; i < 8; i++) {
+                if (j0 + i < L) {
+                    const float sum = __fadd_rn(fv[i], sv[i]);
+                    ss = __fadd_rn(ss, __fmul_rn(sum, sum));
+                    cml = __fadd_rn(cml, __fmul_rn(sum, wv[i]));
                 }
             }
-            __syncwarp();
         }
-        if (lane == 0 && (double)ss > 0.0)                             // .cl:627-630
-            cml = __double2float_rn(__dsub_rn((double)cml, __dmul_rn(0.5, (double)ss)));
+        if ((double)ss > 0.0) cml = __double2float_rn(__dsub_rn((double)cml, __dmul_rn(0.5, (double)ss)));
     }
-    return __shfl_sync(0xffffffffu, cml, 0);
+    return cml;
 }
 
 constexpr int kRefineThreads = 256;
 
 // Exact values of the pooled contenders whose upper bound reaches their
-// candidate's final lower bound, one warp each, in the reference's order of
-// operations; each candidate keeps the largest value above its current best,
-// lowest item id on ties (the parse kernel's strict-greater scan over
-// single-item groups, .cl:699-706).
+// candidate's final lower bound, one thread each (the sums are sequential,
+// so many items in flight hide them best); each candidate keeps the largest
+// value above its current best, lowest item id on ties (the parse kernel's
+// strict-greater scan over single-item groups, .cl:699-706).
 __global__ void __launch_bounds__(kRefineThreads)
 k_ov_refine(OvArgs A) {
-    __shared__ float rbuf[kRefineThreads / 32][2 * kWarpChunk];
-    const u32 lane = threadIdx.x & 31;
-    float *buf = rbuf[threadIdx.x >> 5];
     const u32 m = min(*A.pool_total, A.pool_cap);
-    const u32 nwarps = gridDim.x * (blockDim.x >> 5);
-    for (u32 e = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); e < m; e += nwarps) {
+    for (u32 e = blockIdx.x * blockDim.x + threadIdx.x; e < m; e += gridDim.x * blockDim.x) {
         const u32 g = A.pool_slot[e];
         if (A.fallback[g]) continue;
         if (A.pool_hi[e] < A.cand_lb[g]) continue;      // below another item's lower bound
+        atomicAdd(A.refined, 1u);
         const u32 it = A.pool_item[e];
         const u32 id = A.cand[g];
         const u32 t = it % A.K, a = (it / A.K) % A.S, b = it / (A.K * A.S);
-        const float ll = warp_overlap_item_exact(A, A.best_lab[id], A.best_idx[id], t, a, b, buf);
-        if (lane == 0) {
-            atomicAdd(A.refined, 1u);
-            if (ll > A.best_ll[id]) atomicMax(&A.best_key[g], ov_pack(ll, it));
-        }
+        const float ll = overlap_item_exact_global(A, A.best_lab[id], A.best_idx[id], t, a, b);
+        if (ll > A.best_ll[id]) atomicMax(&A.best_key[g], ov_pack(ll, it));
     }
 }
 
