@@ -345,6 +345,7 @@ OvArgs ov_args(const Workspace &w, const float *v, u32 n, u32 C, const float *T,
     A.seed_a1 = w.seed_a1;
     A.pool_slot = w.pool_slot; A.pool_item = w.pool_item; A.pool_hi = w.pool_hi; A.pool_cap = w.pool_cap;
     A.refined = &cnt->ov_ref;
+    A.scan_next = &cnt->scan_next;
     A.best_key = w.best_key; A.fallback = w.fallback;
     A.items_evaluated = &cnt->ov_items;
     A.pool_total = &cnt->pool_total;
@@ -383,6 +384,7 @@ int ov_fast_pass(const Workspace &w, const OvArgs &A, Counters *cnt, cudaStream_
     FBP_CUDA(cudaMemsetAsync(w.fallback, 0, align_up((size_t)slots + FBP_WINDOW_PAD, kCompactTile), st));
     FBP_CUDA(cudaMemsetAsync(&cnt->pool_total, 0, 4, st));
     FBP_CUDA(cudaMemsetAsync(&cnt->ov_ref, 0, 4, st));
+    FBP_CUDA(cudaMemsetAsync(&cnt->scan_next, 0, 8, st));
     k_ov_prep<<<grid_for((u64)slots * 32, 256), 256, 0, st>>>(A);
     FBP_LAUNCH_CHECK();
     if (w.tc) {

@@ -36,7 +36,9 @@ struct Counters {
     u32 pad0;
     u64 lazy_ref;     // approximate likelihood entries refined on demand (whole chunk)
     u32 ov_ref;       // overlap contenders evaluated exactly this pass
-    u32 pad[15];
+    u32 pad1;
+    u64 scan_next;    // work counter of the overlap scan
+    u32 pad[12];
 };
 static_assert(sizeof(Counters) == 128, "Counters is one 128-byte line");
 

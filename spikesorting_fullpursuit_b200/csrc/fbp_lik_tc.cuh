@@ -274,18 +274,46 @@ k_lik_tc(TcArgs A) {
             if (named_bar_or(1, kTcProdThreads, *(volatile u32 *)abort_flag != 0)) break;
             float *rowsq = rowsq_all + (size_t)b * rows_pad, *rowab = rowab_all + (size_t)b * rows_pad;
             unsigned char *As = tsm + lay.As + (size_t)b * rows_pad * Cg2 * 16;
+            // ---- the next tile's voltage rows into L2 (one 128-byte line per thread)
+            {
+                const u64 nx = item + gridDim.x;
+                if (MODE == 0 && nx < nitems) {
+                    const u32 w2 = A.win[nx / sub];
+                    const long long p0 = (long long)w2 * L + (u32)(nx % sub) * kTcM;
+                    const u32 lines = (rows_pad + 31) / 32;
+                    for (u32 e = pt; e < A.C * lines; e += kTcProdThreads) {
+                        const u32 c = e / lines, ln = e % lines;
+                        const long long pos = p0 + (long long)ln * 32;
+                        if (pos < n) asm volatile("prefetch.global.L2 [%0];" ::"l"(A.v + (size_t)c * n + pos));
+                    }
+                }
+            }
             // ---- row sums (energy, absolute) and the tile's largest magnitude
             float mx = 0.0f;
             for (u32 x = pt; x < rows_pad; x += kTcProdThreads) {
                 const long long pos = s0 + x;
                 float e2 = 0.0f, ab = 0.0f;
-                if (pos >= m_lo && pos < m_hi && pos < n)
-                    for (u32 c = 0; c < A.C; c++) {
-                        const float f = A.v[(size_t)c * n + pos];
+                if (pos >= m_lo && pos < m_hi && pos < n) {
+                    const float *vp = A.v + pos;
+                    u32 c = 0;
+                    for (; c + 8 <= A.C; c += 8) {
+                        float f[8];
+#pragma unroll
+                        for (int j = 0; j < 8; j++) f[j] = vp[(size_t)(c + j) * n];
+#pragma unroll
+                        for (int j = 0; j < 8; j++) {
+                            e2 = fmaf(f[j], f[j], e2);
+                            ab += fabsf(f[j]);
+                            mx = fmaxf(mx, fabsf(f[j]));
+                        }
+                    }
+                    for (; c < A.C; c++) {
+                        const float f = vp[(size_t)c * n];
                         e2 = fmaf(f, f, e2);
                         ab += fabsf(f);
                         mx = fmaxf(mx, fabsf(f));
                     }
+                }
                 rowsq[x] = e2;
                 rowab[x] = ab;
             }

@@ -61,6 +61,7 @@ struct OvArgs {
     float *ga_lo, *ga_hi;            // [slot][S]  interval of G(a) = H[k0][a]
     u32 *ga_bits;                    // [slot][ceil(S/32)] rows a with L[k0][afix] not <= 0
     float *ga_max, *ga_abs;          // [slot]     largest in-bounds hi(a), largest |hi(a)|
+    unsigned long long *scan_next;   // next (candidate, template) pair of the scan
     u32 *seed_a1;                    // [slot]     in-bounds row a of largest lower bound
     u32 *pool_total;                 // appended entries this pass
     u32 pool_cap;
@@ -554,10 +555,14 @@ k_ov_scan(OvArgs A) {
     u32 *bbits = abits + NB;
     const u32 nc = *A.n_cand;
     const u64 total = (u64)nc * K;
-    const u64 nwarps = (u64)gridDim.x * (blockDim.x >> 5);
     const float krm = ov_krm(A), kx = ov_kx(A);
     u32 evaluated = 0;
-    for (u64 e = (u64)blockIdx.x * (blockDim.x >> 5) + warp; e < total; e += nwarps) {
+    for (;;) {
+        // pairs are taken dynamically: their cost varies by orders of magnitude
+        u64 e = 0;
+        if (lane == 0) e = atomicAdd(A.scan_next, 1ull);
+        e = __shfl_sync(0xffffffffu, e, 0);
+        if (e >= total) break;
         const u32 g = (u32)(e / K), t = (u32)(e % K);
         if (A.cskip[g]) continue;
         const float mA = A.ga_max[g];
@@ -618,14 +623,19 @@ k_ov_scan(OvArgs A) {
         const float *q = A.Q + pair * R * (L + 1);
         const u32 P = na * nb;
         float lbmax = -INFINITY;
+        // pair p = ai * nb + bi; each lane steps its (ai, bi) by 32 pairs
+        u32 ai = 0, bi = lane, dq = 0, dr = 32;
+        if (nb) {
+            ai = lane / nb; bi = lane - ai * nb;
+            dq = 32 / nb; dr = 32 - dq * nb;
+        }
         for (u32 p0 = 0; p0 < P; p0 += 32) {
             const u32 p = p0 + lane;
             bool valid = false;
             u32 a = 0, b = 0;
             if (p < P) {
-                const u32 ai = p / nb;
                 a = alist[ai];
-                b = blist[p - ai * nb];
+                b = blist[bi];
                 valid = (a > b ? a - b : b - a) <= L &&                                    // .cl:543-556
                         (((abits[a >> 5] >> (a & 31)) | (bbits[b >> 5] >> (b & 31))) & 1u);  // .cl:572-576
                 if (valid) {
@@ -633,6 +643,9 @@ k_ov_scan(OvArgs A) {
                     valid = ga_hi[a] + hb_hi[b] + xr + slack + kPruneSlack * fabsf(xr) >= TH;
                 }
             }
+            ai += dq;
+            bi += dr;
+            if (bi >= nb) { bi -= nb; ai++; }
             float lo = -INFINITY, hi = -INFINITY;
             if (valid) {
                 ov_item_bounds(q, L, (int)a - (int)nmax, (int)a - (int)b, ga_lo[a], ga_hi[a], hb_lo[b], hb_hi[b],
