@@ -372,26 +372,10 @@ k_window_argmax(u32 n, u32 L, u32 K, const u32 *__restrict__ win,
             float *row = Lk + (size_t)t * n;
             float lv = -INFINITY;
             u32 li = 0xffffffffu;
-            // the template's whole range is loaded up front (up to 16 chunks
-            // of 32 samples): the scan is bound by memory latency, not work
-            float pre[16];
-            const u32 nchunk = (stop - start + 31) / 32;
-#pragma unroll
-            for (int i = 0; i < 16; i++) {
-                const u32 s = start + 32u * i + lane;
-                pre[i] = ((u32)i < nchunk && s < stop) ? row[s] : -INFINITY;
-            }
-            for (u32 ci = 0; ci < nchunk; ci++) {
-                const u32 s = start + 32u * ci + lane;
+            for (u32 s0 = start; s0 < stop; s0 += 32) {
+                const u32 s = s0 + lane;
                 const bool in = s < stop;
-                float cur;
-                if (ci < 16) {
-#pragma unroll
-                    for (int i = 0; i < 16; i++)
-                        if ((u32)i == ci) cur = pre[i];
-                } else {
-                    cur = in ? row[s] : -INFINITY;
-                }
+                float cur = in ? row[s] : -INFINITY;
                 check |= in && cur > 0.0f && s >= sw && s < ew;   // a flagged entry is > 0 either way
                 bool need = false;
                 if (z.apx && in && cur + z.bm[s] >= lb) {

@@ -35,13 +35,16 @@
 
 namespace fbp {
 
-// Warp roles of the tensor-core kernel: warps 0-3 produce tiles (stage the
-// fp16 strip, issue the MMAs), warps 4-11 drain accumulators (epilogue).
-// Epilogue warp w reads TMEM lanes [32(w%4), 32(w%4)+32) -- the lanes a warp
-// may access -- and every other 16-column chunk starting at 16 * ((w-4)/4).
-constexpr int kTcProdWarps = 4;
+// Warp roles of the tensor-core kernel: warps 0-7 stage tiles (the fp16
+// strip, row sums, per-tile factors), warp 8 issues the MMAs, warps 9-16
+// drain accumulators (epilogue).  Epilogue warp w reads TMEM lanes
+// [32(w%4), 32(w%4)+32) -- the lanes a warp may access -- and every other
+// 16-column chunk starting at 16 * ((w-9)/4).
+constexpr int kTcProdWarps = 8;
+constexpr int kTcMmaWarp = kTcProdWarps;
 constexpr int kTcEpiWarps = 8;
-constexpr int kTcThreads = 32 * (kTcProdWarps + kTcEpiWarps);
+constexpr int kTcEpiWarp0 = kTcMmaWarp + 1;
+constexpr int kTcThreads = 32 * (kTcProdWarps + 1 + kTcEpiWarps);
 constexpr int kTcProdThreads = 32 * kTcProdWarps;
 constexpr int kTcEpiThreads = 32 * kTcEpiWarps;
 constexpr int kTcM = 128;            // samples per tile
@@ -106,7 +109,7 @@ __host__ __device__ inline TcSmem tc_smem_layout(u32 L, u32 Cg2, u32 Np, u32 nbu
     m.cta = o;   o += (size_t)Np * 4;                       // 2^-22 * |SS_t / 2|
     m.tinfo = o; o += (size_t)nbuf * 32;                    // per buffer: s0, ew, g, kexp
     o = (o + 7) / 8 * 8;
-    m.bars = o;  o += 8 * 8;                                // full[2], empty[2], templates
+    m.bars = o;  o += 8 * 8;                                // full[2], empty[2], staged[2], templates
     m.misc = o;  o += 64;                                   // tmem slot, segment info, reductions, abort
     m.tcnt = o;  o += (size_t)Np * 4;                       // per-template counters of the tile
     m.bmh = o;   o += (size_t)kTcM * 4;                     // second half's largest flagged bound per row
@@ -174,12 +177,13 @@ __device__ __forceinline__ bool mbar_wait_bounded(u32 bar, u32 parity, u32 limit
 //         its error bound goes into the overlap intervals).
 //
 // Persistent, one CTA per SM.  Producer warps stage tile i into strip buffer
-// i % nbuf and issue its MMAs into accumulator i % nbuf while the epilogue
-// warps drain tile i-1.  full[b] completes when the producer has published
-// the tile's data (one arrive) and its MMAs are done (tcgen05.commit);
-// empty[b] completes when all epilogue warps have read accumulator b and the
-// buffer's row sums.  Every wait is bounded; a wait that gives up sets err
-// and the abort flag, and both roles leave their loops.
+// i % nbuf; the MMA warp multiplies it into accumulator i % nbuf while the
+// producers stage tile i+1 and the epilogue warps drain tile i-1.
+// staged[b] completes when the producers have written buffer b; full[b] when
+// the MMA warp has published it (one arrive) and its MMAs are done
+// (tcgen05.commit); empty[b] when all epilogue warps have read accumulator b
+// and the buffer's row sums.  Every wait is bounded; a wait that gives up
+// sets err and the abort flag, and every role leaves its loop.
 template <int MODE>
 __global__ void __launch_bounds__(kTcThreads, 1)
 k_lik_tc(TcArgs A) {
@@ -194,19 +198,21 @@ k_lik_tc(TcArgs A) {
     int *tinfo = (int *)(tsm + lay.tinfo);                 // [nbuf][8]: s0 lo, s0 hi, ew, g, kexp
     u64 *bars = (u64 *)(tsm + lay.bars);
     u32 *misc = (u32 *)(tsm + lay.misc);
-    u32 *tmem_slot = misc, *seg_info = misc + 1, *pred = misc + 4, *abort_flag = misc + 8;
+    u32 *tmem_slot = misc, *seg_info = misc + 1, *pred = misc + 4, *abort_flag = misc + 12;
     u32 *tcnt = (u32 *)(tsm + lay.tcnt);
     float *bmh = (float *)(tsm + lay.bmh);
     const u32 tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     const u32 kWaitLimit = 1u << 24;
     auto bar_full = [&](u32 b) { return smem_u32(&bars[b]); };
     auto bar_empty = [&](u32 b) { return smem_u32(&bars[2 + b]); };
-    const u32 bar_tb = smem_u32(&bars[4]);
+    auto bar_staged = [&](u32 b) { return smem_u32(&bars[4 + b]); };
+    const u32 bar_tb = smem_u32(&bars[6]);
 
     if (tid == 0) {
         for (u32 b = 0; b < 2; b++) {
-            mbar_init(bar_full(b), 2);                // producer arrive + MMA commit
+            mbar_init(bar_full(b), 2);                // MMA warp arrive + MMA commit
             mbar_init(bar_empty(b), kTcEpiWarps);     // one arrive per epilogue warp
+            mbar_init(bar_staged(b), 1);              // producers (after their barrier)
         }
         mbar_init(bar_tb, 1);
         *abort_flag = 0;
@@ -241,8 +247,8 @@ k_lik_tc(TcArgs A) {
 
     const u32 sub = MODE == 0 ? (L + kTcM - 1) / kTcM : A.stiles;   // tiles per window / candidate
     const u64 nitems = (u64)(MODE == 0 ? *A.n_win : *A.n_cand) * sub;
-    u32 last_full_parity[2] = {2u, 2u};              // producer thread 0: outstanding commits
-    bool tb_ready = false;                           // thread 0: the template copy has landed
+    u32 last_full_parity[2] = {2u, 2u};              // MMA thread: outstanding commits
+    bool tb_ready = false;                           // MMA thread: the template copy has landed
 
     if (warp < kTcProdWarps) {
         // =========================== producer ===========================
@@ -332,6 +338,7 @@ k_lik_tc(TcArgs A) {
             }
             if (MODE == 1 && pt == 0) A.kexp_tile[(size_t)g * sub + (u32)(item % sub)] = kexp;
             // ---- the strip: rows x -> samples s0 + x, 8 fp16 channels per row
+            const float kscale = ldexpf(1.0f, kexp);         // exact: |kexp| <= 126
             for (u32 e = pt; e < rows_pad * Cg2; e += kTcProdThreads) {
                 const u32 x = e % rows_pad, cg = e / rows_pad;
                 const long long pos = s0 + x;
@@ -341,7 +348,7 @@ k_lik_tc(TcArgs A) {
                 for (int j = 0; j < 8; j++) {
                     const u32 c = cg * 8 + j;
                     const float f = (c < A.C && inside) ? A.v[(size_t)c * n + pos] : 0.0f;
-                    h[j] = __half_as_ushort(__float2half_rn(ldexpf(f, kexp)));
+                    h[j] = __half_as_ushort(__float2half_rn(__fmul_rn(f, kscale)));
                 }
                 uint4 q;
                 q.x = ((u32)h[1] << 16) | h[0];
@@ -387,45 +394,67 @@ k_lik_tc(TcArgs A) {
             }
             asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
             named_bar(1, kTcProdThreads);
-            // ---- issue the MMAs: for each lag m, each channel pair j
-            if (pt == 0) {
-                if (!tb_ready) {
-                    tb_ready = mbar_wait_bounded(bar_tb, 0, kWaitLimit);
-                    if (!tb_ready) { atomicExch(A.err, 1u); atomicExch(abort_flag, 1u); }
-                }
-                if (tb_ready) {
-                    // instruction descriptor: D f32, A/B f16, both K-major, M = 128, N = Np
-                    const u32 idesc = (1u << 4) | ((Np >> 3) << 17) | ((u32)(kTcM >> 4) << 24);
-                    const u32 lbo_a = rows_pad * 16, lbo_b = Np * 16;
-                    const u32 a_base = smem_u32(As), b_base = smem_u32(Bs);
-                    const u32 dst = tmem + b * Np;
-                    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-                    for (u32 m = 0; m < L; m++) {
-                        for (u32 j = 0; j < Cg2 / 2; j++) {
-                            const u64 da = umma_desc(a_base + 2 * j * lbo_a + m * 16, lbo_a, 128);
-                            const u64 db = umma_desc(b_base + (m * Cg2 + 2 * j) * lbo_b, lbo_b, 128);
-                            const u32 acc = (m | j) ? 1u : 0u;
-                            asm volatile(
-                                "{\n\t.reg .pred p;\n\t"
-                                "setp.ne.b32 p, %4, 0;\n\t"
-                                "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}"
-                                ::"r"(dst), "l"(da), "l"(db), "r"(idesc), "r"(acc) : "memory");
-                        }
-                    }
-                    mbar_arrive(bar_full(b));
-                    asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];"
-                                 ::"r"(bar_full(b)) : "memory");
-                    last_full_parity[b] = use[b] & 1u;
-                } else {
-                    mbar_arrive(bar_full(b));        // let a waiting epilogue see the abort
-                }
+            if (pt == 0) mbar_arrive(bar_staged(b));   // release: the barrier ordered every write
+            use[b]++;
+        }
+    } else if (warp == kTcMmaWarp) {
+        // =========================== MMA issue ===========================
+        // instruction descriptor: D f32, A/B f16, both K-major, M = 128, N = Np
+        const u32 idesc = (1u << 4) | ((Np >> 3) << 17) | ((u32)(kTcM >> 4) << 24);
+        const u32 lbo_a = rows_pad * 16, lbo_b = Np * 16;
+        // descriptors differ only in their start address (16-byte units,
+        // low 14 bits; every operand lies below 256 KB of shared memory)
+        const u64 db0 = umma_desc(smem_u32(Bs), lbo_b, 128);
+        u32 use[2] = {0u, 0u};
+        u32 it = 0;
+        for (u64 item = blockIdx.x; item < nitems; item += gridDim.x) {
+            if (MODE == 1) {
+                const u32 gg = (u32)(item / sub);
+                if (A.cskip[gg]) continue;
             }
+            const u32 b = nbuf == 2 ? (it & 1u) : 0u;
+            it++;
+            u32 ok = 1;
+            if (lane == 0) {
+                ok = mbar_wait_bounded(bar_staged(b), use[b] & 1u, kWaitLimit) ? 1u : 0u;
+                if (!ok) atomicExch(A.err, 4u);
+                if (ok && !tb_ready) {
+                    tb_ready = mbar_wait_bounded(bar_tb, 0, kWaitLimit);
+                    if (!tb_ready) { atomicExch(A.err, 1u); ok = 0; }
+                }
+                if (!ok) atomicExch(abort_flag, 1u);
+                if (*(volatile u32 *)abort_flag) ok = 0;
+            }
+            ok = __shfl_sync(0xffffffffu, ok, 0);
+            if (!ok) break;
+            if (lane == 0) {
+                asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+                const u64 da0 = umma_desc(smem_u32(tsm + lay.As + (size_t)b * rows_pad * Cg2 * 16), lbo_a, 128);
+                const u32 dst = tmem + b * Np;
+                for (u32 m = 0; m < L; m++) {
+                    for (u32 j = 0; j < Cg2 / 2; j++) {
+                        const u64 da = da0 + (u64)(2 * j * rows_pad + m);
+                        const u64 db = db0 + (u64)((m * Cg2 + 2 * j) * Np);
+                        const u32 acc = (m | j) ? 1u : 0u;
+                        asm volatile(
+                            "{\n\t.reg .pred p;\n\t"
+                            "setp.ne.b32 p, %4, 0;\n\t"
+                            "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}"
+                            ::"r"(dst), "l"(da), "l"(db), "r"(idesc), "r"(acc) : "memory");
+                    }
+                }
+                mbar_arrive(bar_full(b));
+                asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];"
+                             ::"r"(bar_full(b)) : "memory");
+                last_full_parity[b] = use[b] & 1u;
+            }
+            __syncwarp();
             use[b]++;
         }
     } else {
         // =========================== epilogue ===========================
-        const u32 et = tid - kTcProdThreads;         // 0..255
-        const u32 ew_ = warp - kTcProdWarps;         // 0..7
+        const u32 et = tid - 32 * kTcEpiWarp0;       // 0..255
+        const u32 ew_ = warp - kTcEpiWarp0;          // 0..7
         const u32 quad = warp & 3u;                  // TMEM lanes [32 quad, 32 quad + 32)
         const u32 half = ew_ >> 2;                   // column chunks 16 * (half + 2k)
         const u32 row = quad * 32 + lane;
@@ -599,7 +628,7 @@ k_lik_tc(TcArgs A) {
         }
     }
     __syncthreads();
-    if (tid == 0) {
+    if (tid == 32 * kTcMmaWarp) {
         // the template copy must land before this CTA's shared memory is released
         if (!tb_ready) mbar_wait_bounded(bar_tb, 0, kWaitLimit);
         // MMAs must finish before their TMEM is freed
