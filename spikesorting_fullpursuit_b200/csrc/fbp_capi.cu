@@ -89,7 +89,7 @@ struct Workspace {
     u8 *apx;
     float *wn_s, *wa_s, *bm_s, *wlb;
     signed char *kx_s;
-    u32 *tc_ref_t, *tc_ref_s, *tc_seg_s0, *tc_seg_base, *tc_seg_cnt, *tc_seg_count;
+    u32 *tc_ref_t, *tc_ref_s, *tc_seg_s0, *tc_seg_base, *tc_seg_cnt;
     u32 tc_seg_cap;
     size_t bytes;
 };
@@ -206,7 +206,6 @@ Workspace layout(char *base, u32 n, u32 K, u32 L, u32 nmax, bool want_fast, u32 
         w.tc_seg_s0 = (u32 *)take((size_t)w.tc_seg_cap * 4);
         w.tc_seg_base = (u32 *)take((size_t)w.tc_seg_cap * 4);
         w.tc_seg_cnt = (u32 *)take((size_t)w.tc_seg_cap * 4);
-        w.tc_seg_count = (u32 *)take(4);
     }
     w.bytes = off;
     return w;
@@ -455,8 +454,9 @@ __global__ void k_tnorm(const float *__restrict__ T, u32 K, u32 CL, float *__res
     }
 }
 
-__global__ void k_tc_gate(Counters *cnt, u32 cap, const u32 *seg_count, u32 seg_cap) {
-    cnt->tc_overflow = (cnt->tc_ref > cap || *seg_count > seg_cap) ? 1u : 0u;
+__global__ void k_tc_gate(Counters *cnt, u32 cap, u32 seg_cap) {
+    const u64 rs = cnt->tc_refseg;
+    cnt->tc_overflow = ((u32)(rs >> 32) > cap || (u32)rs > seg_cap) ? 1u : 0u;
 }
 
 int tc_chunk_setup(const Workspace &w, const float *T, u32 K, u32 C, u32 L, cudaStream_t st) {
@@ -494,14 +494,13 @@ int tc_likelihood_pass(const Workspace &w, const float *v, u32 n, u32 C, const f
     A.v = v; A.T = T; A.tss = tss; A.tnorm = w.tc_tnorm; A.tabs = w.tc_tabs; A.texp = w.tc_texp; A.Tb = w.Tb;
     A.tb_bytes = (u32)((size_t)L * w.tc_Cg2 * w.tc_Np * 16);
     A.win = win; A.n_win = n_win; A.Lk = Lk;
-    A.ref_t = w.tc_ref_t; A.ref_s = w.tc_ref_s; A.ref_count = &cnt->tc_ref; A.ref_cap = w.tc_ref_cap;
+    A.ref_t = w.tc_ref_t; A.ref_s = w.tc_ref_s; A.refseg = &cnt->tc_refseg; A.ref_cap = w.tc_ref_cap;
     A.seg_s0 = w.tc_seg_s0; A.seg_base = w.tc_seg_base; A.seg_cnt = w.tc_seg_cnt;
-    A.seg_count = w.tc_seg_count; A.seg_overflow = &cnt->tc_overflow; A.seg_cap = w.tc_seg_cap;
+    A.seg_overflow = &cnt->tc_overflow; A.seg_cap = w.tc_seg_cap;
     A.err = &cnt->tc_err;
     A.apx = w.apx; A.wn_s = w.wn_s; A.wa_s = w.wa_s; A.kx_s = w.kx_s; A.bm_s = w.bm_s; A.wlb = w.wlb;
     const size_t smem = tc_smem_bytes(L, w.tc_Cg2, w.tc_Np, w.tc_nbuf);
-    FBP_CUDA(cudaMemsetAsync(&cnt->tc_ref, 0, 4, st));
-    FBP_CUDA(cudaMemsetAsync(w.tc_seg_count, 0, 4, st));
+    FBP_CUDA(cudaMemsetAsync(&cnt->tc_refseg, 0, 8, st));
     FBP_CUDA(cudaFuncSetAttribute(k_lik_tc<0>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     k_lik_tc<0><<<sm_count(), kTcThreads, smem, st>>>(A);
     FBP_LAUNCH_CHECK();
@@ -510,8 +509,9 @@ int tc_likelihood_pass(const Workspace &w, const float *v, u32 n, u32 C, const f
         FBP_CUDA(cudaFuncSetAttribute(k_tc_refine, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)rsmem));
     k_tc_refine<<<sm_count() * 8, kRefThreads, rsmem, st>>>(v, n, C, T, K, L, tss, w.tc_ref_t, w.tc_ref_s,
                                                             w.tc_seg_s0, w.tc_seg_base, w.tc_seg_cnt,
-                                                            w.tc_seg_count, w.tc_seg_cap, Lk);
-    k_tc_gate<<<1, 1, 0, st>>>(cnt, w.tc_ref_cap, w.tc_seg_count, w.tc_seg_cap);
+                                                            reinterpret_cast<const u32 *>(&cnt->tc_refseg),
+                                                            w.tc_seg_cap, Lk);
+    k_tc_gate<<<1, 1, 0, st>>>(cnt, w.tc_ref_cap, w.tc_seg_cap);
     FBP_LAUNCH_CHECK();
     int rc = launch_likelihood(v, n, C, T, K, L, tss, win, n_win, max_windows, Lk, st, &cnt->tc_overflow, w.apx);
     *launches = 4;
@@ -734,7 +734,7 @@ int fbp_pursuit_chunk(float *voltage, uint32_t n, uint32_t C, const float *templ
         if (w.tc) {
             const Counters *hc = (const Counters *)h_counts;
             if (hc->tc_err) { rc = fail(FBP_ERR_CUDA, "tensor-core likelihood: bounded wait %u gave up", hc->tc_err); break; }
-            S.lik_refined += std::min(hc->tc_ref, w.tc_ref_cap);
+            S.lik_refined += std::min((u32)(hc->tc_refseg >> 32), w.tc_ref_cap);
             S.lik_exact_passes += hc->tc_overflow;
         }
         S.work[FBP_STAGE_LIKELIHOOD] += (u64)nwin * L * K;

@@ -30,7 +30,7 @@ struct Counters {
     u32 pool_total;   // overlap contenders appended this pass (may exceed the pool)
     u32 fb_count;     // overlap candidates sent to the exact kernel this pass
     u64 ov_items;     // overlap items evaluated (after the skip rules)
-    u32 tc_ref;       // tensor-core likelihood entries queued for exact refinement this pass
+    u32 pad2;
     u32 tc_err;       // non-zero: a bounded wait in the tensor-core kernel gave up
     u32 tc_overflow;  // refinement list overflowed: the exact kernel redoes the pass
     u32 pad0;
@@ -38,7 +38,8 @@ struct Counters {
     u32 ov_ref;       // overlap contenders evaluated exactly this pass
     u32 pad1;
     u64 scan_next;    // work counter of the overlap scan
-    u32 pad[12];
+    u64 tc_refseg;    // tensor-core refinement list: entries queued (high half), tile segments (low half)
+    u32 pad[10];
 };
 static_assert(sizeof(Counters) == 128, "Counters is one 128-byte line");
 

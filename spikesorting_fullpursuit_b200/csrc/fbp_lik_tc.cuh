@@ -69,10 +69,10 @@ struct TcArgs {
     const u32 *n_win;
     float *Lk;                       // [K][n]
     u32 *ref_t, *ref_s;              // refinement list (one contiguous segment per tile)
-    u32 *ref_count;
+    unsigned long long *refseg;      // entries queued (high half) and tile segments (low half)
     u32 ref_cap;
     u32 *seg_s0, *seg_base, *seg_cnt;  // tile segments of the refinement list
-    u32 *seg_count, *seg_overflow;
+    u32 *seg_overflow;
     u32 seg_cap;
     u32 *err;                        // non-zero: a bounded wait gave up
     u8 *apx;                         // [K][n] approximate-entry flags
@@ -223,8 +223,9 @@ k_lik_tc(TcArgs A) {
                      ::"r"(smem_u32(tmem_slot)), "r"(A.tmem_cols));
         asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
     }
-    // per-chunk template constants (epilogue)
+    // per-chunk template constants (epilogue); tile counters start at zero
     for (u32 t = tid; t < Np; t += blockDim.x) {
+        tcnt[t] = 0;
         const bool real = t < A.K;
         if (MODE == 0) {
             ctk[t] = real ? A.kappa_b * A.tnorm[t] : 0.0f;
@@ -574,57 +575,78 @@ k_lik_tc(TcArgs A) {
             if (lane == 0) mbar_arrive(bar_empty(b));
             if (in_win && lomax > 0.0f) atomicMax(reinterpret_cast<int *>(A.wlb) + s / L, __float_as_int(lomax));
             if (half == 1) bmh[row] = bmax;
-            // phase 2: one contiguous segment of (template, sample) entries per
-            // tile, ordered by template so the refinement shares template rows
-            for (u32 t = et; t < Np; t += kTcEpiThreads) tcnt[t] = 0;
-            named_bar(2, kTcEpiThreads);
+            u32 nwant = 0;
+#pragma unroll
+            for (int wd = 0; wd < 8; wd++) nwant += __popc(wantbits[wd]);
+            const bool anywant = named_bar_or(2, kTcEpiThreads, nwant != 0);   // also publishes bmh
             if (half == 0 && in_win) A.bm_s[s] = fmaxf(bmax, bmh[row]);
-            for (u32 wd = 0; wd < 8; wd++) {
-                u32 bits = wantbits[wd];
-                while (bits) {
-                    const u32 bb = __ffs(bits) - 1;
-                    bits &= bits - 1;
-                    atomicAdd(&tcnt[wd * 32 + bb], 1u);
-                }
-            }
-            named_bar(2, kTcEpiThreads);
-            if (et == 0) {
-                u32 off = 0;                             // template offsets inside the segment
-                for (u32 t = 0; t < Np; t++) {
-                    const u32 c = tcnt[t];
-                    tcnt[t] = off;
-                    off += c;
-                }
-                const u32 base = off ? atomicAdd(A.ref_count, off) : 0u;
-                seg_info[0] = base;
-                seg_info[1] = off;
-                if (off && base + off <= A.ref_cap) {
-                    const u32 si = atomicAdd(A.seg_count, 1u);
-                    if (si < A.seg_cap) {
-                        A.seg_s0[si] = (u32)s0;
-                        A.seg_base[si] = base;
-                        A.seg_cnt[si] = off;
-                    } else {
-                        atomicExch(A.seg_overflow, 1u);
-                    }
-                }
-            }
-            named_bar(2, kTcEpiThreads);
-            const u32 seg_base = seg_info[0], seg_total = seg_info[1];
-            if (seg_total && seg_base + seg_total <= A.ref_cap) {
+            if (anywant) {
+                // phase 2: one contiguous segment of (template, sample)
+                // entries per tile, ordered by template so the refinement
+                // shares template rows (tcnt is zero here)
                 for (u32 wd = 0; wd < 8; wd++) {
                     u32 bits = wantbits[wd];
                     while (bits) {
                         const u32 bb = __ffs(bits) - 1;
                         bits &= bits - 1;
-                        const u32 t = wd * 32 + bb;
-                        const u32 p = seg_base + atomicAdd(&tcnt[t], 1u);
-                        A.ref_t[p] = t;
-                        A.ref_s[p] = s;
+                        atomicAdd(&tcnt[wd * 32 + bb], 1u);
                     }
                 }
+                named_bar(2, kTcEpiThreads);
+                if (ew_ == 0) {
+                    // template offsets: lane l scans templates [8l, 8l+8)
+                    u32 c[8], sum = 0;
+#pragma unroll
+                    for (int i = 0; i < 8; i++) {
+                        const u32 t = lane * 8 + i;
+                        c[i] = t < Np ? tcnt[t] : 0u;
+                        sum += c[i];
+                    }
+                    const u32 incl = warp_incl_scan(sum);
+                    u32 off = incl - sum;
+#pragma unroll
+                    for (int i = 0; i < 8; i++) {
+                        const u32 t = lane * 8 + i;
+                        if (t < Np) tcnt[t] = off;
+                        off += c[i];
+                    }
+                    const u32 total = __shfl_sync(0xffffffffu, incl, 31);
+                    if (lane == 0) {
+                        // one atomic reserves the entries and the segment slot
+                        const unsigned long long old =
+                            atomicAdd(A.refseg, ((unsigned long long)total << 32) | 1ull);
+                        const u32 base = (u32)(old >> 32), si = (u32)old;
+                        seg_info[0] = base;
+                        seg_info[1] = total;
+                        seg_info[2] = 0;
+                        if (base + total <= A.ref_cap && si < A.seg_cap) {
+                            A.seg_s0[si] = (u32)s0;
+                            A.seg_base[si] = base;
+                            A.seg_cnt[si] = total;
+                            seg_info[2] = 1;
+                        } else {
+                            atomicExch(A.seg_overflow, 1u);
+                        }
+                    }
+                }
+                named_bar(2, kTcEpiThreads);
+                const u32 seg_base = seg_info[0];
+                if (seg_info[2]) {
+                    for (u32 wd = 0; wd < 8; wd++) {
+                        u32 bits = wantbits[wd];
+                        while (bits) {
+                            const u32 bb = __ffs(bits) - 1;
+                            bits &= bits - 1;
+                            const u32 t = wd * 32 + bb;
+                            const u32 p = seg_base + atomicAdd(&tcnt[t], 1u);
+                            A.ref_t[p] = t;
+                            A.ref_s[p] = s;
+                        }
+                    }
+                }
+                named_bar(2, kTcEpiThreads);         // tcnt / seg_info are done with
+                for (u32 t = et; t < Np; t += kTcEpiThreads) tcnt[t] = 0;
             }
-            named_bar(2, kTcEpiThreads);             // tcnt / seg_info are reused by the next tile
         }
     }
     __syncthreads();
