@@ -248,13 +248,13 @@ k_lik_tc(TcArgs A) {
 
     const u32 sub = MODE == 0 ? (L + kTcM - 1) / kTcM : A.stiles;   // tiles per window / candidate
     const u64 nitems = (u64)(MODE == 0 ? *A.n_win : *A.n_cand) * sub;
-    u32 last_full_parity[2] = {2u, 2u};              // MMA thread: outstanding commits
+    u32 lfp0 = 2u, lfp1 = 2u;                         // MMA thread: parity of the last commit per buffer
     bool tb_ready = false;                           // MMA thread: the template copy has landed
 
     if (warp < kTcProdWarps) {
         // =========================== producer ===========================
         const u32 pt = tid;                          // 0..127
-        u32 use[2] = {0u, 0u};
+        u32 use0 = 0u, use1 = 0u;                    // uses of each buffer so far
         u32 it = 0;
         for (u64 item = blockIdx.x; item < nitems; item += gridDim.x) {
             long long s0;
@@ -274,8 +274,9 @@ k_lik_tc(TcArgs A) {
             }
             const u32 b = nbuf == 2 ? (it & 1u) : 0u;
             it++;
-            if (use[b] > 0) {
-                bool ok = mbar_wait_bounded(bar_empty(b), (use[b] - 1) & 1u, kWaitLimit);
+            const u32 ub = b ? use1 : use0;
+            if (ub > 0) {
+                bool ok = mbar_wait_bounded(bar_empty(b), (ub - 1) & 1u, kWaitLimit);
                 if (!ok) { atomicExch(A.err, 3u); atomicExch(abort_flag, 1u); }
             }
             if (named_bar_or(1, kTcProdThreads, *(volatile u32 *)abort_flag != 0)) break;
@@ -396,7 +397,7 @@ k_lik_tc(TcArgs A) {
             asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
             named_bar(1, kTcProdThreads);
             if (pt == 0) mbar_arrive(bar_staged(b));   // release: the barrier ordered every write
-            use[b]++;
+            if (b) use1++; else use0++;
         }
     } else if (warp == kTcMmaWarp) {
         // =========================== MMA issue ===========================
@@ -406,7 +407,7 @@ k_lik_tc(TcArgs A) {
         // descriptors differ only in their start address (16-byte units,
         // low 14 bits; every operand lies below 256 KB of shared memory)
         const u64 db0 = umma_desc(smem_u32(Bs), lbo_b, 128);
-        u32 use[2] = {0u, 0u};
+        u32 use0 = 0u, use1 = 0u;
         u32 it = 0;
         for (u64 item = blockIdx.x; item < nitems; item += gridDim.x) {
             if (MODE == 1) {
@@ -415,9 +416,10 @@ k_lik_tc(TcArgs A) {
             }
             const u32 b = nbuf == 2 ? (it & 1u) : 0u;
             it++;
+            const u32 ub = b ? use1 : use0;
             u32 ok = 1;
             if (lane == 0) {
-                ok = mbar_wait_bounded(bar_staged(b), use[b] & 1u, kWaitLimit) ? 1u : 0u;
+                ok = mbar_wait_bounded(bar_staged(b), ub & 1u, kWaitLimit) ? 1u : 0u;
                 if (!ok) atomicExch(A.err, 4u);
                 if (ok && !tb_ready) {
                     tb_ready = mbar_wait_bounded(bar_tb, 0, kWaitLimit);
@@ -447,10 +449,10 @@ k_lik_tc(TcArgs A) {
                 mbar_arrive(bar_full(b));
                 asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];"
                              ::"r"(bar_full(b)) : "memory");
-                last_full_parity[b] = use[b] & 1u;
+                if (b) lfp1 = ub & 1u; else lfp0 = ub & 1u;
             }
             __syncwarp();
-            use[b]++;
+            if (b) use1++; else use0++;
         }
     } else {
         // =========================== epilogue ===========================
@@ -459,7 +461,7 @@ k_lik_tc(TcArgs A) {
         const u32 quad = warp & 3u;                  // TMEM lanes [32 quad, 32 quad + 32)
         const u32 half = ew_ >> 2;                   // column chunks 16 * (half + 2k)
         const u32 row = quad * 32 + lane;
-        u32 use[2] = {0u, 0u};
+        u32 use0 = 0u, use1 = 0u;
         u32 it = 0;
         for (u64 item = blockIdx.x; item < nitems; item += gridDim.x) {
             if (MODE == 1) {
@@ -468,8 +470,8 @@ k_lik_tc(TcArgs A) {
             }
             const u32 b = nbuf == 2 ? (it & 1u) : 0u;
             it++;
-            const bool ok = mbar_wait_bounded(bar_full(b), use[b] & 1u, kWaitLimit);
-            use[b]++;
+            const bool ok = mbar_wait_bounded(bar_full(b), (b ? use1 : use0) & 1u, kWaitLimit);
+            if (b) use1++; else use0++;
             if (!ok) { atomicExch(A.err, 2u); atomicExch(abort_flag, 1u); }
             if (named_bar_or(2, kTcEpiThreads, *(volatile u32 *)abort_flag != 0)) break;
             asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
@@ -526,11 +528,17 @@ k_lik_tc(TcArgs A) {
                 A.wa_s[s] = wa;
                 A.kx_s[s] = (signed char)kexp;
             }
-            // phase 1: store the values whose sign is certain, mark the others
-            u32 wantbits[8] = {0, 0, 0, 0, 0, 0, 0, 0};  // Np <= 256
+            // phase 1: every entry gets its approximation and flag; the ones
+            // whose sign is uncertain are marked for refinement (which
+            // overwrites them before anything reads them).  Branch-free, and
+            // every index is known at compile time (no local memory).
+            u32 wantbits[8] = {0, 0, 0, 0, 0, 0, 0, 0};  // Np <= 256: word k holds chunks k of both halves
             float lomax = 0.0f, bmax = 0.0f;
             const bool tail = s + L >= n;                // .cl:231-234
-            for (u32 c0 = 16 * half; c0 < Np; c0 += 32) {
+#pragma unroll
+            for (int k = 0; k < 8; k++) {
+                const u32 c0 = 16 * half + 32 * k;
+                if (c0 >= Np) break;                     // uniform in the warp
                 u32 r[16];
                 asm volatile(
                     "tcgen05.ld.sync.aligned.32x32b.x16.b32 "
@@ -541,13 +549,13 @@ k_lik_tc(TcArgs A) {
                     : "r"(acc0 + c0));
                 asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
                 if (!in_win) continue;
+                float *dst0 = A.Lk + (size_t)c0 * n + s;
+                u8 *fl0 = A.apx + (size_t)c0 * n + s;
+                u32 cw = 0;
 #pragma unroll
                 for (int q = 0; q < 16; q++) {
                     const u32 t = c0 + q;
-                    if (t >= A.K) continue;
-                    float *dst = A.Lk + (size_t)t * n + s;
-                    u8 *fl = A.apx + (size_t)t * n + s;
-                    if (tail) { *dst = 0.0f; *fl = 0; continue; }
+                    if (t >= A.K) break;                 // padding templates
                     const float a = __uint_as_float(r[q]);
                     const float sc = tsc[t];
                     const float approx = __fadd_rn(sc != 0.0f ? __fmul_rn(a, sc) : ldexpf(a, -(kexp + A.texp[t])),
@@ -555,19 +563,16 @@ k_lik_tc(TcArgs A) {
                     // E = kappa ||t|| ||w|| + 2^-25 (|t|_1 / s_v + |w|_1 / s_t) * 1.001 + 2^-22 (|SS/2| + |approx|)
                     const float E = fmaf(ctk[t], wn, fmaf(ctb[t], wa, tsa[t]) + cta[t] +
                                                          2.384185791015625e-07f * fabsf(approx));
+                    const bool pos = approx - E > 0.0f;      // certainly > 0: refined when a decision needs it
+                    const bool neg = approx + E <= 0.0f;     // certainly <= 0: only its sign is read
                     lomax = fmaxf(lomax, approx - E);
-                    if (approx + E <= 0.0f) {            // certainly <= 0: only its sign is read
-                        *dst = approx;
-                        *fl = 0;
-                    } else if (approx - E > 0.0f) {      // certainly > 0: refined when a decision needs it
-                        *dst = approx;
-                        *fl = 1;
-                        bmax = fmaxf(bmax, E);
-                    } else {                             // sign uncertain: refined now
-                        wantbits[t >> 5] |= 1u << (t & 31);
-                        *fl = 0;
-                    }
+                    bmax = pos ? fmaxf(bmax, E) : bmax;
+                    cw |= (!tail && !pos && !neg) ? (1u << q) : 0u;
+                    dst0[(size_t)q * n] = tail ? 0.0f : approx;
+                    fl0[(size_t)q * n] = (!tail && pos) ? (u8)1 : (u8)0;
                 }
+                if (tail) lomax = 0.0f, bmax = 0.0f;
+                wantbits[k] |= cw << (16 * half);
             }
             // accumulator b and the row sums are no longer needed
             asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
@@ -584,12 +589,13 @@ k_lik_tc(TcArgs A) {
                 // phase 2: one contiguous segment of (template, sample)
                 // entries per tile, ordered by template so the refinement
                 // shares template rows (tcnt is zero here)
-                for (u32 wd = 0; wd < 8; wd++) {
-                    u32 bits = wantbits[wd];
-                    while (bits) {
+#pragma unroll
+                for (int k = 0; k < 8; k++) {
+                    u32 bits = wantbits[k];
+                    while (bits) {                       // word k: chunk k of each half
                         const u32 bb = __ffs(bits) - 1;
                         bits &= bits - 1;
-                        atomicAdd(&tcnt[wd * 32 + bb], 1u);
+                        atomicAdd(&tcnt[32 * k + (bb & 15) + 16 * (bb >> 4)], 1u);
                     }
                 }
                 named_bar(2, kTcEpiThreads);
@@ -632,12 +638,13 @@ k_lik_tc(TcArgs A) {
                 named_bar(2, kTcEpiThreads);
                 const u32 seg_base = seg_info[0];
                 if (seg_info[2]) {
-                    for (u32 wd = 0; wd < 8; wd++) {
-                        u32 bits = wantbits[wd];
+#pragma unroll
+                    for (int k = 0; k < 8; k++) {
+                        u32 bits = wantbits[k];
                         while (bits) {
                             const u32 bb = __ffs(bits) - 1;
                             bits &= bits - 1;
-                            const u32 t = wd * 32 + bb;
+                            const u32 t = 32 * k + (bb & 15) + 16 * (bb >> 4);
                             const u32 p = seg_base + atomicAdd(&tcnt[t], 1u);
                             A.ref_t[p] = t;
                             A.ref_s[p] = s;
@@ -654,9 +661,10 @@ k_lik_tc(TcArgs A) {
         // the template copy must land before this CTA's shared memory is released
         if (!tb_ready) mbar_wait_bounded(bar_tb, 0, kWaitLimit);
         // MMAs must finish before their TMEM is freed
-        if (*(volatile u32 *)abort_flag)
-            for (u32 b = 0; b < 2; b++)
-                if (last_full_parity[b] < 2u) mbar_wait_bounded(bar_full(b), last_full_parity[b], kWaitLimit);
+        if (*(volatile u32 *)abort_flag) {
+            if (lfp0 < 2u) mbar_wait_bounded(bar_full(0), lfp0, kWaitLimit);
+            if (lfp1 < 2u) mbar_wait_bounded(bar_full(1), lfp1, kWaitLimit);
+        }
     }
     __syncthreads();
     if (warp == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(A.tmem_cols));
