@@ -339,6 +339,7 @@ def main():
                            "overlap_fallback_candidates": int(stats[-1].fallback_candidates),
                            "likelihood_refined": int(stats[-1].lik_refined),
                            "likelihood_lazy_refined": int(stats[-1].lik_lazy_refined),
+                           "likelihood_seq_refined": int(stats[-1].lik_seq_refined),
                            "likelihood_exact_passes": int(stats[-1].lik_exact_passes),
                            "parallelism": "segment-parallel x%d" % world},
                 "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": gpu_launches,

@@ -104,6 +104,9 @@ typedef struct fbp_stage_stats {
     uint64_t lik_lazy_refined;  /* likelihood entries left approximate (certainly > 0) and
                                    re-evaluated exactly when a decision needed them
                                    (FBP_PREC_BF16_REFINE) */
+    uint64_t lik_seq_refined;   /* entries of lik_refined whose sign a double-precision
+                                   interval could not settle, re-evaluated in the
+                                   reference's order (FBP_PREC_BF16_REFINE) */
 } fbp_stage_stats;
 
 /* Library version (major*10000 + minor*100 + patch). */

@@ -61,14 +61,14 @@ class StageStats(ctypes.Structure):
                 ("refined_items", ctypes.c_uint64), ("fallback_candidates", ctypes.c_uint64),
                 ("lik_refined", ctypes.c_uint64), ("lik_exact_passes", ctypes.c_uint64),
                 ("passes", ctypes.c_uint32), ("spikes", ctypes.c_uint32),
-                ("lik_lazy_refined", ctypes.c_uint64)]
+                ("lik_lazy_refined", ctypes.c_uint64), ("lik_seq_refined", ctypes.c_uint64)]
 
     def as_dict(self):
         return {"passes": self.passes, "spikes": self.spikes, "candidates": int(self.candidates),
                 "refined_items": int(self.refined_items),
                 "fallback_candidates": int(self.fallback_candidates),
                 "lik_refined": int(self.lik_refined), "lik_exact_passes": int(self.lik_exact_passes),
-                "lik_lazy_refined": int(self.lik_lazy_refined),
+                "lik_lazy_refined": int(self.lik_lazy_refined), "lik_seq_refined": int(self.lik_seq_refined),
                 "ms": {STAGE_NAMES[i]: self.ms[i] for i in range(N_STAGES)},
                 "launches": {STAGE_NAMES[i]: int(self.launches[i]) for i in range(N_STAGES)},
                 "work": {STAGE_NAMES[i]: int(self.work[i]) for i in range(N_STAGES)}}

@@ -313,6 +313,7 @@ int launch_accept(u32 n, u32 C, u32 L, const float *thr, const u32 *win, const u
 }
 
 float tc_kappa(u32 C, u32 L, u32 Cg2);
+float tc_kappa_s(u32 C, u32 L);
 
 // Context for likelihood entries the tensor-core path left approximate.
 LazyLk lazy_ctx(const Workspace &w, const float *v, const float *T, const float *tss, u32 C, u32 L, u32 pass) {
@@ -322,6 +323,7 @@ LazyLk lazy_ctx(const Workspace &w, const float *v, const float *T, const float 
     z.tnorm = w.tc_tnorm; z.tabs = w.tc_tabs; z.tss = tss; z.texp = w.tc_texp;
     z.v = v; z.T = T; z.C = C; z.L = L;
     z.kappa_b = tc_kappa(C, L, w.tc_Cg2);
+    z.kappa_s = tc_kappa_s(C, L);
     z.refined = &w.cnt->lazy_ref;
     z.wlb = w.wlb; z.bm = w.bm_s;
     z.tag = 2u + (pass & 1u);
@@ -480,6 +482,16 @@ float tc_kappa(u32 C, u32 L, u32 Cg2) {
     return (float)(k * 1.01);
 }
 
+// Bound per unit of |SS_t / 2|: the reference's running sum starts at
+// -SS_t/2, and each of its C*L + 1 roundings is relative to a partial sum
+// that may be as large as |SS_t/2| + sum|t v| (the sum|t v| part is in
+// tc_kappa); plus the final fp32 addition of the approximation.
+float tc_kappa_s(u32 C, u32 L) {
+    const double u = 1.0 / 16777216.0;
+    const double n_ref = (double)C * L + 2;
+    return (float)((1.01 * n_ref * u + 4.0 * u) * 1.01);
+}
+
 // One pass of the tensor-core likelihood over the listed windows.
 int tc_likelihood_pass(const Workspace &w, const float *v, u32 n, u32 C, const float *T, u32 K, u32 L,
                        const float *tss, const u32 *win, const u32 *n_win, u32 max_windows, float *Lk,
@@ -491,6 +503,7 @@ int tc_likelihood_pass(const Workspace &w, const float *v, u32 n, u32 C, const f
     A.tmem_cols = w.tc_cols;
     A.nbuf = w.tc_nbuf;
     A.kappa_b = tc_kappa(C, L, w.tc_Cg2);
+    A.kappa_s = tc_kappa_s(C, L);
     A.v = v; A.T = T; A.tss = tss; A.tnorm = w.tc_tnorm; A.tabs = w.tc_tabs; A.texp = w.tc_texp; A.Tb = w.Tb;
     A.tb_bytes = (u32)((size_t)L * w.tc_Cg2 * w.tc_Np * 16);
     A.win = win; A.n_win = n_win; A.Lk = Lk;
@@ -507,10 +520,15 @@ int tc_likelihood_pass(const Workspace &w, const float *v, u32 n, u32 C, const f
     const size_t rsmem = tc_refine_smem_bytes(C, L);
     if (rsmem > 48 * 1024)
         FBP_CUDA(cudaFuncSetAttribute(k_tc_refine, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)rsmem));
+    // gamma: the reference's recursive sum of C*L + 1 terms (products
+    // rounded once each), plus the double sums' own error
+    const double u = 1.0 / 16777216.0, nr = (double)C * L + 2;
+    const double gamma = 1.01 * (nr * u / (1.0 - nr * u)) + 4.0 * nr * 1.1102230246251565e-16;
     k_tc_refine<<<sm_count() * 8, kRefThreads, rsmem, st>>>(v, n, C, T, K, L, tss, w.tc_ref_t, w.tc_ref_s,
                                                             w.tc_seg_s0, w.tc_seg_base, w.tc_seg_cnt,
                                                             reinterpret_cast<const u32 *>(&cnt->tc_refseg),
-                                                            w.tc_seg_cap, Lk);
+                                                            w.tc_seg_cap, Lk, lazy_ctx(w, v, T, tss, C, L, 0),
+                                                            gamma, &cnt->tc_seq);
     k_tc_gate<<<1, 1, 0, st>>>(cnt, w.tc_ref_cap, w.tc_seg_cap);
     FBP_LAUNCH_CHECK();
     int rc = launch_likelihood(v, n, C, T, K, L, tss, win, n_win, max_windows, Lk, st, &cnt->tc_overflow, w.apx);
@@ -789,6 +807,7 @@ int fbp_pursuit_chunk(float *voltage, uint32_t n, uint32_t C, const float *templ
             S.spikes = h_counts[3];
             S.work[FBP_STAGE_OVERLAP] = *(const u64 *)(h_counts + 8);
             S.lik_lazy_refined = ((const Counters *)h_counts)->lazy_ref;
+            S.lik_seq_refined = ((const Counters *)h_counts)->tc_seq;
             if (h_counts[4]) rc = fail(FBP_ERR_CAPACITY, "spike output holds %u spikes; more were found", spike_cap);
         }
     }

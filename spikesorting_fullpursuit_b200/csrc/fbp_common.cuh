@@ -39,7 +39,8 @@ struct Counters {
     u32 pad1;
     u64 scan_next;    // work counter of the overlap scan
     u64 tc_refseg;    // tensor-core refinement list: entries queued (high half), tile segments (low half)
-    u32 pad[10];
+    u64 tc_seq;       // refinement entries whose sign needed the reference's own sum (whole chunk)
+    u32 pad[8];
 };
 static_assert(sizeof(Counters) == 128, "Counters is one 128-byte line");
 

@@ -195,7 +195,8 @@ struct LazyLk {
     const int *texp;                  // [K]
     const float *v, *T;               // voltage (residual) and templates
     u32 C, L;
-    float kappa_b;
+    float kappa_b;                    // bound per unit of ||t|| ||window||
+    float kappa_s;                    // bound per unit of |SS_t / 2| (the reference's running sum starts there)
     u64 *refined;                     // count of entries refined on demand (may be NULL)
     const float *wlb;                 // [W] largest lower bound over each window's entries
     const float *bm;                  // [n] largest bound of a flagged entry of each sample
@@ -205,7 +206,8 @@ struct LazyLk {
 // The bound the tensor-core epilogue used for entry (t, s) (same formula).
 __device__ __forceinline__ float lazy_bound(const LazyLk &z, u32 t, u32 s, float approx) {
     const float sub = 2.98023223876953125e-08f * (ldexpf(z.tabs[t], -(int)z.kx[s]) + ldexpf(z.wa[s], -z.texp[t])) * 1.001f;
-    return z.kappa_b * z.tnorm[t] * z.wn[s] + sub + 2.384185791015625e-07f * (fabsf(z.tss[t]) + fabsf(approx));
+    return z.kappa_b * z.tnorm[t] * z.wn[s] + sub + z.kappa_s * fabsf(z.tss[t]) +
+           2.384185791015625e-07f * fabsf(approx);
 }
 
 // compute_maximum_likelihood (binary_pursuit.cl:216-252), reference order.

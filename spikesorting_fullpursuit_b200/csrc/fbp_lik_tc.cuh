@@ -18,17 +18,21 @@
 // fp16's 11 significant bits give a 2^-10 product bound where bf16 would give
 // 2^-7, with the same shared-memory footprint.
 //
-// Exactness: every value is either re-evaluated in the reference's order
-// (IEEE binary32, .cl:239-249) or provably <= 0.  With
-//   E(t,s) = kappa * ||t|| * ||window(s)|| + 2^-25 (||t||_1 / s_v + |window|_1 / s_t)
-//            + 2^-22 (|SS_t/2| + |approx|)
-// bounding |approx - reference| (fp16 rounding of both operands including
+// Exactness.  With
+//   E(t,s) = kappa * ||t|| * ||window(s)|| + 2^-25 (||t||_1 / s_v + |window|_1 / s_t) * 1.001
+//            + kappa_s * |SS_t/2| + 2^-22 |approx|
+// bounding |approx - reference| -- fp16 rounding of both operands including
 // subnormals, FP32 accumulation in any order, and the reference's own
-// rounding), entries
-// with approx + E > 0 go to the refinement list; the rest are stored as
-// approx, which is < 0 like the reference value.  Every later decision reads
-// such an entry only through "> 0" / "<= 0" tests (window argmax, check flag,
-// overlap skip rules and parse), so the pursuit is unchanged.
+// recursive sum (.cl:239-249), whose running value starts at -SS_t/2 and so
+// carries up to n*u*|SS_t/2| besides n*u*sum|t v| -- every entry is one of
+//   certainly <= 0  (approx + E <= 0): stored as approx; only its sign is
+//                   ever read (window argmax, check flag, overlap skip rules
+//                   and parse);
+//   certainly > 0   (approx - E > 0): stored as approx with a flag; its
+//                   reference value is computed when a decision needs it
+//                   (see LazyLk in fbp_kernels.cuh);
+//   uncertain       : queued and re-evaluated in the reference's order.
+// So the pursuit reads the reference's values wherever they matter.
 #pragma once
 #include <cuda_fp16.h>
 #include "fbp_kernels.cuh"
@@ -56,7 +60,8 @@ struct TcArgs {
     u32 rows_pad;                    // strip rows (128 + L - 1) padded to 8
     u32 nbuf;                        // strip / accumulator buffers (2: staging overlaps the epilogue)
     u32 tmem_cols;
-    float kappa_b;
+    float kappa_b;                   // bound per unit of ||t|| ||window||
+    float kappa_s;                   // bound per unit of |SS_t / 2|
     const float *v;                  // [C][n]
     const float *T;                  // [K][C][L] (exact refinement)
     const float *tss;                // [K]
@@ -231,7 +236,7 @@ k_lik_tc(TcArgs A) {
             ctk[t] = real ? A.kappa_b * A.tnorm[t] : 0.0f;
             ctb[t] = real ? 2.98023223876953125e-08f * 1.001f * ldexpf(1.0f, -A.texp[t]) : 0.0f;
             ctss[t] = real ? A.tss[t] : 0.0f;
-            cta[t] = real ? 2.384185791015625e-07f * fabsf(A.tss[t]) : 0.0f;
+            cta[t] = real ? A.kappa_s * fabsf(A.tss[t]) : 0.0f;
         }
     }
     __syncthreads();
@@ -560,7 +565,8 @@ k_lik_tc(TcArgs A) {
                     const float sc = tsc[t];
                     const float approx = __fadd_rn(sc != 0.0f ? __fmul_rn(a, sc) : ldexpf(a, -(kexp + A.texp[t])),
                                                    ctss[t]);
-                    // E = kappa ||t|| ||w|| + 2^-25 (|t|_1 / s_v + |w|_1 / s_t) * 1.001 + 2^-22 (|SS/2| + |approx|)
+                    // E = kappa ||t|| ||w|| + 2^-25 (|t|_1 / s_v + |w|_1 / s_t) * 1.001
+                    //     + kappa_s |SS/2| + 2^-22 |approx|
                     const float E = fmaf(ctk[t], wn, fmaf(ctb[t], wa, tsa[t]) + cta[t] +
                                                          2.384185791015625e-07f * fabsf(approx));
                     const bool pos = approx - E > 0.0f;      // certainly > 0: refined when a decision needs it
@@ -694,25 +700,37 @@ __global__ void k_tc_pack_templates(const float *__restrict__ T, u32 K, u32 C, u
     }
 }
 
-// Exact reference-order values of the refinement list
-// (compute_maximum_likelihood, binary_pursuit.cl:216-252).  One tile
-// segment per block; its entries are ordered by template.  The tile's
-// voltage (all channels) is staged once; each warp takes 32 consecutive
-// entries -- mostly one template, so the template reads are broadcasts --
-// and every lane advances its own entry's chain in the reference's
-// channel-major, lag-minor order.
+// The refinement list (entries whose tensor-core interval straddles 0).
+// One tile segment per block; its entries are ordered by template.  The
+// tile's voltage (all channels) is staged once; a warp takes one entry:
+//   1. its lanes form X = -SS_t/2 + sum t*v and S = |SS_t/2| + sum |t*v| in
+//      double (each product exact, the sums' own error negligible);
+//      the reference value R (compute_maximum_likelihood,
+//      binary_pursuit.cl:216-252) satisfies |R - X| <= gamma * S;
+//   2. X + gamma S <= 0: R <= 0, stored as float(X) (only its sign is read);
+//      X - gamma S > 0: R > 0, stored as float(X) and flagged approximate --
+//      the lazy bound E of the entry covers gamma * S, so its reference
+//      value is computed when a decision needs it;
+//   3. otherwise the warp computes R itself: lanes form the products (each
+//      rounded as in the reference), lane 0 adds them in the reference's
+//      order.
 constexpr int kRefThreads = 256;
 __host__ __device__ inline size_t tc_refine_smem_bytes(u32 C, u32 L) {
-    return ((size_t)C * (kTcM + L) + 8) * 4;
+    return ((size_t)C * (kTcM + L) + 8) * 4 + (size_t)(kRefThreads / 32) * kWarpChunk * 4;
 }
 __global__ void __launch_bounds__(kRefThreads)
 k_tc_refine(const float *__restrict__ v, u32 n, u32 C, const float *__restrict__ T, u32 K, u32 L,
             const float *__restrict__ tss, const u32 *__restrict__ ref_t, const u32 *__restrict__ ref_s,
             const u32 *__restrict__ seg_s0, const u32 *__restrict__ seg_base, const u32 *__restrict__ seg_cnt,
-            const u32 *__restrict__ seg_count, u32 seg_cap, float *__restrict__ Lk) {
+            const u32 *__restrict__ seg_count, u32 seg_cap, float *__restrict__ Lk, LazyLk z, double gamma,
+            u64 *__restrict__ n_seq) {
     extern __shared__ float rsm[];
     const u32 rl = kTcM + L;               // strip row length
+    const u32 CL = C * L;
+    const u32 lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    float *wbuf = rsm + ((size_t)C * rl + 8) + (size_t)warp * kWarpChunk;
     const u32 nseg = min(*seg_count, seg_cap);
+    u32 nseq = 0;
     for (u32 sg = blockIdx.x; sg < nseg; sg += gridDim.x) {
         const u32 s0 = seg_s0[sg], base = seg_base[sg], cnt = seg_cnt[sg];
         __syncthreads();
@@ -721,17 +739,57 @@ k_tc_refine(const float *__restrict__ v, u32 n, u32 C, const float *__restrict__
             rsm[x] = pos < n ? v[(size_t)c * n + pos] : 0.0f;
         }
         __syncthreads();
-        for (u32 e = threadIdx.x; e < cnt; e += blockDim.x) {
+        for (u32 e = warp; e < cnt; e += kRefThreads / 32) {
             const u32 t = ref_t[base + e], so = ref_s[base + e] - s0;
-            float acc = tss[t];
-            for (u32 c = 0; c < C; c++) {
-                const float *tp = T + ((size_t)t * C + c) * L;
-                const float *sp = rsm + (size_t)c * rl + so;
-                for (u32 i = 0; i < L; i++) acc = __fadd_rn(acc, __fmul_rn(__ldg(tp + i), sp[i]));
+            const float *tp = T + (size_t)t * CL;
+            double X = 0.0, S = 0.0;
+            for (u32 q = lane; q < CL; q += 32) {
+                const u32 c = q / L, i = q - c * L;
+                const double p = (double)__ldg(tp + q) * (double)rsm[(size_t)c * rl + so + i];
+                X += p;
+                S += fabs(p);
             }
-            Lk[(size_t)t * n + s0 + so] = acc;
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) {
+                X += __shfl_xor_sync(0xffffffffu, X, o);
+                S += __shfl_xor_sync(0xffffffffu, S, o);
+            }
+            X += (double)tss[t];
+            S += fabs((double)tss[t]);
+            const double bnd = gamma * S;
+            const size_t idx = (size_t)t * n + s0 + so;
+            if (X + bnd <= 0.0 || X - bnd > 0.0) {
+                if (lane == 0) {
+                    const float xf = (float)X;
+                    Lk[idx] = xf;
+                    if (X - bnd > 0.0) {                 // certainly > 0: refined on demand
+                        z.apx[idx] = 1;
+                        const u32 s = s0 + so;
+                        atomicMax(reinterpret_cast<int *>(const_cast<float *>(z.bm)) + s,
+                                  __float_as_int(lazy_bound(z, t, s, xf)));
+                    }
+                }
+                continue;
+            }
+            // sign still uncertain: the reference's own sum
+            float acc = tss[t];
+            for (u32 q0 = 0; q0 < CL; q0 += kWarpChunk) {
+                const u32 m = min(kWarpChunk, CL - q0);
+                for (u32 k = lane; k < m; k += 32) {
+                    const u32 q = q0 + k, c = q / L, i = q - c * L;
+                    wbuf[k] = __fmul_rn(__ldg(tp + q), rsm[(size_t)c * rl + so + i]);
+                }
+                __syncwarp();
+                if (lane == 0) acc = warp_chain(acc, wbuf, m);
+                __syncwarp();
+            }
+            if (lane == 0) {
+                Lk[idx] = acc;
+                nseq++;
+            }
         }
     }
+    if (n_seq && nseq) atomicAdd(n_seq, (u64)nseq);
 }
 
 }  // namespace fbp
