@@ -228,15 +228,15 @@ def main():
         step(False)
     torch.cuda.synchronize()
 
+    # timed steps: no per-stage timing, so each pass is one CUDA graph launch
     clocks = ClockSampler(local)
     barrier()
     torch.cuda.synchronize()
     clocks.start()
     ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    stats = []
     ev0.record(stream)
     for _ in range(args.steps):
-        stats.append(step(True))
+        step(False)
     ev1.record(stream)
     torch.cuda.synchronize()
     clock_info = clocks.stop()
@@ -249,38 +249,45 @@ def main():
     units_per_step = world * n * K
     value = units_per_step / (ms_step / 1e3)
 
-    # per-stage CUDA-event times inside the timed steps -> dominant stage roofline
-    stage_ms = np.zeros(_lib.N_STAGES)
-    work = np.zeros(_lib.N_STAGES)
-    launches = np.zeros(_lib.N_STAGES)
-    for s in stats:
-        stage_ms += np.array(s.ms[:])
-        work += np.array(s.work[:], dtype=np.float64)
-        launches += np.array(s.launches[:], dtype=np.float64)
+    # one more step with CUDA events around every stage (outside the timed
+    # region): the per-stage times, work and launches of a step
+    st_prof = step(True)
+    torch.cuda.synchronize()
+    stage_ms = np.array(st_prof.ms[:])
+    work = np.array(st_prof.work[:], dtype=np.float64)
+    launches = np.array(st_prof.launches[:], dtype=np.float64)
+    stats = [st_prof]
     Ct = template_channels(T.reshape(K, -1), C, L)
+    S_sh = 2 * nmax + 1
     hbm, tf_burst, tf_sust, peak_src = measured_peaks()
-    per_unit = {  # name: (bound, algorithmic units -> flops or bytes)
-        0: ("tensor", 2.0 * Ct * L, "TFLOP/s"),       # likelihood: 2*C_t*L flops per sample*template
-        1: ("hbm", 4.0, "GB/s"),                       # argmax: each scanned fp32 likelihood read once
-        2: ("tensor", 5.0 * C * L, "TFLOP/s"),        # overlap: 5*C*L flops per evaluated item
-        5: ("hbm", 8.0 * Ct * L, "GB/s"),             # residual: 8*C_t*L bytes per spike
+    cands = float(st_prof.candidates)
+    # stage: (bound, algorithmic flops or bytes of the stage per step)
+    alg_of = {
+        0: ("tensor", work[0] * 2.0 * Ct * L),          # likelihood: 2*C_t*L flops per sample*template
+        8: ("tensor", cands * 2.0 * Ct * L * K * S_sh),  # overlap tables: C_t*L MACs per (template, shift)
+        1: ("hbm", work[1] / 3.0 * 4.0),                # argmax: each likelihood entry of a listed window once
+        2: ("hbm", cands * 8.0 * K * S_sh),             # overlap search: tables and likelihood signs per candidate
+        5: ("hbm", work[5] * 8.0 * Ct * L),             # residual: read and write C_t*L fp32 per spike
     }
-    dom = max(per_unit, key=lambda i: stage_ms[i])
-    bound, per, unit = per_unit[dom]
-    alg = work[dom] * per
-    secs = stage_ms[dom] / 1e3
-    if bound == "tensor":
-        achieved = alg / secs / 1e12 if secs > 0 else 0.0
-        peak = tf_sust
-    else:
-        achieved = alg / secs / 1e9 if secs > 0 else 0.0
-        peak = hbm
-    roofline = {"bound": bound, "achieved": achieved, "peak": peak, "unit": unit,
-                "frac": achieved / peak if peak else None, "traffic": None,
-                "kernel": _lib.STAGE_NAMES[dom], "peak_source": peak_src + (" sustained" if bound == "tensor" else ""),
-                "launches_in_timed_region": int(launches[dom]),
-                "stage_ms_per_step": {_lib.STAGE_NAMES[i]: stage_ms[i] / args.steps for i in range(_lib.N_STAGES)}}
-    gpu_launches = int(launches.sum())
+    per_stage = {}
+    for i, (bound, alg) in alg_of.items():
+        secs = stage_ms[i] / 1e3
+        if secs <= 0 or alg <= 0:
+            continue
+        if bound == "tensor":
+            ach, peak, unit = alg / secs / 1e12, tf_sust, "TFLOP/s"
+        else:
+            ach, peak, unit = alg / secs / 1e9, hbm, "GB/s"
+        per_stage[_lib.STAGE_NAMES[i]] = {"bound": bound, "achieved": ach, "peak": peak, "unit": unit,
+                                          "frac": ach / peak if peak else None, "ms": stage_ms[i]}
+    dom = max(per_stage, key=lambda k: per_stage[k]["ms"])
+    d = per_stage[dom]
+    roofline = {"bound": d["bound"], "achieved": d["achieved"], "peak": d["peak"], "unit": d["unit"],
+                "frac": d["frac"], "traffic": None, "kernel": dom,
+                "peak_source": peak_src + (" sustained" if d["bound"] == "tensor" else ""),
+                "stages": per_stage,
+                "stage_ms_per_step": {_lib.STAGE_NAMES[i]: stage_ms[i] for i in range(_lib.N_STAGES)}}
+    gpu_launches = int(launches.sum()) * args.steps
 
     # end to end through the public API: host voltage (pinned) -> spikes on the host
     e2e = None

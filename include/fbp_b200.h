@@ -75,7 +75,10 @@ enum {
     FBP_STAGE_ACCEPT = 4,       /* accept, flags, spike compaction         */
     FBP_STAGE_RESIDUAL = 5,     /* path (c): residual subtract             */
     FBP_STAGE_LISTS = 6,        /* window/candidate list compaction, resets */
-    FBP_N_STAGES = 7
+    FBP_STAGE_LIK_REFINE = 7,   /* FBP_PREC_BF16_REFINE: entries whose sign the tensor-core
+                                   interval left open, settled exactly             */
+    FBP_STAGE_OVERLAP_TABLES = 8, /* FBP_OVERLAP_FAST: per-candidate correlation tables */
+    FBP_N_STAGES = 9
 };
 
 /* Per-stage counters of one fbp_pursuit_chunk call.  `ms` holds CUDA-event

@@ -50,8 +50,9 @@ SIGNATURES = {
 }
 
 
-N_STAGES = 7
-STAGE_NAMES = ["likelihood", "argmax", "overlap", "check", "accept", "residual", "lists"]
+N_STAGES = 9
+STAGE_NAMES = ["likelihood", "argmax", "overlap", "check", "accept", "residual", "lists", "lik_refine",
+               "overlap_tables"]
 
 
 class StageStats(ctypes.Structure):

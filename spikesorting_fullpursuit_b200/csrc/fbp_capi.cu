@@ -72,6 +72,7 @@ struct Workspace {
     u32 slots;
     float *NT, *sNT, *tnorm, *Q, *XMr, *XM, *H, *vn, *cand_lb, *ga_lo, *ga_hi, *ga_max, *ga_abs, *pool_hi;
     u32 *ga_bits, *seed_a1;
+    Counters *snap;                  // counts of the last pass
     OvConst *oc;
     u8 *cskip, *fallback, *need;
     u32 *pool_slot, *pool_item, *fb_slots, *fb_list;
@@ -129,6 +130,7 @@ Workspace layout(char *base, u32 n, u32 K, u32 L, u32 nmax, bool want_fast, u32 
         return p;
     };
     w.cnt = (Counters *)take(sizeof(Counters));
+    w.snap = (Counters *)take(sizeof(Counters));
     w.Lk = (float *)take((size_t)K * n * sizeof(float));
     w.best_idx = (u32 *)take(Wp * 4);
     w.best_lab = (u32 *)take(Wp * 4);
@@ -379,7 +381,7 @@ int ov_chunk_setup(const Workspace &w, const float *T, u32 K, u32 C, u32 L, u32 
 
 // One pass of the fast overlap recheck over the candidate list (device count
 // n_cand).  Returns the number of kernels launched in *launches.
-int ov_fast_pass(const Workspace &w, const OvArgs &A, Counters *cnt, cudaStream_t st, int *launches) {
+int ov_fast_tables(const Workspace &w, const OvArgs &A, Counters *cnt, cudaStream_t st, int *launches) {
     const u32 slots = w.slots;
     const u32 S = A.S;
     FBP_CUDA(cudaMemsetAsync(w.fallback, 0, align_up((size_t)slots + FBP_WINDOW_PAD, kCompactTile), st));
@@ -412,6 +414,16 @@ int ov_fast_pass(const Workspace &w, const OvArgs &A, Counters *cnt, cudaStream_
         k_ov_tables<<<grid_for((u64)slots * kTabThreads, kTabThreads, 4), kTabThreads, smem, st>>>(A);
         FBP_LAUNCH_CHECK();
     }
+    *launches = 2;
+    return FBP_OK;
+}
+
+// The search over the tables: rows, seed, scan, exact refinement of the
+// contenders, parse, and the exact kernel for candidates whose contenders did
+// not fit.
+int ov_fast_pass(const Workspace &w, const OvArgs &A, Counters *cnt, cudaStream_t st, int *launches) {
+    const u32 slots = w.slots;
+    const u32 S = A.S;
     k_ov_rows<<<grid_for((u64)slots * 32, kSeedThreads, 8), kSeedThreads, 0, st>>>(A);
     k_ov_seed<<<grid_for((u64)slots * A.K * 32, kSeedThreads, 8), kSeedThreads, 0, st>>>(A);
     const size_t scan_smem = scan_smem_bytes(S);
@@ -428,7 +440,7 @@ int ov_fast_pass(const Workspace &w, const OvArgs &A, Counters *cnt, cudaStream_
     fbp_window_state s{A.best_idx, A.best_lab, A.best_ll, A.ov_idx, A.ov_lab, nullptr, A.ovr};
     rc = launch_overlap(A.v, A.n, A.C, A.T, A.K, A.L, w.fb_list, &cnt->fb_count, slots, s, A.Lk, A.nmax, A.thr,
                         A.items_evaluated, st, A.lazy);
-    *launches = 15;
+    *launches = 10;
     return rc;
 }
 
@@ -492,7 +504,7 @@ float tc_kappa_s(u32 C, u32 L) {
     return (float)((1.01 * n_ref * u + 4.0 * u) * 1.01);
 }
 
-// One pass of the tensor-core likelihood over the listed windows.
+// One pass of the tensor-core likelihood over the listed windows: the tiles.
 int tc_likelihood_pass(const Workspace &w, const float *v, u32 n, u32 C, const float *T, u32 K, u32 L,
                        const float *tss, const u32 *win, const u32 *n_win, u32 max_windows, float *Lk,
                        Counters *cnt, cudaStream_t st, int *launches) {
@@ -517,6 +529,15 @@ int tc_likelihood_pass(const Workspace &w, const float *v, u32 n, u32 C, const f
     FBP_CUDA(cudaFuncSetAttribute(k_lik_tc<0>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     k_lik_tc<0><<<sm_count(), kTcThreads, smem, st>>>(A);
     FBP_LAUNCH_CHECK();
+    *launches = 1;
+    return FBP_OK;
+}
+
+// The same pass: the refinement list, and the FP32 kernel over the listed
+// windows when that list overflowed.
+int tc_refine_pass(const Workspace &w, const float *v, u32 n, u32 C, const float *T, u32 K, u32 L,
+                   const float *tss, const u32 *win, const u32 *n_win, u32 max_windows, float *Lk,
+                   Counters *cnt, cudaStream_t st, int *launches) {
     const size_t rsmem = tc_refine_smem_bytes(C, L);
     if (rsmem > 48 * 1024)
         FBP_CUDA(cudaFuncSetAttribute(k_tc_refine, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)rsmem));
@@ -532,7 +553,7 @@ int tc_likelihood_pass(const Workspace &w, const float *v, u32 n, u32 C, const f
     k_tc_gate<<<1, 1, 0, st>>>(cnt, w.tc_ref_cap, w.tc_seg_cap);
     FBP_LAUNCH_CHECK();
     int rc = launch_likelihood(v, n, C, T, K, L, tss, win, n_win, max_windows, Lk, st, &cnt->tc_overflow, w.apx);
-    *launches = 4;
+    *launches = 3;
     return rc;
 }
 
@@ -686,66 +707,142 @@ int fbp_pursuit_chunk(float *voltage, uint32_t n, uint32_t C, const float *templ
     const u32 R = overlap_neighbours(L, nmax);
     int rc = FBP_OK;
     u32 passes = 0;
-    for (;;) {
-        if (passes >= max_passes) { rc = fail(FBP_ERR_ITER_CAP, "no convergence after %u passes", passes); break; }
-        passes++;
+    // One pass (.py:538-731), entirely device-driven: every kernel reads its
+    // counts from device memory, so the same launches serve every pass.  The
+    // counts of the pass are snapshotted (w.snap) before the next pass's
+    // window list overwrites them.  `launched` receives the launches per stage.
+    auto enqueue_pass = [&](u32 pass, uint64_t *launched) -> int {
+        int rc2 = FBP_OK;
         // 1. likelihood over the listed windows (.py:538-549)
         timer.begin(FBP_STAGE_LIKELIHOOD);
         if (w.tc) {
             int nl = 0;
-            if ((rc = tc_likelihood_pass(w, voltage, n, C, templates, K, L, neg_half_ss, w.win, &w.cnt->n_win, W,
-                                         w.Lk, w.cnt, st, &nl)))
-                break;
-            S.launches[FBP_STAGE_LIKELIHOOD] += nl;
+            if ((rc2 = tc_likelihood_pass(w, voltage, n, C, templates, K, L, neg_half_ss, w.win, &w.cnt->n_win, W,
+                                          w.Lk, w.cnt, st, &nl)))
+                return rc2;
+            launched[FBP_STAGE_LIKELIHOOD] += nl;
+            timer.end(FBP_STAGE_LIKELIHOOD);
+            timer.begin(FBP_STAGE_LIK_REFINE);
+            if ((rc2 = tc_refine_pass(w, voltage, n, C, templates, K, L, neg_half_ss, w.win, &w.cnt->n_win, W,
+                                      w.Lk, w.cnt, st, &nl)))
+                return rc2;
+            launched[FBP_STAGE_LIK_REFINE] += nl;
+            timer.end(FBP_STAGE_LIK_REFINE);
+            timer.begin(FBP_STAGE_LIKELIHOOD);
         } else {
-            if ((rc = launch_likelihood(voltage, n, C, templates, K, L, neg_half_ss, w.win, &w.cnt->n_win, W,
-                                        w.Lk, st)))
-                break;
-            S.launches[FBP_STAGE_LIKELIHOOD] += 1;
+            if ((rc2 = launch_likelihood(voltage, n, C, templates, K, L, neg_half_ss, w.win, &w.cnt->n_win, W,
+                                         w.Lk, st)))
+                return rc2;
+            launched[FBP_STAGE_LIKELIHOOD] += 1;
         }
         timer.end(FBP_STAGE_LIKELIHOOD);
         // 2. per-window argmax over all templates (.py:551-562)
         timer.begin(FBP_STAGE_ARGMAX);
-        const LazyLk lz = lazy_ctx(w, voltage, templates, neg_half_ss, C, L, passes);
-        if ((rc = launch_argmax(n, L, K, w.win, &w.cnt->n_win, W, s, w.Lk, st, lz))) break;
-        S.launches[FBP_STAGE_ARGMAX] += 1;
+        const LazyLk lz = lazy_ctx(w, voltage, templates, neg_half_ss, C, L, pass);
+        if ((rc2 = launch_argmax(n, L, K, w.win, &w.cnt->n_win, W, s, w.Lk, st, lz))) return rc2;
+        launched[FBP_STAGE_ARGMAX] += 1;
         timer.end(FBP_STAGE_ARGMAX);
         // 3. candidates = nonzero(overlap_recheck) (.py:565-569), 4. recheck (.py:570-661)
         if (do_overlap_recheck) {
             timer.begin(FBP_STAGE_LISTS);
-            if ((rc = compact(w.ovr, W, w.cand, &w.cnt->n_cand, w.tile_counts, st))) break;
-            S.launches[FBP_STAGE_LISTS] += 3;
+            if ((rc2 = compact(w.ovr, W, w.cand, &w.cnt->n_cand, w.tile_counts, st))) return rc2;
+            launched[FBP_STAGE_LISTS] += 3;
             timer.end(FBP_STAGE_LISTS);
             timer.begin(FBP_STAGE_OVERLAP);
             if (w.fast) {
                 int nl = 0;
                 OvArgs A = ov_args(w, voltage, n, C, templates, K, L, nmax, thresholds, s, w.Lk, w.cand,
                                    &w.cnt->n_cand, w.cnt, neg_half_ss);
-                if ((rc = ov_fast_pass(w, A, w.cnt, st, &nl))) break;
-                S.launches[FBP_STAGE_OVERLAP] += nl;
+                timer.end(FBP_STAGE_OVERLAP);
+                timer.begin(FBP_STAGE_OVERLAP_TABLES);
+                if ((rc2 = ov_fast_tables(w, A, w.cnt, st, &nl))) return rc2;
+                launched[FBP_STAGE_OVERLAP_TABLES] += nl;
+                timer.end(FBP_STAGE_OVERLAP_TABLES);
+                timer.begin(FBP_STAGE_OVERLAP);
+                if ((rc2 = ov_fast_pass(w, A, w.cnt, st, &nl))) return rc2;
+                launched[FBP_STAGE_OVERLAP] += nl;
             } else {
-                if ((rc = launch_overlap(voltage, n, C, templates, K, L, w.cand, &w.cnt->n_cand, W, s, w.Lk,
-                                         nmax, thresholds, &w.cnt->ov_items, st, lz)))
-                    break;
-                S.launches[FBP_STAGE_OVERLAP] += 1;
+                if ((rc2 = launch_overlap(voltage, n, C, templates, K, L, w.cand, &w.cnt->n_cand, W, s, w.Lk,
+                                          nmax, thresholds, &w.cnt->ov_items, st, lz)))
+                    return rc2;
+                launched[FBP_STAGE_OVERLAP] += 1;
             }
             timer.end(FBP_STAGE_OVERLAP);
             timer.begin(FBP_STAGE_CHECK);
-            if ((rc = launch_check_overlap(n, L, w.cand, &w.cnt->n_cand, W, s, w.ovr2, st))) break;
-            S.launches[FBP_STAGE_CHECK] += 2;
+            if ((rc2 = launch_check_overlap(n, L, w.cand, &w.cnt->n_cand, W, s, w.ovr2, st))) return rc2;
+            launched[FBP_STAGE_CHECK] += 2;
             timer.end(FBP_STAGE_CHECK);
         }
         // 5. accept (.py:663-671)
         timer.begin(FBP_STAGE_ACCEPT);
-        if ((rc = launch_accept(n, C, L, thresholds, w.win, &w.cnt->n_win, W, s, w.active, w.has,
-                                w.flags_out, w.acc_list, w.spk_idx, w.spk_lab, w.spk_win, &w.cnt->n_spk,
-                                w.tile_counts, st)))
-            break;
-        S.launches[FBP_STAGE_ACCEPT] += 6;
+        if ((rc2 = launch_accept(n, C, L, thresholds, w.win, &w.cnt->n_win, W, s, w.active, w.has,
+                                 w.flags_out, w.acc_list, w.spk_idx, w.spk_lab, w.spk_win, &w.cnt->n_spk,
+                                 w.tile_counts, st)))
+            return rc2;
+        launched[FBP_STAGE_ACCEPT] += 6;
         timer.end(FBP_STAGE_ACCEPT);
-        // 6. count; stop when nothing was added (.py:673-676)
-        FBP_CUDA(cudaMemcpyAsync(h_counts, w.cnt, sizeof(Counters), cudaMemcpyDeviceToHost, st));
-        FBP_CUDA(cudaStreamSynchronize(st));
+        // 6. the pass's counts (.py:673-676 stops when nothing was added)
+        FBP_CUDA(cudaMemcpyAsync(w.snap, w.cnt, sizeof(Counters), cudaMemcpyDeviceToDevice, st));
+        // 7. reset overlap flags, next list = nonzero(flags), reset flags (.py:678-700)
+        timer.begin(FBP_STAGE_LISTS);
+        FBP_CUDA(cudaMemsetAsync(w.ovr, 0, wb, st));
+        if ((rc2 = compact(w.flags_out, W, w.win, &w.cnt->n_win, w.tile_counts, st))) return rc2;
+        k_mark_active<<<grid_for(W, 256), 256, 0, st>>>(w.flags_out, w.active, W, w.tc ? w.wlb : nullptr);
+        FBP_CUDA(cudaMemsetAsync(w.flags, 0, wb, st));
+        // 8. keep the spikes (.py:702-710)
+        k_append_spikes<<<grid_for(W, 256), 256, 0, st>>>(w.spk_idx, w.spk_lab, w.cnt, spike_idx, spike_lab,
+                                                           spike_cap);
+        k_commit_total<<<1, 1, 0, st>>>(w.cnt, spike_cap);
+        FBP_LAUNCH_CHECK();
+        launched[FBP_STAGE_LISTS] += 6;
+        timer.end(FBP_STAGE_LISTS);
+        // 9. subtract them (.py:712-731)
+        timer.begin(FBP_STAGE_RESIDUAL);
+        if (lz.apx) {
+            k_lazy_freeze<<<grid_for((u64)W * 32, 256, 8), 256, 0, st>>>(n, L, K, w.spk_idx, w.spk_lab,
+                                                                        &w.cnt->n_spk, w.active, W, w.Lk, lz);
+            FBP_LAUNCH_CHECK();
+            launched[FBP_STAGE_RESIDUAL] += 1;
+        }
+        k_residual<<<grid_for((u64)W * 256, 256, 16), 256, 0, st>>>(voltage, n, C, templates, K, L, w.spk_idx,
+                                                                    w.spk_lab, &w.cnt->n_spk, 0, R);
+        FBP_LAUNCH_CHECK();
+        launched[FBP_STAGE_RESIDUAL] += 1;
+        timer.end(FBP_STAGE_RESIDUAL);
+        return FBP_OK;
+    };
+    // Without per-stage timing each pass is one CUDA graph launch (one graph
+    // per pass parity: the parity is the only thing that differs).
+    const bool use_graph = profile == 0;
+    cudaGraphExec_t gx[2] = {nullptr, nullptr};
+    uint64_t glaunch[2][FBP_N_STAGES] = {};
+    for (;;) {
+        if (passes >= max_passes) { rc = fail(FBP_ERR_ITER_CAP, "no convergence after %u passes", passes); break; }
+        passes++;
+        const u32 par = passes & 1u;
+        if (use_graph) {
+            if (!gx[par]) {
+                cudaError_t e = cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal);
+                if (e != cudaSuccess) { rc = fail(FBP_ERR_CUDA, "graph capture: %s", cudaGetErrorString(e)); break; }
+                const int rc2 = enqueue_pass(passes, glaunch[par]);
+                cudaGraph_t g = nullptr;
+                e = cudaStreamEndCapture(st, &g);
+                if (rc2) { if (g) cudaGraphDestroy(g); rc = rc2; break; }
+                if (e == cudaSuccess) e = cudaGraphInstantiate(&gx[par], g, 0);
+                if (g) cudaGraphDestroy(g);
+                if (e != cudaSuccess) { rc = fail(FBP_ERR_CUDA, "graph capture: %s", cudaGetErrorString(e)); break; }
+            }
+            cudaError_t e = cudaGraphLaunch(gx[par], st);
+            if (e != cudaSuccess) { rc = fail(FBP_ERR_CUDA, "graph launch: %s", cudaGetErrorString(e)); break; }
+            for (int k = 0; k < FBP_N_STAGES; k++) S.launches[k] += glaunch[par][k];
+        } else {
+            if ((rc = enqueue_pass(passes, S.launches))) break;
+        }
+        {
+            cudaError_t e = cudaMemcpyAsync(h_counts, w.snap, sizeof(Counters), cudaMemcpyDeviceToHost, st);
+            if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+            if (e != cudaSuccess) { rc = fail(FBP_ERR_CUDA, "pass %u: %s", passes, cudaGetErrorString(e)); break; }
+        }
         timer.collect();
         const u32 added = h_counts[2];
         const u32 nwin = h_counts[0];
@@ -753,50 +850,28 @@ int fbp_pursuit_chunk(float *voltage, uint32_t n, uint32_t C, const float *templ
             const Counters *hc = (const Counters *)h_counts;
             if (hc->tc_err) { rc = fail(FBP_ERR_CUDA, "tensor-core likelihood: bounded wait %u gave up", hc->tc_err); break; }
             S.lik_refined += std::min((u32)(hc->tc_refseg >> 32), w.tc_ref_cap);
+            S.work[FBP_STAGE_LIK_REFINE] += std::min((u32)(hc->tc_refseg >> 32), w.tc_ref_cap);
             S.lik_exact_passes += hc->tc_overflow;
         }
         S.work[FBP_STAGE_LIKELIHOOD] += (u64)nwin * L * K;
         S.work[FBP_STAGE_ARGMAX] += (u64)nwin * 3 * L * K;
         S.work[FBP_STAGE_ACCEPT] += nwin;
+        S.work[FBP_STAGE_RESIDUAL] += added;
         if (do_overlap_recheck) {
             S.work[FBP_STAGE_CHECK] += h_counts[1];
             S.candidates += h_counts[1];
+            if (w.fast) S.work[FBP_STAGE_OVERLAP_TABLES] += h_counts[1];
             if (w.fast) {
                 S.refined_items += ((const Counters *)h_counts)->ov_ref;
                 S.fallback_candidates += h_counts[7];
             }
         }
         if (pass_counts)
-            FBP_CUDA(cudaMemcpyAsync(pass_counts + passes - 1, &w.cnt->n_spk, 4, cudaMemcpyDeviceToDevice, st));
+            FBP_CUDA(cudaMemcpyAsync(pass_counts + passes - 1, &w.snap->n_spk, 4, cudaMemcpyDeviceToDevice, st));
         if (added == 0) break;
-        // 7. reset overlap flags, next list = nonzero(flags), reset flags (.py:678-700)
-        timer.begin(FBP_STAGE_LISTS);
-        FBP_CUDA(cudaMemsetAsync(w.ovr, 0, wb, st));
-        if ((rc = compact(w.flags_out, W, w.win, &w.cnt->n_win, w.tile_counts, st))) break;
-        k_mark_active<<<grid_for(W, 256), 256, 0, st>>>(w.flags_out, w.active, W, w.tc ? w.wlb : nullptr);
-        FBP_CUDA(cudaMemsetAsync(w.flags, 0, wb, st));
-        // 8. keep the spikes (.py:702-710)
-        k_append_spikes<<<grid_for(added, 256), 256, 0, st>>>(w.spk_idx, w.spk_lab, w.cnt, spike_idx,
-                                                               spike_lab, spike_cap);
-        k_commit_total<<<1, 1, 0, st>>>(w.cnt, spike_cap);
-        FBP_LAUNCH_CHECK();
-        S.launches[FBP_STAGE_LISTS] += 6;
-        timer.end(FBP_STAGE_LISTS);
-        // 9. subtract them (.py:712-731)
-        timer.begin(FBP_STAGE_RESIDUAL);
-        if (lz.apx) {
-            k_lazy_freeze<<<grid_for((u64)added * 32, 256, 8), 256, 0, st>>>(n, L, K, w.spk_idx, w.spk_lab, added,
-                                                                           w.active, W, w.Lk, lz);
-            FBP_LAUNCH_CHECK();
-            S.launches[FBP_STAGE_RESIDUAL] += 1;
-        }
-        k_residual<<<grid_for((u64)added * 256, 256, 16), 256, 0, st>>>(
-            voltage, n, C, templates, K, L, w.spk_idx, w.spk_lab, nullptr, added, R);
-        FBP_LAUNCH_CHECK();
-        S.launches[FBP_STAGE_RESIDUAL] += 1;
-        S.work[FBP_STAGE_RESIDUAL] += added;
-        timer.end(FBP_STAGE_RESIDUAL);
     }
+    for (auto &g : gx)
+        if (g) cudaGraphExecDestroy(g);
     if (rc == FBP_OK || rc == FBP_ERR_ITER_CAP) {
         cudaError_t e = cudaMemcpyAsync(h_counts, w.cnt, sizeof(Counters), cudaMemcpyDeviceToHost, st);
         if (e == cudaSuccess) e = cudaStreamSynchronize(st);

@@ -290,7 +290,9 @@ __device__ __forceinline__ float warp_lk_exact(const LazyLk &z, const float *Lk,
 // now, from the voltage it was computed from.
 __global__ void __launch_bounds__(256)
 k_lazy_freeze(u32 n, u32 L, u32 K, const u32 *__restrict__ idx, const u32 *__restrict__ lab,
-              u32 m, const u8 *__restrict__ next_active, u32 W, float *__restrict__ Lk, LazyLk z) {
+              const u32 *__restrict__ m_dev, const u8 *__restrict__ next_active, u32 W, float *__restrict__ Lk,
+              LazyLk z) {
+    const u32 m = *m_dev;
     __shared__ float fbuf[8][kWarpChunk];
     const u32 lane = threadIdx.x & 31;
     const u32 warps_per_block = blockDim.x >> 5;
