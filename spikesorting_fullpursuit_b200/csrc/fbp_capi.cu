@@ -711,27 +711,27 @@ int fbp_pursuit_chunk(float *voltage, uint32_t n, uint32_t C, const float *templ
     // counts from device memory, so the same launches serve every pass.  The
     // counts of the pass are snapshotted (w.snap) before the next pass's
     // window list overwrites them.  `launched` receives the launches per stage.
-    auto enqueue_pass = [&](u32 pass, uint64_t *launched) -> int {
+    auto enqueue_pass = [&](u32 pass, uint64_t *launched, cudaStream_t q) -> int {
         int rc2 = FBP_OK;
         // 1. likelihood over the listed windows (.py:538-549)
         timer.begin(FBP_STAGE_LIKELIHOOD);
         if (w.tc) {
             int nl = 0;
             if ((rc2 = tc_likelihood_pass(w, voltage, n, C, templates, K, L, neg_half_ss, w.win, &w.cnt->n_win, W,
-                                          w.Lk, w.cnt, st, &nl)))
+                                          w.Lk, w.cnt, q, &nl)))
                 return rc2;
             launched[FBP_STAGE_LIKELIHOOD] += nl;
             timer.end(FBP_STAGE_LIKELIHOOD);
             timer.begin(FBP_STAGE_LIK_REFINE);
             if ((rc2 = tc_refine_pass(w, voltage, n, C, templates, K, L, neg_half_ss, w.win, &w.cnt->n_win, W,
-                                      w.Lk, w.cnt, st, &nl)))
+                                      w.Lk, w.cnt, q, &nl)))
                 return rc2;
             launched[FBP_STAGE_LIK_REFINE] += nl;
             timer.end(FBP_STAGE_LIK_REFINE);
             timer.begin(FBP_STAGE_LIKELIHOOD);
         } else {
             if ((rc2 = launch_likelihood(voltage, n, C, templates, K, L, neg_half_ss, w.win, &w.cnt->n_win, W,
-                                         w.Lk, st)))
+                                         w.Lk, q)))
                 return rc2;
             launched[FBP_STAGE_LIKELIHOOD] += 1;
         }
@@ -739,13 +739,13 @@ int fbp_pursuit_chunk(float *voltage, uint32_t n, uint32_t C, const float *templ
         // 2. per-window argmax over all templates (.py:551-562)
         timer.begin(FBP_STAGE_ARGMAX);
         const LazyLk lz = lazy_ctx(w, voltage, templates, neg_half_ss, C, L, pass);
-        if ((rc2 = launch_argmax(n, L, K, w.win, &w.cnt->n_win, W, s, w.Lk, st, lz))) return rc2;
+        if ((rc2 = launch_argmax(n, L, K, w.win, &w.cnt->n_win, W, s, w.Lk, q, lz))) return rc2;
         launched[FBP_STAGE_ARGMAX] += 1;
         timer.end(FBP_STAGE_ARGMAX);
         // 3. candidates = nonzero(overlap_recheck) (.py:565-569), 4. recheck (.py:570-661)
         if (do_overlap_recheck) {
             timer.begin(FBP_STAGE_LISTS);
-            if ((rc2 = compact(w.ovr, W, w.cand, &w.cnt->n_cand, w.tile_counts, st))) return rc2;
+            if ((rc2 = compact(w.ovr, W, w.cand, &w.cnt->n_cand, w.tile_counts, q))) return rc2;
             launched[FBP_STAGE_LISTS] += 3;
             timer.end(FBP_STAGE_LISTS);
             timer.begin(FBP_STAGE_OVERLAP);
@@ -755,21 +755,21 @@ int fbp_pursuit_chunk(float *voltage, uint32_t n, uint32_t C, const float *templ
                                    &w.cnt->n_cand, w.cnt, neg_half_ss);
                 timer.end(FBP_STAGE_OVERLAP);
                 timer.begin(FBP_STAGE_OVERLAP_TABLES);
-                if ((rc2 = ov_fast_tables(w, A, w.cnt, st, &nl))) return rc2;
+                if ((rc2 = ov_fast_tables(w, A, w.cnt, q, &nl))) return rc2;
                 launched[FBP_STAGE_OVERLAP_TABLES] += nl;
                 timer.end(FBP_STAGE_OVERLAP_TABLES);
                 timer.begin(FBP_STAGE_OVERLAP);
-                if ((rc2 = ov_fast_pass(w, A, w.cnt, st, &nl))) return rc2;
+                if ((rc2 = ov_fast_pass(w, A, w.cnt, q, &nl))) return rc2;
                 launched[FBP_STAGE_OVERLAP] += nl;
             } else {
                 if ((rc2 = launch_overlap(voltage, n, C, templates, K, L, w.cand, &w.cnt->n_cand, W, s, w.Lk,
-                                          nmax, thresholds, &w.cnt->ov_items, st, lz)))
+                                          nmax, thresholds, &w.cnt->ov_items, q, lz)))
                     return rc2;
                 launched[FBP_STAGE_OVERLAP] += 1;
             }
             timer.end(FBP_STAGE_OVERLAP);
             timer.begin(FBP_STAGE_CHECK);
-            if ((rc2 = launch_check_overlap(n, L, w.cand, &w.cnt->n_cand, W, s, w.ovr2, st))) return rc2;
+            if ((rc2 = launch_check_overlap(n, L, w.cand, &w.cnt->n_cand, W, s, w.ovr2, q))) return rc2;
             launched[FBP_STAGE_CHECK] += 2;
             timer.end(FBP_STAGE_CHECK);
         }
@@ -777,34 +777,34 @@ int fbp_pursuit_chunk(float *voltage, uint32_t n, uint32_t C, const float *templ
         timer.begin(FBP_STAGE_ACCEPT);
         if ((rc2 = launch_accept(n, C, L, thresholds, w.win, &w.cnt->n_win, W, s, w.active, w.has,
                                  w.flags_out, w.acc_list, w.spk_idx, w.spk_lab, w.spk_win, &w.cnt->n_spk,
-                                 w.tile_counts, st)))
+                                 w.tile_counts, q)))
             return rc2;
         launched[FBP_STAGE_ACCEPT] += 6;
         timer.end(FBP_STAGE_ACCEPT);
         // 6. the pass's counts (.py:673-676 stops when nothing was added)
-        FBP_CUDA(cudaMemcpyAsync(w.snap, w.cnt, sizeof(Counters), cudaMemcpyDeviceToDevice, st));
+        FBP_CUDA(cudaMemcpyAsync(w.snap, w.cnt, sizeof(Counters), cudaMemcpyDeviceToDevice, q));
         // 7. reset overlap flags, next list = nonzero(flags), reset flags (.py:678-700)
         timer.begin(FBP_STAGE_LISTS);
-        FBP_CUDA(cudaMemsetAsync(w.ovr, 0, wb, st));
-        if ((rc2 = compact(w.flags_out, W, w.win, &w.cnt->n_win, w.tile_counts, st))) return rc2;
-        k_mark_active<<<grid_for(W, 256), 256, 0, st>>>(w.flags_out, w.active, W, w.tc ? w.wlb : nullptr);
-        FBP_CUDA(cudaMemsetAsync(w.flags, 0, wb, st));
+        FBP_CUDA(cudaMemsetAsync(w.ovr, 0, wb, q));
+        if ((rc2 = compact(w.flags_out, W, w.win, &w.cnt->n_win, w.tile_counts, q))) return rc2;
+        k_mark_active<<<grid_for(W, 256), 256, 0, q>>>(w.flags_out, w.active, W, w.tc ? w.wlb : nullptr);
+        FBP_CUDA(cudaMemsetAsync(w.flags, 0, wb, q));
         // 8. keep the spikes (.py:702-710)
-        k_append_spikes<<<grid_for(W, 256), 256, 0, st>>>(w.spk_idx, w.spk_lab, w.cnt, spike_idx, spike_lab,
+        k_append_spikes<<<grid_for(W, 256), 256, 0, q>>>(w.spk_idx, w.spk_lab, w.cnt, spike_idx, spike_lab,
                                                            spike_cap);
-        k_commit_total<<<1, 1, 0, st>>>(w.cnt, spike_cap);
+        k_commit_total<<<1, 1, 0, q>>>(w.cnt, spike_cap);
         FBP_LAUNCH_CHECK();
         launched[FBP_STAGE_LISTS] += 6;
         timer.end(FBP_STAGE_LISTS);
         // 9. subtract them (.py:712-731)
         timer.begin(FBP_STAGE_RESIDUAL);
         if (lz.apx) {
-            k_lazy_freeze<<<grid_for((u64)W * 32, 256, 8), 256, 0, st>>>(n, L, K, w.spk_idx, w.spk_lab,
+            k_lazy_freeze<<<grid_for((u64)W * 32, 256, 8), 256, 0, q>>>(n, L, K, w.spk_idx, w.spk_lab,
                                                                         &w.cnt->n_spk, w.active, W, w.Lk, lz);
             FBP_LAUNCH_CHECK();
             launched[FBP_STAGE_RESIDUAL] += 1;
         }
-        k_residual<<<grid_for((u64)W * 256, 256, 16), 256, 0, st>>>(voltage, n, C, templates, K, L, w.spk_idx,
+        k_residual<<<grid_for((u64)W * 256, 256, 16), 256, 0, q>>>(voltage, n, C, templates, K, L, w.spk_idx,
                                                                     w.spk_lab, &w.cnt->n_spk, 0, R);
         FBP_LAUNCH_CHECK();
         launched[FBP_STAGE_RESIDUAL] += 1;
@@ -812,9 +812,12 @@ int fbp_pursuit_chunk(float *voltage, uint32_t n, uint32_t C, const float *templ
         return FBP_OK;
     };
     // Without per-stage timing each pass is one CUDA graph launch (one graph
-    // per pass parity: the parity is the only thing that differs).
+    // per pass parity: the parity is the only thing that differs).  Graphs
+    // are captured on a private stream (the caller's may be the legacy
+    // default stream, which cannot capture) and launched on the caller's.
     const bool use_graph = profile == 0;
     cudaGraphExec_t gx[2] = {nullptr, nullptr};
+    cudaStream_t cs = nullptr;
     uint64_t glaunch[2][FBP_N_STAGES] = {};
     for (;;) {
         if (passes >= max_passes) { rc = fail(FBP_ERR_ITER_CAP, "no convergence after %u passes", passes); break; }
@@ -822,11 +825,12 @@ int fbp_pursuit_chunk(float *voltage, uint32_t n, uint32_t C, const float *templ
         const u32 par = passes & 1u;
         if (use_graph) {
             if (!gx[par]) {
-                cudaError_t e = cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal);
+                cudaError_t e = cs ? cudaSuccess : cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking);
+                if (e == cudaSuccess) e = cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal);
                 if (e != cudaSuccess) { rc = fail(FBP_ERR_CUDA, "graph capture: %s", cudaGetErrorString(e)); break; }
-                const int rc2 = enqueue_pass(passes, glaunch[par]);
+                const int rc2 = enqueue_pass(passes, glaunch[par], cs);
                 cudaGraph_t g = nullptr;
-                e = cudaStreamEndCapture(st, &g);
+                e = cudaStreamEndCapture(cs, &g);
                 if (rc2) { if (g) cudaGraphDestroy(g); rc = rc2; break; }
                 if (e == cudaSuccess) e = cudaGraphInstantiate(&gx[par], g, 0);
                 if (g) cudaGraphDestroy(g);
@@ -836,7 +840,7 @@ int fbp_pursuit_chunk(float *voltage, uint32_t n, uint32_t C, const float *templ
             if (e != cudaSuccess) { rc = fail(FBP_ERR_CUDA, "graph launch: %s", cudaGetErrorString(e)); break; }
             for (int k = 0; k < FBP_N_STAGES; k++) S.launches[k] += glaunch[par][k];
         } else {
-            if ((rc = enqueue_pass(passes, S.launches))) break;
+            if ((rc = enqueue_pass(passes, S.launches, st))) break;
         }
         {
             cudaError_t e = cudaMemcpyAsync(h_counts, w.snap, sizeof(Counters), cudaMemcpyDeviceToHost, st);
@@ -872,6 +876,7 @@ int fbp_pursuit_chunk(float *voltage, uint32_t n, uint32_t C, const float *templ
     }
     for (auto &g : gx)
         if (g) cudaGraphExecDestroy(g);
+    if (cs) cudaStreamDestroy(cs);
     if (rc == FBP_OK || rc == FBP_ERR_ITER_CAP) {
         cudaError_t e = cudaMemcpyAsync(h_counts, w.cnt, sizeof(Counters), cudaMemcpyDeviceToHost, st);
         if (e == cudaSuccess) e = cudaStreamSynchronize(st);
