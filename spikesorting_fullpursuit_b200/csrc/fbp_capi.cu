@@ -613,6 +613,40 @@ u32 overlap_neighbours(u32 L, u32 nmax) {
     return 3 + ceil_div(2 * nmax, L);
 }
 
+// Instantiated pass graphs of recent calls.  A graph holds the pointers and
+// sizes it was captured with, so it is reused only by a call with all of them
+// equal (device, buffers, sizes and modes): it then enqueues exactly the
+// launches a fresh capture would.
+struct PassGraphs {
+    std::vector<uint64_t> key;
+    cudaGraphExec_t gx[2] = {nullptr, nullptr};
+    uint64_t launches[2][FBP_N_STAGES] = {};
+};
+std::mutex g_graph_mu;
+std::vector<PassGraphs> g_graphs;            // most recent last
+constexpr size_t kGraphCacheSize = 8;
+
+// Pinned host copy of the counters and a capture stream, per thread and device.
+struct HostScratch {
+    int dev = -1;
+    u32 *counts = nullptr;
+    cudaStream_t capture = nullptr;
+};
+thread_local HostScratch t_scratch;
+int host_scratch(HostScratch **out) {
+    int dev = 0;
+    FBP_CUDA(cudaGetDevice(&dev));
+    HostScratch &h = t_scratch;
+    if (h.dev != dev) {
+        if (!h.counts) FBP_CUDA(cudaMallocHost(&h.counts, sizeof(Counters)));
+        h.capture = nullptr;                 // streams belong to the device they were made on
+        FBP_CUDA(cudaStreamCreateWithFlags(&h.capture, cudaStreamNonBlocking));
+        h.dev = dev;
+    }
+    *out = &h;
+    return FBP_OK;
+}
+
 }  // namespace
 
 extern "C" {
@@ -702,8 +736,9 @@ int fbp_pursuit_chunk(float *voltage, uint32_t n, uint32_t C, const float *templ
         timer.end(FBP_STAGE_OVERLAP);
     }
 
-    u32 *h_counts = nullptr;
-    FBP_CUDA(cudaMallocHost(&h_counts, sizeof(Counters)));
+    HostScratch *hs = nullptr;
+    if (int e = host_scratch(&hs)) return e;
+    u32 *h_counts = hs->counts;
     const u32 R = overlap_neighbours(L, nmax);
     int rc = FBP_OK;
     u32 passes = 0;
@@ -816,17 +851,33 @@ int fbp_pursuit_chunk(float *voltage, uint32_t n, uint32_t C, const float *templ
     // are captured on a private stream (the caller's may be the legacy
     // default stream, which cannot capture) and launched on the caller's.
     const bool use_graph = profile == 0;
-    cudaGraphExec_t gx[2] = {nullptr, nullptr};
-    cudaStream_t cs = nullptr;
-    uint64_t glaunch[2][FBP_N_STAGES] = {};
+    PassGraphs pg;
+    if (use_graph) {
+        int dev = 0;
+        cudaGetDevice(&dev);
+        pg.key = {(uint64_t)dev, (uint64_t)(uintptr_t)voltage, n, C, (uint64_t)(uintptr_t)templates, K, L,
+                  (uint64_t)(uintptr_t)neg_half_ss, (uint64_t)(uintptr_t)thresholds, nmax,
+                  (uint64_t)do_overlap_recheck, (uint64_t)precision, (uint64_t)overlap_method,
+                  (uint64_t)(uintptr_t)workspace, (uint64_t)workspace_bytes, (uint64_t)(uintptr_t)spike_idx,
+                  (uint64_t)(uintptr_t)spike_lab, spike_cap};
+        std::lock_guard<std::mutex> lk(g_graph_mu);
+        for (size_t i = 0; i < g_graphs.size(); i++)
+            if (g_graphs[i].key == pg.key) {
+                pg = g_graphs[i];
+                g_graphs.erase(g_graphs.begin() + i);   // back in the cache when this call ends
+                break;
+            }
+    }
+    cudaGraphExec_t *gx = pg.gx;
+    uint64_t (*glaunch)[FBP_N_STAGES] = pg.launches;
+    cudaStream_t cs = hs->capture;
     for (;;) {
         if (passes >= max_passes) { rc = fail(FBP_ERR_ITER_CAP, "no convergence after %u passes", passes); break; }
         passes++;
         const u32 par = passes & 1u;
         if (use_graph) {
             if (!gx[par]) {
-                cudaError_t e = cs ? cudaSuccess : cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking);
-                if (e == cudaSuccess) e = cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal);
+                cudaError_t e = cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal);
                 if (e != cudaSuccess) { rc = fail(FBP_ERR_CUDA, "graph capture: %s", cudaGetErrorString(e)); break; }
                 const int rc2 = enqueue_pass(passes, glaunch[par], cs);
                 cudaGraph_t g = nullptr;
@@ -874,9 +925,15 @@ int fbp_pursuit_chunk(float *voltage, uint32_t n, uint32_t C, const float *templ
             FBP_CUDA(cudaMemcpyAsync(pass_counts + passes - 1, &w.snap->n_spk, 4, cudaMemcpyDeviceToDevice, st));
         if (added == 0) break;
     }
-    for (auto &g : gx)
-        if (g) cudaGraphExecDestroy(g);
-    if (cs) cudaStreamDestroy(cs);
+    if (use_graph && (gx[0] || gx[1])) {
+        std::lock_guard<std::mutex> lk(g_graph_mu);
+        g_graphs.push_back(pg);
+        if (g_graphs.size() > kGraphCacheSize) {
+            for (auto &g : g_graphs.front().gx)
+                if (g) cudaGraphExecDestroy(g);
+            g_graphs.erase(g_graphs.begin());
+        }
+    }
     if (rc == FBP_OK || rc == FBP_ERR_ITER_CAP) {
         cudaError_t e = cudaMemcpyAsync(h_counts, w.cnt, sizeof(Counters), cudaMemcpyDeviceToHost, st);
         if (e == cudaSuccess) e = cudaStreamSynchronize(st);
@@ -893,7 +950,6 @@ int fbp_pursuit_chunk(float *voltage, uint32_t n, uint32_t C, const float *templ
     }
     *n_passes_host = passes;
     S.passes = passes;
-    cudaFreeHost(h_counts);
     return rc;
 }
 
