@@ -73,6 +73,9 @@ struct Workspace {
     float *NT, *sNT, *tnorm, *Q, *XMr, *XM, *H, *vn, *cand_lb, *ga_lo, *ga_hi, *ga_max, *ga_abs, *pool_hi;
     u32 *ga_bits, *seed_a1;
     Counters *snap;                  // counts of the last pass
+    u32 *tsup, *tperm, *grange;      // template channel supports, order, group ranges
+    u32 *grange32;                   // group ranges of 32 slots (masked overlap tables)
+    bool masked_tables = false;      // templates occupy narrow channel ranges
     OvConst *oc;
     u8 *cskip, *fallback, *need;
     u32 *pool_slot, *pool_item, *fb_slots, *fb_list;
@@ -131,6 +134,10 @@ Workspace layout(char *base, u32 n, u32 K, u32 L, u32 nmax, bool want_fast, u32 
     };
     w.cnt = (Counters *)take(sizeof(Counters));
     w.snap = (Counters *)take(sizeof(Counters));
+    w.tsup = (u32 *)take((size_t)K * 8);
+    w.tperm = (u32 *)take((size_t)K * 4);
+    w.grange = (u32 *)take((size_t)ceil_div(K, kLikTplPerBlock) * 8);
+    w.grange32 = (u32 *)take((size_t)ceil_div(K, kTabMGroup) * 8);
     w.Lk = (float *)take((size_t)K * n * sizeof(float));
     w.best_idx = (u32 *)take(Wp * 4);
     w.best_lab = (u32 *)take(Wp * 4);
@@ -237,7 +244,8 @@ int compact(const u8 *f, u32 W, u32 *list, u32 *count_dev, u32 *tile_counts, cud
 
 int launch_likelihood(const float *v, u32 n, u32 C, const float *T, u32 K, u32 L, const float *tss,
                       const u32 *win, const u32 *n_win_dev, u32 max_windows, float *Lk,
-                      cudaStream_t st, const u32 *gate = nullptr, u8 *apx = nullptr) {
+                      cudaStream_t st, const u32 *gate = nullptr, u8 *apx = nullptr,
+                      const u32 *tperm = nullptr, const u32 *grange = nullptr) {
     const size_t smem = (size_t)kLikChanChunk * (kLikTile + L) * sizeof(float);
     static size_t configured = 0;
     if (smem > 48 * 1024 && smem > configured) {
@@ -247,7 +255,8 @@ int launch_likelihood(const float *v, u32 n, u32 C, const float *T, u32 K, u32 L
     }
     const u64 items = (u64)max_windows * ceil_div(K, kLikTplPerBlock);
     const int grid = grid_for(items * kLikThreads, kLikThreads, 16);
-    k_likelihood_fp32<<<grid, kLikThreads, smem, st>>>(v, n, C, T, K, L, tss, win, n_win_dev, Lk, gate, apx);
+    k_likelihood_fp32<<<grid, kLikThreads, smem, st>>>(v, n, C, T, K, L, tss, win, n_win_dev, Lk, gate, apx,
+                                                       tperm, grange);
     FBP_LAUNCH_CHECK();
     return FBP_OK;
 }
@@ -346,6 +355,7 @@ OvArgs ov_args(const Workspace &w, const float *v, u32 n, u32 C, const float *T,
     A.cand_lb = w.cand_lb;
     A.ga_lo = w.ga_lo; A.ga_hi = w.ga_hi; A.ga_bits = w.ga_bits; A.ga_max = w.ga_max; A.ga_abs = w.ga_abs;
     A.seed_a1 = w.seed_a1;
+    A.tsup = w.tsup;
     A.pool_slot = w.pool_slot; A.pool_item = w.pool_item; A.pool_hi = w.pool_hi; A.pool_cap = w.pool_cap;
     A.refined = &cnt->ov_ref;
     A.scan_next = &cnt->scan_next;
@@ -367,9 +377,10 @@ OvArgs ov_args(const Workspace &w, const float *v, u32 n, u32 C, const float *T,
 // Per-chunk tables of the fast overlap recheck (templates are fixed).
 int ov_chunk_setup(const Workspace &w, const float *T, u32 K, u32 C, u32 L, u32 nmax, cudaStream_t st) {
     const u32 S = 2 * nmax + 1;
-    k_ov_chunk_tables<<<grid_for((u64)K * S, 256), 256, 0, st>>>(T, K, C, L, nmax, w.NT, w.sNT, w.tnorm, w.oc);
+    k_ov_chunk_tables<<<grid_for((u64)K * S, 256), 256, 0, st>>>(T, K, C, L, nmax, w.NT, w.sNT, w.tnorm, w.oc,
+                                                                  w.tsup);
     const u64 rows = (u64)K * K * (2 * L - 1);
-    k_ov_q_table<<<grid_for(rows, 128, 16), 128, 0, st>>>(T, K, C, L, w.Q);
+    k_ov_q_table<<<grid_for(rows, 128, 16), 128, 0, st>>>(T, K, C, L, w.Q, w.tsup);
     const size_t xm_smem = (size_t)(2 * L - 1) * (L + 1) * 4;
     if (xm_smem > 48 * 1024)
         FBP_CUDA(cudaFuncSetAttribute(k_ov_xm, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)xm_smem));
@@ -406,6 +417,13 @@ int ov_fast_tables(const Workspace &w, const OvArgs &A, Counters *cnt, cudaStrea
         const size_t smem = tc_smem_bytes(A.L, w.tc_Cg2, w.tc_Np, w.tc_nbuf);
         FBP_CUDA(cudaFuncSetAttribute(k_lik_tc<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
         k_lik_tc<1><<<sm_count(), kTcThreads, smem, st>>>(T);
+        FBP_LAUNCH_CHECK();
+    } else if (w.masked_tables) {
+        const size_t smem = tables_m_smem_bytes(S, A.L);
+        if (smem > 48 * 1024)
+            FBP_CUDA(cudaFuncSetAttribute(k_ov_tables_m, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        k_ov_tables_m<<<grid_for((u64)slots * ceil_div(A.K, kTabMGroup) * kTabMThreads, kTabMThreads, 4),
+                        kTabMThreads, smem, st>>>(A, w.tperm, w.tsup, w.grange32);
         FBP_LAUNCH_CHECK();
     } else {
         const size_t smem = tables_smem_bytes(S, A.K, A.L);
@@ -552,7 +570,8 @@ int tc_refine_pass(const Workspace &w, const float *v, u32 n, u32 C, const float
                                                             gamma, &cnt->tc_seq);
     k_tc_gate<<<1, 1, 0, st>>>(cnt, w.tc_ref_cap, w.tc_seg_cap);
     FBP_LAUNCH_CHECK();
-    int rc = launch_likelihood(v, n, C, T, K, L, tss, win, n_win, max_windows, Lk, st, &cnt->tc_overflow, w.apx);
+    int rc = launch_likelihood(v, n, C, T, K, L, tss, win, n_win, max_windows, Lk, st, &cnt->tc_overflow, w.apx,
+                               w.tperm, w.grange);
     *launches = 3;
     return rc;
 }
@@ -716,7 +735,20 @@ int fbp_pursuit_chunk(float *voltage, uint32_t n, uint32_t C, const float *templ
     FBP_CUDA(cudaMemsetAsync(w.ovr2, 0, wb, st));
     FBP_CUDA(cudaMemsetAsync(w.active, 0, wb, st));
     k_iota_windows<<<grid_for(W, 256), 256, 0, st>>>(w.win, w.active, W, w.cnt);
+    k_template_support<<<1, 256, 0, st>>>(templates, K, C, L, w.tsup, w.tperm, w.grange, kLikTplPerBlock,
+                                          w.grange32, kTabMGroup);
     FBP_LAUNCH_CHECK();
+    if (w.fast && do_overlap_recheck && !w.tc) {
+        // the masked overlap tables pay off when the template groups touch
+        // well under all channels (one small read-back per chunk)
+        const u32 ng = ceil_div(K, kTabMGroup);
+        std::vector<u32> gr(2 * (size_t)ng);
+        FBP_CUDA(cudaMemcpyAsync(gr.data(), w.grange32, gr.size() * 4, cudaMemcpyDeviceToHost, st));
+        FBP_CUDA(cudaStreamSynchronize(st));
+        u64 span = 0;
+        for (u32 g = 0; g < ng; g++) span += gr[2 * g + 1] - gr[2 * g];
+        w.masked_tables = 2 * span < (u64)ng * C && 2 * nmax + 1 <= 32u * kTabMShiftChunks;
+    }
     S.launches[FBP_STAGE_LISTS] += 1;
     timer.end(FBP_STAGE_LISTS);
     if (w.tc) {
@@ -766,7 +798,7 @@ int fbp_pursuit_chunk(float *voltage, uint32_t n, uint32_t C, const float *templ
             timer.begin(FBP_STAGE_LIKELIHOOD);
         } else {
             if ((rc2 = launch_likelihood(voltage, n, C, templates, K, L, neg_half_ss, w.win, &w.cnt->n_win, W,
-                                         w.Lk, q)))
+                                         w.Lk, q, nullptr, nullptr, w.tperm, w.grange)))
                 return rc2;
             launched[FBP_STAGE_LIKELIHOOD] += 1;
         }
@@ -859,7 +891,7 @@ int fbp_pursuit_chunk(float *voltage, uint32_t n, uint32_t C, const float *templ
                   (uint64_t)(uintptr_t)neg_half_ss, (uint64_t)(uintptr_t)thresholds, nmax,
                   (uint64_t)do_overlap_recheck, (uint64_t)precision, (uint64_t)overlap_method,
                   (uint64_t)(uintptr_t)workspace, (uint64_t)workspace_bytes, (uint64_t)(uintptr_t)spike_idx,
-                  (uint64_t)(uintptr_t)spike_lab, spike_cap};
+                  (uint64_t)(uintptr_t)spike_lab, spike_cap, (uint64_t)w.masked_tables};
         std::lock_guard<std::mutex> lk(g_graph_mu);
         for (size_t i = 0; i < g_graphs.size(); i++)
             if (g_graphs[i].key == pg.key) {

@@ -95,6 +95,56 @@ __global__ void k_mark_active(const u8 *__restrict__ flags, u8 *__restrict__ act
 // starting from float32(-0.5*SS) -- exactly the reference's sequence.
 // ---------------------------------------------------------------------------
 constexpr int kLikThreads = 128;
+
+// Per chunk: each template's non-zero channel range [lo, hi) (tsup), the
+// template order sorted by (lo, id) (tperm), and per group of kLikTplPerBlock
+// consecutive slots the union of their ranges (grange).  One block.
+__global__ void k_template_support(const float *__restrict__ T, u32 K, u32 C, u32 L, u32 *__restrict__ tsup,
+                                   u32 *__restrict__ tperm, u32 *__restrict__ grange, u32 group,
+                                   u32 *__restrict__ grange2, u32 group2) {
+    for (u32 t = threadIdx.x; t < K; t += blockDim.x) {
+        u32 lo = C, hi = 0;
+        for (u32 c = 0; c < C; c++) {
+            const float *tp = T + ((size_t)t * C + c) * L;
+            bool nz = false;
+            for (u32 i = 0; i < L && !nz; i++) nz = tp[i] != 0.0f;
+            if (nz) { lo = min(lo, c); hi = c + 1; }
+        }
+        if (hi == 0) lo = 0;                         // all-zero template: empty range
+        tsup[2 * t] = lo;
+        tsup[2 * t + 1] = hi;
+    }
+    __syncthreads();
+    for (u32 t = threadIdx.x; t < K; t += blockDim.x) {
+        const u32 lo = tsup[2 * t];
+        u32 rank = 0;
+        for (u32 o = 0; o < K; o++) {
+            const u32 lo2 = tsup[2 * o];
+            rank += (lo2 < lo || (lo2 == lo && o < t)) ? 1u : 0u;
+        }
+        tperm[rank] = t;
+    }
+    __syncthreads();
+    for (int pass = 0; pass < 2; pass++) {
+        const u32 gs = pass ? group2 : group;
+        u32 *gr = pass ? grange2 : grange;
+        if (!gr) continue;
+        const u32 ng = (K + gs - 1) / gs;
+        for (u32 g = threadIdx.x; g < ng; g += blockDim.x) {
+            u32 lo = C, hi = 0;
+            for (u32 j = g * gs; j < min(K, (g + 1) * gs); j++) {
+                const u32 t = tperm[j];
+                if (tsup[2 * t + 1] > tsup[2 * t]) {
+                    lo = min(lo, tsup[2 * t]);
+                    hi = max(hi, tsup[2 * t + 1]);
+                }
+            }
+            if (hi == 0) lo = 0;
+            gr[2 * g] = lo;
+            gr[2 * g + 1] = hi;
+        }
+    }
+}
 constexpr int kLikQ = 4;             // templates per warp
 constexpr int kLikR = 4;             // samples per lane
 constexpr int kLikTile = 32 * kLikR; // 128 samples
@@ -105,7 +155,7 @@ __global__ void __launch_bounds__(kLikThreads)
 k_likelihood_fp32(const float *__restrict__ v, u32 n, u32 C, const float *__restrict__ T, u32 K, u32 L,
                   const float *__restrict__ tss, const u32 *__restrict__ win,
                   const u32 *__restrict__ n_win_dev, float *__restrict__ Lk, const u32 *__restrict__ gate,
-                  u8 *__restrict__ apx) {
+                  u8 *__restrict__ apx, const u32 *__restrict__ tperm, const u32 *__restrict__ grange) {
     extern __shared__ float strip[];   // kLikChanChunk x (kLikTile + L)
     if (gate && *gate == 0) return;    // only run when the gate asks for it
     const u32 n_win = *n_win_dev;
@@ -118,15 +168,25 @@ k_likelihood_fp32(const float *__restrict__ v, u32 n, u32 C, const float *__rest
         const u32 kg = (u32)(item % kgroups);
         const u32 sw = w * L;
         const u32 ew = min((w + 1) * L, n);
-        const u32 t0 = kg * kLikTplPerBlock + warp * kLikQ;
+        const u32 slot0 = kg * kLikTplPerBlock + warp * kLikQ;
+        // templates of this warp (slot order sorted by support when masked)
+        u32 tq[kLikQ];
+#pragma unroll
+        for (int q = 0; q < kLikQ; q++) {
+            const u32 sl = min(slot0 + q, K - 1);
+            tq[q] = tperm ? tperm[sl] : sl;
+        }
+        // channels where some template of the group is non-zero (the others
+        // add exact zeros to the reference's sum)
+        const u32 cbeg = grange ? grange[2 * kg] : 0u, cend = grange ? grange[2 * kg + 1] : C;
         for (u32 s0 = sw; s0 < ew; s0 += kLikTile) {
             float acc[kLikQ][kLikR];
 #pragma unroll
             for (int q = 0; q < kLikQ; q++)
 #pragma unroll
-                for (int r = 0; r < kLikR; r++) acc[q][r] = (t0 + q < K) ? tss[t0 + q] : 0.0f;
-            for (u32 c0 = 0; c0 < C; c0 += kLikChanChunk) {
-                const u32 cc = min((u32)kLikChanChunk, C - c0);
+                for (int r = 0; r < kLikR; r++) acc[q][r] = (slot0 + q < K) ? tss[tq[q]] : 0.0f;
+            for (u32 c0 = cbeg; c0 < cend; c0 += kLikChanChunk) {
+                const u32 cc = min((u32)kLikChanChunk, cend - c0);
                 __syncthreads();
                 for (u32 e = threadIdx.x; e < cc * stride; e += blockDim.x) {
                     const u32 c = e / stride, x = e % stride;
@@ -138,8 +198,7 @@ k_likelihood_fp32(const float *__restrict__ v, u32 n, u32 C, const float *__rest
                     const float *sp = strip + c * stride + lane;
                     const float *tp[kLikQ];
 #pragma unroll
-                    for (int q = 0; q < kLikQ; q++)
-                        tp[q] = T + ((size_t)min(t0 + q, K - 1) * C + (c0 + c)) * L;
+                    for (int q = 0; q < kLikQ; q++) tp[q] = T + ((size_t)tq[q] * C + (c0 + c)) * L;
                     for (u32 i = 0; i < L; i++) {
                         float tv[kLikQ], vv[kLikR];
 #pragma unroll
@@ -156,13 +215,13 @@ k_likelihood_fp32(const float *__restrict__ v, u32 n, u32 C, const float *__rest
             }
 #pragma unroll
             for (int q = 0; q < kLikQ; q++) {
-                if (t0 + q >= K) continue;
+                if (slot0 + q >= K) continue;
 #pragma unroll
                 for (int r = 0; r < kLikR; r++) {
                     const u32 s = s0 + lane + 32 * r;
                     if (s < ew && s < s0 + kLikTile) {
-                        Lk[(size_t)(t0 + q) * n + s] = (s + L >= n) ? 0.0f : acc[q][r];
-                        if (apx) apx[(size_t)(t0 + q) * n + s] = 0;
+                        Lk[(size_t)tq[q] * n + s] = (s + L >= n) ? 0.0f : acc[q][r];
+                        if (apx) apx[(size_t)tq[q] * n + s] = 0;
                     }
                 }
             }

@@ -63,6 +63,7 @@ struct OvArgs {
     float *ga_max, *ga_abs;          // [slot]     largest in-bounds hi(a), largest |hi(a)|
     unsigned long long *scan_next;   // next (candidate, template) pair of the scan
     u32 *seed_a1;                    // [slot]     in-bounds row a of largest lower bound
+    const u32 *tsup;                 // [K][2] non-zero channel range of each template (may be NULL)
     u32 *pool_total;                 // appended entries this pass
     u32 pool_cap;
     u32 *pool_slot;                  // [pool_cap]
@@ -95,14 +96,15 @@ __device__ __forceinline__ float warp_max_f(float x) {
 // square root, tnorm[t] = ||t||; kappa from the number of non-zero channels.
 __global__ void k_ov_chunk_tables(const float *__restrict__ T, u32 K, u32 C, u32 L, u32 nmax,
                                   float *__restrict__ NT, float *__restrict__ sNT,
-                                  float *__restrict__ tnorm, OvConst *oc) {
+                                  float *__restrict__ tnorm, OvConst *oc, const u32 *__restrict__ tsup) {
     const u32 S = 2 * nmax + 1;
     for (u32 e = blockIdx.x * blockDim.x + threadIdx.x; e < K * S; e += gridDim.x * blockDim.x) {
         const u32 t = e / S, b = e % S;
         const int d = (int)b - (int)nmax;
         const int j0 = max(0, d), j1 = min((int)L, (int)L + d);
         double acc = 0.0;
-        for (u32 c = 0; c < C; c++) {
+        const u32 clo = tsup ? tsup[2 * t] : 0u, chi = tsup ? tsup[2 * t + 1] : C;
+        for (u32 c = clo; c < chi; c++) {
             const float *tp = T + ((size_t)t * C + c) * L;
             for (int j = j0; j < j1; j++) {
                 const double x = tp[j - d];
@@ -148,13 +150,17 @@ __global__ void k_ov_chunk_tables(const float *__restrict__ T, u32 K, u32 C, u32
 
 // Q[k0][t][ri][m] = sum_{m' < m} sum_c T[k0][c][m'] * T[t][c][m'+r], r = ri-(L-1).
 // One thread per (k0, t, ri) row, accumulated in double, stored in float.
-__global__ void k_ov_q_table(const float *__restrict__ T, u32 K, u32 C, u32 L, float *__restrict__ Q) {
+__global__ void k_ov_q_table(const float *__restrict__ T, u32 K, u32 C, u32 L, float *__restrict__ Q,
+                             const u32 *__restrict__ tsup) {
     const u32 R = 2 * L - 1;
     const u64 rows = (u64)K * K * R;
     for (u64 e = (u64)blockIdx.x * blockDim.x + threadIdx.x; e < rows; e += (u64)gridDim.x * blockDim.x) {
         const u32 ri = (u32)(e % R);
         const u32 t = (u32)((e / R) % K);
         const u32 k0 = (u32)(e / ((u64)R * K));
+        // channels where both templates can be non-zero (tsup: [lo, hi) per template)
+        const u32 clo = tsup ? max(tsup[2 * k0], tsup[2 * t]) : 0u;
+        const u32 chi = tsup ? min(tsup[2 * k0 + 1], tsup[2 * t + 1]) : C;
         const int r = (int)ri - (int)(L - 1);
         float *q = Q + e * (L + 1);
         double acc = 0.0;
@@ -162,7 +168,7 @@ __global__ void k_ov_q_table(const float *__restrict__ T, u32 K, u32 C, u32 L, f
         for (u32 m = 0; m < L; m++) {
             const int mt = (int)m + r;
             if (mt >= 0 && mt < (int)L) {
-                for (u32 c = 0; c < C; c++)
+                for (u32 c = clo; c < chi; c++)
                     acc += (double)T[((size_t)k0 * C + c) * L + m] * (double)T[((size_t)t * C + c) * L + mt];
             }
             q[m + 1] = (float)acc;
@@ -279,6 +285,100 @@ k_ov_tables(OvArgs A) {
                             A.H[((size_t)g * K + t) * S + b] = acc[i][j] - 0.5f * A.NT[(size_t)t * S + b];
                     }
                 }
+            }
+        }
+    }
+}
+
+// H[g][t][b] for masked templates (each non-zero on a narrow channel range):
+// block = (candidate, group of 32 templates in support order); the group's
+// channels of the window, zero-padded by n_max on both sides, are staged in
+// chunks; warp w takes slots 4w..4w+3 of the group, lane l the shifts
+// b = l + 32k, and each (channel, lag) step is one broadcast template value
+// times a contiguous row of the window.  Only the templates' own channels
+// are summed (the others add zero).  FP32 FMA in any order: the error bound
+// of the tables covers it.
+constexpr int kTabMThreads = 256;
+constexpr int kTabMGroup = 32;
+constexpr int kTabMChan = 16;            // staged channels per chunk
+constexpr int kTabMShiftChunks = 16;     // S <= 512
+__host__ __device__ inline size_t tables_m_smem_bytes(u32 S, u32 L) {
+    return (size_t)kTabMChan * (S + L - 1) * 4;
+}
+__global__ void __launch_bounds__(kTabMThreads)
+k_ov_tables_m(OvArgs A, const u32 *__restrict__ tperm, const u32 *__restrict__ tsup,
+              const u32 *__restrict__ grange32) {
+    extern __shared__ float wp[];                   // [kTabMChan][S + L - 1]
+    const u32 S = A.S, K = A.K, L = A.L, nmax = A.nmax;
+    const u32 P = S + L - 1;
+    const u32 warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const u32 nk = (S + 31) / 32;
+    const u32 ng = (K + kTabMGroup - 1) / kTabMGroup;
+    const u32 nc = *A.n_cand;
+    for (u64 item = blockIdx.x; item < (u64)nc * ng; item += gridDim.x) {
+        const u32 g = (u32)(item / ng), tg = (u32)(item % ng);
+        if (A.cskip[g]) continue;
+        const u32 i0 = A.best_idx[A.cand[g]];
+        const u32 glo = grange32[2 * tg], ghi = grange32[2 * tg + 1];
+        u32 tq[4], lo[4], hi[4];
+        u32 wlo = 0xffffffffu, whi = 0;
+#pragma unroll
+        for (int q = 0; q < 4; q++) {
+            const u32 sl = tg * kTabMGroup + warp * 4 + q;
+            tq[q] = sl < K ? tperm[sl] : 0u;
+            lo[q] = sl < K ? tsup[2 * tq[q]] : 0u;
+            hi[q] = sl < K ? tsup[2 * tq[q] + 1] : 0u;
+            if (hi[q] > lo[q]) { wlo = min(wlo, lo[q]); whi = max(whi, hi[q]); }
+        }
+        float acc[4][kTabMShiftChunks];
+#pragma unroll
+        for (int q = 0; q < 4; q++)
+#pragma unroll
+            for (int k = 0; k < kTabMShiftChunks; k++) acc[q][k] = 0.0f;
+        for (u32 c0 = glo; c0 < ghi; c0 += kTabMChan) {
+            const u32 cc = min((u32)kTabMChan, ghi - c0);
+            __syncthreads();
+            for (u32 e = threadIdx.x; e < cc * P; e += blockDim.x) {
+                const u32 c = e / P, x = e % P;
+                const int rel = (int)x - (int)nmax;          // position relative to i0
+                wp[e] = (rel >= 0 && rel < (int)L) ? A.v[(size_t)(c0 + c) * A.n + i0 + rel] : 0.0f;
+            }
+            __syncthreads();
+            const u32 cb = max(c0, wlo), ce = min(c0 + cc, whi);
+            for (u32 c = cb; c < ce; c++) {
+                const float *row = wp + (size_t)(c - c0) * P + lane;
+                const float *tp[4];
+                bool on[4];
+#pragma unroll
+                for (int q = 0; q < 4; q++) {
+                    on[q] = c >= lo[q] && c < hi[q];
+                    tp[q] = A.T + ((size_t)tq[q] * A.C + c) * L;
+                }
+                for (u32 m = 0; m < L; m++) {
+                    float tv[4];
+#pragma unroll
+                    for (int q = 0; q < 4; q++) tv[q] = on[q] ? __ldg(tp[q] + m) : 0.0f;
+#pragma unroll
+                    for (int k = 0; k < kTabMShiftChunks; k++) {
+                        if ((u32)k >= nk) break;
+                        // m + b <= P - 1 for every b < S; lanes past S read nothing
+                        const float wv = (lane + 32u * k < S) ? row[m + 32 * k] : 0.0f;
+#pragma unroll
+                        for (int q = 0; q < 4; q++) acc[q][k] = fmaf(tv[q], wv, acc[q][k]);
+                    }
+                }
+            }
+        }
+#pragma unroll
+        for (int q = 0; q < 4; q++) {
+            const u32 sl = tg * kTabMGroup + warp * 4 + q;
+            if (sl >= K) continue;
+            const u32 t = tq[q];
+#pragma unroll
+            for (int k = 0; k < kTabMShiftChunks; k++) {
+                const u32 b = lane + 32 * k;
+                if ((u32)k < nk && b < S)
+                    A.H[((size_t)g * K + t) * S + b] = acc[q][k] - 0.5f * A.NT[(size_t)t * S + b];
             }
         }
     }
@@ -701,8 +801,14 @@ __device__ float overlap_item_exact_global(const OvArgs &A, u32 lab, u32 bidx, u
     const u32 L = A.L, C = A.C;
     const u32 afix = bidx + a - A.nmax, ashift = bidx + b - A.nmax;
     const int fa = (int)bidx - (int)afix, sa = (int)bidx - (int)ashift;
+    // channels where either template is non-zero (elsewhere both terms are 0)
+    u32 clo = 0, chi = C;
+    if (A.tsup) {
+        clo = min(A.tsup[2 * lab], A.tsup[2 * t]);
+        chi = max(A.tsup[2 * lab + 1], A.tsup[2 * t + 1]);
+    }
     float cml = 0.0f;
-    for (u32 c = 0; c < C; c++) {
+    for (u32 c = clo; c < chi; c++) {
         const float *f = A.T + ((size_t)lab * C + c) * L;
         const float *sp = A.T + ((size_t)t * C + c) * L;
         const float *vv = A.v + (size_t)c * A.n + bidx;
