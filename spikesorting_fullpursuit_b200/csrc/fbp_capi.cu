@@ -59,6 +59,13 @@ int sm_count() {
     return cached;
 }
 
+// A template group of the tensor-core likelihood: columns t0..t0+nt of the
+// support order (tperm), channels [clo, clo + Cg) of the recording.
+struct TcGroup {
+    u32 t0, nt, clo, Cg, Cg2, Np, nbuf, cols;
+    size_t tb_off;                   // offset of its packed templates in Tb (uint4 units)
+};
+
 // Device workspace of one chunk: sub-buffers at 256-byte boundaries.
 struct Workspace {
     float *Lk;
@@ -86,7 +93,13 @@ struct Workspace {
     u32 stiles;
     // tensor-core likelihood (present when `tc`)
     bool tc;
-    u32 tc_Cg2, tc_Np, tc_cols, tc_ref_cap, tc_nbuf;
+    u32 tc_ref_cap;
+    u32 tc_gmax;                     // template groups the buffers hold
+    std::vector<TcGroup> tcg;        // this chunk's groups (planned from the template supports)
+    u32 tc_cg2max, tc_cmax;          // largest channel groups / channels of a group
+    u32 *tc_gdesc;                   // [group][3]: t0, clo, Cg (device)
+    u32 *tgrp;                       // [K] group of each template (device)
+    u32 *tc_seg_grp;                 // [seg_cap] group of each refinement segment
     uint4 *Tb;
     float *tc_tnorm, *tc_tabs;
     int *tc_texp;
@@ -95,6 +108,7 @@ struct Workspace {
     signed char *kx_s;
     u32 *tc_ref_t, *tc_ref_s, *tc_seg_s0, *tc_seg_base, *tc_seg_cnt;
     u32 tc_seg_cap;
+    u32 n;                           // samples of the chunk
     size_t bytes;
 };
 
@@ -110,16 +124,59 @@ bool fast_overlap_fits(u32 K, u32 L, u32 nmax) {
 
 size_t window_bytes_u8(u32 W) { return align_up((size_t)W + FBP_WINDOW_PAD, kCompactTile); }
 
-// The tensor-core likelihood keeps all templates of a chunk in shared memory.
-// Two strip / accumulator buffers when they fit (staging overlaps the
-// epilogue), else one.
-bool tc_fits(u32 C, u32 K, u32 L, u32 *Cg2, u32 *Np, u32 *nbuf) {
-    *Cg2 = ((C + 15) / 16) * 2;
-    *Np = ((K + 15) / 16) * 16;
-    if (*Np > 256) return false;
-    if (tc_refine_smem_bytes(C, L) > 227 * 1024) return false;
-    *nbuf = tc_smem_bytes(L, *Cg2, *Np, 2) <= 227 * 1024 ? 2 : 1;
-    return tc_smem_bytes(L, *Cg2, *Np, *nbuf) <= 227 * 1024;
+// Tensor-core template groups.  Templates in support order (tperm) are cut
+// into groups of GS consecutive columns; a group's channel range is the union
+// of its templates' supports.  Every GS from all templates down to 16 is
+// tried; the plan whose groups all fit shared memory (templates, two or one
+// strip buffers; the refinement's strip) with the least padded MMA work per
+// tile (columns x channel groups, plus a fixed cost per group) wins.
+bool plan_tc_groups(const std::vector<u32> &tsup, const std::vector<u32> &tperm, u32 K, u32 C, u32 L, u32 gmax,
+                    std::vector<TcGroup> &out) {
+    double best = 1e300;
+    std::vector<TcGroup> cur;
+    const u32 kall = (K + 15) / 16 * 16;
+    const u32 sizes[] = {kall, 256, 128, 64, 32, 16};
+    for (u32 GS : sizes) {
+        if (GS > 256 || GS == 0) continue;
+        if ((K + GS - 1) / GS > gmax) continue;
+        cur.clear();
+        double cost = 0;
+        bool ok = true;
+        size_t off = 0;
+        for (u32 t0 = 0; t0 < K && ok; t0 += GS) {
+            TcGroup g{};
+            g.t0 = t0;
+            g.nt = std::min(GS, K - t0);
+            u32 lo = C, hi = 0;
+            for (u32 j = t0; j < t0 + g.nt; j++) {
+                const u32 t = tperm[j];
+                if (tsup[2 * t + 1] > tsup[2 * t]) {
+                    lo = std::min(lo, tsup[2 * t]);
+                    hi = std::max(hi, tsup[2 * t + 1]);
+                }
+            }
+            if (hi <= lo) { lo = 0; hi = std::min(C, 8u); }   // all-zero templates: zero products
+            g.clo = lo;
+            g.Cg = hi - lo;
+            g.Cg2 = (g.Cg + 15) / 16 * 2;
+            g.Np = (g.nt + 15) / 16 * 16;
+            if (tc_smem_bytes(L, g.Cg2, g.Np, 2) <= 227 * 1024) g.nbuf = 2;
+            else if (tc_smem_bytes(L, g.Cg2, g.Np, 1) <= 227 * 1024) g.nbuf = 1;
+            else ok = false;
+            if (tc_refine_smem_bytes(g.Cg, L) > 227 * 1024) ok = false;
+            g.cols = 32;
+            while (g.cols < g.nbuf * g.Np) g.cols <<= 1;
+            g.tb_off = off;
+            off += (size_t)L * g.Cg2 * g.Np;
+            cost += (double)g.Np * g.Cg2 + 8.0 * g.Cg2 + 2.0 * g.Np + 64.0;
+            cur.push_back(g);
+        }
+        if (ok && cost < best) {
+            best = cost;
+            out = cur;
+        }
+    }
+    return best < 1e300;
 }
 
 Workspace layout(char *base, u32 n, u32 K, u32 L, u32 nmax, bool want_fast, u32 C = 0, bool want_tc = false) {
@@ -192,30 +249,36 @@ Workspace layout(char *base, u32 n, u32 K, u32 L, u32 nmax, bool want_fast, u32 
         w.fb_list = (u32 *)take(sl * 4);
         w.ua = (float *)take(sl * 4);
         w.stiles = (S + kTcM - 1) / kTcM;
-        w.kexp_tile = (int *)take(sl * w.stiles * 4);
+        w.kexp_tile = (int *)take(sl * w.stiles * 4 * (want_tc ? std::max(1u, ceil_div(K, 16)) : 1u));
     }
-    w.tc = want_tc && tc_fits(C, K, L, &w.tc_Cg2, &w.tc_Np, &w.tc_nbuf);
+    w.tc = want_tc && C > 0;
     if (w.tc) {
-        w.tc_cols = 32;
-        while (w.tc_cols < w.tc_nbuf * w.tc_Np) w.tc_cols <<= 1;
-        w.Tb = (uint4 *)take((size_t)L * w.tc_Cg2 * w.tc_Np * 16);
+        // buffers for up to one group per 16 templates (the plan is made per
+        // chunk from the template supports)
+        w.tc_gmax = std::max(1u, ceil_div(K, 16));
+        const u32 cg2all = ceil_div(C, 16) * 2;
+        w.Tb = (uint4 *)take((size_t)L * cg2all * (2 * (size_t)K + 16) * 16);
         w.apx = (u8 *)take((size_t)K * n);
-        w.wn_s = (float *)take((size_t)n * 4);
+        w.wn_s = (float *)take((size_t)w.tc_gmax * n * 4);
         w.bm_s = (float *)take((size_t)n * 4);
         w.wlb = (float *)take((size_t)ceil_div(n, L) * 4);
-        w.wa_s = (float *)take((size_t)n * 4);
-        w.kx_s = (signed char *)take((size_t)n);
+        w.wa_s = (float *)take((size_t)w.tc_gmax * n * 4);
+        w.kx_s = (signed char *)take((size_t)w.tc_gmax * n);
         w.tc_tnorm = (float *)take((size_t)K * 4);
         w.tc_tabs = (float *)take((size_t)K * 4);
         w.tc_texp = (int *)take((size_t)K * 4);
         w.tc_ref_cap = (u32)std::min<u64>(0x7fffffffull, std::max<u64>(1u << 20, (u64)n * K / 4));
         w.tc_ref_t = (u32 *)take((size_t)w.tc_ref_cap * 4);
         w.tc_ref_s = (u32 *)take((size_t)w.tc_ref_cap * 4);
-        w.tc_seg_cap = W * ((L + kTcM - 1) / kTcM) + 16;
+        w.tc_seg_cap = (W * ((L + kTcM - 1) / kTcM) + 16) * w.tc_gmax;
         w.tc_seg_s0 = (u32 *)take((size_t)w.tc_seg_cap * 4);
         w.tc_seg_base = (u32 *)take((size_t)w.tc_seg_cap * 4);
         w.tc_seg_cnt = (u32 *)take((size_t)w.tc_seg_cap * 4);
+        w.tc_seg_grp = (u32 *)take((size_t)w.tc_seg_cap * 4);
+        w.tc_gdesc = (u32 *)take((size_t)w.tc_gmax * 12);
+        w.tgrp = (u32 *)take((size_t)K * 4);
     }
+    w.n = n;
     w.bytes = off;
     return w;
 }
@@ -325,6 +388,8 @@ int launch_accept(u32 n, u32 C, u32 L, const float *thr, const u32 *win, const u
 
 float tc_kappa(u32 C, u32 L, u32 Cg2);
 float tc_kappa_s(u32 C, u32 L);
+TcArgs tc_group_args(const Workspace &w, u32 gi, const float *v, u32 n, u32 C, const float *T, u32 K, u32 L,
+                     const float *tss, float *Lk, Counters *cnt);
 
 // Context for likelihood entries the tensor-core path left approximate.
 LazyLk lazy_ctx(const Workspace &w, const float *v, const float *T, const float *tss, u32 C, u32 L, u32 pass) {
@@ -333,8 +398,9 @@ LazyLk lazy_ctx(const Workspace &w, const float *v, const float *T, const float 
     z.apx = w.apx; z.wn = w.wn_s; z.wa = w.wa_s; z.kx = w.kx_s;
     z.tnorm = w.tc_tnorm; z.tabs = w.tc_tabs; z.tss = tss; z.texp = w.tc_texp;
     z.v = v; z.T = T; z.C = C; z.L = L;
-    z.kappa_b = tc_kappa(C, L, w.tc_Cg2);
+    z.kappa_b = tc_kappa(C, L, w.tc_cg2max);
     z.kappa_s = tc_kappa_s(C, L);
+    z.tgrp = w.tgrp; z.gstride = w.n; z.tsup = w.tsup;
     z.refined = &w.cnt->lazy_ref;
     z.wlb = w.wlb; z.bm = w.bm_s;
     z.tag = 2u + (pass & 1u);
@@ -365,7 +431,9 @@ OvArgs ov_args(const Workspace &w, const float *v, u32 n, u32 C, const float *T,
     A.ua = w.ua;
     A.lazy = lazy_ctx(w, v, T, tss, C, L, 0);   // read only: the tag is not used
     if (w.tc) {                      // H from the tensor cores
-        A.km_override = tc_kappa(C, L, w.tc_Cg2);
+        A.km_override = tc_kappa(C, L, w.tc_cg2max);
+        A.tgrp = w.tgrp;
+        A.kt_slots = w.slots;
         A.tabs = w.tc_tabs;
         A.texp = w.tc_texp;
         A.kexp_tile = w.kexp_tile;
@@ -402,22 +470,17 @@ int ov_fast_tables(const Workspace &w, const OvArgs &A, Counters *cnt, cudaStrea
     k_ov_prep<<<grid_for((u64)slots * 32, 256), 256, 0, st>>>(A);
     FBP_LAUNCH_CHECK();
     if (w.tc) {
-        TcArgs T{};
-        T.n = A.n; T.C = A.C; T.K = A.K; T.L = A.L;
-        T.Cg2 = w.tc_Cg2; T.Np = w.tc_Np;
-        T.rows_pad = (kTcM + A.L - 1 + 7) / 8 * 8;
-        T.tmem_cols = w.tc_cols;
-        T.nbuf = w.tc_nbuf;
-        T.v = A.v; T.T = A.T; T.texp = w.tc_texp; T.Tb = w.Tb;
-        T.tb_bytes = (u32)((size_t)A.L * w.tc_Cg2 * w.tc_Np * 16);
-        T.err = &cnt->tc_err;
-        T.S = S; T.nmax = A.nmax; T.stiles = w.stiles;
-        T.cand = A.cand; T.n_cand = A.n_cand; T.best_idx = A.best_idx; T.cskip = A.cskip;
-        T.NT = A.NT; T.H = A.H; T.kexp_tile = w.kexp_tile;
-        const size_t smem = tc_smem_bytes(A.L, w.tc_Cg2, w.tc_Np, w.tc_nbuf);
-        FBP_CUDA(cudaFuncSetAttribute(k_lik_tc<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-        k_lik_tc<1><<<sm_count(), kTcThreads, smem, st>>>(T);
-        FBP_LAUNCH_CHECK();
+        for (u32 gi = 0; gi < (u32)w.tcg.size(); gi++) {
+            TcArgs T = tc_group_args(w, gi, A.v, A.n, A.C, A.T, A.K, A.L, nullptr, nullptr, cnt);
+            T.S = S; T.nmax = A.nmax; T.stiles = w.stiles;
+            T.cand = A.cand; T.n_cand = A.n_cand; T.best_idx = A.best_idx; T.cskip = A.cskip;
+            T.NT = A.NT; T.H = A.H;
+            T.kexp_tile = w.kexp_tile + (size_t)gi * slots * w.stiles;
+            const size_t smem = tc_smem_bytes(A.L, T.Cg2, T.Np, T.nbuf);
+            FBP_CUDA(cudaFuncSetAttribute(k_lik_tc<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+            k_lik_tc<1><<<sm_count(), kTcThreads, smem, st>>>(T);
+            FBP_LAUNCH_CHECK();
+        }
     } else if (w.masked_tables) {
         const size_t smem = tables_m_smem_bytes(S, A.L);
         if (smem > 48 * 1024)
@@ -432,7 +495,7 @@ int ov_fast_tables(const Workspace &w, const OvArgs &A, Counters *cnt, cudaStrea
         k_ov_tables<<<grid_for((u64)slots * kTabThreads, kTabThreads, 4), kTabThreads, smem, st>>>(A);
         FBP_LAUNCH_CHECK();
     }
-    *launches = 2;
+    *launches = 1 + (w.tc ? (int)w.tcg.size() : 1);
     return FBP_OK;
 }
 
@@ -492,11 +555,42 @@ __global__ void k_tc_gate(Counters *cnt, u32 cap, u32 seg_cap) {
 }
 
 int tc_chunk_setup(const Workspace &w, const float *T, u32 K, u32 C, u32 L, cudaStream_t st) {
-    const u64 total = (u64)L * w.tc_Cg2 * w.tc_Np;
     k_tnorm<<<grid_for(K, 64), 64, 0, st>>>(T, K, C * L, w.tc_tnorm, w.tc_tabs, w.tc_texp);
-    k_tc_pack_templates<<<grid_for(total, 256), 256, 0, st>>>(T, K, C, L, w.tc_Cg2, w.tc_Np, w.tc_texp, w.Tb);
+    for (const TcGroup &g : w.tcg) {
+        const u64 total = (u64)L * g.Cg2 * g.Np;
+        k_tc_pack_templates<<<grid_for(total, 256), 256, 0, st>>>(T, g.nt, C, g.clo, g.Cg, L, g.Cg2, g.Np,
+                                                                   w.tc_texp, w.tperm + g.t0, w.Tb + g.tb_off);
+    }
     FBP_LAUNCH_CHECK();
     return FBP_OK;
+}
+
+// Launch arguments of one template group of the tensor-core kernel.
+TcArgs tc_group_args(const Workspace &w, u32 gi, const float *v, u32 n, u32 C, const float *T, u32 K, u32 L,
+                     const float *tss, float *Lk, Counters *cnt) {
+    const TcGroup &g = w.tcg[gi];
+    TcArgs A{};
+    A.n = n; A.C = g.Cg; A.K = g.nt; A.L = L;
+    A.trow = w.tperm + g.t0; A.Kall = K; A.tstride = C * L;
+    A.Cg2 = g.Cg2; A.Np = g.Np;
+    A.rows_pad = (kTcM + L - 1 + 7) / 8 * 8;
+    A.tmem_cols = g.cols;
+    A.nbuf = g.nbuf;
+    A.kappa_b = tc_kappa(C, L, w.tc_cg2max);
+    A.kappa_s = tc_kappa_s(C, L);
+    A.v = v + (size_t)g.clo * n; A.T = T; A.tss = tss;
+    A.tnorm = w.tc_tnorm; A.tabs = w.tc_tabs; A.texp = w.tc_texp;
+    A.Tb = w.Tb + g.tb_off;
+    A.tb_bytes = (u32)((size_t)L * g.Cg2 * g.Np * 16);
+    A.Lk = Lk;
+    A.ref_t = w.tc_ref_t; A.ref_s = w.tc_ref_s; A.refseg = &cnt->tc_refseg; A.ref_cap = w.tc_ref_cap;
+    A.seg_s0 = w.tc_seg_s0; A.seg_base = w.tc_seg_base; A.seg_cnt = w.tc_seg_cnt; A.seg_grp = w.tc_seg_grp;
+    A.grp = gi;
+    A.seg_overflow = &cnt->tc_overflow; A.seg_cap = w.tc_seg_cap;
+    A.err = &cnt->tc_err;
+    A.apx = w.apx; A.bm_s = w.bm_s; A.wlb = w.wlb;
+    A.wn_s = w.wn_s + (size_t)gi * n; A.wa_s = w.wa_s + (size_t)gi * n; A.kx_s = w.kx_s + (size_t)gi * n;
+    return A;
 }
 
 // Bound on |tensor-core value - reference value| per unit of
@@ -522,32 +616,22 @@ float tc_kappa_s(u32 C, u32 L) {
     return (float)((1.01 * n_ref * u + 4.0 * u) * 1.01);
 }
 
-// One pass of the tensor-core likelihood over the listed windows: the tiles.
+// One pass of the tensor-core likelihood over the listed windows: the tiles,
+// one launch per template group.
 int tc_likelihood_pass(const Workspace &w, const float *v, u32 n, u32 C, const float *T, u32 K, u32 L,
                        const float *tss, const u32 *win, const u32 *n_win, u32 max_windows, float *Lk,
                        Counters *cnt, cudaStream_t st, int *launches) {
-    TcArgs A{};
-    A.n = n; A.C = C; A.K = K; A.L = L;
-    A.Cg2 = w.tc_Cg2; A.Np = w.tc_Np;
-    A.rows_pad = (kTcM + L - 1 + 7) / 8 * 8;
-    A.tmem_cols = w.tc_cols;
-    A.nbuf = w.tc_nbuf;
-    A.kappa_b = tc_kappa(C, L, w.tc_Cg2);
-    A.kappa_s = tc_kappa_s(C, L);
-    A.v = v; A.T = T; A.tss = tss; A.tnorm = w.tc_tnorm; A.tabs = w.tc_tabs; A.texp = w.tc_texp; A.Tb = w.Tb;
-    A.tb_bytes = (u32)((size_t)L * w.tc_Cg2 * w.tc_Np * 16);
-    A.win = win; A.n_win = n_win; A.Lk = Lk;
-    A.ref_t = w.tc_ref_t; A.ref_s = w.tc_ref_s; A.refseg = &cnt->tc_refseg; A.ref_cap = w.tc_ref_cap;
-    A.seg_s0 = w.tc_seg_s0; A.seg_base = w.tc_seg_base; A.seg_cnt = w.tc_seg_cnt;
-    A.seg_overflow = &cnt->tc_overflow; A.seg_cap = w.tc_seg_cap;
-    A.err = &cnt->tc_err;
-    A.apx = w.apx; A.wn_s = w.wn_s; A.wa_s = w.wa_s; A.kx_s = w.kx_s; A.bm_s = w.bm_s; A.wlb = w.wlb;
-    const size_t smem = tc_smem_bytes(L, w.tc_Cg2, w.tc_Np, w.tc_nbuf);
+    (void)max_windows;
     FBP_CUDA(cudaMemsetAsync(&cnt->tc_refseg, 0, 8, st));
-    FBP_CUDA(cudaFuncSetAttribute(k_lik_tc<0>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    k_lik_tc<0><<<sm_count(), kTcThreads, smem, st>>>(A);
-    FBP_LAUNCH_CHECK();
-    *launches = 1;
+    for (u32 gi = 0; gi < (u32)w.tcg.size(); gi++) {
+        TcArgs A = tc_group_args(w, gi, v, n, C, T, K, L, tss, Lk, cnt);
+        A.win = win; A.n_win = n_win;
+        const size_t smem = tc_smem_bytes(L, A.Cg2, A.Np, A.nbuf);
+        FBP_CUDA(cudaFuncSetAttribute(k_lik_tc<0>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        k_lik_tc<0><<<sm_count(), kTcThreads, smem, st>>>(A);
+        FBP_LAUNCH_CHECK();
+    }
+    *launches = (int)w.tcg.size();
     return FBP_OK;
 }
 
@@ -556,18 +640,17 @@ int tc_likelihood_pass(const Workspace &w, const float *v, u32 n, u32 C, const f
 int tc_refine_pass(const Workspace &w, const float *v, u32 n, u32 C, const float *T, u32 K, u32 L,
                    const float *tss, const u32 *win, const u32 *n_win, u32 max_windows, float *Lk,
                    Counters *cnt, cudaStream_t st, int *launches) {
-    const size_t rsmem = tc_refine_smem_bytes(C, L);
+    const size_t rsmem = tc_refine_smem_bytes(w.tc_cmax, L);
     if (rsmem > 48 * 1024)
         FBP_CUDA(cudaFuncSetAttribute(k_tc_refine, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)rsmem));
     // gamma: the reference's recursive sum of C*L + 1 terms (products
     // rounded once each), plus the double sums' own error
     const double u = 1.0 / 16777216.0, nr = (double)C * L + 2;
     const double gamma = 1.01 * (nr * u / (1.0 - nr * u)) + 4.0 * nr * 1.1102230246251565e-16;
-    k_tc_refine<<<sm_count() * 8, kRefThreads, rsmem, st>>>(v, n, C, T, K, L, tss, w.tc_ref_t, w.tc_ref_s,
-                                                            w.tc_seg_s0, w.tc_seg_base, w.tc_seg_cnt,
-                                                            reinterpret_cast<const u32 *>(&cnt->tc_refseg),
-                                                            w.tc_seg_cap, Lk, lazy_ctx(w, v, T, tss, C, L, 0),
-                                                            gamma, &cnt->tc_seq);
+    k_tc_refine<<<sm_count() * 8, kRefThreads, rsmem, st>>>(
+        v, n, C, w.tc_cmax, T, K, L, tss, w.tc_ref_t, w.tc_ref_s, w.tc_seg_s0, w.tc_seg_base, w.tc_seg_cnt,
+        w.tc_seg_grp, w.tc_gdesc, w.tperm, reinterpret_cast<const u32 *>(&cnt->tc_refseg), w.tc_seg_cap, Lk,
+        lazy_ctx(w, v, T, tss, C, L, 0), gamma, &cnt->tc_seq);
     k_tc_gate<<<1, 1, 0, st>>>(cnt, w.tc_ref_cap, w.tc_seg_cap);
     FBP_LAUNCH_CHECK();
     int rc = launch_likelihood(v, n, C, T, K, L, tss, win, n_win, max_windows, Lk, st, &cnt->tc_overflow, w.apx,
@@ -738,16 +821,40 @@ int fbp_pursuit_chunk(float *voltage, uint32_t n, uint32_t C, const float *templ
     k_template_support<<<1, 256, 0, st>>>(templates, K, C, L, w.tsup, w.tperm, w.grange, kLikTplPerBlock,
                                           w.grange32, kTabMGroup);
     FBP_LAUNCH_CHECK();
-    if (w.fast && do_overlap_recheck && !w.tc) {
-        // the masked overlap tables pay off when the template groups touch
-        // well under all channels (one small read-back per chunk)
+    if (w.tc || (w.fast && do_overlap_recheck)) {
+        // template supports on the host (one small read-back per chunk): the
+        // tensor-core group plan and the choice of overlap-table kernel
         const u32 ng = ceil_div(K, kTabMGroup);
-        std::vector<u32> gr(2 * (size_t)ng);
+        std::vector<u32> tsup(2 * (size_t)K), tperm(K), gr(2 * (size_t)ng);
+        FBP_CUDA(cudaMemcpyAsync(tsup.data(), w.tsup, tsup.size() * 4, cudaMemcpyDeviceToHost, st));
+        FBP_CUDA(cudaMemcpyAsync(tperm.data(), w.tperm, tperm.size() * 4, cudaMemcpyDeviceToHost, st));
         FBP_CUDA(cudaMemcpyAsync(gr.data(), w.grange32, gr.size() * 4, cudaMemcpyDeviceToHost, st));
         FBP_CUDA(cudaStreamSynchronize(st));
-        u64 span = 0;
-        for (u32 g = 0; g < ng; g++) span += gr[2 * g + 1] - gr[2 * g];
-        w.masked_tables = 2 * span < (u64)ng * C && 2 * nmax + 1 <= 32u * kTabMShiftChunks;
+        if (w.tc) {
+            if (!plan_tc_groups(tsup, tperm, K, C, L, w.tc_gmax, w.tcg)) {
+                w.tc = false;                        // no group fits: the FP32 kernel
+            } else {
+                w.tc_cg2max = w.tc_cmax = 0;
+                std::vector<u32> gdesc(3 * w.tcg.size()), tgrp(K);
+                for (u32 gi = 0; gi < (u32)w.tcg.size(); gi++) {
+                    const TcGroup &g = w.tcg[gi];
+                    w.tc_cg2max = std::max(w.tc_cg2max, g.Cg2);
+                    w.tc_cmax = std::max(w.tc_cmax, g.Cg);
+                    gdesc[3 * gi] = g.t0; gdesc[3 * gi + 1] = g.clo; gdesc[3 * gi + 2] = g.Cg;
+                    for (u32 j = g.t0; j < g.t0 + g.nt; j++) tgrp[tperm[j]] = gi;
+                }
+                FBP_CUDA(cudaMemcpyAsync(w.tc_gdesc, gdesc.data(), gdesc.size() * 4, cudaMemcpyHostToDevice, st));
+                FBP_CUDA(cudaMemcpyAsync(w.tgrp, tgrp.data(), tgrp.size() * 4, cudaMemcpyHostToDevice, st));
+                FBP_CUDA(cudaStreamSynchronize(st));   // the host vectors go out of scope
+            }
+        }
+        if (w.fast && do_overlap_recheck && !w.tc) {
+            // the masked overlap tables pay off when the template groups
+            // touch well under all channels
+            u64 span = 0;
+            for (u32 g = 0; g < ng; g++) span += gr[2 * g + 1] - gr[2 * g];
+            w.masked_tables = 2 * span < (u64)ng * C && 2 * nmax + 1 <= 32u * kTabMShiftChunks;
+        }
     }
     S.launches[FBP_STAGE_LISTS] += 1;
     timer.end(FBP_STAGE_LISTS);
@@ -755,6 +862,7 @@ int fbp_pursuit_chunk(float *voltage, uint32_t n, uint32_t C, const float *templ
         timer.begin(FBP_STAGE_LIKELIHOOD);
         FBP_CUDA(cudaMemsetAsync(w.apx, 0, (size_t)K * n, st));
         FBP_CUDA(cudaMemsetAsync(w.wlb, 0, (size_t)W * 4, st));
+        FBP_CUDA(cudaMemsetAsync(w.bm_s, 0, (size_t)n * 4, st));
         int rc0 = tc_chunk_setup(w, templates, K, C, L, st);
         if (rc0) return rc0;
         S.launches[FBP_STAGE_LIKELIHOOD] += 2;
@@ -854,7 +962,8 @@ int fbp_pursuit_chunk(float *voltage, uint32_t n, uint32_t C, const float *templ
         timer.begin(FBP_STAGE_LISTS);
         FBP_CUDA(cudaMemsetAsync(w.ovr, 0, wb, q));
         if ((rc2 = compact(w.flags_out, W, w.win, &w.cnt->n_win, w.tile_counts, q))) return rc2;
-        k_mark_active<<<grid_for(W, 256), 256, 0, q>>>(w.flags_out, w.active, W, w.tc ? w.wlb : nullptr);
+        k_mark_active<<<grid_for(W, 256), 256, 0, q>>>(w.flags_out, w.active, W, w.tc ? w.wlb : nullptr,
+                                                       w.tc ? w.bm_s : nullptr, L, n);
         FBP_CUDA(cudaMemsetAsync(w.flags, 0, wb, q));
         // 8. keep the spikes (.py:702-710)
         k_append_spikes<<<grid_for(W, 256), 256, 0, q>>>(w.spk_idx, w.spk_lab, w.cnt, spike_idx, spike_lab,
@@ -891,7 +1000,9 @@ int fbp_pursuit_chunk(float *voltage, uint32_t n, uint32_t C, const float *templ
                   (uint64_t)(uintptr_t)neg_half_ss, (uint64_t)(uintptr_t)thresholds, nmax,
                   (uint64_t)do_overlap_recheck, (uint64_t)precision, (uint64_t)overlap_method,
                   (uint64_t)(uintptr_t)workspace, (uint64_t)workspace_bytes, (uint64_t)(uintptr_t)spike_idx,
-                  (uint64_t)(uintptr_t)spike_lab, spike_cap, (uint64_t)w.masked_tables};
+                  (uint64_t)(uintptr_t)spike_lab, spike_cap, (uint64_t)w.masked_tables, (uint64_t)w.tc};
+        for (const TcGroup &g : w.tcg)               // the group plan follows the template supports
+            if (w.tc) pg.key.insert(pg.key.end(), {g.t0, g.nt, g.clo, g.Cg, g.nbuf});
         std::lock_guard<std::mutex> lk(g_graph_mu);
         for (size_t i = 0; i < g_graphs.size(); i++)
             if (g_graphs[i].key == pg.key) {

@@ -76,10 +76,13 @@ __global__ void k_iota_windows(u32 *__restrict__ win, u8 *__restrict__ active, u
 // active = flags != 0; windows about to be recomputed also drop their
 // lower bound (wlb, tensor-core path; may be NULL).
 __global__ void k_mark_active(const u8 *__restrict__ flags, u8 *__restrict__ active, u32 W,
-                              float *__restrict__ wlb) {
+                              float *__restrict__ wlb, float *__restrict__ bm, u32 L, u32 n) {
     for (u32 i = blockIdx.x * blockDim.x + threadIdx.x; i < W; i += gridDim.x * blockDim.x) {
         active[i] = flags[i] != 0;
-        if (wlb && flags[i]) wlb[i] = 0.0f;
+        if (wlb && flags[i]) {
+            wlb[i] = 0.0f;
+            for (u32 s = i * L; s < min((i + 1) * L, n); s++) bm[s] = 0.0f;
+        }
     }
 }
 
@@ -260,19 +263,25 @@ struct LazyLk {
     const float *wlb;                 // [W] largest lower bound over each window's entries
     const float *bm;                  // [n] largest bound of a flagged entry of each sample
     u32 tag;                          // 2 + pass % 2
+    const u32 *tgrp;                  // [K] template group; wn/wa/kx are [group][n] (NULL: one group)
+    u64 gstride;                      // n
+    const u32 *tsup;                  // [K][2] non-zero channel range (NULL: all channels)
 };
 
 // The bound the tensor-core epilogue used for entry (t, s) (same formula).
 __device__ __forceinline__ float lazy_bound(const LazyLk &z, u32 t, u32 s, float approx) {
-    const float sub = 2.98023223876953125e-08f * (ldexpf(z.tabs[t], -(int)z.kx[s]) + ldexpf(z.wa[s], -z.texp[t])) * 1.001f;
-    return z.kappa_b * z.tnorm[t] * z.wn[s] + sub + z.kappa_s * fabsf(z.tss[t]) +
+    const size_t i = (z.tgrp ? (size_t)z.tgrp[t] * z.gstride : 0) + s;
+    const float sub = 2.98023223876953125e-08f * (ldexpf(z.tabs[t], -(int)z.kx[i]) + ldexpf(z.wa[i], -z.texp[t])) * 1.001f;
+    return z.kappa_b * z.tnorm[t] * z.wn[i] + sub + z.kappa_s * fabsf(z.tss[t]) +
            2.384185791015625e-07f * fabsf(approx);
 }
 
 // compute_maximum_likelihood (binary_pursuit.cl:216-252), reference order.
 __device__ __forceinline__ float exact_likelihood(const LazyLk &z, u32 n, u32 t, u32 s) {
     float acc = z.tss[t];
-    for (u32 c = 0; c < z.C; c++) {
+    // channels outside the template's support add exact zeros
+    const u32 clo = z.tsup ? z.tsup[2 * t] : 0u, chi = z.tsup ? z.tsup[2 * t + 1] : z.C;
+    for (u32 c = clo; c < chi; c++) {
         const float *tp = z.T + ((size_t)t * z.C + c) * z.L;
         const float *vp = z.v + (size_t)c * n + s;
         for (u32 i = 0; i < z.L; i++) acc = __fadd_rn(acc, __fmul_rn(__ldg(tp + i), vp[i]));
@@ -310,8 +319,11 @@ __device__ __forceinline__ float warp_chain(float acc, const float *buf, u32 m) 
 __device__ float warp_exact_likelihood(const LazyLk &z, u32 n, u32 t, u32 s, float *buf) {
     static_assert(kWarpChunk == 256, "eight products per lane");
     const u32 lane = threadIdx.x & 31;
-    const u32 CL = z.C * z.L;
-    const float *tp = z.T + (size_t)t * CL;
+    // the template's support: channels outside it add exact zeros
+    const u32 clo = z.tsup ? z.tsup[2 * t] : 0u, chi = z.tsup ? z.tsup[2 * t + 1] : z.C;
+    const u32 CL = (chi > clo ? chi - clo : 0u) * z.L;
+    const float *tp = z.T + ((size_t)t * z.C + clo) * z.L;
+    const float *vb = z.v + (size_t)clo * n;
     float acc = z.tss[t];
     for (u32 q0 = 0; q0 < CL; q0 += kWarpChunk) {
         const u32 m = min(kWarpChunk, CL - q0);
@@ -323,7 +335,7 @@ __device__ float warp_exact_likelihood(const LazyLk &z, u32 n, u32 t, u32 s, flo
             if (k < m) {
                 const u32 q = q0 + k, c = q / z.L, j = q - c * z.L;
                 tv[i] = __ldg(tp + q);
-                vv[i] = z.v[(size_t)c * n + s + j];
+                vv[i] = vb[(size_t)c * n + s + j];
             }
         }
 #pragma unroll

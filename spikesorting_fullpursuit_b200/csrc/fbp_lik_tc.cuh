@@ -54,7 +54,10 @@ constexpr int kTcEpiThreads = 32 * kTcEpiWarps;
 constexpr int kTcM = 128;            // samples per tile
 
 struct TcArgs {
-    u32 n, C, K, L;
+    u32 n, C, K, L;                  // C: the group's channels; K: the group's templates
+    const u32 *trow;                 // [K] template of each group column (NULL: column = template)
+    u32 Kall;                        // templates of the chunk (row stride of the overlap tables)
+    u32 tstride;                     // floats between consecutive templates in T (all channels)
     u32 Cg2;                         // channel groups of 8, padded to even
     u32 Np;                          // templates padded to a multiple of 16
     u32 rows_pad;                    // strip rows (128 + L - 1) padded to 8
@@ -77,6 +80,8 @@ struct TcArgs {
     unsigned long long *refseg;      // entries queued (high half) and tile segments (low half)
     u32 ref_cap;
     u32 *seg_s0, *seg_base, *seg_cnt;  // tile segments of the refinement list
+    u32 *seg_grp;                      // template group of each segment
+    u32 grp;                           // this launch's template group
     u32 *seg_overflow;
     u32 seg_cap;
     u32 *err;                        // non-zero: a bounded wait gave up
@@ -96,7 +101,7 @@ struct TcArgs {
 
 // Shared memory of the tensor-core kernel (nbuf strip buffers).
 struct TcSmem {
-    size_t Bs, As, rowsq, rowab, tsc, tsa, ctk, ctb, ctss, cta, tinfo, bars, misc, tcnt, bmh, total;
+    size_t Bs, As, rowsq, rowab, tsc, tsa, ctk, ctb, ctss, cta, ctrow, tinfo, bars, misc, tcnt, bmh, total;
 };
 __host__ __device__ inline TcSmem tc_smem_layout(u32 L, u32 Cg2, u32 Np, u32 nbuf) {
     const size_t rows_pad = (kTcM + L - 1 + 7) / 8 * 8;
@@ -111,7 +116,8 @@ __host__ __device__ inline TcSmem tc_smem_layout(u32 L, u32 Cg2, u32 Np, u32 nbu
     m.ctk = o;   o += (size_t)Np * 4;                       // kappa * ||t||
     m.ctb = o;   o += (size_t)Np * 4;                       // 2^-25 * 1.001 * 2^-texp[t]
     m.ctss = o;  o += (size_t)Np * 4;                       // -SS_t / 2
-    m.cta = o;   o += (size_t)Np * 4;                       // 2^-22 * |SS_t / 2|
+    m.cta = o;   o += (size_t)Np * 4;                       // kappa_s * |SS_t / 2|
+    m.ctrow = o; o += (size_t)Np * 4;                       // template of each column
     m.tinfo = o; o += (size_t)nbuf * 32;                    // per buffer: s0, ew, g, kexp
     o = (o + 7) / 8 * 8;
     m.bars = o;  o += 8 * 8;                                // full[2], empty[2], staged[2], templates
@@ -200,6 +206,7 @@ k_lik_tc(TcArgs A) {
     float *tsc_all = (float *)(tsm + lay.tsc), *tsa_all = (float *)(tsm + lay.tsa);
     float *ctk = (float *)(tsm + lay.ctk), *ctb = (float *)(tsm + lay.ctb);
     float *ctss = (float *)(tsm + lay.ctss), *cta = (float *)(tsm + lay.cta);
+    u32 *ctrow = (u32 *)(tsm + lay.ctrow);
     int *tinfo = (int *)(tsm + lay.tinfo);                 // [nbuf][8]: s0 lo, s0 hi, ew, g, kexp
     u64 *bars = (u64 *)(tsm + lay.bars);
     u32 *misc = (u32 *)(tsm + lay.misc);
@@ -232,11 +239,13 @@ k_lik_tc(TcArgs A) {
     for (u32 t = tid; t < Np; t += blockDim.x) {
         tcnt[t] = 0;
         const bool real = t < A.K;
+        const u32 gt = real ? (A.trow ? A.trow[t] : t) : 0u;
+        ctrow[t] = gt;
         if (MODE == 0) {
-            ctk[t] = real ? A.kappa_b * A.tnorm[t] : 0.0f;
-            ctb[t] = real ? 2.98023223876953125e-08f * 1.001f * ldexpf(1.0f, -A.texp[t]) : 0.0f;
-            ctss[t] = real ? A.tss[t] : 0.0f;
-            cta[t] = real ? A.kappa_s * fabsf(A.tss[t]) : 0.0f;
+            ctk[t] = real ? A.kappa_b * A.tnorm[gt] : 0.0f;
+            ctb[t] = real ? 2.98023223876953125e-08f * 1.001f * ldexpf(1.0f, -A.texp[gt]) : 0.0f;
+            ctss[t] = real ? A.tss[gt] : 0.0f;
+            cta[t] = real ? A.kappa_s * fabsf(A.tss[gt]) : 0.0f;
         }
     }
     __syncthreads();
@@ -368,10 +377,11 @@ k_lik_tc(TcArgs A) {
             for (u32 t = pt; t < Np; t += kTcProdThreads) {
                 float sc = 0.0f;
                 if (t < A.K) {
-                    const int ex = -(kexp + A.texp[t]);
+                    const u32 gt = ctrow[t];
+                    const int ex = -(kexp + A.texp[gt]);
                     if (ex >= -149 && ex <= 127) sc = ldexpf(1.0f, ex);   // exact power of two
                     if (MODE == 0) tsa_all[(size_t)b * Np + t] =
-                                       2.98023223876953125e-08f * 1.001f * ldexpf(A.tabs[t], -kexp);
+                                       2.98023223876953125e-08f * 1.001f * ldexpf(A.tabs[gt], -kexp);
                 }
                 tsc_all[(size_t)b * Np + t] = sc;
             }
@@ -505,10 +515,11 @@ k_lik_tc(TcArgs A) {
                         for (int q = 0; q < 16; q++) {
                             const u32 t = c0 + q;
                             if (t >= A.K) continue;
+                            const u32 gt = ctrow[t];
                             const float a = __uint_as_float(r[q]);
                             const float sc = tsc[t];
-                            const float x = sc != 0.0f ? __fmul_rn(a, sc) : ldexpf(a, -(kexp + A.texp[t]));
-                            A.H[((size_t)g * A.K + t) * A.S + brow] = x - 0.5f * A.NT[(size_t)t * A.S + brow];
+                            const float x = sc != 0.0f ? __fmul_rn(a, sc) : ldexpf(a, -(kexp + A.texp[gt]));
+                            A.H[((size_t)g * A.Kall + gt) * A.S + brow] = x - 0.5f * A.NT[(size_t)gt * A.S + brow];
                         }
                     }
                 }
@@ -554,16 +565,17 @@ k_lik_tc(TcArgs A) {
                     : "r"(acc0 + c0));
                 asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
                 if (!in_win) continue;
-                float *dst0 = A.Lk + (size_t)c0 * n + s;
-                u8 *fl0 = A.apx + (size_t)c0 * n + s;
                 u32 cw = 0;
 #pragma unroll
                 for (int q = 0; q < 16; q++) {
                     const u32 t = c0 + q;
                     if (t >= A.K) break;                 // padding templates
+                    const u32 gt = ctrow[t];
+                    float *dst = A.Lk + (size_t)gt * n + s;
+                    u8 *fl = A.apx + (size_t)gt * n + s;
                     const float a = __uint_as_float(r[q]);
                     const float sc = tsc[t];
-                    const float approx = __fadd_rn(sc != 0.0f ? __fmul_rn(a, sc) : ldexpf(a, -(kexp + A.texp[t])),
+                    const float approx = __fadd_rn(sc != 0.0f ? __fmul_rn(a, sc) : ldexpf(a, -(kexp + A.texp[gt])),
                                                    ctss[t]);
                     // E = kappa ||t|| ||w|| + 2^-25 (|t|_1 / s_v + |w|_1 / s_t) * 1.001
                     //     + kappa_s |SS/2| + 2^-22 |approx|
@@ -574,8 +586,8 @@ k_lik_tc(TcArgs A) {
                     lomax = fmaxf(lomax, approx - E);
                     bmax = pos ? fmaxf(bmax, E) : bmax;
                     cw |= (!tail && !pos && !neg) ? (1u << q) : 0u;
-                    dst0[(size_t)q * n] = tail ? 0.0f : approx;
-                    fl0[(size_t)q * n] = (!tail && pos) ? (u8)1 : (u8)0;
+                    *dst = tail ? 0.0f : approx;
+                    *fl = (!tail && pos) ? (u8)1 : (u8)0;
                 }
                 if (tail) lomax = 0.0f, bmax = 0.0f;
                 wantbits[k] |= cw << (16 * half);
@@ -590,7 +602,12 @@ k_lik_tc(TcArgs A) {
 #pragma unroll
             for (int wd = 0; wd < 8; wd++) nwant += __popc(wantbits[wd]);
             const bool anywant = named_bar_or(2, kTcEpiThreads, nwant != 0);   // also publishes bmh
-            if (half == 0 && in_win) A.bm_s[s] = fmaxf(bmax, bmh[row]);
+            // largest flagged bound of the sample over every template group
+            // (reset when its window is listed for recomputation)
+            if (half == 0 && in_win) {
+                const float bmv = fmaxf(bmax, bmh[row]);
+                if (bmv > 0.0f) atomicMax(reinterpret_cast<int *>(A.bm_s) + s, __float_as_int(bmv));
+            }
             if (anywant) {
                 // phase 2: one contiguous segment of (template, sample)
                 // entries per tile, ordered by template so the refinement
@@ -635,6 +652,7 @@ k_lik_tc(TcArgs A) {
                             A.seg_s0[si] = (u32)s0;
                             A.seg_base[si] = base;
                             A.seg_cnt[si] = total;
+                            A.seg_grp[si] = A.grp;
                             seg_info[2] = 1;
                         } else {
                             atomicExch(A.seg_overflow, 1u);
@@ -676,19 +694,21 @@ k_lik_tc(TcArgs A) {
     if (warp == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(A.tmem_cols));
 }
 
-// Templates in the UMMA B layout: Tb[m][g][t] = 8 fp16 channels 8g..8g+7 of
-// template t at lag m, scaled by 2^texp[t] (zero padding for channels >= C
-// and t >= K).
-__global__ void k_tc_pack_templates(const float *__restrict__ T, u32 K, u32 C, u32 L, u32 Cg2, u32 Np,
-                                    const int *__restrict__ texp, uint4 *__restrict__ Tb) {
+// Templates in the UMMA B layout: Tb[m][g][t] = 8 fp16 channels 8g..8g+7
+// (of the group's range, starting at channel clo) of template trow[t] at lag
+// m, scaled by 2^texp (zero padding for channels >= Cg and columns >= K).
+__global__ void k_tc_pack_templates(const float *__restrict__ T, u32 K, u32 Call, u32 clo, u32 Cg, u32 L,
+                                    u32 Cg2, u32 Np, const int *__restrict__ texp, const u32 *__restrict__ trow,
+                                    uint4 *__restrict__ Tb) {
     const u64 total = (u64)L * Cg2 * Np;
     for (u64 e = (u64)blockIdx.x * blockDim.x + threadIdx.x; e < total; e += (u64)gridDim.x * blockDim.x) {
         const u32 t = (u32)(e % Np), g = (u32)((e / Np) % Cg2), m = (u32)(e / ((u64)Np * Cg2));
+        const u32 gt = t < K ? (trow ? trow[t] : t) : 0u;
         u16 h[8];
 #pragma unroll
         for (int j = 0; j < 8; j++) {
             const u32 c = g * 8 + j;
-            const float f = (t < K && c < C) ? ldexpf(T[((size_t)t * C + c) * L + m], texp[t]) : 0.0f;
+            const float f = (t < K && c < Cg) ? ldexpf(T[((size_t)gt * Call + clo + c) * L + m], texp[gt]) : 0.0f;
             h[j] = __half_as_ushort(__float2half_rn(f));
         }
         uint4 q;
@@ -719,20 +739,28 @@ __host__ __device__ inline size_t tc_refine_smem_bytes(u32 C, u32 L) {
     return ((size_t)C * (kTcM + L) + 8) * 4 + (size_t)(kRefThreads / 32) * kWarpChunk * 4;
 }
 __global__ void __launch_bounds__(kRefThreads)
-k_tc_refine(const float *__restrict__ v, u32 n, u32 C, const float *__restrict__ T, u32 K, u32 L,
-            const float *__restrict__ tss, const u32 *__restrict__ ref_t, const u32 *__restrict__ ref_s,
+k_tc_refine(const float *__restrict__ vall, u32 n, u32 Call, u32 Cmax, const float *__restrict__ Tall, u32 K,
+            u32 L, const float *__restrict__ tss, const u32 *__restrict__ ref_t, const u32 *__restrict__ ref_s,
             const u32 *__restrict__ seg_s0, const u32 *__restrict__ seg_base, const u32 *__restrict__ seg_cnt,
+            const u32 *__restrict__ seg_grp, const u32 *__restrict__ gdesc, const u32 *__restrict__ tperm,
             const u32 *__restrict__ seg_count, u32 seg_cap, float *__restrict__ Lk, LazyLk z, double gamma,
             u64 *__restrict__ n_seq) {
     extern __shared__ float rsm[];
     const u32 rl = kTcM + L;               // strip row length
-    const u32 CL = C * L;
     const u32 lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    float *wbuf = rsm + ((size_t)C * rl + 8) + (size_t)warp * kWarpChunk;
+    float *wbuf = rsm + ((size_t)Cmax * rl + 8) + (size_t)warp * kWarpChunk;
     const u32 nseg = min(*seg_count, seg_cap);
+    const u32 tstride = Call * L;          // floats between templates in T
     u32 nseq = 0;
     for (u32 sg = blockIdx.x; sg < nseg; sg += gridDim.x) {
         const u32 s0 = seg_s0[sg], base = seg_base[sg], cnt = seg_cnt[sg];
+        // the segment's template group: columns t0.., channels [clo, clo + C)
+        const u32 gi = seg_grp[sg];
+        const u32 t0 = gdesc[3 * gi], clo = gdesc[3 * gi + 1], C = gdesc[3 * gi + 2];
+        const float *v = vall + (size_t)clo * n;
+        const float *T = Tall + (size_t)clo * L;
+        const u32 *trow = tperm ? tperm + t0 : nullptr;
+        const u32 CL = C * L;
         __syncthreads();
         for (u32 x = threadIdx.x; x < C * rl; x += blockDim.x) {
             const u32 c = x / rl, i = x % rl, pos = s0 + i;
@@ -740,8 +768,8 @@ k_tc_refine(const float *__restrict__ v, u32 n, u32 C, const float *__restrict__
         }
         __syncthreads();
         for (u32 e = warp; e < cnt; e += kRefThreads / 32) {
-            const u32 t = ref_t[base + e], so = ref_s[base + e] - s0;
-            const float *tp = T + (size_t)t * CL;
+            const u32 t = trow ? trow[ref_t[base + e]] : ref_t[base + e], so = ref_s[base + e] - s0;
+            const float *tp = T + (size_t)t * tstride;      // the group's channels of template t
             double X = 0.0, S = 0.0;
             for (u32 q = lane; q < CL; q += 32) {
                 const u32 c = q / L, i = q - c * L;

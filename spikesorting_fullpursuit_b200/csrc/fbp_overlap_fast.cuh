@@ -78,7 +78,9 @@ struct OvArgs {
     float km_override;               // > 0: bound of the tensor-core tables
     const float *tabs;               // [K] ||t||_1
     const int *texp;                 // [K] template scale exponents
-    const int *kexp_tile;            // [slot][stiles] window scale exponents
+    const int *kexp_tile;            // [group][slot][stiles] window scale exponents
+    const u32 *tgrp;                 // [K] template group of the tensor-core tables (NULL: one group)
+    u32 kt_slots;                    // slots per group in kexp_tile
     u32 stiles;
     float *ua;                       // [slot] ||window||_1
     LazyLk lazy;                     // approximate likelihood entries (tensor-core path)
@@ -427,11 +429,15 @@ __device__ __forceinline__ void ov_item_bounds(const float *__restrict__ q, u32 
 // Interval of a row term: G(a) = H[k0][a] (extra = 0) or H[t][b] (extra =
 // the cross term's own rounding), with the fp16 subnormal terms of
 // tensor-core tables (sub0 / sub1 scaled by the tile's voltage exponent).
-__device__ __forceinline__ void ov_row_interval(const OvArgs &A, u32 g, u32 x, float Hv, float nt, float snt,
-                                                float vn, float krm, float extra, float sub0, float sub1,
+__device__ __forceinline__ void ov_row_interval(const OvArgs &A, u32 g, u32 tmpl, u32 x, float Hv, float nt,
+                                                float snt, float vn, float krm, float extra, float sub0, float sub1,
                                                 float &lo, float &hi) {
     float sx = 0.0f;
-    if (A.kexp_tile) sx = sub0 * ldexpf(1.0f, -A.kexp_tile[(size_t)g * A.stiles + x / 128]) + sub1;
+    if (A.kexp_tile) {
+        // scale exponent of the table tile: per template group, candidate, tile of 128 shifts
+        const size_t grp = A.tgrp ? (size_t)A.tgrp[tmpl] * A.kt_slots : 0;
+        sx = sub0 * ldexpf(1.0f, -A.kexp_tile[(grp + g) * A.stiles + x / 128]) + sub1;
+    }
     const float e = krm * (snt * vn + nt) + 4.0f * kUnitRoundoff * fabsf(Hv) + extra + sx;
     lo = Hv - e;
     hi = Hv + e;
@@ -543,7 +549,7 @@ k_ov_rows(OvArgs A) {
             bool ap = false;
             if (x < S) {
                 float lo, hi;
-                ov_row_interval(A, g, x, Hg[x], A.NT[(size_t)c.k0 * S + x], A.sNT[(size_t)c.k0 * S + x], c.vn,
+                ov_row_interval(A, g, c.k0, x, Hg[x], A.NT[(size_t)c.k0 * S + x], A.sNT[(size_t)c.k0 * S + x], c.vn,
                                 krm, 0.0f, c.subA0, c.subA1, lo, hi);
                 A.ga_lo[(size_t)g * S + x] = lo;
                 A.ga_hi[(size_t)g * S + x] = hi;
@@ -598,7 +604,7 @@ k_ov_seed(OvArgs A) {
         u32 b1 = 0, b2 = 0;
         for (u32 x = c.xlo + lane; x < xend; x += 32) {
             float lo, hi;
-            ov_row_interval(A, g, x, Hg[x], A.NT[(size_t)t * S + x], A.sNT[(size_t)t * S + x], c.vn, krm, eqt,
+            ov_row_interval(A, g, t, x, Hg[x], A.NT[(size_t)t * S + x], A.sNT[(size_t)t * S + x], c.vn, krm, eqt,
                             subB0, subB1, lo, hi);
             if (lo > v1) { v1 = lo; b1 = x; }
             if ((x > a1 ? x - a1 : a1 - x) <= L && lo > v2) { v2 = lo; b2 = x; }
@@ -685,7 +691,7 @@ k_ov_scan(OvArgs A) {
                 ga_lo[x] = A.ga_lo[(size_t)g * S + x];
                 ga_hi[x] = A.ga_hi[(size_t)g * S + x];
                 float lo, hi;
-                ov_row_interval(A, g, x, Hg[x], A.NT[(size_t)t * S + x], A.sNT[(size_t)t * S + x], c.vn, krm, eqt,
+                ov_row_interval(A, g, t, x, Hg[x], A.NT[(size_t)t * S + x], A.sNT[(size_t)t * S + x], c.vn, krm, eqt,
                                 subB0, subB1, lo, hi);
                 hb_lo[x] = lo;
                 hb_hi[x] = hi;
