@@ -215,6 +215,9 @@ k_lik_tc(TcArgs A) {
     float *bmh = (float *)(tsm + lay.bmh);
     const u32 tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     const u32 kWaitLimit = 1u << 24;
+    const u32 sub = MODE == 0 ? (L + kTcM - 1) / kTcM : A.stiles;   // tiles per window / candidate
+    const u64 nitems = (u64)(MODE == 0 ? *A.n_win : *A.n_cand) * sub;
+    if ((u64)blockIdx.x >= nitems) return;           // no tile for this CTA: no set-up at all
     auto bar_full = [&](u32 b) { return smem_u32(&bars[b]); };
     auto bar_empty = [&](u32 b) { return smem_u32(&bars[2 + b]); };
     auto bar_staged = [&](u32 b) { return smem_u32(&bars[4 + b]); };
@@ -260,8 +263,6 @@ k_lik_tc(TcArgs A) {
                      ::"r"(smem_u32(Bs)), "l"(A.Tb), "r"(A.tb_bytes), "r"(bar_tb) : "memory");
     }
 
-    const u32 sub = MODE == 0 ? (L + kTcM - 1) / kTcM : A.stiles;   // tiles per window / candidate
-    const u64 nitems = (u64)(MODE == 0 ? *A.n_win : *A.n_cand) * sub;
     u32 lfp0 = 2u, lfp1 = 2u;                         // MMA thread: parity of the last commit per buffer
     bool tb_ready = false;                           // MMA thread: the template copy has landed
 
@@ -721,8 +722,9 @@ __global__ void k_tc_pack_templates(const float *__restrict__ T, u32 K, u32 Call
 }
 
 // The refinement list (entries whose tensor-core interval straddles 0).
-// One tile segment per block; its entries are ordered by template.  The
-// tile's voltage (all channels) is staged once; a warp takes one entry:
+// One tile segment per block; its entries are ordered by template (so the
+// template reads of neighbouring warps hit the same lines); a warp takes one
+// entry, its lanes reading the voltage coalesced:
 //   1. its lanes form X = -SS_t/2 + sum t*v and S = |SS_t/2| + sum |t*v| in
 //      double (each product exact, the sums' own error negligible);
 //      the reference value R (compute_maximum_likelihood,
@@ -736,7 +738,8 @@ __global__ void k_tc_pack_templates(const float *__restrict__ T, u32 K, u32 Call
 //      order.
 constexpr int kRefThreads = 256;
 __host__ __device__ inline size_t tc_refine_smem_bytes(u32 C, u32 L) {
-    return ((size_t)C * (kTcM + L) + 8) * 4 + (size_t)(kRefThreads / 32) * kWarpChunk * 4;
+    (void)C; (void)L;
+    return (size_t)(kRefThreads / 32) * kWarpChunk * 4;
 }
 __global__ void __launch_bounds__(kRefThreads)
 k_tc_refine(const float *__restrict__ vall, u32 n, u32 Call, u32 Cmax, const float *__restrict__ Tall, u32 K,
@@ -746,9 +749,8 @@ k_tc_refine(const float *__restrict__ vall, u32 n, u32 Call, u32 Cmax, const flo
             const u32 *__restrict__ seg_count, u32 seg_cap, float *__restrict__ Lk, LazyLk z, double gamma,
             u64 *__restrict__ n_seq) {
     extern __shared__ float rsm[];
-    const u32 rl = kTcM + L;               // strip row length
     const u32 lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    float *wbuf = rsm + ((size_t)Cmax * rl + 8) + (size_t)warp * kWarpChunk;
+    float *wbuf = rsm + (size_t)warp * kWarpChunk;
     const u32 nseg = min(*seg_count, seg_cap);
     const u32 tstride = Call * L;          // floats between templates in T
     u32 nseq = 0;
@@ -761,19 +763,13 @@ k_tc_refine(const float *__restrict__ vall, u32 n, u32 Call, u32 Cmax, const flo
         const float *T = Tall + (size_t)clo * L;
         const u32 *trow = tperm ? tperm + t0 : nullptr;
         const u32 CL = C * L;
-        __syncthreads();
-        for (u32 x = threadIdx.x; x < C * rl; x += blockDim.x) {
-            const u32 c = x / rl, i = x % rl, pos = s0 + i;
-            rsm[x] = pos < n ? v[(size_t)c * n + pos] : 0.0f;
-        }
-        __syncthreads();
         for (u32 e = warp; e < cnt; e += kRefThreads / 32) {
             const u32 t = trow ? trow[ref_t[base + e]] : ref_t[base + e], so = ref_s[base + e] - s0;
             const float *tp = T + (size_t)t * tstride;      // the group's channels of template t
             double X = 0.0, S = 0.0;
             for (u32 q = lane; q < CL; q += 32) {
                 const u32 c = q / L, i = q - c * L;
-                const double p = (double)__ldg(tp + q) * (double)rsm[(size_t)c * rl + so + i];
+                const double p = (double)__ldg(tp + q) * (double)__ldg(v + (size_t)c * n + s0 + so + i);
                 X += p;
                 S += fabs(p);
             }
@@ -805,7 +801,7 @@ k_tc_refine(const float *__restrict__ vall, u32 n, u32 Call, u32 Cmax, const flo
                 const u32 m = min(kWarpChunk, CL - q0);
                 for (u32 k = lane; k < m; k += 32) {
                     const u32 q = q0 + k, c = q / L, i = q - c * L;
-                    wbuf[k] = __fmul_rn(__ldg(tp + q), rsm[(size_t)c * rl + so + i]);
+                    wbuf[k] = __fmul_rn(__ldg(tp + q), __ldg(v + (size_t)c * n + s0 + so + i));
                 }
                 __syncwarp();
                 if (lane == 0) acc = warp_chain(acc, wbuf, m);

@@ -807,14 +807,20 @@ __device__ float overlap_item_exact_global(const OvArgs &A, u32 lab, u32 bidx, u
     const u32 L = A.L, C = A.C;
     const u32 afix = bidx + a - A.nmax, ashift = bidx + b - A.nmax;
     const int fa = (int)bidx - (int)afix, sa = (int)bidx - (int)ashift;
-    // channels where either template is non-zero (elsewhere both terms are 0)
-    u32 clo = 0, chi = C;
+    // channels where either template is non-zero, in channel order: the two
+    // supports as one range when they meet, else one after the other
+    // (elsewhere both terms are 0 and the reference's sums do not change)
+    u32 r0 = 0, r1 = C, r2 = C, r3 = C;
     if (A.tsup) {
-        clo = min(A.tsup[2 * lab], A.tsup[2 * t]);
-        chi = max(A.tsup[2 * lab + 1], A.tsup[2 * t + 1]);
+        u32 al = A.tsup[2 * lab], ah = A.tsup[2 * lab + 1], bl = A.tsup[2 * t], bh = A.tsup[2 * t + 1];
+        if (ah <= al) { al = bl; ah = bh; }
+        if (bh <= bl) { bl = al; bh = ah; }
+        if (bl < al) { u32 x = al; al = bl; bl = x; x = ah; ah = bh; bh = x; }
+        if (bl <= ah) { r0 = al; r1 = max(ah, bh); r2 = r3 = r1; }
+        else { r0 = al; r1 = ah; r2 = bl; r3 = bh; }
     }
     float cml = 0.0f;
-    for (u32 c = clo; c < chi; c++) {
+    for (u32 c = r0; c < r3; c = (c + 1 == r1) ? r2 : c + 1) {
         const float *f = A.T + ((size_t)lab * C + c) * L;
         const float *sp = A.T + ((size_t)t * C + c) * L;
         const float *vv = A.v + (size_t)c * A.n + bidx;
