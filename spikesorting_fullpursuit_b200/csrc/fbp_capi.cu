@@ -97,6 +97,7 @@ struct Workspace {
     u32 tc_gmax;                     // template groups the buffers hold
     std::vector<TcGroup> tcg;        // this chunk's groups (planned from the template supports)
     u32 tc_cg2max, tc_cmax;          // largest channel groups / channels of a group
+    u32 tc_nz;                       // widest template support (channels): only non-zero products round
     u32 *tc_gdesc;                   // [group][3]: t0, clo, Cg (device)
     u32 *tgrp;                       // [K] group of each template (device)
     u32 *tc_seg_grp;                 // [seg_cap] group of each refinement segment
@@ -105,6 +106,8 @@ struct Workspace {
     int *tc_texp;
     u8 *apx;
     float *wn_s, *wa_s, *bm_s, *wlb;
+    float *umax;                     // [W][K] largest upper bound of a template's entries per window
+    u8 *wpos;                        // [W] some entry of the window is > 0
     signed char *kx_s;
     u32 *tc_ref_t, *tc_ref_s, *tc_seg_s0, *tc_seg_base, *tc_seg_cnt;
     u32 tc_seg_cap;
@@ -191,6 +194,9 @@ Workspace layout(char *base, u32 n, u32 K, u32 L, u32 nmax, bool want_fast, u32 
     };
     w.cnt = (Counters *)take(sizeof(Counters));
     w.snap = (Counters *)take(sizeof(Counters));
+    w.wlb = (float *)take((size_t)W * 4);
+    w.umax = (float *)take((size_t)W * K * 4);
+    w.wpos = (u8 *)take((size_t)W);
     w.tsup = (u32 *)take((size_t)K * 8);
     w.tperm = (u32 *)take((size_t)K * 4);
     w.grange = (u32 *)take((size_t)ceil_div(K, kLikTplPerBlock) * 8);
@@ -261,7 +267,6 @@ Workspace layout(char *base, u32 n, u32 K, u32 L, u32 nmax, bool want_fast, u32 
         w.apx = (u8 *)take((size_t)K * n);
         w.wn_s = (float *)take((size_t)w.tc_gmax * n * 4);
         w.bm_s = (float *)take((size_t)n * 4);
-        w.wlb = (float *)take((size_t)ceil_div(n, L) * 4);
         w.wa_s = (float *)take((size_t)w.tc_gmax * n * 4);
         w.kx_s = (signed char *)take((size_t)w.tc_gmax * n);
         w.tc_tnorm = (float *)take((size_t)K * 4);
@@ -308,7 +313,7 @@ int compact(const u8 *f, u32 W, u32 *list, u32 *count_dev, u32 *tile_counts, cud
 int launch_likelihood(const float *v, u32 n, u32 C, const float *T, u32 K, u32 L, const float *tss,
                       const u32 *win, const u32 *n_win_dev, u32 max_windows, float *Lk,
                       cudaStream_t st, const u32 *gate = nullptr, u8 *apx = nullptr,
-                      const u32 *tperm = nullptr, const u32 *grange = nullptr) {
+                      const u32 *tperm = nullptr, const u32 *grange = nullptr, WinBounds wb = WinBounds{}) {
     const size_t smem = (size_t)kLikChanChunk * (kLikTile + L) * sizeof(float);
     static size_t configured = 0;
     if (smem > 48 * 1024 && smem > configured) {
@@ -319,17 +324,18 @@ int launch_likelihood(const float *v, u32 n, u32 C, const float *T, u32 K, u32 L
     const u64 items = (u64)max_windows * ceil_div(K, kLikTplPerBlock);
     const int grid = grid_for(items * kLikThreads, kLikThreads, 16);
     k_likelihood_fp32<<<grid, kLikThreads, smem, st>>>(v, n, C, T, K, L, tss, win, n_win_dev, Lk, gate, apx,
-                                                       tperm, grange);
+                                                       tperm, grange, wb);
     FBP_LAUNCH_CHECK();
     return FBP_OK;
 }
 
 int launch_argmax(u32 n, u32 L, u32 K, const u32 *win, const u32 *n_win_dev, u32 max_windows,
-                  const fbp_window_state &s, float *Lk, cudaStream_t st, const LazyLk &z = LazyLk{}) {
+                  const fbp_window_state &s, float *Lk, cudaStream_t st, const LazyLk &z = LazyLk{},
+                  WinBounds wb = WinBounds{}) {
     const int threads = kArgmaxThreads;
     const int grid = grid_for((u64)max_windows * 32, threads, 8);
     k_window_argmax<<<grid, threads, 0, st>>>(n, L, K, win, n_win_dev, s.best_idx, s.best_lab, s.best_ll,
-                                              s.flags, s.overlap_recheck, s.ov_idx, s.ov_lab, Lk, z);
+                                              s.flags, s.overlap_recheck, s.ov_idx, s.ov_lab, Lk, z, wb);
     FBP_LAUNCH_CHECK();
     return FBP_OK;
 }
@@ -398,8 +404,8 @@ LazyLk lazy_ctx(const Workspace &w, const float *v, const float *T, const float 
     z.apx = w.apx; z.wn = w.wn_s; z.wa = w.wa_s; z.kx = w.kx_s;
     z.tnorm = w.tc_tnorm; z.tabs = w.tc_tabs; z.tss = tss; z.texp = w.tc_texp;
     z.v = v; z.T = T; z.C = C; z.L = L;
-    z.kappa_b = tc_kappa(C, L, w.tc_cg2max);
-    z.kappa_s = tc_kappa_s(C, L);
+    z.kappa_b = tc_kappa(w.tc_nz, L, ceil_div(w.tc_nz, 8));
+    z.kappa_s = tc_kappa_s(w.tc_nz, L);
     z.tgrp = w.tgrp; z.gstride = w.n; z.tsup = w.tsup;
     z.refined = &w.cnt->lazy_ref;
     z.wlb = w.wlb; z.bm = w.bm_s;
@@ -431,7 +437,7 @@ OvArgs ov_args(const Workspace &w, const float *v, u32 n, u32 C, const float *T,
     A.ua = w.ua;
     A.lazy = lazy_ctx(w, v, T, tss, C, L, 0);   // read only: the tag is not used
     if (w.tc) {                      // H from the tensor cores
-        A.km_override = tc_kappa(C, L, w.tc_cg2max);
+        A.km_override = tc_kappa(w.tc_nz, L, ceil_div(w.tc_nz, 8));
         A.tgrp = w.tgrp;
         A.kt_slots = w.slots;
         A.tabs = w.tc_tabs;
@@ -576,8 +582,8 @@ TcArgs tc_group_args(const Workspace &w, u32 gi, const float *v, u32 n, u32 C, c
     A.rows_pad = (kTcM + L - 1 + 7) / 8 * 8;
     A.tmem_cols = g.cols;
     A.nbuf = g.nbuf;
-    A.kappa_b = tc_kappa(C, L, w.tc_cg2max);
-    A.kappa_s = tc_kappa_s(C, L);
+    A.kappa_b = tc_kappa(w.tc_nz, L, ceil_div(w.tc_nz, 8));
+    A.kappa_s = tc_kappa_s(w.tc_nz, L);
     A.v = v + (size_t)g.clo * n; A.T = T; A.tss = tss;
     A.tnorm = w.tc_tnorm; A.tabs = w.tc_tabs; A.texp = w.tc_texp;
     A.Tb = w.Tb + g.tb_off;
@@ -588,7 +594,7 @@ TcArgs tc_group_args(const Workspace &w, u32 gi, const float *v, u32 n, u32 C, c
     A.grp = gi;
     A.seg_overflow = &cnt->tc_overflow; A.seg_cap = w.tc_seg_cap;
     A.err = &cnt->tc_err;
-    A.apx = w.apx; A.bm_s = w.bm_s; A.wlb = w.wlb;
+    A.apx = w.apx; A.bm_s = w.bm_s; A.wlb = w.wlb; A.umax = w.umax; A.wpos = w.wpos;
     A.wn_s = w.wn_s + (size_t)gi * n; A.wa_s = w.wa_s + (size_t)gi * n; A.kx_s = w.kx_s + (size_t)gi * n;
     return A;
 }
@@ -597,6 +603,8 @@ TcArgs tc_group_args(const Workspace &w, u32 gi, const float *v, u32 n, u32 C, c
 // ||t|| * ||window||: both operands rounded to fp16 (normal range; the
 // subnormal part is a separate absolute term), FP32 accumulation of every
 // product allowed one ulp of error, and the reference's own recursive sum.
+// C is the number of channels whose products can be non-zero (a template's
+// support): zero products add nothing and round nothing.
 float tc_kappa(u32 C, u32 L, u32 Cg2) {
     const double u_h = 1.0 / 2048.0, u = 1.0 / 16777216.0;
     const double prod = 2.0 * u_h + u_h * u_h;
@@ -645,16 +653,16 @@ int tc_refine_pass(const Workspace &w, const float *v, u32 n, u32 C, const float
         FBP_CUDA(cudaFuncSetAttribute(k_tc_refine, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)rsmem));
     // gamma: the reference's recursive sum of C*L + 1 terms (products
     // rounded once each), plus the double sums' own error
-    const double u = 1.0 / 16777216.0, nr = (double)C * L + 2;
+    const double u = 1.0 / 16777216.0, nr = (double)w.tc_nz * L + 2;
     const double gamma = 1.01 * (nr * u / (1.0 - nr * u)) + 4.0 * nr * 1.1102230246251565e-16;
     k_tc_refine<<<sm_count() * 8, kRefThreads, rsmem, st>>>(
         v, n, C, w.tc_cmax, T, K, L, tss, w.tc_ref_t, w.tc_ref_s, w.tc_seg_s0, w.tc_seg_base, w.tc_seg_cnt,
         w.tc_seg_grp, w.tc_gdesc, w.tperm, reinterpret_cast<const u32 *>(&cnt->tc_refseg), w.tc_seg_cap, Lk,
-        lazy_ctx(w, v, T, tss, C, L, 0), gamma, &cnt->tc_seq);
+        lazy_ctx(w, v, T, tss, C, L, 0), gamma, &cnt->tc_seq, w.wpos);
     k_tc_gate<<<1, 1, 0, st>>>(cnt, w.tc_ref_cap, w.tc_seg_cap);
     FBP_LAUNCH_CHECK();
     int rc = launch_likelihood(v, n, C, T, K, L, tss, win, n_win, max_windows, Lk, st, &cnt->tc_overflow, w.apx,
-                               w.tperm, w.grange);
+                               w.tperm, w.grange, WinBounds{w.wlb, w.umax, w.wpos});
     *launches = 3;
     return rc;
 }
@@ -817,7 +825,11 @@ int fbp_pursuit_chunk(float *voltage, uint32_t n, uint32_t C, const float *templ
     FBP_CUDA(cudaMemsetAsync(w.ovr, 0, wb, st));
     FBP_CUDA(cudaMemsetAsync(w.ovr2, 0, wb, st));
     FBP_CUDA(cudaMemsetAsync(w.active, 0, wb, st));
+    FBP_CUDA(cudaMemsetAsync(w.wlb, 0, (size_t)W * 4, st));
+    FBP_CUDA(cudaMemsetAsync(w.umax, 0, (size_t)W * K * 4, st));
+    FBP_CUDA(cudaMemsetAsync(w.wpos, 0, (size_t)W, st));
     k_iota_windows<<<grid_for(W, 256), 256, 0, st>>>(w.win, w.active, W, w.cnt);
+    k_template_ranges<<<grid_for((u64)K * 32, 256), 256, 0, st>>>(templates, K, C, L, w.tsup);
     k_template_support<<<1, 256, 0, st>>>(templates, K, C, L, w.tsup, w.tperm, w.grange, kLikTplPerBlock,
                                           w.grange32, kTabMGroup);
     FBP_LAUNCH_CHECK();
@@ -835,6 +847,12 @@ int fbp_pursuit_chunk(float *voltage, uint32_t n, uint32_t C, const float *templ
                 w.tc = false;                        // no group fits: the FP32 kernel
             } else {
                 w.tc_cg2max = w.tc_cmax = 0;
+                // adding an exact zero product is exact (in the reference's
+                // sum and in any accumulation order), so the rounding bounds
+                // count the widest support's products, not C*L
+                w.tc_nz = 1;
+                for (u32 t = 0; t < K; t++)
+                    if (tsup[2 * t + 1] > tsup[2 * t]) w.tc_nz = std::max(w.tc_nz, tsup[2 * t + 1] - tsup[2 * t]);
                 std::vector<u32> gdesc(3 * w.tcg.size()), tgrp(K);
                 for (u32 gi = 0; gi < (u32)w.tcg.size(); gi++) {
                     const TcGroup &g = w.tcg[gi];
@@ -861,7 +879,6 @@ int fbp_pursuit_chunk(float *voltage, uint32_t n, uint32_t C, const float *templ
     if (w.tc) {
         timer.begin(FBP_STAGE_LIKELIHOOD);
         FBP_CUDA(cudaMemsetAsync(w.apx, 0, (size_t)K * n, st));
-        FBP_CUDA(cudaMemsetAsync(w.wlb, 0, (size_t)W * 4, st));
         FBP_CUDA(cudaMemsetAsync(w.bm_s, 0, (size_t)n * 4, st));
         int rc0 = tc_chunk_setup(w, templates, K, C, L, st);
         if (rc0) return rc0;
@@ -906,7 +923,8 @@ int fbp_pursuit_chunk(float *voltage, uint32_t n, uint32_t C, const float *templ
             timer.begin(FBP_STAGE_LIKELIHOOD);
         } else {
             if ((rc2 = launch_likelihood(voltage, n, C, templates, K, L, neg_half_ss, w.win, &w.cnt->n_win, W,
-                                         w.Lk, q, nullptr, nullptr, w.tperm, w.grange)))
+                                         w.Lk, q, nullptr, nullptr, w.tperm, w.grange,
+                                         WinBounds{w.wlb, w.umax, w.wpos})))
                 return rc2;
             launched[FBP_STAGE_LIKELIHOOD] += 1;
         }
@@ -914,7 +932,8 @@ int fbp_pursuit_chunk(float *voltage, uint32_t n, uint32_t C, const float *templ
         // 2. per-window argmax over all templates (.py:551-562)
         timer.begin(FBP_STAGE_ARGMAX);
         const LazyLk lz = lazy_ctx(w, voltage, templates, neg_half_ss, C, L, pass);
-        if ((rc2 = launch_argmax(n, L, K, w.win, &w.cnt->n_win, W, s, w.Lk, q, lz))) return rc2;
+        if ((rc2 = launch_argmax(n, L, K, w.win, &w.cnt->n_win, W, s, w.Lk, q, lz, WinBounds{w.wlb, w.umax, w.wpos})))
+            return rc2;
         launched[FBP_STAGE_ARGMAX] += 1;
         timer.end(FBP_STAGE_ARGMAX);
         // 3. candidates = nonzero(overlap_recheck) (.py:565-569), 4. recheck (.py:570-661)
@@ -962,8 +981,8 @@ int fbp_pursuit_chunk(float *voltage, uint32_t n, uint32_t C, const float *templ
         timer.begin(FBP_STAGE_LISTS);
         FBP_CUDA(cudaMemsetAsync(w.ovr, 0, wb, q));
         if ((rc2 = compact(w.flags_out, W, w.win, &w.cnt->n_win, w.tile_counts, q))) return rc2;
-        k_mark_active<<<grid_for(W, 256), 256, 0, q>>>(w.flags_out, w.active, W, w.tc ? w.wlb : nullptr,
-                                                       w.tc ? w.bm_s : nullptr, L, n);
+        k_mark_active<<<grid_for(W, 256), 256, 0, q>>>(w.flags_out, w.active, W, WinBounds{w.wlb, w.umax, w.wpos},
+                                                       w.tc ? w.bm_s : nullptr, L, n, K);
         FBP_CUDA(cudaMemsetAsync(w.flags, 0, wb, q));
         // 8. keep the spikes (.py:702-710)
         k_append_spikes<<<grid_for(W, 256), 256, 0, q>>>(w.spk_idx, w.spk_lab, w.cnt, spike_idx, spike_lab,
@@ -981,7 +1000,7 @@ int fbp_pursuit_chunk(float *voltage, uint32_t n, uint32_t C, const float *templ
             launched[FBP_STAGE_RESIDUAL] += 1;
         }
         k_residual<<<grid_for((u64)W * 256, 256, 16), 256, 0, q>>>(voltage, n, C, templates, K, L, w.spk_idx,
-                                                                    w.spk_lab, &w.cnt->n_spk, 0, R);
+                                                                    w.spk_lab, &w.cnt->n_spk, 0, R, w.tsup);
         FBP_LAUNCH_CHECK();
         launched[FBP_STAGE_RESIDUAL] += 1;
         timer.end(FBP_STAGE_RESIDUAL);
@@ -1104,7 +1123,7 @@ int fbp_compute_residual(float *voltage, uint32_t n, uint32_t C, const float *te
     if (!voltage || !templates || !spike_idx || !spike_lab)
         return fail(FBP_ERR_BAD_ARG, "fbp_compute_residual: null pointer argument");
     k_residual<<<grid_for((u64)n_spikes * 256, 256, 16), 256, 0, (cudaStream_t)stream>>>(
-        voltage, n, C, templates, K, L, spike_idx, spike_lab, nullptr, n_spikes, max_overlap_neighbours);
+        voltage, n, C, templates, K, L, spike_idx, spike_lab, nullptr, n_spikes, max_overlap_neighbours, nullptr);
     FBP_LAUNCH_CHECK();
     return FBP_OK;
 }

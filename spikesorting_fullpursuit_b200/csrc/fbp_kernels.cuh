@@ -15,6 +15,18 @@
 
 namespace fbp {
 
+// Per-window bounds written by the likelihood kernels (both paths) for the
+// window argmax: wlb[w] the largest lower bound of an entry of window w,
+// umax[w][t] the largest upper bound of template t's entries there (>= 0),
+// wpos[w] whether any entry of the window is > 0.  Reset when the window is
+// listed for recomputation; entries only move inside their intervals later.
+struct WinBounds {
+    float *wlb;
+    float *umax;
+    u8 *wpos;
+};
+
+
 // ---------------------------------------------------------------------------
 // Ordered compaction: list of indices j < W with f[j] != 0, ascending.
 // Three launches: per-tile counts, one-block scan of the tile counts, write.
@@ -75,14 +87,17 @@ __global__ void k_iota_windows(u32 *__restrict__ win, u8 *__restrict__ active, u
 // active[j] = (flags[j] != 0) for the next pass.
 // active = flags != 0; windows about to be recomputed also drop their
 // lower bound (wlb, tensor-core path; may be NULL).
-__global__ void k_mark_active(const u8 *__restrict__ flags, u8 *__restrict__ active, u32 W,
-                              float *__restrict__ wlb, float *__restrict__ bm, u32 L, u32 n) {
+__global__ void k_mark_active(const u8 *__restrict__ flags, u8 *__restrict__ active, u32 W, WinBounds wb,
+                              float *__restrict__ bm, u32 L, u32 n, u32 K) {
     for (u32 i = blockIdx.x * blockDim.x + threadIdx.x; i < W; i += gridDim.x * blockDim.x) {
         active[i] = flags[i] != 0;
-        if (wlb && flags[i]) {
-            wlb[i] = 0.0f;
+        if (!flags[i]) continue;
+        if (wb.wlb) wb.wlb[i] = 0.0f;
+        if (wb.wpos) wb.wpos[i] = 0;
+        if (wb.umax)
+            for (u32 t = 0; t < K; t++) wb.umax[(size_t)i * K + t] = 0.0f;
+        if (bm)
             for (u32 s = i * L; s < min((i + 1) * L, n); s++) bm[s] = 0.0f;
-        }
     }
 }
 
@@ -97,27 +112,40 @@ __global__ void k_mark_active(const u8 *__restrict__ flags, u8 *__restrict__ act
 // accumulators of a thread is an independent chain in (channel, lag) order,
 // starting from float32(-0.5*SS) -- exactly the reference's sequence.
 // ---------------------------------------------------------------------------
+__device__ __forceinline__ float warp_max_float(float x) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) x = fmaxf(x, __shfl_xor_sync(0xffffffffu, x, o));
+    return x;
+}
+
 constexpr int kLikThreads = 128;
 
 // Per chunk: each template's non-zero channel range [lo, hi) (tsup), the
 // template order sorted by (lo, id) (tperm), and per group of kLikTplPerBlock
 // consecutive slots the union of their ranges (grange).  One block.
-__global__ void k_template_support(const float *__restrict__ T, u32 K, u32 C, u32 L, u32 *__restrict__ tsup,
-                                   u32 *__restrict__ tperm, u32 *__restrict__ grange, u32 group,
-                                   u32 *__restrict__ grange2, u32 group2) {
-    for (u32 t = threadIdx.x; t < K; t += blockDim.x) {
+// Non-zero channel range of each template: one warp per template.
+__global__ void k_template_ranges(const float *__restrict__ T, u32 K, u32 C, u32 L, u32 *__restrict__ tsup) {
+    const u32 lane = threadIdx.x & 31;
+    for (u32 t = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); t < K; t += gridDim.x * (blockDim.x >> 5)) {
         u32 lo = C, hi = 0;
         for (u32 c = 0; c < C; c++) {
             const float *tp = T + ((size_t)t * C + c) * L;
             bool nz = false;
-            for (u32 i = 0; i < L && !nz; i++) nz = tp[i] != 0.0f;
-            if (nz) { lo = min(lo, c); hi = c + 1; }
+            for (u32 i = lane; i < L; i += 32) nz |= tp[i] != 0.0f;
+            if (__any_sync(0xffffffffu, nz)) { lo = min(lo, c); hi = c + 1; }
         }
         if (hi == 0) lo = 0;                         // all-zero template: empty range
-        tsup[2 * t] = lo;
-        tsup[2 * t + 1] = hi;
+        if (lane == 0) {
+            tsup[2 * t] = lo;
+            tsup[2 * t + 1] = hi;
+        }
     }
-    __syncthreads();
+}
+
+// The template order and group ranges from the supports (one block).
+__global__ void k_template_support(const float *__restrict__ T, u32 K, u32 C, u32 L, u32 *__restrict__ tsup,
+                                   u32 *__restrict__ tperm, u32 *__restrict__ grange, u32 group,
+                                   u32 *__restrict__ grange2, u32 group2) {
     for (u32 t = threadIdx.x; t < K; t += blockDim.x) {
         const u32 lo = tsup[2 * t];
         u32 rank = 0;
@@ -158,7 +186,8 @@ __global__ void __launch_bounds__(kLikThreads)
 k_likelihood_fp32(const float *__restrict__ v, u32 n, u32 C, const float *__restrict__ T, u32 K, u32 L,
                   const float *__restrict__ tss, const u32 *__restrict__ win,
                   const u32 *__restrict__ n_win_dev, float *__restrict__ Lk, const u32 *__restrict__ gate,
-                  u8 *__restrict__ apx, const u32 *__restrict__ tperm, const u32 *__restrict__ grange) {
+                  u8 *__restrict__ apx, const u32 *__restrict__ tperm, const u32 *__restrict__ grange,
+                  WinBounds wb) {
     extern __shared__ float strip[];   // kLikChanChunk x (kLikTile + L)
     if (gate && *gate == 0) return;    // only run when the gate asks for it
     const u32 n_win = *n_win_dev;
@@ -215,6 +244,26 @@ k_likelihood_fp32(const float *__restrict__ v, u32 n, u32 C, const float *__rest
                                 acc[q][r] = __fadd_rn(acc[q][r], __fmul_rn(tv[q], vv[r]));
                     }
                 }
+            }
+            if (wb.umax) {
+                // window bounds: the values are exact (lower = upper bound)
+                bool anypos = false;
+#pragma unroll
+                for (int q = 0; q < kLikQ; q++) {
+                    float mq = 0.0f;
+#pragma unroll
+                    for (int r = 0; r < kLikR; r++) {
+                        const u32 s = s0 + lane + 32 * r;
+                        if (s < ew && s < s0 + kLikTile && s + L < n) mq = fmaxf(mq, acc[q][r]);
+                    }
+                    mq = warp_max_float(mq);
+                    anypos |= mq > 0.0f;
+                    if (lane == 0 && mq > 0.0f && slot0 + q < K) {
+                        atomicMax(reinterpret_cast<int *>(wb.umax) + (size_t)w * K + tq[q], __float_as_int(mq));
+                        atomicMax(reinterpret_cast<int *>(wb.wlb) + w, __float_as_int(mq));
+                    }
+                }
+                if (lane == 0 && anypos) wb.wpos[w] = 1;
             }
 #pragma unroll
             for (int q = 0; q < kLikQ; q++) {
@@ -414,7 +463,7 @@ k_window_argmax(u32 n, u32 L, u32 K, const u32 *__restrict__ win,
                                 u32 *__restrict__ best_lab, float *__restrict__ best_ll,
                                 u8 *__restrict__ flags, u8 *__restrict__ ovr,
                                 u32 *__restrict__ ov_idx, u32 *__restrict__ ov_lab,
-                                float *__restrict__ Lk, LazyLk z) {
+                                float *__restrict__ Lk, LazyLk z, WinBounds wb) {
     __shared__ float abuf[kArgmaxThreads / 32][kWarpChunk];
     const u32 n_win = *n_win_dev;
     const u32 lane = threadIdx.x & 31;
@@ -434,16 +483,32 @@ k_window_argmax(u32 n, u32 L, u32 K, const u32 *__restrict__ win,
         // cannot hold it, so only entries that reach lb need their
         // reference value; every other one is read as stored (< lb).
         float lb = 0.0f;
-        if (z.apx) {
-            lb = z.wlb[id];
-            if (id > 0) lb = fmaxf(lb, z.wlb[id - 1]);
-            if (id + 1 < W) lb = fmaxf(lb, z.wlb[id + 1]);
+        if (wb.wlb) {
+            lb = wb.wlb[id];
+            if (id > 0) lb = fmaxf(lb, wb.wlb[id - 1]);
+            if (id + 1 < W) lb = fmaxf(lb, wb.wlb[id + 1]);
         }
+        // With window bounds only templates whose upper bound over windows
+        // id-1..id+1 reaches lb (and 0) can hold the maximum or tie it: the
+        // others are skipped, the rest scanned in template order.
+        const bool bounded = wb.umax != nullptr;
         u32 nref = 0;
         float bl = 0.0f;                                 // .cl:389-393 (template 0 resets)
         u32 blab = best_lab[id], bidx = best_idx[id];
-        bool check = false;
-        for (u32 t = 0; t < K; t++) {
+        bool check = bounded && wb.wpos[id] != 0;
+        for (u32 t0 = 0; t0 < K; t0 += 32) {
+          bool cand = t0 + lane < K;
+          if (bounded && cand) {
+              const u32 tt = t0 + lane;
+              float u = wb.umax[(size_t)id * K + tt];
+              if (id > 0) u = fmaxf(u, wb.umax[(size_t)(id - 1) * K + tt]);
+              if (id + 1 < W) u = fmaxf(u, wb.umax[(size_t)(id + 1) * K + tt]);
+              cand = u > 0.0f && u >= lb;
+          }
+          u32 tmask = __ballot_sync(0xffffffffu, cand);
+          while (tmask) {
+            const u32 t = t0 + __ffs(tmask) - 1;
+            tmask &= tmask - 1;
             float *row = Lk + (size_t)t * n;
             float lv = -INFINITY;
             u32 li = 0xffffffffu;
@@ -479,6 +544,7 @@ k_window_argmax(u32 n, u32 L, u32 K, const u32 *__restrict__ win,
                 if (ov > lv || (ov == lv && oi < li)) { lv = ov; li = oi; }
             }
             if (lv > bl) { bl = lv; blab = t; bidx = li; }
+          }
         }
         check = __any_sync(0xffffffffu, check);
         if (z.refined) {
@@ -805,27 +871,39 @@ __global__ void k_commit_total(Counters *cnt, u32 cap) {
 // covering it, which applies every covering spike's subtraction in list
 // order -- the sequential reference's result, with no atomics.
 // ---------------------------------------------------------------------------
+// With template supports (tsup, may be NULL), a spike only touches its
+// template's channels: elsewhere it subtracts zeros, which change nothing.
+// Sample (c, x) is then written by the last covering spike whose support
+// holds c, applying every such spike in list order.
+__device__ __forceinline__ bool res_touches(const u32 *tsup, u32 lab, u32 c) {
+    return !tsup || (c >= tsup[2 * lab] && c < tsup[2 * lab + 1]);
+}
 __global__ void k_residual(float *__restrict__ v, u32 n, u32 C, const float *__restrict__ T, u32 K, u32 L,
                            const u32 *__restrict__ idx, const u32 *__restrict__ lab,
-                           const u32 *__restrict__ n_spk_dev, u32 n_spk_host, u32 R) {
+                           const u32 *__restrict__ n_spk_dev, u32 n_spk_host, u32 R,
+                           const u32 *__restrict__ tsup) {
     const u32 m = n_spk_dev ? *n_spk_dev : n_spk_host;
     for (u32 s = blockIdx.x; s < m; s += gridDim.x) {
         const u32 p = idx[s];
         if (lab[s] >= K) continue;                                       // .cl:78-81
         const u32 jlo = s > R ? s - R : 0;
         const u32 jhi = min(m - 1, s + R);
-        for (u32 e = threadIdx.x; e < C * L; e += blockDim.x) {
+        const u32 clo = tsup ? tsup[2 * lab[s]] : 0u, chi = tsup ? tsup[2 * lab[s] + 1] : C;
+        for (u32 e = clo * L + threadIdx.x; e < chi * L; e += blockDim.x) {
             const u32 c = e / L, i = e % L;
             const u32 x = p + i;
             if (x >= n) continue;                                        // .cl:93-96
             bool owner = true;
             for (u32 j = s + 1; j <= jhi; j++)
-                if (lab[j] < K && idx[j] <= x && x < idx[j] + L) { owner = false; break; }
+                if (lab[j] < K && idx[j] <= x && x < idx[j] + L && res_touches(tsup, lab[j], c)) {
+                    owner = false;
+                    break;
+                }
             if (!owner) continue;
             float val = v[(size_t)c * n + x];
             for (u32 j = jlo; j <= s; j++) {
                 const u32 pj = idx[j];
-                if (lab[j] < K && pj <= x && x < pj + L)
+                if (lab[j] < K && pj <= x && x < pj + L && res_touches(tsup, lab[j], c))
                     val = __fsub_rn(val, T[((size_t)lab[j] * C + c) * L + (x - pj)]);
             }
             v[(size_t)c * n + x] = val;

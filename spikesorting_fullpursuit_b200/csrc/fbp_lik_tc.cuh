@@ -89,6 +89,8 @@ struct TcArgs {
     float *wn_s, *wa_s;              // [n] per-sample window norms
     float *bm_s;                     // [n] largest bound of a flagged entry of the sample
     float *wlb;                      // [W] largest lower bound over a window's entries
+    float *umax;                     // [W][Kall] largest upper bound of a template's entries in a window
+    u8 *wpos;                        // [W] some entry of the window is > 0
     signed char *kx_s;               // [n] per-sample fp16 scale exponent
     // overlap-table tiles (MODE 1): rows are the shifts b of a candidate window
     u32 S, nmax, stiles;
@@ -552,10 +554,15 @@ k_lik_tc(TcArgs A) {
             u32 wantbits[8] = {0, 0, 0, 0, 0, 0, 0, 0};  // Np <= 256: word k holds chunks k of both halves
             float lomax = 0.0f, bmax = 0.0f;
             const bool tail = s + L >= n;                // .cl:231-234
+            const u32 wcur = (u32)(s0 / L);               // the tile's window
+            bool anypos = false;
 #pragma unroll
             for (int k = 0; k < 8; k++) {
                 const u32 c0 = 16 * half + 32 * k;
                 if (c0 >= Np) break;                     // uniform in the warp
+                float uq[16];
+#pragma unroll
+                for (int q = 0; q < 16; q++) uq[q] = 0.0f;
                 u32 r[16];
                 asm volatile(
                     "tcgen05.ld.sync.aligned.32x32b.x16.b32 "
@@ -565,8 +572,8 @@ k_lik_tc(TcArgs A) {
                       "=r"(r[14]), "=r"(r[15])
                     : "r"(acc0 + c0));
                 asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
-                if (!in_win) continue;
                 u32 cw = 0;
+                if (in_win) {
 #pragma unroll
                 for (int q = 0; q < 16; q++) {
                     const u32 t = c0 + q;
@@ -589,10 +596,22 @@ k_lik_tc(TcArgs A) {
                     cw |= (!tail && !pos && !neg) ? (1u << q) : 0u;
                     *dst = tail ? 0.0f : approx;
                     *fl = (!tail && pos) ? (u8)1 : (u8)0;
+                    uq[q] = tail ? 0.0f : fmaxf(0.0f, approx + E);
+                    anypos |= !tail && pos;
                 }
                 if (tail) lomax = 0.0f, bmax = 0.0f;
                 wantbits[k] |= cw << (16 * half);
+                }
+                // per (window, template): the largest upper bound over the tile's rows
+#pragma unroll
+                for (int q = 0; q < 16; q++) {
+                    const float u = warp_max_f(uq[q]);
+                    if (lane == 0 && u > 0.0f && c0 + q < A.K)
+                        atomicMax(reinterpret_cast<int *>(A.umax) + (size_t)wcur * A.Kall + ctrow[c0 + q],
+                                  __float_as_int(u));
+                }
             }
+            if (__any_sync(0xffffffffu, anypos) && lane == 0) A.wpos[wcur] = 1;
             // accumulator b and the row sums are no longer needed
             asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
             __syncwarp();
@@ -747,7 +766,7 @@ k_tc_refine(const float *__restrict__ vall, u32 n, u32 Call, u32 Cmax, const flo
             const u32 *__restrict__ seg_s0, const u32 *__restrict__ seg_base, const u32 *__restrict__ seg_cnt,
             const u32 *__restrict__ seg_grp, const u32 *__restrict__ gdesc, const u32 *__restrict__ tperm,
             const u32 *__restrict__ seg_count, u32 seg_cap, float *__restrict__ Lk, LazyLk z, double gamma,
-            u64 *__restrict__ n_seq) {
+            u64 *__restrict__ n_seq, u8 *__restrict__ wpos) {
     extern __shared__ float rsm[];
     const u32 lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     float *wbuf = rsm + (size_t)warp * kWarpChunk;
@@ -788,6 +807,7 @@ k_tc_refine(const float *__restrict__ vall, u32 n, u32 Call, u32 Cmax, const flo
                     Lk[idx] = xf;
                     if (X - bnd > 0.0) {                 // certainly > 0: refined on demand
                         z.apx[idx] = 1;
+                        wpos[(s0 + so) / L] = 1;
                         const u32 s = s0 + so;
                         atomicMax(reinterpret_cast<int *>(const_cast<float *>(z.bm)) + s,
                                   __float_as_int(lazy_bound(z, t, s, xf)));
@@ -809,6 +829,7 @@ k_tc_refine(const float *__restrict__ vall, u32 n, u32 Call, u32 Cmax, const flo
             }
             if (lane == 0) {
                 Lk[idx] = acc;
+                if (acc > 0.0f) wpos[(s0 + so) / L] = 1;
                 nseq++;
             }
         }
