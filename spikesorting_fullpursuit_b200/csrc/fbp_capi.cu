@@ -99,6 +99,8 @@ struct Workspace {
     u32 tc_cg2max, tc_cmax;          // largest channel groups / channels of a group
     u32 tc_nz;                       // widest template support (channels): only non-zero products round
     u32 *tc_gdesc;                   // [group][3]: t0, clo, Cg (device)
+    TcArgs *tc_args0, *tc_args1;     // [group] launch arguments: likelihood tiles, overlap tables (device)
+    size_t tc_smem;                  // dynamic shared memory of the largest group
     u32 *tgrp;                       // [K] group of each template (device)
     u32 *tc_seg_grp;                 // [seg_cap] group of each refinement segment
     uint4 *Tb;
@@ -282,6 +284,8 @@ Workspace layout(char *base, u32 n, u32 K, u32 L, u32 nmax, bool want_fast, u32 
         w.tc_seg_grp = (u32 *)take((size_t)w.tc_seg_cap * 4);
         w.tc_gdesc = (u32 *)take((size_t)w.tc_gmax * 12);
         w.tgrp = (u32 *)take((size_t)K * 4);
+        w.tc_args0 = (TcArgs *)take((size_t)w.tc_gmax * sizeof(TcArgs));
+        w.tc_args1 = (TcArgs *)take((size_t)w.tc_gmax * sizeof(TcArgs));
     }
     w.n = n;
     w.bytes = off;
@@ -476,17 +480,10 @@ int ov_fast_tables(const Workspace &w, const OvArgs &A, Counters *cnt, cudaStrea
     k_ov_prep<<<grid_for((u64)slots * 32, 256), 256, 0, st>>>(A);
     FBP_LAUNCH_CHECK();
     if (w.tc) {
-        for (u32 gi = 0; gi < (u32)w.tcg.size(); gi++) {
-            TcArgs T = tc_group_args(w, gi, A.v, A.n, A.C, A.T, A.K, A.L, nullptr, nullptr, cnt);
-            T.S = S; T.nmax = A.nmax; T.stiles = w.stiles;
-            T.cand = A.cand; T.n_cand = A.n_cand; T.best_idx = A.best_idx; T.cskip = A.cskip;
-            T.NT = A.NT; T.H = A.H;
-            T.kexp_tile = w.kexp_tile + (size_t)gi * slots * w.stiles;
-            const size_t smem = tc_smem_bytes(A.L, T.Cg2, T.Np, T.nbuf);
-            FBP_CUDA(cudaFuncSetAttribute(k_lik_tc<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-            k_lik_tc<1><<<sm_count(), kTcThreads, smem, st>>>(T);
-            FBP_LAUNCH_CHECK();
-        }
+        FBP_CUDA(cudaFuncSetAttribute(k_lik_tc<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)w.tc_smem));
+        const u32 G = (u32)w.tcg.size();
+        k_lik_tc<1><<<std::max<u32>(sm_count(), G), kTcThreads, w.tc_smem, st>>>(w.tc_args1, G);
+        FBP_LAUNCH_CHECK();
     } else if (w.masked_tables) {
         const size_t smem = tables_m_smem_bytes(S, A.L);
         if (smem > 48 * 1024)
@@ -501,7 +498,7 @@ int ov_fast_tables(const Workspace &w, const OvArgs &A, Counters *cnt, cudaStrea
         k_ov_tables<<<grid_for((u64)slots * kTabThreads, kTabThreads, 4), kTabThreads, smem, st>>>(A);
         FBP_LAUNCH_CHECK();
     }
-    *launches = 1 + (w.tc ? (int)w.tcg.size() : 1);
+    *launches = 2;
     return FBP_OK;
 }
 
@@ -631,15 +628,12 @@ int tc_likelihood_pass(const Workspace &w, const float *v, u32 n, u32 C, const f
                        Counters *cnt, cudaStream_t st, int *launches) {
     (void)max_windows;
     FBP_CUDA(cudaMemsetAsync(&cnt->tc_refseg, 0, 8, st));
-    for (u32 gi = 0; gi < (u32)w.tcg.size(); gi++) {
-        TcArgs A = tc_group_args(w, gi, v, n, C, T, K, L, tss, Lk, cnt);
-        A.win = win; A.n_win = n_win;
-        const size_t smem = tc_smem_bytes(L, A.Cg2, A.Np, A.nbuf);
-        FBP_CUDA(cudaFuncSetAttribute(k_lik_tc<0>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-        k_lik_tc<0><<<sm_count(), kTcThreads, smem, st>>>(A);
-        FBP_LAUNCH_CHECK();
-    }
-    *launches = (int)w.tcg.size();
+    (void)v; (void)n; (void)C; (void)T; (void)K; (void)L; (void)tss; (void)win; (void)n_win; (void)Lk;
+    FBP_CUDA(cudaFuncSetAttribute(k_lik_tc<0>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)w.tc_smem));
+    const u32 G = (u32)w.tcg.size();
+    k_lik_tc<0><<<std::max<u32>(sm_count(), G), kTcThreads, w.tc_smem, st>>>(w.tc_args0, G);
+    FBP_LAUNCH_CHECK();
+    *launches = 1;
     return FBP_OK;
 }
 
@@ -882,6 +876,28 @@ int fbp_pursuit_chunk(float *voltage, uint32_t n, uint32_t C, const float *templ
         FBP_CUDA(cudaMemsetAsync(w.bm_s, 0, (size_t)n * 4, st));
         int rc0 = tc_chunk_setup(w, templates, K, C, L, st);
         if (rc0) return rc0;
+        // launch arguments of every template group (constant for the chunk)
+        {
+            const u32 G = (u32)w.tcg.size();
+            std::vector<TcArgs> a0(G), a1(G);
+            w.tc_smem = 0;
+            for (u32 gi = 0; gi < G; gi++) {
+                a0[gi] = tc_group_args(w, gi, voltage, n, C, templates, K, L, neg_half_ss, w.Lk, w.cnt);
+                a0[gi].win = w.win;
+                a0[gi].n_win = &w.cnt->n_win;
+                a1[gi] = tc_group_args(w, gi, voltage, n, C, templates, K, L, nullptr, nullptr, w.cnt);
+                if (w.fast && do_overlap_recheck) {
+                    a1[gi].S = 2 * nmax + 1; a1[gi].nmax = nmax; a1[gi].stiles = w.stiles;
+                    a1[gi].cand = w.cand; a1[gi].n_cand = &w.cnt->n_cand; a1[gi].best_idx = w.best_idx;
+                    a1[gi].cskip = w.cskip; a1[gi].NT = w.NT; a1[gi].H = w.H;
+                    a1[gi].kexp_tile = w.kexp_tile + (size_t)gi * w.slots * w.stiles;
+                }
+                w.tc_smem = std::max(w.tc_smem, tc_smem_bytes(L, a0[gi].Cg2, a0[gi].Np, a0[gi].nbuf));
+            }
+            FBP_CUDA(cudaMemcpyAsync(w.tc_args0, a0.data(), G * sizeof(TcArgs), cudaMemcpyHostToDevice, st));
+            FBP_CUDA(cudaMemcpyAsync(w.tc_args1, a1.data(), G * sizeof(TcArgs), cudaMemcpyHostToDevice, st));
+            FBP_CUDA(cudaStreamSynchronize(st));   // the host vectors go out of scope
+        }
         S.launches[FBP_STAGE_LIKELIHOOD] += 2;
         timer.end(FBP_STAGE_LIKELIHOOD);
     }

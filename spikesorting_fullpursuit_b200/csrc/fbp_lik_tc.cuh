@@ -199,7 +199,24 @@ __device__ __forceinline__ bool mbar_wait_bounded(u32 bar, u32 parity, u32 limit
 // sets err and the abort flag, and every role leaves its loop.
 template <int MODE>
 __global__ void __launch_bounds__(kTcThreads, 1)
-k_lik_tc(TcArgs A) {
+k_lik_tc(const TcArgs *__restrict__ gargs, u32 ngroups) {
+    // CTAs are split over the template groups in proportion (the first
+    // gridDim % ngroups groups get one more); a CTA loads its group's
+    // templates once and takes that group's tiles bi, bi + cnt, ...
+    u32 gi, bi, cnt;
+    {
+        const u32 b = blockIdx.x, base = gridDim.x / ngroups, rem = gridDim.x % ngroups;
+        if (base == 0) {
+            gi = b; bi = 0; cnt = 1;
+        } else if (b < rem * (base + 1)) {
+            gi = b / (base + 1); bi = b % (base + 1); cnt = base + 1;
+        } else {
+            const u32 b2 = b - rem * (base + 1);
+            gi = rem + b2 / base; bi = b2 % base; cnt = base;
+        }
+        if (gi >= ngroups) return;
+    }
+    const TcArgs &A = gargs[gi];
     extern __shared__ __align__(128) unsigned char tsm[];
     const u32 L = A.L, Cg2 = A.Cg2, Np = A.Np, rows_pad = A.rows_pad, n = A.n, nbuf = A.nbuf;
     const TcSmem lay = tc_smem_layout(L, Cg2, Np, nbuf);
@@ -219,7 +236,7 @@ k_lik_tc(TcArgs A) {
     const u32 kWaitLimit = 1u << 24;
     const u32 sub = MODE == 0 ? (L + kTcM - 1) / kTcM : A.stiles;   // tiles per window / candidate
     const u64 nitems = (u64)(MODE == 0 ? *A.n_win : *A.n_cand) * sub;
-    if ((u64)blockIdx.x >= nitems) return;           // no tile for this CTA: no set-up at all
+    if ((u64)bi >= nitems) return;                   // no tile for this CTA: no set-up at all
     auto bar_full = [&](u32 b) { return smem_u32(&bars[b]); };
     auto bar_empty = [&](u32 b) { return smem_u32(&bars[2 + b]); };
     auto bar_staged = [&](u32 b) { return smem_u32(&bars[4 + b]); };
@@ -273,7 +290,7 @@ k_lik_tc(TcArgs A) {
         const u32 pt = tid;                          // 0..127
         u32 use0 = 0u, use1 = 0u;                    // uses of each buffer so far
         u32 it = 0;
-        for (u64 item = blockIdx.x; item < nitems; item += gridDim.x) {
+        for (u64 item = bi; item < nitems; item += cnt) {
             long long s0;
             u32 ew = 0, g = 0;
             long long m_lo = 0, m_hi = n;
@@ -301,7 +318,7 @@ k_lik_tc(TcArgs A) {
             unsigned char *As = tsm + lay.As + (size_t)b * rows_pad * Cg2 * 16;
             // ---- the next tile's voltage rows into L2 (one 128-byte line per thread)
             {
-                const u64 nx = item + gridDim.x;
+                const u64 nx = item + cnt;
                 if (MODE == 0 && nx < nitems) {
                     const u32 w2 = A.win[nx / sub];
                     const long long p0 = (long long)w2 * L + (u32)(nx % sub) * kTcM;
@@ -427,7 +444,7 @@ k_lik_tc(TcArgs A) {
         const u64 db0 = umma_desc(smem_u32(Bs), lbo_b, 128);
         u32 use0 = 0u, use1 = 0u;
         u32 it = 0;
-        for (u64 item = blockIdx.x; item < nitems; item += gridDim.x) {
+        for (u64 item = bi; item < nitems; item += cnt) {
             if (MODE == 1) {
                 const u32 gg = (u32)(item / sub);
                 if (A.cskip[gg]) continue;
@@ -481,7 +498,7 @@ k_lik_tc(TcArgs A) {
         const u32 row = quad * 32 + lane;
         u32 use0 = 0u, use1 = 0u;
         u32 it = 0;
-        for (u64 item = blockIdx.x; item < nitems; item += gridDim.x) {
+        for (u64 item = bi; item < nitems; item += cnt) {
             if (MODE == 1) {
                 const u32 gg = (u32)(item / sub);
                 if (A.cskip[gg]) continue;
