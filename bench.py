@@ -50,6 +50,16 @@ def parse():
                     help="seconds of recording timed on the CPU baseline")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--mode", choices=["pursuit", "batch", "serve"], default="pursuit",
+                    help="pursuit: one segment per step (the headline line); batch: many uneven segments "
+                         "sorted concurrently; serve: Poisson request arrivals, p50/p99 latency")
+    ap.add_argument("--segments", type=int, default=None,
+                    help="batch: segments (default 256); serve: requests (default 48)")
+    ap.add_argument("--time-scale", type=float, default=0.05,
+                    help="batch/serve: factor on the segment durations of the workload")
+    ap.add_argument("--slots", type=int, default=4, help="batch/serve: concurrent requests on the GPU")
+    ap.add_argument("--rates", default="0.5,0.8,0.95",
+                    help="serve: arrival rates as fractions of the measured saturated request rate")
     return ap.parse_args()
 
 
@@ -165,6 +175,108 @@ def run_reference_arm(args, rank, world):
     print(json.dumps(line), flush=True)
 
 
+# ---------------------------------------------------------------- batch / serve
+
+def _make_segment(spec_dict):
+    from spikesorting_fullpursuit_b200 import synthetic
+    rec = synthetic.SegmentSpec(**spec_dict).make()
+    return (np.ascontiguousarray(rec.voltage), rec.sort_info(), rec.fresh_metrics(),
+            rec.n_samples_per_chan - 1)
+
+
+def make_segments(specs):
+    """Generate the segments on the host cores (spawned workers, before any
+    CUDA call of this process)."""
+    import multiprocessing as mp
+    from concurrent.futures import ProcessPoolExecutor
+    workers = max(1, min(len(specs), os.cpu_count() or 1))
+    with ProcessPoolExecutor(max_workers=workers, mp_context=mp.get_context("spawn")) as ex:
+        return list(ex.map(_make_segment, [sp.as_dict() for sp in specs], chunksize=1))
+
+
+def _same(a, b):
+    if isinstance(a[0], list) or isinstance(b[0], list):
+        return len(a[0]) == len(b[0]) == 0
+    return np.array_equal(a[0], b[0]) and np.array_equal(a[1], b[1])
+
+
+def run_mix(args):
+    """Batched sorting (uneven segments, all submitted at once) or serving
+    (Poisson arrivals at rates swept up to the saturated rate) through the
+    continuous-batching server; bf16+refine and plain fp32 side by side.
+    Every request's spikes are compared across precisions and runs."""
+    from spikesorting_fullpursuit_b200 import synthetic
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    serve = args.mode == "serve"
+    nseg = args.segments or (48 if serve else 256)
+    specs = (synthetic.serve_mix(nseg, seed=4 + rank, time_scale=args.time_scale) if serve else
+             synthetic.batch_mix(nseg, seed=3 + rank, time_scale=args.time_scale))
+    t_gen = time.perf_counter()
+    segs = make_segments(specs)
+    t_gen = time.perf_counter() - t_gen
+
+    import torch
+    from spikesorting_fullpursuit_b200 import build as B
+    from spikesorting_fullpursuit_b200.serving import PursuitServer, drive, latency_summary, poisson_arrivals
+    if B.needs_build():
+        B.build()
+    torch.cuda.set_device(local)
+    units = float(sum(sp.units for sp in specs))
+    clocks = ClockSampler(local)
+    out = {}
+    reference_outputs = None
+    identical = True
+    clocks.start()
+    for prec in ("bf16", "fp32"):
+        with PursuitServer(slots=args.slots, precision=prec, overlap=args.overlap) as srv:
+            drive(srv, segs[: 2 * args.slots])                        # warm-up (untimed)
+            torch.cuda.synchronize()
+            res, wall = drive(srv, segs)                                # saturated: all at once
+            torch.cuda.synchronize()
+            summ = latency_summary(res, wall)
+            summ.update({"wall_s": wall, "requests_per_s": len(res) / wall, "max_running": srv.max_running,
+                         "max_hbm_in_use_gb": srv.max_in_use / 1e9, "hbm_budget_gb": srv.hbm_budget / 1e9})
+            outs = [r.outputs for r in res]
+            if reference_outputs is None:
+                reference_outputs = outs
+            identical &= all(_same(a, b) for a, b in zip(outs, reference_outputs))
+            entry = {"saturated": summ}
+            if serve:
+                sweep = []
+                cap = len(res) / wall
+                for j, frac in enumerate(float(x) for x in args.rates.split(",")):
+                    arr = poisson_arrivals(frac * cap, len(segs), seed=100 + j)
+                    r2, w2 = drive(srv, segs, arr)
+                    torch.cuda.synchronize()
+                    s2 = latency_summary(r2, w2)
+                    s2.update({"rate_fraction": frac, "rate_per_s": frac * cap, "max_running": srv.max_running})
+                    identical &= all(_same(a.outputs, b) for a, b in zip(r2, reference_outputs))
+                    sweep.append(s2)
+                entry["poisson"] = sweep
+            out[prec] = entry
+    clock_info = clocks.stop()
+    bf, fp = out["bf16"]["saturated"], out["fp32"]["saturated"]
+    line = {"metric": ("serving p50/p99 segment latency vs pursuit sample*template/s" if serve
+                       else "batched pursuit sample*template/s"),
+            "value": bf["throughput"], "unit": UNIT, "n_gpus": 1, "higher_is_better": True,
+            "fp32_value": fp["throughput"], "bf16_over_fp32": bf["throughput"] / fp["throughput"],
+            "spikes_identical_bf16_fp32_and_across_runs": bool(identical),
+            "data": "synthetic (seeded per request)",
+            "config": {"workload": "serve_mix" if serve else "batch_mix", "requests": nseg,
+                       "time_scale": args.time_scale, "slots": args.slots, "overlap": args.overlap,
+                       "n_max_shift": "L-1", "units": units,
+                       "channels": [min(sp.n_chans for sp in specs), max(sp.n_chans for sp in specs)],
+                       "templates": [min(sp.n_templates for sp in specs), max(sp.n_templates for sp in specs)],
+                       "durations_s": [min(sp.duration_s for sp in specs), max(sp.duration_s for sp in specs)],
+                       "generation_s": t_gen,
+                       "timing": "wall clock from first arrival to last completion, GPU synchronised; "
+                                 "host voltage copied to the device inside each request"},
+            "bf16": out["bf16"], "fp32": out["fp32"], "clocks": clock_info}
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+
+
 # ---------------------------------------------------------------- our arm
 
 def main():
@@ -174,6 +286,9 @@ def main():
     local = int(os.environ.get("LOCAL_RANK", "0"))
     if args.impl == "reference":
         run_reference_arm(args, rank, world)
+        return
+    if args.mode != "pursuit":
+        run_mix(args)
         return
 
     import torch

@@ -49,13 +49,13 @@ int fail(int code, const char *fmt, ...) {
     } while (0)
 
 int sm_count() {
-    static int cached = 0;
-    if (!cached) {
-        int dev = 0;
+    // initialised once, thread-safely (calls may come from several host threads)
+    static const int cached = [] {
+        int dev = 0, n = 0;
         cudaGetDevice(&dev);
-        cudaDeviceGetAttribute(&cached, cudaDevAttrMultiProcessorCount, dev);
-        if (cached <= 0) cached = 148;
-    }
+        cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev);
+        return n > 0 ? n : 148;
+    }();
     return cached;
 }
 
@@ -319,11 +319,9 @@ int launch_likelihood(const float *v, u32 n, u32 C, const float *T, u32 K, u32 L
                       cudaStream_t st, const u32 *gate = nullptr, u8 *apx = nullptr,
                       const u32 *tperm = nullptr, const u32 *grange = nullptr, WinBounds wb = WinBounds{}) {
     const size_t smem = (size_t)kLikChanChunk * (kLikTile + L) * sizeof(float);
-    static size_t configured = 0;
-    if (smem > 48 * 1024 && smem > configured) {
+    if (smem > 48 * 1024) {
         FBP_CUDA(cudaFuncSetAttribute(k_likelihood_fp32, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                       (int)smem));
-        configured = smem;
     }
     const u64 items = (u64)max_windows * ceil_div(K, kLikTplPerBlock);
     const int grid = grid_for(items * kLikThreads, kLikThreads, 16);
@@ -351,11 +349,9 @@ int launch_overlap(const float *v, u32 n, u32 C, const float *T, u32 K, u32 L, c
     const size_t smem = (size_t)2 * C * L * sizeof(float);
     if (smem > 227 * 1024)
         return fail(FBP_ERR_BAD_ARG, "overlap recheck: C*L = %u too large for shared memory", C * L);
-    static size_t configured = 0;
-    if (smem > 48 * 1024 && smem > configured) {
+    if (smem > 48 * 1024) {
         FBP_CUDA(cudaFuncSetAttribute(k_overlap_exact, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                       (int)smem));
-        configured = smem;
     }
     const int grid = grid_for((u64)max_cand * kOvThreads, kOvThreads, 4);
     k_overlap_exact<<<grid, kOvThreads, smem, st>>>(v, n, C, T, K, L, cand, n_cand_dev, s.best_idx,

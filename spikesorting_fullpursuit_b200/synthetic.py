@@ -212,7 +212,7 @@ def make_recording(*, n_chans, duration_s, fs, n_templates, L, pre_fraction,
                    amp_range=(3.0, 10.0), amp_lognormal_median=None,
                    rate_range=(5.0, 50.0), gain="uniform", mask_chans=None,
                    overlap_fraction=0.0, overlap_window_s=1e-3,
-                   int16_scale=None, seed=0, name="") -> Recording:
+                   int16_scale=None, autocov_chans=None, seed=0, name="") -> Recording:
     rng = np.random.Generator(np.random.PCG64(seed))
     n = int(round(duration_s * fs))
     C, K = n_chans, n_templates
@@ -220,7 +220,9 @@ def make_recording(*, n_chans, duration_s, fs, n_templates, L, pre_fraction,
     align = int(round(pre_fraction * (L - 1)))
 
     noise = bandlimited_noise(rng, C, n, fs)
-    acov = noise_autocov(noise[:, : min(n, 400000)], L)
+    # the noise is i.i.d. across channels: autocov_chans (None = all) bounds
+    # the channels the average is taken over
+    acov = noise_autocov(noise[: (C if autocov_chans is None else min(C, autocov_chans)), : min(n, 400000)], L)
     idx = np.abs(np.subtract.outer(np.arange(L), np.arange(L)))
     cov = acov[idx]
 
@@ -331,3 +333,66 @@ def hd384(duration_s=300.0, seed=2, **kw):
                 name="hd384_300u")
     args.update(kw)
     return make_recording(**args)
+
+
+# --- request mixes for batched sorting and serving -------------------------
+
+class SegmentSpec:
+    """Shape of one request segment; `make()` generates it from its seed."""
+
+    __slots__ = ("seed", "model", "n_chans", "duration_s", "fs", "n_templates", "L")
+
+    def __init__(self, seed, model, n_chans, duration_s, fs, n_templates, L):
+        self.seed, self.model, self.n_chans = int(seed), model, int(n_chans)
+        self.duration_s, self.fs = float(duration_s), float(fs)
+        self.n_templates, self.L = int(n_templates), int(L)
+
+    @property
+    def units(self):
+        """samples x templates of the segment."""
+        return int(round(self.duration_s * self.fs)) * self.n_templates
+
+    def make(self):
+        common = dict(n_chans=self.n_chans, duration_s=self.duration_s, fs=self.fs,
+                      n_templates=self.n_templates, L=self.L, seed=self.seed, autocov_chans=16)
+        if self.model == "tetrode":
+            return make_recording(pre_fraction=0.4, amp_range=(3.0, 10.0), rate_range=(5.0, 50.0),
+                                  gain="uniform", name="seg_tetrode", **common)
+        return make_recording(pre_fraction=0.4, amp_lognormal_median=6.0, rate_range=(0.5, 100.0),
+                              gain="mask", mask_chans=16, name="seg_hd", **common)
+
+    def as_dict(self):
+        return {k: getattr(self, k) for k in self.__slots__}
+
+
+def batch_mix(n_segments=256, seed=3, time_scale=1.0):
+    """Uneven segments of the batched-sorting workload: durations uniform
+    1-60 s (times `time_scale`) at 40 kHz, 4-32 channels, 2-40 templates,
+    61-101-sample clips; the tetrode generative model."""
+    rng = np.random.Generator(np.random.PCG64(seed))
+    out = []
+    for i in range(n_segments):
+        out.append(SegmentSpec(seed * 1000003 + i, "tetrode", rng.integers(4, 33),
+                               rng.uniform(1.0, 60.0) * time_scale, 40000.0, rng.integers(2, 41),
+                               rng.integers(61, 102)))
+    return out
+
+
+def serve_mix(n_requests, seed=4, time_scale=1.0):
+    """Requests of the serving workload, each with its own seed: 4-384
+    channels, 2-120 s (times `time_scale`) at 30 or 40 kHz float32, 4-300
+    templates.  Up to 32 channels the tetrode model (templates on all
+    channels, at most 40 of them, 40 kHz); above, the high-density model
+    (16-channel masks, 61-sample clips, 30 kHz)."""
+    rng = np.random.Generator(np.random.PCG64(seed))
+    out = []
+    for i in range(n_requests):
+        C = int(rng.integers(4, 385))
+        dur = rng.uniform(2.0, 120.0) * time_scale
+        if C <= 32:
+            spec = SegmentSpec(seed * 1000003 + i, "tetrode", C, dur, 40000.0, rng.integers(4, 41),
+                               rng.integers(61, 102))
+        else:
+            spec = SegmentSpec(seed * 1000003 + i, "hd", C, dur, 30000.0, rng.integers(4, 301), 61)
+        out.append(spec)
+    return out
