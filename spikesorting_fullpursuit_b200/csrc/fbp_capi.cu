@@ -59,6 +59,34 @@ int sm_count() {
     return cached;
 }
 
+// Raises the dynamic shared memory limit of `func` to the device's opt-in
+// maximum, once per kernel and device.  The limit is a process-wide kernel
+// attribute: setting it per call to the call's own size would let one host
+// thread shrink it under another thread's launch (or captured graph) of the
+// same kernel with a larger size.
+std::mutex g_attr_mu;
+std::vector<std::pair<const void *, int>> g_attr_done;
+int allow_smem(const void *func) {
+    int dev = 0;
+    FBP_CUDA(cudaGetDevice(&dev));
+    std::lock_guard<std::mutex> lk(g_attr_mu);
+    for (const auto &d : g_attr_done)
+        if (d.first == func && d.second == dev) return FBP_OK;
+    int mx = 0;
+    FBP_CUDA(cudaDeviceGetAttribute(&mx, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev));
+    cudaFuncAttributes fa;
+    FBP_CUDA(cudaFuncGetAttributes(&fa, func));          // the kernel's static shared memory counts too
+    FBP_CUDA(cudaFuncSetAttribute(func, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  mx - (int)fa.sharedSizeBytes));
+    g_attr_done.emplace_back(func, dev);
+    return FBP_OK;
+}
+#define FBP_ALLOW_SMEM(kern)                                                               \
+    do {                                                                                   \
+        const int rc_ = allow_smem((const void *)&kern);                                 \
+        if (rc_ != FBP_OK) return rc_;                                                     \
+    } while (0)
+
 // A template group of the tensor-core likelihood: columns t0..t0+nt of the
 // support order (tperm), channels [clo, clo + Cg) of the recording.
 struct TcGroup {
@@ -320,8 +348,7 @@ int launch_likelihood(const float *v, u32 n, u32 C, const float *T, u32 K, u32 L
                       const u32 *tperm = nullptr, const u32 *grange = nullptr, WinBounds wb = WinBounds{}) {
     const size_t smem = (size_t)kLikChanChunk * (kLikTile + L) * sizeof(float);
     if (smem > 48 * 1024) {
-        FBP_CUDA(cudaFuncSetAttribute(k_likelihood_fp32, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                      (int)smem));
+        FBP_ALLOW_SMEM(k_likelihood_fp32);
     }
     const u64 items = (u64)max_windows * ceil_div(K, kLikTplPerBlock);
     const int grid = grid_for(items * kLikThreads, kLikThreads, 16);
@@ -350,8 +377,7 @@ int launch_overlap(const float *v, u32 n, u32 C, const float *T, u32 K, u32 L, c
     if (smem > 227 * 1024)
         return fail(FBP_ERR_BAD_ARG, "overlap recheck: C*L = %u too large for shared memory", C * L);
     if (smem > 48 * 1024) {
-        FBP_CUDA(cudaFuncSetAttribute(k_overlap_exact, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                      (int)smem));
+        FBP_ALLOW_SMEM(k_overlap_exact);
     }
     const int grid = grid_for((u64)max_cand * kOvThreads, kOvThreads, 4);
     k_overlap_exact<<<grid, kOvThreads, smem, st>>>(v, n, C, T, K, L, cand, n_cand_dev, s.best_idx,
@@ -457,7 +483,7 @@ int ov_chunk_setup(const Workspace &w, const float *T, u32 K, u32 C, u32 L, u32 
     k_ov_q_table<<<grid_for(rows, 128, 16), 128, 0, st>>>(T, K, C, L, w.Q, w.tsup);
     const size_t xm_smem = (size_t)(2 * L - 1) * (L + 1) * 4;
     if (xm_smem > 48 * 1024)
-        FBP_CUDA(cudaFuncSetAttribute(k_ov_xm, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)xm_smem));
+        FBP_ALLOW_SMEM(k_ov_xm);
     k_ov_xm<<<(int)std::min<u64>((u64)K * K, (u64)sm_count() * 2), 256, xm_smem, st>>>(w.Q, K, L, nmax, w.oc, w.XMr,
                                                                                         w.XM);
     FBP_LAUNCH_CHECK();
@@ -476,21 +502,21 @@ int ov_fast_tables(const Workspace &w, const OvArgs &A, Counters *cnt, cudaStrea
     k_ov_prep<<<grid_for((u64)slots * 32, 256), 256, 0, st>>>(A);
     FBP_LAUNCH_CHECK();
     if (w.tc) {
-        FBP_CUDA(cudaFuncSetAttribute(k_lik_tc<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)w.tc_smem));
+        FBP_ALLOW_SMEM(k_lik_tc<1>);
         const u32 G = (u32)w.tcg.size();
         k_lik_tc<1><<<std::max<u32>(sm_count(), G), kTcThreads, w.tc_smem, st>>>(w.tc_args1, G);
         FBP_LAUNCH_CHECK();
     } else if (w.masked_tables) {
         const size_t smem = tables_m_smem_bytes(S, A.L);
         if (smem > 48 * 1024)
-            FBP_CUDA(cudaFuncSetAttribute(k_ov_tables_m, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+            FBP_ALLOW_SMEM(k_ov_tables_m);
         k_ov_tables_m<<<grid_for((u64)slots * ceil_div(A.K, kTabMGroup) * kTabMThreads, kTabMThreads, 4),
                         kTabMThreads, smem, st>>>(A, w.tperm, w.tsup, w.grange32);
         FBP_LAUNCH_CHECK();
     } else {
         const size_t smem = tables_smem_bytes(S, A.K, A.L);
         if (smem > 48 * 1024)
-            FBP_CUDA(cudaFuncSetAttribute(k_ov_tables, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+            FBP_ALLOW_SMEM(k_ov_tables);
         k_ov_tables<<<grid_for((u64)slots * kTabThreads, kTabThreads, 4), kTabThreads, smem, st>>>(A);
         FBP_LAUNCH_CHECK();
     }
@@ -508,7 +534,7 @@ int ov_fast_pass(const Workspace &w, const OvArgs &A, Counters *cnt, cudaStream_
     k_ov_seed<<<grid_for((u64)slots * A.K * 32, kSeedThreads, 8), kSeedThreads, 0, st>>>(A);
     const size_t scan_smem = scan_smem_bytes(S);
     if (scan_smem > 48 * 1024)
-        FBP_CUDA(cudaFuncSetAttribute(k_ov_scan, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)scan_smem));
+        FBP_ALLOW_SMEM(k_ov_scan);
     k_ov_scan<<<grid_for((u64)slots * A.K * 32, kScanThreads, 8), kScanThreads, scan_smem, st>>>(A);
     k_ov_refine<<<(int)sm_count() * 16, kRefineThreads, 0, st>>>(A);
     k_ov_finalize<<<grid_for((u64)slots * 32, kRefineThreads, 8), kRefineThreads, 0, st>>>(A);
@@ -625,7 +651,7 @@ int tc_likelihood_pass(const Workspace &w, const float *v, u32 n, u32 C, const f
     (void)max_windows;
     FBP_CUDA(cudaMemsetAsync(&cnt->tc_refseg, 0, 8, st));
     (void)v; (void)n; (void)C; (void)T; (void)K; (void)L; (void)tss; (void)win; (void)n_win; (void)Lk;
-    FBP_CUDA(cudaFuncSetAttribute(k_lik_tc<0>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)w.tc_smem));
+    FBP_ALLOW_SMEM(k_lik_tc<0>);
     const u32 G = (u32)w.tcg.size();
     k_lik_tc<0><<<std::max<u32>(sm_count(), G), kTcThreads, w.tc_smem, st>>>(w.tc_args0, G);
     FBP_LAUNCH_CHECK();
@@ -640,7 +666,7 @@ int tc_refine_pass(const Workspace &w, const float *v, u32 n, u32 C, const float
                    Counters *cnt, cudaStream_t st, int *launches) {
     const size_t rsmem = tc_refine_smem_bytes(w.tc_cmax, L);
     if (rsmem > 48 * 1024)
-        FBP_CUDA(cudaFuncSetAttribute(k_tc_refine, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)rsmem));
+        FBP_ALLOW_SMEM(k_tc_refine);
     // gamma: the reference's recursive sum of C*L + 1 terms (products
     // rounded once each), plus the double sums' own error
     const double u = 1.0 / 16777216.0, nr = (double)w.tc_nz * L + 2;
