@@ -907,6 +907,9 @@ int fbp_pursuit_chunk(float *voltage, uint32_t n, uint32_t C, const float *templ
                 a0[gi] = tc_group_args(w, gi, voltage, n, C, templates, K, L, neg_half_ss, w.Lk, w.cnt);
                 a0[gi].win = w.win;
                 a0[gi].n_win = &w.cnt->n_win;
+                // short templates: a tile holds the rows of wpt aligned windows
+                a0[gi].wpt = (L >= 32 && 2 * L <= (u32)kTcM) ? (u32)kTcM / L : 1u;
+                a0[gi].active = w.active;
                 a1[gi] = tc_group_args(w, gi, voltage, n, C, templates, K, L, nullptr, nullptr, w.cnt);
                 if (w.fast && do_overlap_recheck) {
                     a1[gi].S = 2 * nmax + 1; a1[gi].nmax = nmax; a1[gi].stiles = w.stiles;

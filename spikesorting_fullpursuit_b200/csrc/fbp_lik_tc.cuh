@@ -75,6 +75,9 @@ struct TcArgs {
     u32 tb_bytes;
     const u32 *win;
     const u32 *n_win;
+    u32 wpt;                         // MODE 0: windows per tile (> 1: tiles are aligned blocks of
+                                     // wpt windows, of which the listed ones are computed)
+    const u8 *active;                // [W] window listed in this pass (block tiles)
     float *Lk;                       // [K][n]
     u32 *ref_t, *ref_s;              // refinement list (one contiguous segment per tile)
     unsigned long long *refseg;      // entries queued (high half) and tile segments (low half)
@@ -234,9 +237,25 @@ k_lik_tc(const TcArgs *__restrict__ gargs, u32 ngroups) {
     float *bmh = (float *)(tsm + lay.bmh);
     const u32 tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     const u32 kWaitLimit = 1u << 24;
-    const u32 sub = MODE == 0 ? (L + kTcM - 1) / kTcM : A.stiles;   // tiles per window / candidate
-    const u64 nitems = (u64)(MODE == 0 ? *A.n_win : *A.n_cand) * sub;
+    // MODE 0 tiles: one listed window (L > 64 may take several tiles), or
+    // with wpt > 1 the aligned block of windows [wpt q, wpt q + wpt) when
+    // one of them is listed (short templates: both windows' rows in one tile)
+    const u32 wpt = MODE == 0 ? A.wpt : 1u;
+    const u32 Wn = (n + L - 1) / L;
+    const u32 sub = MODE == 0 ? (wpt > 1 ? 1u : (L + kTcM - 1) / kTcM) : A.stiles;   // tiles per window / candidate
+    const u64 nitems = MODE == 0 ? (wpt > 1 ? (u64)((Wn + wpt - 1) / wpt) : (u64)*A.n_win * sub)
+                                 : (u64)*A.n_cand * sub;
     if ((u64)bi >= nitems) return;                   // no tile for this CTA: no set-up at all
+    // every role skips the same items: candidates without a table (MODE 1),
+    // blocks without a listed window (MODE 0, wpt > 1)
+    auto live = [&](u64 item) -> bool {
+        if (MODE == 1) return !A.cskip[(u32)(item / sub)];
+        if (wpt <= 1) return true;
+        const u32 w0 = (u32)item * wpt;
+        bool any = false;
+        for (u32 k = 0; k < wpt && w0 + k < Wn; k++) any |= A.active[w0 + k] != 0;
+        return any;
+    };
     auto bar_full = [&](u32 b) { return smem_u32(&bars[b]); };
     auto bar_empty = [&](u32 b) { return smem_u32(&bars[2 + b]); };
     auto bar_staged = [&](u32 b) { return smem_u32(&bars[4 + b]); };
@@ -294,13 +313,17 @@ k_lik_tc(const TcArgs *__restrict__ gargs, u32 ngroups) {
             long long s0;
             u32 ew = 0, g = 0;
             long long m_lo = 0, m_hi = n;
-            if (MODE == 0) {
+            if (!live(item)) continue;
+            if (MODE == 0 && wpt > 1) {
+                const u32 w0 = (u32)item * wpt;
+                s0 = (long long)w0 * L;
+                ew = (u32)min((u64)(w0 + wpt) * L, (u64)n);
+            } else if (MODE == 0) {
                 const u32 w = A.win[item / sub];
                 s0 = (long long)w * L + (u32)(item % sub) * kTcM;
                 ew = min((w + 1) * L, n);
             } else {
                 g = (u32)(item / sub);
-                if (A.cskip[g]) continue;
                 const u32 i0 = A.best_idx[A.cand[g]];
                 s0 = (long long)i0 - (long long)A.nmax + (long long)(item % sub) * kTcM;
                 m_lo = i0;
@@ -320,8 +343,8 @@ k_lik_tc(const TcArgs *__restrict__ gargs, u32 ngroups) {
             {
                 const u64 nx = item + cnt;
                 if (MODE == 0 && nx < nitems) {
-                    const u32 w2 = A.win[nx / sub];
-                    const long long p0 = (long long)w2 * L + (u32)(nx % sub) * kTcM;
+                    const long long p0 = wpt > 1 ? (long long)nx * wpt * L
+                                                 : (long long)A.win[nx / sub] * L + (u32)(nx % sub) * kTcM;
                     const u32 lines = (rows_pad + 31) / 32;
                     for (u32 e = pt; e < A.C * lines; e += kTcProdThreads) {
                         const u32 c = e / lines, ln = e % lines;
@@ -445,10 +468,7 @@ k_lik_tc(const TcArgs *__restrict__ gargs, u32 ngroups) {
         u32 use0 = 0u, use1 = 0u;
         u32 it = 0;
         for (u64 item = bi; item < nitems; item += cnt) {
-            if (MODE == 1) {
-                const u32 gg = (u32)(item / sub);
-                if (A.cskip[gg]) continue;
-            }
+            if (!live(item)) continue;
             const u32 b = nbuf == 2 ? (it & 1u) : 0u;
             it++;
             const u32 ub = b ? use1 : use0;
@@ -469,16 +489,26 @@ k_lik_tc(const TcArgs *__restrict__ gargs, u32 ngroups) {
                 asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
                 const u64 da0 = umma_desc(smem_u32(tsm + lay.As + (size_t)b * rows_pad * Cg2 * 16), lbo_a, 128);
                 const u32 dst = tmem + b * Np;
-                for (u32 m = 0; m < L; m++) {
-                    for (u32 j = 0; j < Cg2 / 2; j++) {
-                        const u64 da = da0 + (u64)(2 * j * rows_pad + m);
-                        const u64 db = db0 + (u64)((m * Cg2 + 2 * j) * Np);
-                        const u32 acc = (m | j) ? 1u : 0u;
+                // The issuing thread is the limit (each MMA of a small N is
+                // shorter than the instructions between two issues), so the
+                // inner loop only steps both descriptors by constants: lag m
+                // moves the strip one row (16 B) and the templates one lag
+                // block.  The first MMA overwrites the accumulator.
+                const u64 bstep = (u64)Cg2 * Np;
+                u32 acc = 0u;
+                for (u32 j = 0; j < Cg2 / 2; j++) {
+                    u64 da = da0 + (u64)(2 * j * rows_pad);
+                    u64 db = db0 + (u64)(2 * j * Np);
+#pragma unroll 4
+                    for (u32 m = 0; m < L; m++) {
                         asm volatile(
                             "{\n\t.reg .pred p;\n\t"
                             "setp.ne.b32 p, %4, 0;\n\t"
                             "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}"
                             ::"r"(dst), "l"(da), "l"(db), "r"(idesc), "r"(acc) : "memory");
+                        acc = 1u;
+                        da += 1u;
+                        db += bstep;
                     }
                 }
                 mbar_arrive(bar_full(b));
@@ -499,10 +529,7 @@ k_lik_tc(const TcArgs *__restrict__ gargs, u32 ngroups) {
         u32 use0 = 0u, use1 = 0u;
         u32 it = 0;
         for (u64 item = bi; item < nitems; item += cnt) {
-            if (MODE == 1) {
-                const u32 gg = (u32)(item / sub);
-                if (A.cskip[gg]) continue;
-            }
+            if (!live(item)) continue;
             const u32 b = nbuf == 2 ? (it & 1u) : 0u;
             it++;
             const bool ok = mbar_wait_bounded(bar_full(b), (b ? use1 : use0) & 1u, kWaitLimit);
@@ -552,7 +579,9 @@ k_lik_tc(const TcArgs *__restrict__ gargs, u32 ngroups) {
             const float *rowsq = rowsq_all + (size_t)b * rows_pad, *rowab = rowab_all + (size_t)b * rows_pad;
             const float *tsa = tsa_all + (size_t)b * Np;
             const u32 s = (u32)s0 + row;
-            const bool in_win = s < ewin && row < kTcM;
+            // block tiles: rows of a window that is not listed keep the values
+            // an earlier pass left (the reference recomputes listed windows only)
+            const bool in_win = s < ewin && row < kTcM && (wpt <= 1 || A.active[s / L] != 0);
             float wn = 0.0f, wa = 0.0f;
             if (in_win) {
                 const u32 hi_i = min(row + L, rows_pad) - 1;
@@ -571,7 +600,11 @@ k_lik_tc(const TcArgs *__restrict__ gargs, u32 ngroups) {
             u32 wantbits[8] = {0, 0, 0, 0, 0, 0, 0, 0};  // Np <= 256: word k holds chunks k of both halves
             float lomax = 0.0f, bmax = 0.0f;
             const bool tail = s + L >= n;                // .cl:231-234
-            const u32 wcur = (u32)(s0 / L);               // the tile's window
+            // this warp's rows lie in windows wlo..whi (one window per tile
+            // when wpt == 1; with block tiles L >= 32, so at most two)
+            const u32 wlo = wpt > 1 ? ((u32)s0 + 32u * quad) / L : (u32)(s0 / L);
+            const u32 whi = wpt > 1 ? ((u32)s0 + 32u * quad + 31u) / L : wlo;
+            const u32 myw = s / L;
             bool anypos = false;
 #pragma unroll
             for (int k = 0; k < 8; k++) {
@@ -622,13 +655,20 @@ k_lik_tc(const TcArgs *__restrict__ gargs, u32 ngroups) {
                 // per (window, template): the largest upper bound over the tile's rows
 #pragma unroll
                 for (int q = 0; q < 16; q++) {
-                    const float u = warp_max_f(uq[q]);
+                    const float u = warp_max_f(myw == wlo ? uq[q] : 0.0f);
                     if (lane == 0 && u > 0.0f && c0 + q < A.K)
-                        atomicMax(reinterpret_cast<int *>(A.umax) + (size_t)wcur * A.Kall + ctrow[c0 + q],
+                        atomicMax(reinterpret_cast<int *>(A.umax) + (size_t)wlo * A.Kall + ctrow[c0 + q],
                                   __float_as_int(u));
+                    if (whi != wlo) {
+                        const float u2 = warp_max_f(myw == whi ? uq[q] : 0.0f);
+                        if (lane == 0 && u2 > 0.0f && c0 + q < A.K)
+                            atomicMax(reinterpret_cast<int *>(A.umax) + (size_t)whi * A.Kall + ctrow[c0 + q],
+                                      __float_as_int(u2));
+                    }
                 }
             }
-            if (__any_sync(0xffffffffu, anypos) && lane == 0) A.wpos[wcur] = 1;
+            if (__any_sync(0xffffffffu, anypos && myw == wlo) && lane == 0) A.wpos[wlo] = 1;
+            if (whi != wlo && __any_sync(0xffffffffu, anypos && myw == whi) && lane == 0) A.wpos[whi] = 1;
             // accumulator b and the row sums are no longer needed
             asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
             __syncwarp();
