@@ -295,6 +295,7 @@ def main():
     import torch.distributed as dist
     from spikesorting_fullpursuit_b200 import _lib, binary_pursuit
     from spikesorting_fullpursuit_b200 import build as B
+    from spikesorting_fullpursuit_b200.parallel.distributed import max_over_ranks
 
     torch.cuda.set_device(local)
     dev = torch.device("cuda", local)
@@ -357,10 +358,7 @@ def main():
     clock_info = clocks.stop()
     barrier()
     ms_total = ev0.elapsed_time(ev1)
-    t = torch.tensor([ms_total], dtype=torch.float64, device=dev)
-    if world > 1:
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    ms_step = float(t.item()) / args.steps
+    ms_step = max_over_ranks(ms_total, device=dev) / args.steps
     units_per_step = world * n * K
     value = units_per_step / (ms_step / 1e3)
 
@@ -429,10 +427,8 @@ def main():
                                  precision=args.precision, overlap=args.overlap)
             e_times.append(time.perf_counter() - t0)
             d2h = 8 * len(out[0])
-        te = torch.tensor([float(np.mean(e_times))], dtype=torch.float64, device=dev)
-        if world > 1:
-            dist.all_reduce(te, op=dist.ReduceOp.MAX)
-        e2e = {"value": units_per_step / float(te.item()), "unit": UNIT,
+        te = max_over_ranks(float(np.mean(e_times)), device=dev)
+        e2e = {"value": units_per_step / te, "unit": UNIT,
                "h2d_bytes_per_step": int(host_v.nbytes + T.nbytes + tss.nbytes + thr.nbytes),
                "d2h_bytes_per_step": int(d2h)}
 
