@@ -48,6 +48,8 @@ def parse():
     ap.add_argument("--overlap", choices=["fast", "exact"], default="fast")
     ap.add_argument("--cpu-sample-s", type=float, default=0.05,
                     help="seconds of recording timed on the CPU baseline")
+    ap.add_argument("--ref-sample-s", type=float, default=0.0125,
+                    help="seconds of recording per step of the reference arm when the reference itself runs")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--mode", choices=["pursuit", "batch", "serve"], default="pursuit",
@@ -139,39 +141,63 @@ def measured_peaks():
 # ---------------------------------------------------------------- reference arm
 
 def run_reference_arm(args, rank, world):
-    """The reference's CPU implementation of the path (the oracle: kernels and
-    host loop of binary_pursuit.cl / binary_pursuit_parallel.py restated in C,
-    pinned to the reference) on the host cores, one bounded sample per step."""
+    """The reference's CPU implementation of the path on the host cores, one
+    bounded sample per step: the reference's own binary_pursuit() host code
+    driving its binary_pursuit.cl kernels compiled for the CPU (one thread,
+    work-items in order), where that build and the staged package are present;
+    else the oracle (kernels and host loop restated in C, pinned to the
+    reference) on all host threads."""
     if rank != 0:
         return
     from oracle import oracle as O
-    rec = workload(args.workload, max(args.cpu_sample_s, 0.01) if args.duration is None else
-                   min(args.duration, args.cpu_sample_s), seed=1)
+    from oracle import reference_harness as RH
+    use_ref = RH.available()
+    sample_s = args.ref_sample_s if use_ref else args.cpu_sample_s
+    rec = workload(args.workload, max(sample_s, 0.01) if args.duration is None else
+                   min(args.duration, sample_s), seed=1)
     L = rec.n_samples_per_chan
     si = rec.sort_info()
     threads = os.cpu_count() or 1
+    note = None
+
+    def one_ref():
+        RH.run_reference(rec.voltage, rec.voltage.dtype, si, rec.fresh_metrics(), n_max_shift_inds=L - 1)
+
+    def one_port():
+        O.binary_pursuit_oracle(rec.voltage, rec.voltage.dtype, si, rec.fresh_metrics(),
+                                n_max_shift_inds=L - 1, nthreads=threads)
+    run = one_ref if use_ref else one_port
+    if use_ref:
+        try:
+            one_ref()
+        except Exception as e:           # the staged reference does not run here: the oracle instead
+            note = "reference harness failed (%s: %s); oracle port timed instead" % (type(e).__name__, e)
+            use_ref, run = False, one_port
     times = []
     for i in range(args.warmup + args.steps):
         t0 = time.perf_counter()
-        O.binary_pursuit_oracle(rec.voltage, rec.voltage.dtype, si, rec.fresh_metrics(),
-                                n_max_shift_inds=L - 1, nthreads=threads)
+        run()
         dt = time.perf_counter() - t0
         if i >= args.warmup:
             times.append(dt)
     sec = float(np.median(times))
     units = rec.n_samples * rec.n_templates
     value = units / sec
-    sample = ("first %.3f s (%d samples) of the %s workload, all passes, n_max_shift=L-1"
-              % (rec.n_samples / rec.sampling_rate, rec.n_samples, args.workload))
+    sample = ("first %.4f s (%d samples) of the %s workload, all passes, n_max_shift=L-1; %s"
+              % (rec.n_samples / rec.sampling_rate, rec.n_samples, args.workload,
+                 "the reference's binary_pursuit() and binary_pursuit.cl compiled for the CPU, one thread"
+                 if use_ref else "the oracle (C restatement of the reference) on %d threads" % threads))
     line = {"impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": sec * 1e3,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
             "data": "synthetic (seeded)",
             "config": {"workload": args.workload, "n_chans": rec.n_chans, "n_samples": rec.n_samples,
                        "n_templates": rec.n_templates, "template_len": L, "n_max_shift": L - 1},
-            "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "port",
-                             "sample": sample},
+            "cpu_baseline": {"value": value, "unit": UNIT, "cores": 1 if use_ref else threads,
+                             "kind": "reference" if use_ref else "port", "sample": sample},
             "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    if note:
+        line["note"] = note
     print(json.dumps(line), flush=True)
 
 

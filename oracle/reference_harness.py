@@ -5,8 +5,8 @@ staged, unmodified reference package (baseline/_ref, made by
 oracle/install_reference.sh) with the stand-in pyopencl of
 oracle/fake_modules, whose kernels are the reference's binary_pursuit.cl
 compiled as C (oracle/_ref/libbp_ref.so, `make -C oracle ref`).  Available
-only where the reference tree exists (not on a machine that only receives
-this repository).
+where the staged package and the compiled kernels exist (both are built in a
+container that has the reference tree, and travel with the repository).
 """
 import contextlib
 import io
@@ -18,7 +18,11 @@ REPO = os.path.dirname(HERE)
 REF_STAGED = os.path.join(REPO, "baseline", "_ref")
 REF_LIB = os.path.join(HERE, "_ref", "libbp_ref.so")
 REF_TREE = os.environ.get("FBP_REFERENCE_TREE", "/root/reference")
-CL_PATH = os.path.join(REF_TREE, "spikesorting_fullpursuit", "kernels", "binary_pursuit.cl")
+# the kernel source as the reference's host code opens it: from the staged
+# package (it travels with the repository), else from the reference tree
+_CL_STAGED = os.path.join(REF_STAGED, "spikesorting_fullpursuit", "kernels", "binary_pursuit.cl")
+CL_PATH = _CL_STAGED if os.path.exists(_CL_STAGED) else os.path.join(
+    REF_TREE, "spikesorting_fullpursuit", "kernels", "binary_pursuit.cl")
 
 
 def available():
