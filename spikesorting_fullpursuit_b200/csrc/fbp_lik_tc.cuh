@@ -306,7 +306,7 @@ k_lik_tc(const TcArgs *__restrict__ gargs, u32 ngroups) {
 
     if (warp < kTcProdWarps) {
         // =========================== producer ===========================
-        const u32 pt = tid;                          // 0..127
+        const u32 pt = tid;                          // 0..255
         u32 use0 = 0u, use1 = 0u;                    // uses of each buffer so far
         u32 it = 0;
         for (u64 item = bi; item < nitems; item += cnt) {
