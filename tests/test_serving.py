@@ -137,3 +137,47 @@ def test_results_same_alone_and_in_the_mix(precision):
         exp = tuple(np.asarray(x) for x in alone[i % len(recs)])
         assert_same_outputs(r.outputs, exp, isinstance(alone[i % len(recs)][0], list))
     torch.cuda.synchronize()
+
+
+def test_request_footprint_counts_workspace_and_buffers():
+    """The admission footprint is the library's workspace for the request's
+    largest chunk plus its voltage, spike buffers and templates; it grows
+    with the segment and the bf16 path's extra buffers are counted."""
+    import ctypes
+    from spikesorting_fullpursuit_b200 import _lib, synthetic
+    from spikesorting_fullpursuit_b200.serving import request_footprint
+    rec = synthetic.tetrode(duration_s=0.2, seed=1)
+    si = rec.sort_info()
+    C, n = rec.voltage.shape
+    L = rec.n_samples_per_chan
+    K = rec.templates.shape[0]
+    ws = ctypes.c_size_t(0)
+    _lib.check(_lib.lib().fbp_pursuit_workspace_bytes(n, C, K, L, 100, 0, ctypes.byref(ws)))
+    W = (n + L - 1) // L
+    fp32 = request_footprint(rec.voltage, si, rec.fresh_metrics(), 100, precision="fp32", total_mem=180e9)
+    assert fp32 == ws.value + 4 * C * n + 8 * (8 * W + 4096) + 4 * K * C * L + 8 * K
+    bf16 = request_footprint(rec.voltage, si, rec.fresh_metrics(), 100, precision="bf16", total_mem=180e9)
+    assert bf16 > fp32
+    # a chunk length caps what one request holds at a time
+    capped = request_footprint(rec.voltage, si, rec.fresh_metrics(), 100, precision="fp32", chunk_samples=2000)
+    assert capped < fp32
+    longer = synthetic.tetrode(duration_s=0.4, seed=1)
+    assert request_footprint(longer.voltage, longer.sort_info(), longer.fresh_metrics(), 100,
+                             precision="fp32", total_mem=180e9) > fp32
+
+
+def test_batch_and_serve_mixes_follow_the_stated_ranges():
+    from spikesorting_fullpursuit_b200 import synthetic
+    b = synthetic.batch_mix(256, seed=3, time_scale=1.0)
+    assert len(b) == 256 and len({s.seed for s in b}) == 256
+    assert all(4 <= s.n_chans <= 32 and 2 <= s.n_templates <= 40 and 61 <= s.L <= 101 for s in b)
+    assert all(1.0 <= s.duration_s <= 60.0 and s.fs == 40000.0 for s in b)
+    r = synthetic.serve_mix(500, seed=4, time_scale=1.0)
+    assert all(4 <= s.n_chans <= 384 and 2.0 <= s.duration_s <= 120.0 for s in r)
+    assert all((s.model == "tetrode") == (s.n_chans <= 32) for s in r)
+    assert all(s.fs == (40000.0 if s.model == "tetrode" else 30000.0) for s in r)
+    assert all(4 <= s.n_templates <= (40 if s.model == "tetrode" else 300) for s in r)
+    small = synthetic.batch_mix(3, seed=3, time_scale=0.001)[0]
+    rec = small.make()
+    assert rec.voltage.shape == (small.n_chans, int(round(small.duration_s * small.fs)))
+    assert rec.templates.shape == (small.n_templates, small.n_chans * small.L)
