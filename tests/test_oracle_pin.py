@@ -31,6 +31,8 @@ LIVE = [
     dict(kind="linear16", seed=23, L=31, dur=0.08, nmax=30, overlap=True, K=16),
     dict(kind="hd384", seed=24, L=21, dur=0.1, nmax=10, overlap=True, K=12, C=48, mask=8),
     dict(kind="tetrode", seed=25, L=41, dur=0.25, nmax=40, overlap=False),
+    # the 384-channel workload's template structure: 16-channel masks, L = 61, 30 kHz, int16
+    dict(kind="hd384", seed=26, L=61, dur=0.05, nmax=10, overlap=True, K=24, C=64, mask=16),
 ]
 
 
