@@ -185,6 +185,25 @@ __device__ __forceinline__ bool mbar_wait_bounded(u32 bar, u32 parity, u32 limit
     return false;
 }
 
+// Max over the warp of 16 values per lane, all 16 columns at once: at each
+// step a lane keeps half of its columns (the half picked by its lane bit)
+// and takes the partner's values for them, so 8 + 4 + 2 + 1 shuffles leave
+// column (lane >> 1) & 15 reduced over the lanes that differ in bits 1-4;
+// a last shuffle adds bit 0.  Returns that column's maximum.
+__device__ __forceinline__ float warp_max16(float (&v)[16], u32 lane) {
+#pragma unroll
+    for (int o = 16, h = 8; h >= 1; o >>= 1, h >>= 1) {
+        const bool hi = (lane & (u32)o) != 0;
+#pragma unroll
+        for (int i = 0; i < h; i++) {
+            const float send = hi ? v[i] : v[i + h];
+            const float keep = hi ? v[i + h] : v[i];
+            v[i] = fmaxf(keep, __shfl_xor_sync(0xffffffffu, send, o));
+        }
+    }
+    return fmaxf(v[0], __shfl_xor_sync(0xffffffffu, v[0], 1));
+}
+
 // MODE 0: likelihood tiles (128 samples of a listed window).
 // MODE 1: overlap tables -- tile = (candidate, 128 shifts b); the strip is the
 //         candidate window [i0, i0+L) with zeros around it, so row b of the
@@ -627,7 +646,9 @@ k_lik_tc(const TcArgs *__restrict__ gargs, u32 ngroups) {
 #pragma unroll
                 for (int q = 0; q < 16; q++) {
                     const u32 t = c0 + q;
-                    if (t >= A.K) break;                 // padding templates
+                    // padding columns (t >= K) are computed and dropped, so the
+                    // loop has no exit and its shared-memory reads can be issued early
+                    const bool real = t < A.K;
                     const u32 gt = ctrow[t];
                     float *dst = A.Lk + (size_t)gt * n + s;
                     u8 *fl = A.apx + (size_t)gt * n + s;
@@ -641,28 +662,37 @@ k_lik_tc(const TcArgs *__restrict__ gargs, u32 ngroups) {
                                                          2.384185791015625e-07f * fabsf(approx));
                     const bool pos = approx - E > 0.0f;      // certainly > 0: refined when a decision needs it
                     const bool neg = approx + E <= 0.0f;     // certainly <= 0: only its sign is read
-                    lomax = fmaxf(lomax, approx - E);
-                    bmax = pos ? fmaxf(bmax, E) : bmax;
-                    cw |= (!tail && !pos && !neg) ? (1u << q) : 0u;
-                    *dst = tail ? 0.0f : approx;
-                    *fl = (!tail && pos) ? (u8)1 : (u8)0;
-                    uq[q] = tail ? 0.0f : fmaxf(0.0f, approx + E);
-                    anypos |= !tail && pos;
+                    lomax = real ? fmaxf(lomax, approx - E) : lomax;
+                    bmax = (real && pos) ? fmaxf(bmax, E) : bmax;
+                    cw |= (real && !tail && !pos && !neg) ? (1u << q) : 0u;
+                    if (real) {
+                        *dst = tail ? 0.0f : approx;
+                        *fl = (!tail && pos) ? (u8)1 : (u8)0;
+                    }
+                    uq[q] = (real && !tail) ? fmaxf(0.0f, approx + E) : 0.0f;
+                    anypos |= real && !tail && pos;
                 }
                 if (tail) lomax = 0.0f, bmax = 0.0f;
                 wantbits[k] |= cw << (16 * half);
                 }
-                // per (window, template): the largest upper bound over the tile's rows
+                // per (window, template): the largest upper bound over the
+                // tile's rows -- the 16 columns reduced over the warp together
+                // (16 shuffles), column (lane >> 1) & 15 ending in lanes 2j, 2j+1
+                {
+                    const u32 col = (lane >> 1) & 15u;
+                    float vv[16];
 #pragma unroll
-                for (int q = 0; q < 16; q++) {
-                    const float u = warp_max_f(myw == wlo ? uq[q] : 0.0f);
-                    if (lane == 0 && u > 0.0f && c0 + q < A.K)
-                        atomicMax(reinterpret_cast<int *>(A.umax) + (size_t)wlo * A.Kall + ctrow[c0 + q],
+                    for (int q = 0; q < 16; q++) vv[q] = myw == wlo ? uq[q] : 0.0f;
+                    const float u = warp_max16(vv, lane);
+                    if ((lane & 1u) == 0 && u > 0.0f && c0 + col < A.K)
+                        atomicMax(reinterpret_cast<int *>(A.umax) + (size_t)wlo * A.Kall + ctrow[c0 + col],
                                   __float_as_int(u));
-                    if (whi != wlo) {
-                        const float u2 = warp_max_f(myw == whi ? uq[q] : 0.0f);
-                        if (lane == 0 && u2 > 0.0f && c0 + q < A.K)
-                            atomicMax(reinterpret_cast<int *>(A.umax) + (size_t)whi * A.Kall + ctrow[c0 + q],
+                    if (whi != wlo) {                    // uniform in the warp
+#pragma unroll
+                        for (int q = 0; q < 16; q++) vv[q] = myw == whi ? uq[q] : 0.0f;
+                        const float u2 = warp_max16(vv, lane);
+                        if ((lane & 1u) == 0 && u2 > 0.0f && c0 + col < A.K)
+                            atomicMax(reinterpret_cast<int *>(A.umax) + (size_t)whi * A.Kall + ctrow[c0 + col],
                                       __float_as_int(u2));
                     }
                 }
