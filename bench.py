@@ -234,6 +234,13 @@ def run_mix(args):
     from spikesorting_fullpursuit_b200 import synthetic
     rank = int(os.environ.get("RANK", "0"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
+    if int(os.environ.get("WORLD_SIZE", "1")) > 1:
+        # one server per GPU; several GPUs take shares of the segments with
+        # parallel.distributed instead
+        if rank == 0:
+            print(json.dumps({"mode": args.mode, "unavailable": "batch and serve modes run on one GPU"}),
+                  flush=True)
+        return
     serve = args.mode == "serve"
     nseg = args.segments or (48 if serve else 256)
     specs = (synthetic.serve_mix(nseg, seed=4 + rank, time_scale=args.time_scale) if serve else
