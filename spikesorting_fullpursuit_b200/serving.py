@@ -125,7 +125,8 @@ class AdmissionScheduler:
 
     def submit(self, job, footprint, units=0):
         """Queue `job`; returns a Future of `Completed` (its `outputs` are what
-        `run` returned) or of the exception `run` raised."""
+        `run` returned) or of the exception `run` raised.  Cancelling the
+        future before the job starts removes it from the queue."""
         req = _Request(job, int(footprint), int(units), time.perf_counter())
         with self._cv:
             if self._closed:
@@ -150,6 +151,9 @@ class AdmissionScheduler:
         self.close()
 
     def _admissible(self):
+        # a request cancelled while it waited (Future.cancel()) leaves the queue unrun
+        while self._queue and self._queue[0].future.cancelled():
+            self._queue.popleft()
         if not self._queue:
             return False
         head = self._queue[0]
@@ -165,6 +169,8 @@ class AdmissionScheduler:
                         return
                     self._cv.wait()
                 req = self._queue.popleft()
+                if not req.future.set_running_or_notify_cancel():
+                    continue                    # cancelled between the check and now
                 self._in_use += req.footprint
                 self._running += 1
                 self.max_running = max(self.max_running, self._running)

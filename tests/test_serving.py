@@ -88,6 +88,30 @@ def test_failed_job_reports_and_server_continues():
         s.submit(("late", 1, False), 1)
 
 
+def test_cancelled_queued_job_never_runs():
+    gate = threading.Event()
+    ran = []
+
+    def run(job, slot):
+        if job == "first":
+            assert gate.wait(timeout=30)
+        ran.append(job)
+        return job
+
+    with AdmissionScheduler(slots=1, budget=10, run=run) as s:
+        f1 = s.submit("first", 1)
+        f2 = s.submit("second", 1)
+        f3 = s.submit("third", 1)
+        time.sleep(0.05)                               # "first" is running, the others wait
+        assert f2.cancel()
+        assert not f1.cancel()                         # already running
+        gate.set()
+        assert f1.result(timeout=30).outputs == "first"
+        assert f3.result(timeout=30).outputs == "third"
+    assert f2.cancelled()
+    assert ran == ["first", "third"]
+
+
 def test_jobs_arriving_while_others_run_are_admitted():
     budget = 30
     tr = _Tracker(budget, hold_s=0.05)
