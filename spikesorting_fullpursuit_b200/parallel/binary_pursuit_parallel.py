@@ -114,7 +114,10 @@ def binary_pursuit(voltage, v_dtype, sort_info, separability_metrics, n_max_shif
 
     if chunk_samples is None:
         total_mem = torch.cuda.get_device_properties(dev).total_memory
-        chunk_samples = num_indices_per_chunk(n_chans, K, L, sampling_rate, total_mem, max_gpu_memory)
+        chunk_samples = num_indices_per_chunk(n_chans, K, L, sampling_rate, total_mem, max_gpu_memory,
+                                              n_max_shift=n_max_shift_inds, precision=prec,
+                                              v_itemsize=np.dtype(voltage.dtype).itemsize,
+                                              adjusted_clips=bool(sort_info['get_adjusted_clips']))
     elif chunk_samples < 4 * L:
         raise ValueError("Cannot fit enough data on GPU to run binary pursuit. "
                          "Decrease template samples or get a new GPU.")

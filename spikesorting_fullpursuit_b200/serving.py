@@ -22,14 +22,13 @@ the results in input order.
 """
 import collections
 import concurrent.futures
-import ctypes
 import threading
 import time
 
 import numpy as np
 
 from .parallel.binary_pursuit_parallel import binary_pursuit
-from .parallel.chunking import num_indices_per_chunk
+from .parallel.chunking import chunk_footprint_bytes, num_indices_per_chunk
 
 
 class Completed:
@@ -69,31 +68,29 @@ class _Request:
 
 def request_footprint(voltage, sort_info, separability_metrics, n_max_shift_inds=None, precision="bf16",
                       overlap="fast", chunk_samples=None, total_mem=None, max_gpu_memory=None):
-    """HBM bytes one request holds while it runs (its largest chunk).
-
-    The pursuit workspace comes from the library (`fbp_pursuit_workspace_bytes`);
-    the voltage chunk is float32; the spike buffers are sized as
-    `binary_pursuit()` sizes them; the templates and thresholds are added."""
-    from . import _lib
-    lib = _lib.lib()
+    """HBM bytes one request holds while it runs (its largest chunk), as the
+    chunk planner counts them (parallel.chunking.chunk_footprint_bytes): the
+    library's workspace (`fbp_pursuit_workspace_bytes`), the voltage chunk,
+    the spike buffers sized as `binary_pursuit()` sizes them, the templates
+    and thresholds."""
     C, n_total = int(voltage.shape[0]), int(voltage.shape[1])
     L = int(sort_info['n_samples_per_chan'])
     templates = np.asarray(separability_metrics['templates'])
     K = 1 if templates.ndim == 1 else int(templates.shape[0])
     if n_max_shift_inds is None or n_max_shift_inds < 0:
         n_max_shift_inds = L // 2
+    prec = 0 if precision == "fp32" else 1
     if chunk_samples is None:
         if total_mem is None:
             import torch
             total_mem = torch.cuda.get_device_properties(torch.cuda.current_device()).total_memory
-        chunk_samples = num_indices_per_chunk(C, K, L, sort_info['sampling_rate'], total_mem, max_gpu_memory)
+        chunk_samples = num_indices_per_chunk(C, K, L, sort_info['sampling_rate'], total_mem, max_gpu_memory,
+                                              n_max_shift=int(n_max_shift_inds), precision=prec,
+                                              v_itemsize=np.dtype(voltage.dtype).itemsize,
+                                              adjusted_clips=bool(sort_info['get_adjusted_clips']))
     n = min(n_total, int(chunk_samples))
-    prec = 0 if precision == "fp32" else 1
-    ws = ctypes.c_size_t(0)
-    _lib.check(lib.fbp_pursuit_workspace_bytes(n, C, K, L, int(n_max_shift_inds), prec, ctypes.byref(ws)))
-    W = (n + L - 1) // L
-    spikes = 2 * 4 * (8 * W + 4096)
-    return int(ws.value) + 4 * C * n + spikes + 4 * K * C * L + 8 * K
+    return chunk_footprint_bytes(n, C, K, L, int(n_max_shift_inds), prec, np.dtype(voltage.dtype).itemsize,
+                                 bool(sort_info['get_adjusted_clips']))
 
 
 class AdmissionScheduler:

@@ -30,10 +30,53 @@ def test_chunk_too_small_raises_value_error():
         chunking.num_indices_per_chunk(384, 300, 61, 30000.0, 8 * 1024 ** 3, max_gpu_memory=1e5)
 
 
-def test_chunk_fits_memory():
-    n = chunking.num_indices_per_chunk(16, 64, 101, 40000.0, 180 * 1024 ** 3)
-    assert n * chunking.device_bytes_per_sample(16, 64, 101) < 180 * 1024 ** 3
-    assert n >= 24_000_000            # a 10-minute 16-channel segment is one chunk
+B200_BYTES = 183_359 * 1024 ** 2          # total memory a B200 reports
+
+
+# (channels, templates, L, n_max_shift, voltage itemsize, samples of the segment)
+PLAN_CASES = {
+    "tetrode_30s": (4, 8, 101, 100, 4, 1_200_000),
+    "linear16_10min": (16, 64, 101, 100, 4, 24_000_000),
+    "hd384_5min": (384, 300, 61, 60, 2, 9_000_000),
+    "hd384_60min": (384, 300, 61, 60, 2, 108_000_000),
+}
+
+
+@pytest.mark.parametrize("precision", [0, 1], ids=["fp32", "bf16"])
+@pytest.mark.parametrize("case", sorted(PLAN_CASES))
+def test_planned_chunk_fits_usable_memory(case, precision):
+    """The planner sizes chunks with the library's own workspace: the chunk it
+    picks, with its workspace, voltage and spike buffers, fits the usable
+    memory, and one sample more would not."""
+    C, K, L, nmax, isz, n_seg = PLAN_CASES[case]
+    usable = chunking.usable_bytes(B200_BYTES)
+    n = chunking.num_indices_per_chunk(C, K, L, 30000.0, B200_BYTES, n_max_shift=nmax, precision=precision,
+                                       v_itemsize=isz)
+    need = chunking.chunk_footprint_bytes(n, C, K, L, nmax, precision, isz)
+    assert need <= usable
+    if n < chunking.MAX_CHUNK_SAMPLES:
+        assert chunking.chunk_footprint_bytes(n + 1, C, K, L, nmax, precision, isz) > usable
+    # the footprint counts the library's workspace, which is most of it
+    assert need > chunking.workspace_bytes(n, C, K, L, nmax, precision) > 4 * C * n
+    # the chunk of a segment is at most the segment; every chunk of it fits
+    cs, onsets = chunking.plan_chunks(n_seg, C, K, L, B200_BYTES, n_max_shift=nmax, precision=precision,
+                                      v_itemsize=isz)
+    for o in onsets:
+        m = min(n_seg, o + cs) - o
+        assert chunking.chunk_footprint_bytes(m, C, K, L, nmax, precision, isz) <= usable
+
+
+def test_ten_minute_linear16_segment_is_one_chunk():
+    n = chunking.num_indices_per_chunk(16, 64, 101, 40000.0, B200_BYTES, n_max_shift=100, precision=1)
+    assert n >= 24_000_000
+
+
+def test_max_gpu_memory_caps_the_chunk():
+    big = chunking.num_indices_per_chunk(16, 64, 101, 40000.0, B200_BYTES, n_max_shift=100)
+    capped = chunking.num_indices_per_chunk(16, 64, 101, 40000.0, B200_BYTES, max_gpu_memory=2 * 1024 ** 3,
+                                            n_max_shift=100)
+    assert capped < big
+    assert chunking.chunk_footprint_bytes(capped, 16, 64, 101, 100) <= 2 * 1024 ** 3
 
 
 def test_add_n_spikes_semantics():
