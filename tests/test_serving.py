@@ -90,10 +90,12 @@ def test_failed_job_reports_and_server_continues():
 
 def test_cancelled_queued_job_never_runs():
     gate = threading.Event()
+    started = threading.Event()
     ran = []
 
     def run(job, slot):
         if job == "first":
+            started.set()
             assert gate.wait(timeout=30)
         ran.append(job)
         return job
@@ -102,7 +104,7 @@ def test_cancelled_queued_job_never_runs():
         f1 = s.submit("first", 1)
         f2 = s.submit("second", 1)
         f3 = s.submit("third", 1)
-        time.sleep(0.05)                               # "first" is running, the others wait
+        assert started.wait(timeout=30)                # "first" is running, the others wait
         assert f2.cancel()
         assert not f1.cancel()                         # already running
         gate.set()
