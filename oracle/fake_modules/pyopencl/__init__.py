@@ -4,9 +4,13 @@ It implements exactly the surface that the reference's host driver
 spikesorting_fullpursuit/parallel/binary_pursuit_parallel.py:128-845 touches,
 so that the reference's own `binary_pursuit()` runs unchanged on this CPU.
 Kernels dispatch to the reference's binary_pursuit.cl compiled as C
-(oracle/_ref/libbp_ref.so).  Every kernel reports a WORK_GROUP_SIZE of 1, and
-work-items run one after another in global-id order.  Buffers are host numpy
-arrays, padded by 64 bytes for the reference's known out-of-range reads.
+(oracle/_ref/libbp_ref.so).  Every kernel reports a WORK_GROUP_SIZE of 1.
+Work-items run one after another in global-id order, except those of the
+kernels whose work-items write disjoint outputs (compute_full_likelihood,
+overlap_recheck_indices, get_adjusted_clips), which run on THREADS host threads
+(default: all; FBP_REF_THREADS overrides) with private local memory.  Buffers
+are host numpy arrays, padded by 64 bytes for the reference's known
+out-of-range reads.
 """
 import ctypes
 import os
@@ -22,6 +26,9 @@ _lib = None
 GLOBAL_MEM_SIZE_BYTES = 16 * 1024 ** 3
 ADDRESS_BITS_VALUE = 64
 MAX_COMPUTE_UNITS = 8
+
+# Host threads for the kernels whose work-items are independent.
+THREADS = int(os.environ.get("FBP_REF_THREADS", "0")) or (os.cpu_count() or 1)
 
 # Counters the tests read back (number of kernel launches by name).
 launch_counts = {}
@@ -46,6 +53,10 @@ def _load():
         _lib.bpref_launch.restype = ctypes.c_int
         _lib.bpref_launch.argtypes = [ctypes.c_int, ctypes.c_uint64, ctypes.c_uint64,
                                       ctypes.c_uint64, ctypes.POINTER(ctypes.c_uint64)]
+        _lib.bpref_launch_mt.restype = ctypes.c_int
+        _lib.bpref_launch_mt.argtypes = [ctypes.c_int, ctypes.c_uint64, ctypes.c_uint64, ctypes.c_uint64,
+                                         ctypes.POINTER(ctypes.c_uint64), ctypes.c_int,
+                                         ctypes.POINTER(ctypes.c_uint64), ctypes.c_int]
     return _lib
 
 
@@ -141,6 +152,7 @@ class Buffer:
 
 class LocalMemory:
     def __init__(self, nbytes):
+        self.nbytes = int(nbytes)
         self._raw = np.zeros(int(nbytes) + 64, dtype=np.uint8)
 
     @property
@@ -163,6 +175,12 @@ class Kernel:
 
     def get_work_group_info(self, key, device):
         return 1
+
+    def _local_sizes(self):
+        words = (ctypes.c_uint64 * len(self.args))()
+        for i, a in enumerate(self.args):
+            words[i] = a.nbytes if isinstance(a, LocalMemory) else 0
+        return words
 
     def _pack(self):
         words = (ctypes.c_uint64 * len(self.args))()
@@ -196,7 +214,8 @@ def enqueue_nd_range_kernel(queue, kernel, global_size, local_size, global_work_
     off = 0 if global_work_offset is None else int(global_work_offset[0])
     gsz = int(global_size[0])
     lsz = int(local_size[0]) if local_size is not None else 1
-    rc = _load().bpref_launch(kernel.kid, off, gsz, lsz, kernel._pack())
+    rc = _load().bpref_launch_mt(kernel.kid, off, gsz, lsz, kernel._pack(), len(kernel.args),
+                                 kernel._local_sizes(), THREADS)
     if rc != 0:
         raise RuntimeError("fake pyopencl launch failed: %d" % rc)
     launch_counts[kernel.name] = launch_counts.get(kernel.name, 0) + 1

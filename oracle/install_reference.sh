@@ -5,10 +5,11 @@
 # pkg_resources.require('pyopencl>=2019.1.2') at metadata time and pyopencl is
 # not installable offline.  So the package tree is copied to /tmp, its one
 # Cython extension (c_cython/sort_cython.pyx) is built there, and the result is
-# copied to baseline/_ref/.  Nothing under /root/reference is written.
+# copied to baseline/_ref/.  Nothing in the reference checkout is written.
 set -euo pipefail
-REF=${REF:-/root/reference}
 HERE=$(cd "$(dirname "$0")/.." && pwd)
+# the reference checkout: $REF, else $FBP_REFERENCE_TREE, else `reference` beside this repository
+REF=${REF:-${FBP_REFERENCE_TREE:-$HERE/../reference}}
 DEST="$HERE/baseline/_ref"
 [ -d "$REF/spikesorting_fullpursuit" ] || { echo "reference not found at $REF" >&2; exit 1; }
 TMP=$(mktemp -d /tmp/sfp_ref.XXXXXX)

@@ -17,7 +17,15 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 REPO = os.path.dirname(HERE)
 REF_STAGED = os.path.join(REPO, "baseline", "_ref")
 REF_LIB = os.path.join(HERE, "_ref", "libbp_ref.so")
-REF_TREE = os.environ.get("FBP_REFERENCE_TREE", "/root/reference")
+
+
+def reference_tree():
+    """Root of the reference checkout: $FBP_REFERENCE_TREE, else a checkout
+    named `reference` beside this repository."""
+    return os.environ.get("FBP_REFERENCE_TREE") or os.path.normpath(os.path.join(REPO, "..", "reference"))
+
+
+REF_TREE = reference_tree()
 # the kernel source as the reference's host code opens it: from the staged
 # package (it travels with the repository), else from the reference tree
 _CL_STAGED = os.path.join(REF_STAGED, "spikesorting_fullpursuit", "kernels", "binary_pursuit.cl")
