@@ -39,7 +39,9 @@ typedef enum fbp_status {
     FBP_ERR_ITER_CAP = 3,    /* the pursuit did not converge within max_passes  */
     FBP_ERR_CAPACITY = 4,    /* the spike output buffer is too small            */
     FBP_ERR_NO_DEVICE = 5,   /* no CUDA device                                  */
-    FBP_ERR_OOM = 6          /* reserved: allocation failure in a caller layer  */
+    FBP_ERR_OOM = 6,         /* reserved: allocation failure in a caller layer  */
+    FBP_ERR_TIMEOUT = 7      /* a bounded wait inside a kernel gave up; the
+                                kernel returned and the context stays usable  */
 } fbp_status;
 
 /* Arithmetic of the full-pass likelihood (path (a)).  Both modes produce
@@ -159,6 +161,42 @@ int fbp_pursuit_chunk(float *voltage, uint32_t n_samples, uint32_t n_chans,
                       void *stream);
 
 /* ------------------------------------------------------------------------
+ * Testing hooks (no counterpart in the reference).
+ * ---------------------------------------------------------------------- */
+
+/* Limits that make rarely taken paths of fbp_pursuit_chunk reachable on
+ * small inputs.  Process-wide; they apply to calls made after
+ * fbp_set_test_limits returns (do not change them while another thread is
+ * inside fbp_pursuit_chunk).  Results are unchanged by the capacities: an
+ * overflowing refinement list makes the FP32 kernel redo the pass's windows,
+ * an overflowing contender pool hands the candidate to the exact overlap
+ * kernel. */
+#define FBP_DEFAULT_WAIT_POLLS 16777216u
+typedef struct fbp_test_limits {
+    uint32_t refine_list_cap;    /* tensor-core refinement list entries (0: workspace capacity) */
+    uint32_t contender_pool_cap; /* fast overlap contender pool entries (0: workspace capacity) */
+    uint32_t wait_polls;         /* polls after which a pipeline wait of the tensor-core kernel
+                                    gives up (FBP_DEFAULT_WAIT_POLLS normally; 0 gives up at
+                                    once): the call then returns FBP_ERR_TIMEOUT */
+} fbp_test_limits;
+
+/* Set the limits; NULL restores the defaults ({0, 0, FBP_DEFAULT_WAIT_POLLS}). */
+int fbp_set_test_limits(const fbp_test_limits *limits);
+
+/* One pass of the tensor-core likelihood (FBP_PREC_BF16_REFINE, path (a))
+ * over every window of a chunk, without refinement.  approx[k][s] ([K][n]
+ * float32) receives the tensor-core value and bound[k][s] the error bound E
+ * the pursuit relies on: |approx - R| <= E for R, the reference's IEEE
+ * binary32 likelihood (compute_maximum_likelihood, binary_pursuit.cl:216-252).
+ * Entries with s + L >= n hold 0 in both.  workspace: fbp_pursuit_workspace_bytes
+ * (..., FBP_PREC_BF16_REFINE) bytes.  FBP_ERR_BAD_ARG when no template group
+ * of this shape fits the tensor-core kernel. */
+int fbp_tc_likelihood_bounds(const float *voltage, uint32_t n_samples, uint32_t n_chans,
+                             const float *templates, uint32_t n_templates, uint32_t template_len,
+                             const float *neg_half_ss, void *workspace, size_t workspace_bytes,
+                             float *approx, float *bound, void *stream);
+
+/* ------------------------------------------------------------------------
  * Single stages (the reference kernels one by one).
  * ---------------------------------------------------------------------- */
 
@@ -256,7 +294,9 @@ int fbp_binary_pursuit_accept(uint32_t n_samples, uint32_t n_chans, uint32_t tem
  * FBP_NOALLOC_MAX_WINDOWS windows (n_samples <= FBP_NOALLOC_MAX_WINDOWS * L);
  * larger inputs return FBP_ERR_BAD_ARG.  The first call on a device looks up
  * the array's device address (cudaGetSymbolAddress), so make that first call
- * before any stream capture.  All calls share the one array: calls whose GPU
+ * before any stream capture.  The address is kept for the life of the
+ * process: after cudaDeviceReset it is stale, so do not call this entry point
+ * after resetting the device.  All calls share the one array: calls whose GPU
  * work overlaps (other streams, other threads) race on it; it is cleared
  * at the start of every call, so its leftover contents do not matter. */
 #define FBP_NOALLOC_MAX_WINDOWS 4194300u

@@ -17,6 +17,8 @@ FBP_ERR_ITER_CAP = 3
 FBP_ERR_CAPACITY = 4
 FBP_ERR_NO_DEVICE = 5
 FBP_ERR_OOM = 6
+FBP_ERR_TIMEOUT = 7
+DEFAULT_WAIT_POLLS = 16777216
 NOALLOC_MAX_WINDOWS = 4194300
 PREC_FP32 = 0
 PREC_BF16_REFINE = 1
@@ -46,6 +48,8 @@ SIGNATURES = {
     "fbp_binary_pursuit_accept": (I, [U32, U32, U32, P, P, P, U32, P, P, P, P, P, P, P, P, P, P]),
     "fbp_binary_pursuit_accept_noalloc": (I, [U32, U32, U32, P, P, P, U32, P, P, P, P, P, P, P, P]),
     "fbp_scan_scratch_bytes": (SZ, [U32]),
+    "fbp_set_test_limits": (I, [P]),
+    "fbp_tc_likelihood_bounds": (I, [P, U32, U32, P, U32, U32, P, P, SZ, P, P, P]),
     "fbp_window_u8_bytes": (SZ, [U32]),
 }
 
@@ -73,6 +77,23 @@ class StageStats(ctypes.Structure):
                 "ms": {STAGE_NAMES[i]: self.ms[i] for i in range(N_STAGES)},
                 "launches": {STAGE_NAMES[i]: int(self.launches[i]) for i in range(N_STAGES)},
                 "work": {STAGE_NAMES[i]: int(self.work[i]) for i in range(N_STAGES)}}
+
+
+class TestLimits(ctypes.Structure):
+    """fbp_test_limits of include/fbp_b200.h."""
+    _fields_ = [("refine_list_cap", ctypes.c_uint32), ("contender_pool_cap", ctypes.c_uint32),
+                ("wait_polls", ctypes.c_uint32)]
+
+
+def set_test_limits(refine_list_cap=0, contender_pool_cap=0, wait_polls=DEFAULT_WAIT_POLLS):
+    """Testing hook: shrink the refinement list or contender pool, or shorten
+    the tensor-core kernel's pipeline waits, for the calls that follow."""
+    lim = TestLimits(int(refine_list_cap), int(contender_pool_cap), int(wait_polls))
+    check(lib().fbp_set_test_limits(ctypes.byref(lim)))
+
+
+def reset_test_limits():
+    check(lib().fbp_set_test_limits(None))
 
 
 class WindowState(ctypes.Structure):

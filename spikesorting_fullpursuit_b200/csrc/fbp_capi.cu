@@ -9,6 +9,7 @@
 #include <cstdio>
 #include <cstring>
 #include <algorithm>
+#include <atomic>
 #include <mutex>
 #include <string>
 #include <vector>
@@ -47,6 +48,11 @@ int fail(int code, const char *fmt, ...) {
             return fail(FBP_ERR_CUDA, "kernel launch failed at %s:%d: %s", __FILE__,       \
                         __LINE__, cudaGetErrorString(e_));                                 \
     } while (0)
+
+// Testing limits (fbp_set_test_limits): capacities of the refinement list
+// and the contender pool (0: the workspace's), polls of the tensor-core
+// kernel's pipeline waits.
+std::atomic<u32> g_lim_refine{0}, g_lim_pool{0}, g_lim_wait{FBP_DEFAULT_WAIT_POLLS};
 
 int sm_count() {
     // initialised once, thread-safely (calls may come from several host threads)
@@ -613,6 +619,7 @@ TcArgs tc_group_args(const Workspace &w, u32 gi, const float *v, u32 n, u32 C, c
     A.grp = gi;
     A.seg_overflow = &cnt->tc_overflow; A.seg_cap = w.tc_seg_cap;
     A.err = &cnt->tc_err;
+    A.wait_polls = g_lim_wait.load();
     A.apx = w.apx; A.bm_s = w.bm_s; A.wlb = w.wlb; A.umax = w.umax; A.wpos = w.wpos;
     A.wn_s = w.wn_s + (size_t)gi * n; A.wa_s = w.wa_s + (size_t)gi * n; A.kx_s = w.kx_s + (size_t)gi * n;
     return A;
@@ -773,61 +780,17 @@ int host_scratch(HostScratch **out) {
     return FBP_OK;
 }
 
-}  // namespace
-
-extern "C" {
-
-int fbp_version(void) { return 100; }
-
-const char *fbp_last_error(void) { return g_last_error.c_str(); }
-
-size_t fbp_scan_scratch_bytes(uint32_t n_windows) {
-    return (size_t)(ceil_div(n_windows, kCompactTile) + 1) * 4;
-}
-
-size_t fbp_window_u8_bytes(uint32_t n_windows) { return window_bytes_u8(n_windows); }
-
-int fbp_pursuit_workspace_bytes(uint32_t n, uint32_t C, uint32_t K, uint32_t L, uint32_t nmax,
-                                int precision, size_t *bytes_out) {
-    if (!bytes_out || n == 0 || C == 0 || K == 0 || L == 0)
-        return fail(FBP_ERR_BAD_ARG, "workspace size: bad arguments");
-    *bytes_out = layout(nullptr, n, K, L, nmax, true, C, precision == FBP_PREC_BF16_REFINE).bytes;
-    return FBP_OK;
-}
-
-int fbp_pursuit_chunk(float *voltage, uint32_t n, uint32_t C, const float *templates, uint32_t K,
-                      uint32_t L, const float *neg_half_ss, const float *thresholds, uint32_t nmax,
-                      int do_overlap_recheck, int precision, int overlap_method, uint32_t max_passes,
-                      void *workspace, size_t workspace_bytes, uint32_t *spike_idx, uint32_t *spike_lab,
-                      uint32_t spike_cap, uint32_t *pass_counts, uint32_t *n_spikes_host,
-                      uint32_t *n_passes_host, int profile, fbp_stage_stats *stats, void *stream) {
-    g_last_error.clear();
-    if (!voltage || !templates || !neg_half_ss || !thresholds || !workspace || !spike_idx ||
-        !spike_lab || !n_spikes_host || !n_passes_host)
-        return fail(FBP_ERR_BAD_ARG, "fbp_pursuit_chunk: null pointer argument");
-    if (n == 0 || C == 0 || K == 0 || L == 0)
-        return fail(FBP_ERR_BAD_ARG, "fbp_pursuit_chunk: zero size (n=%u C=%u K=%u L=%u)", n, C, K, L);
-    if (precision != FBP_PREC_FP32 && precision != FBP_PREC_BF16_REFINE)
-        return fail(FBP_ERR_BAD_ARG, "fbp_pursuit_chunk: unknown precision %d", precision);
-    if ((u64)2 * nmax + 1 > 0xffffffffull)
-        return fail(FBP_ERR_BAD_ARG, "fbp_pursuit_chunk: n_max_shift too large");
-    if (overlap_method != FBP_OVERLAP_FAST && overlap_method != FBP_OVERLAP_EXACT)
-        return fail(FBP_ERR_BAD_ARG, "fbp_pursuit_chunk: unknown overlap method %d", overlap_method);
-    Workspace w = layout((char *)workspace, n, K, L, nmax, overlap_method == FBP_OVERLAP_FAST, C,
-                         precision == FBP_PREC_BF16_REFINE);
-    if (workspace_bytes < w.bytes)
-        return fail(FBP_ERR_BAD_ARG, "fbp_pursuit_chunk: workspace has %zu bytes, needs %zu",
-                    workspace_bytes, w.bytes);
-    cudaStream_t st = (cudaStream_t)stream;
+// Per-chunk set-up shared by fbp_pursuit_chunk and fbp_tc_likelihood_bounds:
+// state zeroed as the reference's buffers start (.py:387, :412-423), every
+// window listed, template supports and order, the tensor-core group plan and
+// launch arguments (dbg_bound: the testing output of the bound E), and the
+// fast overlap recheck's template tables.
+int prepare_chunk(Workspace &w, float *voltage, u32 n, u32 C, const float *templates, u32 K, u32 L,
+                  const float *neg_half_ss, u32 nmax, int do_overlap_recheck, cudaStream_t st,
+                  fbp_stage_stats &S, StageTimer &timer, float *dbg_bound) {
     const u32 W = ceil_div(n, L);
     const size_t Wp = (size_t)W + FBP_WINDOW_PAD;
     const size_t wb = window_bytes_u8(W);
-    fbp_window_state s{w.best_idx, w.best_lab, w.best_ll, w.ov_idx, w.ov_lab, w.flags, w.ovr};
-    fbp_stage_stats local_stats;
-    fbp_stage_stats &S = stats ? *stats : local_stats;
-    memset(&S, 0, sizeof(S));
-    StageTimer timer(profile != 0, st, &S);
-
     // reference buffers start zeroed (.py:387, :412-423)
     timer.begin(FBP_STAGE_LISTS);
     FBP_CUDA(cudaMemsetAsync(w.cnt, 0, sizeof(Counters), st));
@@ -910,6 +873,7 @@ int fbp_pursuit_chunk(float *voltage, uint32_t n, uint32_t C, const float *templ
                 // short templates: a tile holds the rows of wpt aligned windows
                 a0[gi].wpt = (L >= 32 && 2 * L <= (u32)kTcM) ? (u32)kTcM / L : 1u;
                 a0[gi].active = w.active;
+                a0[gi].dbgE = dbg_bound;
                 a1[gi] = tc_group_args(w, gi, voltage, n, C, templates, K, L, nullptr, nullptr, w.cnt);
                 if (w.fast && do_overlap_recheck) {
                     a1[gi].S = 2 * nmax + 1; a1[gi].nmax = nmax; a1[gi].stiles = w.stiles;
@@ -934,6 +898,69 @@ int fbp_pursuit_chunk(float *voltage, uint32_t n, uint32_t C, const float *templ
         timer.end(FBP_STAGE_OVERLAP);
     }
 
+    return FBP_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int fbp_version(void) { return 100; }
+
+const char *fbp_last_error(void) { return g_last_error.c_str(); }
+
+size_t fbp_scan_scratch_bytes(uint32_t n_windows) {
+    return (size_t)(ceil_div(n_windows, kCompactTile) + 1) * 4;
+}
+
+size_t fbp_window_u8_bytes(uint32_t n_windows) { return window_bytes_u8(n_windows); }
+
+int fbp_pursuit_workspace_bytes(uint32_t n, uint32_t C, uint32_t K, uint32_t L, uint32_t nmax,
+                                int precision, size_t *bytes_out) {
+    if (!bytes_out || n == 0 || C == 0 || K == 0 || L == 0)
+        return fail(FBP_ERR_BAD_ARG, "workspace size: bad arguments");
+    *bytes_out = layout(nullptr, n, K, L, nmax, true, C, precision == FBP_PREC_BF16_REFINE).bytes;
+    return FBP_OK;
+}
+
+int fbp_pursuit_chunk(float *voltage, uint32_t n, uint32_t C, const float *templates, uint32_t K,
+                      uint32_t L, const float *neg_half_ss, const float *thresholds, uint32_t nmax,
+                      int do_overlap_recheck, int precision, int overlap_method, uint32_t max_passes,
+                      void *workspace, size_t workspace_bytes, uint32_t *spike_idx, uint32_t *spike_lab,
+                      uint32_t spike_cap, uint32_t *pass_counts, uint32_t *n_spikes_host,
+                      uint32_t *n_passes_host, int profile, fbp_stage_stats *stats, void *stream) {
+    g_last_error.clear();
+    if (!voltage || !templates || !neg_half_ss || !thresholds || !workspace || !spike_idx ||
+        !spike_lab || !n_spikes_host || !n_passes_host)
+        return fail(FBP_ERR_BAD_ARG, "fbp_pursuit_chunk: null pointer argument");
+    if (n == 0 || C == 0 || K == 0 || L == 0)
+        return fail(FBP_ERR_BAD_ARG, "fbp_pursuit_chunk: zero size (n=%u C=%u K=%u L=%u)", n, C, K, L);
+    if (precision != FBP_PREC_FP32 && precision != FBP_PREC_BF16_REFINE)
+        return fail(FBP_ERR_BAD_ARG, "fbp_pursuit_chunk: unknown precision %d", precision);
+    if ((u64)2 * nmax + 1 > 0xffffffffull)
+        return fail(FBP_ERR_BAD_ARG, "fbp_pursuit_chunk: n_max_shift too large");
+    if (overlap_method != FBP_OVERLAP_FAST && overlap_method != FBP_OVERLAP_EXACT)
+        return fail(FBP_ERR_BAD_ARG, "fbp_pursuit_chunk: unknown overlap method %d", overlap_method);
+    Workspace w = layout((char *)workspace, n, K, L, nmax, overlap_method == FBP_OVERLAP_FAST, C,
+                         precision == FBP_PREC_BF16_REFINE);
+    if (workspace_bytes < w.bytes)
+        return fail(FBP_ERR_BAD_ARG, "fbp_pursuit_chunk: workspace has %zu bytes, needs %zu",
+                    workspace_bytes, w.bytes);
+    const u32 lim_refine = g_lim_refine.load(), lim_pool = g_lim_pool.load(), lim_wait = g_lim_wait.load();
+    if (lim_refine && w.tc) w.tc_ref_cap = std::min(w.tc_ref_cap, lim_refine);
+    if (lim_pool && w.fast) w.pool_cap = std::min(w.pool_cap, lim_pool);
+    cudaStream_t st = (cudaStream_t)stream;
+    const u32 W = ceil_div(n, L);
+    const size_t wb = window_bytes_u8(W);
+    fbp_window_state s{w.best_idx, w.best_lab, w.best_ll, w.ov_idx, w.ov_lab, w.flags, w.ovr};
+    fbp_stage_stats local_stats;
+    fbp_stage_stats &S = stats ? *stats : local_stats;
+    memset(&S, 0, sizeof(S));
+    StageTimer timer(profile != 0, st, &S);
+
+    if (int e = prepare_chunk(w, voltage, n, C, templates, K, L, neg_half_ss, nmax, do_overlap_recheck, st, S,
+                              timer, nullptr))
+        return e;
     HostScratch *hs = nullptr;
     if (int e = host_scratch(&hs)) return e;
     u32 *h_counts = hs->counts;
@@ -1060,7 +1087,8 @@ int fbp_pursuit_chunk(float *voltage, uint32_t n, uint32_t C, const float *templ
                   (uint64_t)(uintptr_t)neg_half_ss, (uint64_t)(uintptr_t)thresholds, nmax,
                   (uint64_t)do_overlap_recheck, (uint64_t)precision, (uint64_t)overlap_method,
                   (uint64_t)(uintptr_t)workspace, (uint64_t)workspace_bytes, (uint64_t)(uintptr_t)spike_idx,
-                  (uint64_t)(uintptr_t)spike_lab, spike_cap, (uint64_t)w.masked_tables, (uint64_t)w.tc};
+                  (uint64_t)(uintptr_t)spike_lab, spike_cap, (uint64_t)w.masked_tables, (uint64_t)w.tc,
+                  lim_refine, lim_pool, lim_wait};
         for (const TcGroup &g : w.tcg)               // the group plan follows the template supports
             if (w.tc) pg.key.insert(pg.key.end(), {g.t0, g.nt, g.clo, g.Cg, g.nbuf});
         std::lock_guard<std::mutex> lk(g_graph_mu);
@@ -1106,7 +1134,10 @@ int fbp_pursuit_chunk(float *voltage, uint32_t n, uint32_t C, const float *templ
         const u32 nwin = h_counts[0];
         if (w.tc) {
             const Counters *hc = (const Counters *)h_counts;
-            if (hc->tc_err) { rc = fail(FBP_ERR_CUDA, "tensor-core likelihood: bounded wait %u gave up", hc->tc_err); break; }
+            if (hc->tc_err) {
+                rc = fail(FBP_ERR_TIMEOUT, "tensor-core kernel: bounded wait (role code %u) gave up", hc->tc_err);
+                break;
+            }
             S.lik_refined += std::min((u32)(hc->tc_refseg >> 32), w.tc_ref_cap);
             S.work[FBP_STAGE_LIK_REFINE] += std::min((u32)(hc->tc_refseg >> 32), w.tc_ref_cap);
             S.lik_exact_passes += hc->tc_overflow;
@@ -1154,6 +1185,47 @@ int fbp_pursuit_chunk(float *voltage, uint32_t n, uint32_t C, const float *templ
     *n_passes_host = passes;
     S.passes = passes;
     return rc;
+}
+
+int fbp_set_test_limits(const fbp_test_limits *lim) {
+    g_last_error.clear();
+    g_lim_refine.store(lim ? lim->refine_list_cap : 0u);
+    g_lim_pool.store(lim ? lim->contender_pool_cap : 0u);
+    g_lim_wait.store(lim ? lim->wait_polls : FBP_DEFAULT_WAIT_POLLS);
+    return FBP_OK;
+}
+
+int fbp_tc_likelihood_bounds(const float *voltage, uint32_t n, uint32_t C, const float *templates, uint32_t K,
+                             uint32_t L, const float *neg_half_ss, void *workspace, size_t workspace_bytes,
+                             float *approx, float *bound, void *stream) {
+    g_last_error.clear();
+    if (!voltage || !templates || !neg_half_ss || !workspace || !approx || !bound)
+        return fail(FBP_ERR_BAD_ARG, "fbp_tc_likelihood_bounds: null pointer argument");
+    if (n == 0 || C == 0 || K == 0 || L == 0)
+        return fail(FBP_ERR_BAD_ARG, "fbp_tc_likelihood_bounds: zero size");
+    Workspace w = layout((char *)workspace, n, K, L, 0, false, C, true);
+    if (workspace_bytes < w.bytes)
+        return fail(FBP_ERR_BAD_ARG, "fbp_tc_likelihood_bounds: workspace has %zu bytes, needs %zu",
+                    workspace_bytes, w.bytes);
+    cudaStream_t st = (cudaStream_t)stream;
+    fbp_stage_stats S;
+    memset(&S, 0, sizeof(S));
+    StageTimer timer(false, st, &S);
+    FBP_CUDA(cudaMemsetAsync(bound, 0, (size_t)K * n * 4, st));
+    if (int e = prepare_chunk(w, const_cast<float *>(voltage), n, C, templates, K, L, neg_half_ss, 0, 0, st, S,
+                              timer, bound))
+        return e;
+    if (!w.tc) return fail(FBP_ERR_BAD_ARG, "fbp_tc_likelihood_bounds: no tensor-core plan for this shape");
+    int nl = 0;
+    if (int e = tc_likelihood_pass(w, voltage, n, C, templates, K, L, neg_half_ss, w.win, &w.cnt->n_win,
+                                   ceil_div(n, L), w.Lk, w.cnt, st, &nl))
+        return e;
+    FBP_CUDA(cudaMemcpyAsync(approx, w.Lk, (size_t)K * n * 4, cudaMemcpyDeviceToDevice, st));
+    u32 err = 0;
+    FBP_CUDA(cudaMemcpyAsync(&err, &w.cnt->tc_err, 4, cudaMemcpyDeviceToHost, st));
+    FBP_CUDA(cudaStreamSynchronize(st));
+    if (err) return fail(FBP_ERR_TIMEOUT, "tensor-core kernel: bounded wait (role code %u) gave up", err);
+    return FBP_OK;
 }
 
 int fbp_compute_residual(float *voltage, uint32_t n, uint32_t C, const float *templates, uint32_t K,

@@ -52,6 +52,11 @@ constexpr int kTcThreads = 32 * (kTcProdWarps + 1 + kTcEpiWarps);
 constexpr int kTcProdThreads = 32 * kTcProdWarps;
 constexpr int kTcEpiThreads = 32 * kTcEpiWarps;
 constexpr int kTcM = 128;            // samples per tile
+// Polls of the waits a CTA makes before it exits: for its template copy to
+// land and for MMAs it issued to finish.  These stay long even when a test
+// shortens the pipeline waits: shared memory and TMEM are released only
+// after the asynchronous work into them is done.
+constexpr u32 kTcDrainPolls = 1u << 24;
 
 struct TcArgs {
     u32 n, C, K, L;                  // C: the group's channels; K: the group's templates
@@ -88,6 +93,8 @@ struct TcArgs {
     u32 *seg_overflow;
     u32 seg_cap;
     u32 *err;                        // non-zero: a bounded wait gave up
+    u32 wait_polls;                  // polls before a pipeline wait gives up (final drains use kTcDrainPolls)
+    float *dbgE;                     // MODE 0, testing: when set, the bound E of every entry ([K][n])
     u8 *apx;                         // [K][n] approximate-entry flags
     float *wn_s, *wa_s;              // [n] per-sample window norms
     float *bm_s;                     // [n] largest bound of a flagged entry of the sample
@@ -255,7 +262,7 @@ k_lik_tc(const TcArgs *__restrict__ gargs, u32 ngroups) {
     u32 *tcnt = (u32 *)(tsm + lay.tcnt);
     float *bmh = (float *)(tsm + lay.bmh);
     const u32 tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-    const u32 kWaitLimit = 1u << 24;
+    const u32 wlim = A.wait_polls;                   // pipeline waits (a test may shorten them)
     // MODE 0 tiles: one listed window (L > 64 may take several tiles), or
     // with wpt > 1 the aligned block of windows [wpt q, wpt q + wpt) when
     // one of them is listed (short templates: both windows' rows in one tile)
@@ -352,7 +359,7 @@ k_lik_tc(const TcArgs *__restrict__ gargs, u32 ngroups) {
             it++;
             const u32 ub = b ? use1 : use0;
             if (ub > 0) {
-                bool ok = mbar_wait_bounded(bar_empty(b), (ub - 1) & 1u, kWaitLimit);
+                bool ok = mbar_wait_bounded(bar_empty(b), (ub - 1) & 1u, wlim);
                 if (!ok) { atomicExch(A.err, 3u); atomicExch(abort_flag, 1u); }
             }
             if (named_bar_or(1, kTcProdThreads, *(volatile u32 *)abort_flag != 0)) break;
@@ -493,10 +500,10 @@ k_lik_tc(const TcArgs *__restrict__ gargs, u32 ngroups) {
             const u32 ub = b ? use1 : use0;
             u32 ok = 1;
             if (lane == 0) {
-                ok = mbar_wait_bounded(bar_staged(b), ub & 1u, kWaitLimit) ? 1u : 0u;
+                ok = mbar_wait_bounded(bar_staged(b), ub & 1u, wlim) ? 1u : 0u;
                 if (!ok) atomicExch(A.err, 4u);
                 if (ok && !tb_ready) {
-                    tb_ready = mbar_wait_bounded(bar_tb, 0, kWaitLimit);
+                    tb_ready = mbar_wait_bounded(bar_tb, 0, wlim);
                     if (!tb_ready) { atomicExch(A.err, 1u); ok = 0; }
                 }
                 if (!ok) atomicExch(abort_flag, 1u);
@@ -551,7 +558,7 @@ k_lik_tc(const TcArgs *__restrict__ gargs, u32 ngroups) {
             if (!live(item)) continue;
             const u32 b = nbuf == 2 ? (it & 1u) : 0u;
             it++;
-            const bool ok = mbar_wait_bounded(bar_full(b), (b ? use1 : use0) & 1u, kWaitLimit);
+            const bool ok = mbar_wait_bounded(bar_full(b), (b ? use1 : use0) & 1u, wlim);
             if (b) use1++; else use0++;
             if (!ok) { atomicExch(A.err, 2u); atomicExch(abort_flag, 1u); }
             if (named_bar_or(2, kTcEpiThreads, *(volatile u32 *)abort_flag != 0)) break;
@@ -668,6 +675,7 @@ k_lik_tc(const TcArgs *__restrict__ gargs, u32 ngroups) {
                     if (real) {
                         *dst = tail ? 0.0f : approx;
                         *fl = (!tail && pos) ? (u8)1 : (u8)0;
+                        if (A.dbgE) A.dbgE[(size_t)gt * n + s] = tail ? 0.0f : E;
                     }
                     uq[q] = (real && !tail) ? fmaxf(0.0f, approx + E) : 0.0f;
                     anypos |= real && !tail && pos;
@@ -790,11 +798,11 @@ k_lik_tc(const TcArgs *__restrict__ gargs, u32 ngroups) {
     __syncthreads();
     if (tid == 32 * kTcMmaWarp) {
         // the template copy must land before this CTA's shared memory is released
-        if (!tb_ready) mbar_wait_bounded(bar_tb, 0, kWaitLimit);
+        if (!tb_ready) mbar_wait_bounded(bar_tb, 0, kTcDrainPolls);
         // MMAs must finish before their TMEM is freed
         if (*(volatile u32 *)abort_flag) {
-            if (lfp0 < 2u) mbar_wait_bounded(bar_full(0), lfp0, kWaitLimit);
-            if (lfp1 < 2u) mbar_wait_bounded(bar_full(1), lfp1, kWaitLimit);
+            if (lfp0 < 2u) mbar_wait_bounded(bar_full(0), lfp0, kTcDrainPolls);
+            if (lfp1 < 2u) mbar_wait_bounded(bar_full(1), lfp1, kTcDrainPolls);
         }
     }
     __syncthreads();

@@ -60,3 +60,15 @@ def test_null_arguments_rejected_before_any_cuda_call(lib):
 def test_scan_scratch(lib):
     assert lib.fbp_scan_scratch_bytes(4096) == 8
     assert lib.fbp_scan_scratch_bytes(4097) == 12
+
+
+def test_test_limits_host_only(lib):
+    _lib.set_test_limits(refine_list_cap=5, contender_pool_cap=7, wait_polls=0)
+    _lib.reset_test_limits()
+    assert lib.fbp_last_error() == b""
+
+
+def test_bounds_entry_rejects_null_arguments(lib):
+    rc = lib.fbp_tc_likelihood_bounds(None, 100, 4, None, 8, 31, None, None, 0, None, None, None)
+    assert rc == _lib.FBP_ERR_BAD_ARG
+    assert b"null pointer" in lib.fbp_last_error()
