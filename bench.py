@@ -2,11 +2,15 @@
 
 One step = one complete binary pursuit (all passes until convergence,
 overlap recheck and residuals included) of one synthetic recording segment.
-Default workload: 16-channel linear probe, 10 min at 40 kHz (24M samples per
-channel), 64 templates of 101 samples on all channels, Poisson 1-80 Hz with
-15% forced overlaps, n_max_shift_inds = L-1 (the production setting,
-full_binary_pursuit.py:145).  Inputs are seeded synthetic data: the voltage
-(1.5 GB) and the likelihood buffer (6.1 GB) are both far larger than L2.
+Default workload: the 384-channel high-density probe, 5 min at 30 kHz (9M
+samples per channel, int16), 300 templates of 61 samples on 16-channel masks,
+Poisson 0.5-100 Hz, n_max_shift_inds = L-1 (the production setting,
+full_binary_pursuit.py:145).  The headline value is the tensor-core mode
+(bf16 + exact refinement); the same line carries the plain FP32 path on the
+same recording (fp32_value, bf16_over_fp32) and whether the two spike trains
+are identical.  Inputs are seeded synthetic data: the voltage (13.8 GB as
+float32) and the likelihood buffer (10.8 GB) are far larger than L2.
+`--workload linear16` runs the 16-channel, 10-minute, 64-template workload.
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
 
@@ -39,7 +43,7 @@ def parse():
     ap.add_argument("--steps", type=int, default=3)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    ap.add_argument("--workload", choices=["linear16", "tetrode", "hd384"], default="linear16")
+    ap.add_argument("--workload", choices=["hd384", "linear16", "tetrode"], default="hd384")
     ap.add_argument("--duration", type=float, default=None,
                     help="override the segment length in seconds (development only)")
     ap.add_argument("--precision", choices=["fp32", "bf16"], default="bf16",
@@ -48,8 +52,13 @@ def parse():
     ap.add_argument("--overlap", choices=["fast", "exact"], default="fast")
     ap.add_argument("--cpu-sample-s", type=float, default=0.05,
                     help="seconds of recording timed on the CPU baseline")
-    ap.add_argument("--ref-sample-s", type=float, default=0.0125,
-                    help="seconds of recording per step of the reference arm when the reference itself runs")
+    ap.add_argument("--ref-windows", type=int, default=None,
+                    help="windows (of L samples) per step of the reference arm (default: 4 for 384 channels, "
+                         "16 otherwise); each step pursues the next slice of the recording")
+    ap.add_argument("--fp32-steps", type=int, default=1,
+                    help="timed steps of the plain FP32 path reported beside the headline (0: skip)")
+    ap.add_argument("--fp32-warmup", type=int, default=1)
+    ap.add_argument("--e2e-steps", type=int, default=3, help="steps of the end-to-end measurement")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--mode", choices=["pursuit", "batch", "serve"], default="pursuit",
@@ -140,60 +149,85 @@ def measured_peaks():
 
 # ---------------------------------------------------------------- reference arm
 
+def searched_samples(n, L):
+    """Samples of the windows the reference searches in a chunk of n samples:
+    compute_template_maximum_likelihood skips a window whose end is at or
+    past n - L (binary_pursuit.cl:380-383)."""
+    W = (n + L - 1) // L
+    return sum(min((w + 1) * L, n) - w * L for w in range(W) if (w + 1) * L < n - L)
+
+
 def run_reference_arm(args, rank, world):
-    """The reference's CPU implementation of the path on the host cores, one
-    bounded sample per step: the reference's own binary_pursuit() host code
-    driving its binary_pursuit.cl kernels compiled for the CPU (one thread,
-    work-items in order), where that build and the staged package are present;
-    else the oracle (kernels and host loop restated in C, pinned to the
-    reference) on all host threads."""
+    """The reference's CPU implementation of the path on the host cores: its
+    own binary_pursuit() host code (staged unmodified) driving its
+    binary_pursuit.cl kernels compiled for the CPU, the kernels whose
+    work-items write disjoint outputs (full likelihood, overlap recheck,
+    adjusted clips) on all host threads.  Same workload, metric and config as
+    our arm; each step pursues the next slice of `--ref-windows` windows of a
+    recording of that workload, and its units are the samples of the windows
+    the reference searches in the slice (the last two are not searched,
+    .cl:380-383) times the templates.  Where the staged package or the
+    compiled kernels are missing, the oracle (the reference restated in C)
+    stands in, on all host threads."""
     if rank != 0:
         return
     from oracle import oracle as O
     from oracle import reference_harness as RH
     use_ref = RH.available()
-    sample_s = args.ref_sample_s if use_ref else args.cpu_sample_s
-    rec = workload(args.workload, max(sample_s, 0.01) if args.duration is None else
-                   min(args.duration, sample_s), seed=1)
-    L = rec.n_samples_per_chan
+    probe = workload(args.workload, 0.01, seed=1)
+    L, fs, C, K = probe.n_samples_per_chan, probe.sampling_rate, probe.n_chans, probe.n_templates
+    full = workload(args.workload, args.duration, seed=1) if args.duration is not None and args.duration < 5 else None
+    full_n = int(round((args.duration if args.duration is not None else
+                        {"hd384": 300.0, "linear16": 600.0, "tetrode": 30.0}[args.workload]) * fs))
+    nwin = args.ref_windows or (4 if C >= 128 else 16)
+    slice_n = nwin * L
+    nsteps = args.warmup + args.steps
+    # one recording holding every step's slice (same generative model, sizes and seed as our arm)
+    rec = full if full is not None else workload(args.workload, nsteps * slice_n / fs + 1e-6, seed=1)
     si = rec.sort_info()
     threads = os.cpu_count() or 1
     note = None
 
-    def one_ref():
-        RH.run_reference(rec.voltage, rec.voltage.dtype, si, rec.fresh_metrics(), n_max_shift_inds=L - 1)
+    def one(i, use):
+        a = (i * slice_n) % max(1, rec.n_samples - slice_n + 1)
+        sl = np.ascontiguousarray(rec.voltage[:, a:a + slice_n])
+        if use:
+            RH.run_reference(sl, sl.dtype, si, rec.fresh_metrics(), n_max_shift_inds=L - 1)
+        else:
+            O.binary_pursuit_oracle(sl, sl.dtype, si, rec.fresh_metrics(), n_max_shift_inds=L - 1,
+                                    nthreads=threads)
+        return sl.shape[1]
 
-    def one_port():
-        O.binary_pursuit_oracle(rec.voltage, rec.voltage.dtype, si, rec.fresh_metrics(),
-                                n_max_shift_inds=L - 1, nthreads=threads)
-    run = one_ref if use_ref else one_port
     if use_ref:
         try:
-            one_ref()
+            one(0, True)
         except Exception as e:           # the staged reference does not run here: the oracle instead
             note = "reference harness failed (%s: %s); oracle port timed instead" % (type(e).__name__, e)
-            use_ref, run = False, one_port
-    times = []
-    for i in range(args.warmup + args.steps):
+            use_ref = False
+    times, units = [], 0
+    for i in range(nsteps):
         t0 = time.perf_counter()
-        run()
+        m = one(i, use_ref)
         dt = time.perf_counter() - t0
         if i >= args.warmup:
             times.append(dt)
-    sec = float(np.median(times))
-    units = rec.n_samples * rec.n_templates
+            units += searched_samples(m, L) * K
+    sec = float(sum(times))
     value = units / sec
-    sample = ("first %.4f s (%d samples) of the %s workload, all passes, n_max_shift=L-1; %s"
-              % (rec.n_samples / rec.sampling_rate, rec.n_samples, args.workload,
-                 "the reference's binary_pursuit() and binary_pursuit.cl compiled for the CPU, one thread"
+    sample = ("%d steps, each the next %d-window slice (%d samples, %d of them in windows the reference "
+              "searches) of a %s recording (%d ch, %d templates, L=%d, n_max_shift=L-1), all passes; units "
+              "= searched samples x templates; %s"
+              % (args.steps, nwin, slice_n, searched_samples(slice_n, L), args.workload, C, K, L,
+                 "the reference's own binary_pursuit() and binary_pursuit.cl compiled for the CPU, "
+                 "independent work-items on %d threads" % threads
                  if use_ref else "the oracle (C restatement of the reference) on %d threads" % threads))
     line = {"impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
-            "steps": args.steps, "warmup": args.warmup, "ms_per_step": sec * 1e3,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": sec * 1e3 / max(1, len(times)),
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
             "data": "synthetic (seeded)",
-            "config": {"workload": args.workload, "n_chans": rec.n_chans, "n_samples": rec.n_samples,
-                       "n_templates": rec.n_templates, "template_len": L, "n_max_shift": L - 1},
-            "cpu_baseline": {"value": value, "unit": UNIT, "cores": 1 if use_ref else threads,
+            "config": {"workload": probe.name, "n_chans": C, "n_samples": full_n, "n_templates": K,
+                       "template_len": L, "n_max_shift": L - 1},
+            "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads,
                              "kind": "reference" if use_ref else "port", "sample": sample},
             "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     if note:
@@ -338,7 +372,9 @@ def main():
                                 device_id=dev)
     lib = _lib.lib() if not B.needs_build() else (B.build(), _lib.lib())[1]
 
+    t_gen = time.perf_counter()
     rec = workload(args.workload, args.duration, seed=1 + rank)
+    t_gen = time.perf_counter() - t_gen
     C, n, K, L = rec.n_chans, rec.n_samples, rec.n_templates, rec.n_samples_per_chan
     nmax = L - 1
     prec = 0 if args.precision == "fp32" else 1
@@ -351,58 +387,71 @@ def main():
     pristine = torch.from_numpy(np.ascontiguousarray(rec.voltage)).to(dev).to(torch.float32)
     v = torch.empty_like(pristine)
     T_d, tss_d, thr_d = (torch.from_numpy(x).to(dev) for x in (T, tss, thr))
-    wsb = ctypes.c_size_t(0)
-    _lib.check(lib.fbp_pursuit_workspace_bytes(n, C, K, L, nmax, prec, ctypes.byref(wsb)))
-    ws = torch.empty(wsb.value, dtype=torch.uint8, device=dev)
     W = (n + L - 1) // L
     cap = 16 * W + 4096
     out_i = torch.empty(cap, dtype=torch.int32, device=dev)
     out_l = torch.empty(cap, dtype=torch.int32, device=dev)
+    last = {}
 
-    def step(profile):
+    def workspace(p):
+        wsb = ctypes.c_size_t(0)
+        _lib.check(lib.fbp_pursuit_workspace_bytes(n, C, K, L, nmax, p, ctypes.byref(wsb)))
+        return torch.empty(wsb.value, dtype=torch.uint8, device=dev)
+
+    def step(profile, p, ws):
         v.copy_(pristine)
         nspk, npass = ctypes.c_uint32(0), ctypes.c_uint32(0)
         st = _lib.StageStats()
         _lib.check(lib.fbp_pursuit_chunk(
-            _lib.ptr(v), n, C, _lib.ptr(T_d), K, L, _lib.ptr(tss_d), _lib.ptr(thr_d), nmax, 1, prec,
-            0 if args.overlap == "fast" else 1, 1000000, _lib.ptr(ws), ws.numel(), _lib.ptr(out_i), _lib.ptr(out_l), cap, None,
-            ctypes.byref(nspk), ctypes.byref(npass), int(profile), ctypes.byref(st), sp))
+            _lib.ptr(v), n, C, _lib.ptr(T_d), K, L, _lib.ptr(tss_d), _lib.ptr(thr_d), nmax, 1, p,
+            0 if args.overlap == "fast" else 1, 1000000, _lib.ptr(ws), ws.numel(), _lib.ptr(out_i),
+            _lib.ptr(out_l), cap, None, ctypes.byref(nspk), ctypes.byref(npass), int(profile), ctypes.byref(st),
+            sp))
+        last["n"] = int(nspk.value)
         return st
+
+    def spikes_of_last_step():
+        m = last["n"]
+        return out_i[:m].cpu().numpy().copy(), out_l[:m].cpu().numpy().copy()
 
     def barrier():
         if world > 1:
             dist.barrier()
 
-    for _ in range(args.warmup):
-        step(False)
-    torch.cuda.synchronize()
+    def timed(p, ws, warmup, steps, sampler=None):
+        """Device time per step (max over ranks) of `steps` graph-mode steps after `warmup`."""
+        for _ in range(warmup):
+            step(False, p, ws)
+        torch.cuda.synchronize()
+        barrier()
+        torch.cuda.synchronize()
+        if sampler:
+            sampler.start()
+        ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        ev0.record(stream)
+        for _ in range(steps):
+            step(False, p, ws)
+        ev1.record(stream)
+        torch.cuda.synchronize()
+        info = sampler.stop() if sampler else None
+        barrier()
+        return max_over_ranks(ev0.elapsed_time(ev1), device=dev) / steps, info
 
-    # timed steps: no per-stage timing, so each pass is one CUDA graph launch
+    # ---- headline: the requested precision, W warm-up and K timed steps
+    ws = workspace(prec)
     clocks = ClockSampler(local)
-    barrier()
-    torch.cuda.synchronize()
-    clocks.start()
-    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    ev0.record(stream)
-    for _ in range(args.steps):
-        step(False)
-    ev1.record(stream)
-    torch.cuda.synchronize()
-    clock_info = clocks.stop()
-    barrier()
-    ms_total = ev0.elapsed_time(ev1)
-    ms_step = max_over_ranks(ms_total, device=dev) / args.steps
+    ms_step, clock_info = timed(prec, ws, args.warmup, args.steps, clocks)
     units_per_step = world * n * K
     value = units_per_step / (ms_step / 1e3)
+    spikes_main = spikes_of_last_step()
 
     # one more step with CUDA events around every stage (outside the timed
     # region): the per-stage times, work and launches of a step
-    st_prof = step(True)
+    st_prof = step(True, prec, ws)
     torch.cuda.synchronize()
     stage_ms = np.array(st_prof.ms[:])
     work = np.array(st_prof.work[:], dtype=np.float64)
     launches = np.array(st_prof.launches[:], dtype=np.float64)
-    stats = [st_prof]
     Ct = template_channels(T.reshape(K, -1), C, L)
     S_sh = 2 * nmax + 1
     hbm, tf_burst, tf_sust, peak_src = measured_peaks()
@@ -432,6 +481,11 @@ def main():
             # reference's (every entry once), so the ratio to the HBM peak is
             # not a bandwidth fraction
             per_stage[_lib.STAGE_NAMES[i]].update({"frac": None, "achieved_kind": "reference-equivalent bytes"})
+        if i == 2:
+            # the reference's own work unit for the overlap recheck: 5*C_t*L
+            # flops per (a, b, t) item that survives its skip rules
+            per_stage["overlap"]["surviving_items"] = float(work[2])
+            per_stage["overlap"]["reference_equivalent_tflops"] = work[2] * 5.0 * Ct * L / secs / 1e12
     dom = max((k for k in per_stage if per_stage[k]["frac"] is not None), key=lambda k: per_stage[k]["ms"])
     d = per_stage[dom]
     roofline = {"bound": d["bound"], "achieved": d["achieved"], "peak": d["peak"], "unit": d["unit"],
@@ -441,6 +495,24 @@ def main():
                 "stage_ms_per_step": {_lib.STAGE_NAMES[i]: stage_ms[i] for i in range(_lib.N_STAGES)}}
     gpu_launches = int(launches.sum()) * args.steps
 
+    # ---- the plain FP32 path on the same recording (the north star's
+    # denominator): its throughput and whether its spike train is the same
+    fp32 = None
+    if prec != 0 and args.fp32_steps > 0:
+        del ws
+        torch.cuda.empty_cache()
+        ws32 = workspace(0)
+        ms32, _ = timed(0, ws32, args.fp32_warmup, args.fp32_steps)
+        spikes32 = spikes_of_last_step()
+        del ws32
+        torch.cuda.empty_cache()
+        same = (spikes32[0].shape == spikes_main[0].shape and np.array_equal(spikes32[0], spikes_main[0])
+                and np.array_equal(spikes32[1], spikes_main[1]))
+        same = bool(max_over_ranks(0.0 if same else 1.0, device=dev) == 0.0)
+        fp32 = {"value": units_per_step / (ms32 / 1e3), "ms_per_step": ms32, "steps": args.fp32_steps,
+                "warmup": args.fp32_warmup, "spikes": int(spikes32[0].size)}
+        ws = workspace(prec)
+
     # end to end through the public API: host voltage (pinned) -> spikes on the host
     e2e = None
     if not args.no_e2e:
@@ -448,12 +520,15 @@ def main():
         pinned.numpy()[...] = rec.voltage
         host_v = pinned.numpy()
         si = rec.sort_info()
+        del ws, v
+        torch.cuda.empty_cache()
         binary_pursuit(host_v, host_v.dtype, si, rec.fresh_metrics(), n_max_shift_inds=nmax,
                        precision=args.precision, overlap=args.overlap)
         barrier()
         e_times = []
         d2h = 0
-        for _ in range(args.steps):
+        nsteps_e2e = max(1, min(args.steps, args.e2e_steps))
+        for _ in range(nsteps_e2e):
             torch.cuda.synchronize()
             t0 = time.perf_counter()
             out = binary_pursuit(host_v, host_v.dtype, si, rec.fresh_metrics(), n_max_shift_inds=nmax,
@@ -463,7 +538,9 @@ def main():
         te = max_over_ranks(float(np.mean(e_times)), device=dev)
         e2e = {"value": units_per_step / te, "unit": UNIT,
                "h2d_bytes_per_step": int(host_v.nbytes + T.nbytes + tss.nbytes + thr.nbytes),
-               "d2h_bytes_per_step": int(d2h)}
+               "d2h_bytes_per_step": int(d2h), "steps": nsteps_e2e,
+               "timing": "host clock around binary_pursuit() from pinned host voltage to int64 spike "
+                         "arrays on the host, GPU synchronised"}
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
@@ -477,7 +554,9 @@ def main():
                                 nthreads=threads)
         dt = time.perf_counter() - t0
         cpu = {"value": m * K / dt, "unit": UNIT, "cores": threads, "kind": "port",
-               "sample": "first %.3f s (%d samples) of the same recording, all passes" % (sample_s, m)}
+               "sample": "first %.3f s (%d samples) of the same recording, all passes, the oracle (the "
+                         "reference restated in C, zero template rows skipped) on %d threads"
+                         % (sample_s, m, threads)}
 
     if rank == 0:
         line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
@@ -487,20 +566,34 @@ def main():
                 "data": "synthetic (seeded; one independent segment per rank)",
                 "config": {"workload": rec.name, "n_chans": C, "n_samples": n, "n_templates": K,
                            "template_len": L, "n_max_shift": nmax, "precision": args.precision,
-                           "overlap": args.overlap,
+                           "overlap": args.overlap, "voltage_dtype": str(rec.voltage.dtype),
                            "l2": "inputs larger than L2 (voltage %.2f GB, likelihood %.2f GB)"
                                  % (C * n * 4 / 1e9, K * n * 4 / 1e9),
-                           "passes": int(stats[-1].passes), "spikes": int(stats[-1].spikes),
-                           "overlap_candidates": int(stats[-1].candidates),
-                           "overlap_refined_items": int(stats[-1].refined_items),
-                           "overlap_fallback_candidates": int(stats[-1].fallback_candidates),
-                           "likelihood_refined": int(stats[-1].lik_refined),
-                           "likelihood_lazy_refined": int(stats[-1].lik_lazy_refined),
-                           "likelihood_seq_refined": int(stats[-1].lik_seq_refined),
-                           "likelihood_exact_passes": int(stats[-1].lik_exact_passes),
+                           "passes": int(st_prof.passes), "spikes": int(st_prof.spikes),
+                           "overlap_candidates": int(st_prof.candidates),
+                           "overlap_surviving_items": int(st_prof.work[2]),
+                           "overlap_refined_items": int(st_prof.refined_items),
+                           "overlap_fallback_candidates": int(st_prof.fallback_candidates),
+                           "likelihood_refined": int(st_prof.lik_refined),
+                           "likelihood_lazy_refined": int(st_prof.lik_lazy_refined),
+                           "likelihood_seq_refined": int(st_prof.lik_seq_refined),
+                           "likelihood_exact_passes": int(st_prof.lik_exact_passes),
+                           "generation_s": t_gen,
                            "parallelism": "segment-parallel x%d" % world},
                 "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": gpu_launches,
                 "clocks": clock_info}
+        if fp32 is not None:
+            line["fp32_value"] = fp32["value"]
+            line["fp32"] = fp32
+            line["bf16_over_fp32"] = value / fp32["value"]
+            line["spikes_identical"] = same
+            # every decision reads the reference's binary32 value or an
+            # interval that cannot cross the threshold: the margin band is empty
+            line["margin_band"] = {
+                "epsilon": 0.0, "in_band_events": 0,
+                "entries_in_tensor_core_band": int(st_prof.lik_refined),
+                "note": "likelihood entries whose tensor-core interval contained 0 were re-evaluated "
+                        "(double interval, else the reference's own sum) before any decision read them"}
         print(json.dumps(line), flush=True)
     if world > 1:
         dist.destroy_process_group()
