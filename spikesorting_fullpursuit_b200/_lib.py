@@ -32,6 +32,11 @@ P = ctypes.c_void_p
 SZ = ctypes.c_size_t
 I = ctypes.c_int
 
+F32, I16, F64 = 0, 1, 2
+U64 = ctypes.c_uint64
+I32 = ctypes.c_int32
+I64 = ctypes.c_int64
+
 # name -> (restype, argtypes); every symbol declared in include/fbp_b200.h
 SIGNATURES = {
     "fbp_version": (I, []),
@@ -51,6 +56,27 @@ SIGNATURES = {
     "fbp_set_test_limits": (I, [P]),
     "fbp_tc_likelihood_bounds": (I, [P, U32, U32, P, U32, U32, P, P, SZ, P, P, P]),
     "fbp_window_u8_bytes": (SZ, [U32]),
+}
+
+# every symbol declared in include/fbp_prepost.h
+PREPOST_SIGNATURES = {
+    "fbp_get_clips": (I, [P, I, U64, U32, P, U32, P, U32, U32, I32, I32, P, P]),
+    "fbp_robust_scratch_bytes": (SZ, [U32, U32, I]),
+    "fbp_robust_templates": (I, [P, I, U32, U32, P, U32, P, P, SZ, P]),
+    "fbp_noise_cov_scratch_bytes": (SZ, [U32, U32]),
+    "fbp_clip_noise_covariance": (I, [P, I, P, P, P, U32, U32, U32, P, P, SZ, P]),
+    "fbp_remove_duplicates": (I, [I, P, P, P, P, I, U32, P, U32, U32, I64, P, P, P]),
+    "fbp_unit_mean_templates": (I, [P, U32, P, U32, P, P]),
+    "fbp_overlap_template_scratch_bytes": (SZ, [U32, I32, I32]),
+    "fbp_overlap_template_search": (I, [P, U32, U32, U32, I32, I32, P, U32, P, P, P, SZ, P]),
+    "fbp_power_spectrum": (I, [P, U64, U64, P, P]),
+    "fbp_wiener_smooth": (I, [P, U64, U64, I64, P, P]),
+    "fbp_wiener_apply": (I, [P, P, P, U64, U64, P]),
+    "fbp_zca_scratch_bytes": (SZ, [U32]),
+    "fbp_zca_covariance": (I, [P, I, U32, U64, P, I32, P, P, P, SZ, P]),
+    "fbp_zca_apply": (I, [P, P, I, U32, U64, P, P]),
+    "fbp_separability_metrics": (I, [P, U32, U32, U32, P, ctypes.c_double, ctypes.c_double, P, P, P, P, P, P,
+                                     P]),
 }
 
 
@@ -110,7 +136,7 @@ def lib():
                 "libfbp_b200.so not found at %s; build it with "
                 "`python -m spikesorting_fullpursuit_b200.build`" % LIB_PATH)
         L = ctypes.CDLL(LIB_PATH)
-        for name, (res, args) in SIGNATURES.items():
+        for name, (res, args) in list(SIGNATURES.items()) + list(PREPOST_SIGNATURES.items()):
             f = getattr(L, name)
             f.restype = res
             f.argtypes = args

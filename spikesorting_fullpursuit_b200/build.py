@@ -14,7 +14,7 @@ CSRC = os.path.join(HERE, "csrc")
 REPO = os.path.dirname(HERE)
 LIB_NAME = "libfbp_b200.so"
 LIB_PATH = os.path.join(HERE, LIB_NAME)
-SOURCES = ["fbp_capi.cu"]
+SOURCES = ["fbp_capi.cu", "fbp_prepost.cu"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
 
@@ -28,6 +28,7 @@ def nvcc_path():
 def _deps():
     files = [os.path.join(CSRC, f) for f in os.listdir(CSRC)]
     files.append(os.path.join(REPO, "include", "fbp_b200.h"))
+    files.append(os.path.join(REPO, "include", "fbp_prepost.h"))
     return files
 
 

@@ -34,6 +34,19 @@ int fail(int code, const char *fmt, ...) {
     return code;
 }
 
+}  // namespace
+
+// Error text for the entry points of the other translation unit
+// (fbp_prepost.cu): one per-thread string for the whole library.
+namespace fbp {
+int set_last_error(int code, const char *msg) {
+    g_last_error = msg ? msg : "";
+    return code;
+}
+}  // namespace fbp
+
+namespace {
+
 #define FBP_CUDA(call)                                                                     \
     do {                                                                                   \
         cudaError_t e_ = (call);                                                           \

@@ -12,8 +12,8 @@ from spikesorting_fullpursuit_b200 import _lib
 REPO = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 
 
-def declared_functions():
-    src = open(os.path.join(REPO, "include", "fbp_b200.h")).read()
+def declared_functions(header="fbp_b200.h"):
+    src = open(os.path.join(REPO, "include", header)).read()
     src = re.sub(r"/\*.*?\*/", "", src, flags=re.S)
     return sorted(set(re.findall(r"^\s*(?:int|size_t|const char \*)\s*(fbp_\w+)\s*\(", src, flags=re.M)))
 
@@ -25,14 +25,15 @@ def lib():
 
 
 def test_every_declared_symbol_is_exported(lib):
-    names = declared_functions()
-    assert len(names) >= 12
+    names = declared_functions() + declared_functions("fbp_prepost.h")
+    assert len(names) >= 27
     for nm in names:
         assert hasattr(lib, nm), nm
 
 
 def test_binding_table_covers_header():
     assert set(declared_functions()) == set(_lib.SIGNATURES)
+    assert set(declared_functions("fbp_prepost.h")) == set(_lib.PREPOST_SIGNATURES)
 
 
 def test_version_and_error_text(lib):
