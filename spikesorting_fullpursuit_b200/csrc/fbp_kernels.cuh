@@ -878,35 +878,69 @@ __global__ void k_commit_total(Counters *cnt, u32 cap) {
 __device__ __forceinline__ bool res_touches(const u32 *tsup, u32 lab, u32 c) {
     return !tsup || (c >= tsup[2 * lab] && c < tsup[2 * lab + 1]);
 }
-__global__ void k_residual(float *__restrict__ v, u32 n, u32 C, const float *__restrict__ T, u32 K, u32 L,
-                           const u32 *__restrict__ idx, const u32 *__restrict__ lab,
-                           const u32 *__restrict__ n_spk_dev, u32 n_spk_host, u32 R,
-                           const u32 *__restrict__ tsup) {
+// One block per spike: its list neighbours j in [s - R, s + R] (position,
+// label, channel range; an empty range for labels >= K) are staged in shared
+// memory once, then warps take the spike's channels and lanes its L samples
+// (no division per element, coalesced along samples).
+constexpr u32 kResNb = 128;
+__global__ void __launch_bounds__(256)
+k_residual(float *__restrict__ v, u32 n, u32 C, const float *__restrict__ T, u32 K, u32 L,
+           const u32 *__restrict__ idx, const u32 *__restrict__ lab, const u32 *__restrict__ n_spk_dev,
+           u32 n_spk_host, u32 R, const u32 *__restrict__ tsup) {
+    __shared__ u32 nb_p[kResNb], nb_lab[kResNb], nb_lo[kResNb], nb_hi[kResNb];
     const u32 m = n_spk_dev ? *n_spk_dev : n_spk_host;
+    const u32 warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nw = blockDim.x >> 5;
     for (u32 s = blockIdx.x; s < m; s += gridDim.x) {
-        const u32 p = idx[s];
-        if (lab[s] >= K) continue;                                       // .cl:78-81
+        const u32 ls = lab[s];
+        if (ls >= K) continue;                                           // .cl:78-81 (uniform in the block)
         const u32 jlo = s > R ? s - R : 0;
         const u32 jhi = min(m - 1, s + R);
-        const u32 clo = tsup ? tsup[2 * lab[s]] : 0u, chi = tsup ? tsup[2 * lab[s] + 1] : C;
-        for (u32 e = clo * L + threadIdx.x; e < chi * L; e += blockDim.x) {
-            const u32 c = e / L, i = e % L;
-            const u32 x = p + i;
-            if (x >= n) continue;                                        // .cl:93-96
-            bool owner = true;
-            for (u32 j = s + 1; j <= jhi; j++)
-                if (lab[j] < K && idx[j] <= x && x < idx[j] + L && res_touches(tsup, lab[j], c)) {
-                    owner = false;
-                    break;
-                }
-            if (!owner) continue;
-            float val = v[(size_t)c * n + x];
-            for (u32 j = jlo; j <= s; j++) {
-                const u32 pj = idx[j];
-                if (lab[j] < K && pj <= x && x < pj + L && res_touches(tsup, lab[j], c))
-                    val = __fsub_rn(val, T[((size_t)lab[j] * C + c) * L + (x - pj)]);
+        const u32 cnt = jhi - jlo + 1, self = s - jlo;
+        const bool staged = cnt <= kResNb;
+        __syncthreads();                                                 // the previous spike's readers are done
+        if (staged) {
+            for (u32 q = threadIdx.x; q < cnt; q += blockDim.x) {
+                const u32 lj = lab[jlo + q];
+                nb_p[q] = idx[jlo + q];
+                nb_lab[q] = lj;
+                nb_lo[q] = lj < K ? (tsup ? tsup[2 * lj] : 0u) : 1u;
+                nb_hi[q] = lj < K ? (tsup ? tsup[2 * lj + 1] : C) : 0u;
             }
-            v[(size_t)c * n + x] = val;
+        }
+        __syncthreads();
+        // neighbour q covers (c, x) when its label is < K, c is in its
+        // template's support and x lies in its clip
+        auto covers = [&](u32 q, u32 c, u32 x) -> bool {
+            u32 pq, lo, hi;
+            if (staged) {
+                pq = nb_p[q]; lo = nb_lo[q]; hi = nb_hi[q];
+            } else {
+                const u32 lj = lab[jlo + q];
+                pq = idx[jlo + q];
+                lo = lj < K ? (tsup ? tsup[2 * lj] : 0u) : 1u;
+                hi = lj < K ? (tsup ? tsup[2 * lj + 1] : C) : 0u;
+            }
+            return c >= lo && c < hi && pq <= x && x < pq + L;
+        };
+        const u32 p = idx[s];
+        const u32 clo = tsup ? tsup[2 * ls] : 0u, chi = tsup ? tsup[2 * ls + 1] : C;
+        for (u32 c = clo + warp; c < chi; c += nw) {
+            for (u32 i = lane; i < L; i += 32) {
+                const u32 x = p + i;
+                if (x >= n) break;                                       // .cl:93-96
+                bool owner = true;
+                for (u32 q = self + 1; q < cnt && owner; q++) owner = !covers(q, c, x);
+                if (!owner) continue;
+                float val = v[(size_t)c * n + x];
+                for (u32 q = 0; q <= self; q++) {
+                    if (covers(q, c, x)) {
+                        const u32 lq = staged ? nb_lab[q] : lab[jlo + q];
+                        const u32 pq = staged ? nb_p[q] : idx[jlo + q];
+                        val = __fsub_rn(val, T[((size_t)lq * C + c) * L + (x - pq)]);
+                    }
+                }
+                v[(size_t)c * n + x] = val;
+            }
         }
     }
 }
