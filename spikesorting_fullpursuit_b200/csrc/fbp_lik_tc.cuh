@@ -419,38 +419,57 @@ k_lik_tc(const TcArgs *__restrict__ gargs, u32 ngroups) {
                     }
                 }
             }
-            // ---- row sums (energy, absolute) and the tile's largest magnitude
+            // ---- row sums (energy, absolute) and the tile's largest magnitude:
+            // items (row x, group of 8 channels) over all producer threads,
+            // two items at a time; each item's partial sums go to the strip
+            // buffer (free until the strip is written below), then each row
+            // adds its groups in channel order
             float mx = 0.0f;
-            for (u32 x = pt; x < rows_pad; x += kTcProdThreads) {
+            float2 *part = reinterpret_cast<float2 *>(As);       // [cg][x]
+            const u32 nitem8 = rows_pad * Cg2;
+            auto load8 = [&](u32 e, float (&f)[8]) {
+                const u32 x = e % rows_pad, cg = e / rows_pad;
                 const long long pos = s0 + x;
-                float e2 = 0.0f, ab = 0.0f;
-                if (pos >= m_lo && pos < m_hi && pos < n) {
-                    const float *vp = A.v + pos;
-                    u32 c = 0;
-                    for (; c + 8 <= A.C; c += 8) {
-                        float f[8];
+                const bool inside = pos >= m_lo && pos < m_hi && pos < n;
+                const float *vp = A.v + pos;
 #pragma unroll
-                        for (int j = 0; j < 8; j++) f[j] = vp[(size_t)(c + j) * n];
-#pragma unroll
-                        for (int j = 0; j < 8; j++) {
-                            e2 = fmaf(f[j], f[j], e2);
-                            ab += fabsf(f[j]);
-                            mx = fmaxf(mx, fabsf(f[j]));
-                        }
-                    }
-                    for (; c < A.C; c++) {
-                        const float f = vp[(size_t)c * n];
-                        e2 = fmaf(f, f, e2);
-                        ab += fabsf(f);
-                        mx = fmaxf(mx, fabsf(f));
-                    }
+                for (int j = 0; j < 8; j++) {
+                    const u32 c = cg * 8 + j;
+                    f[j] = (inside && c < A.C) ? vp[(size_t)c * n] : 0.0f;
                 }
-                rowsq[x] = e2;
-                rowab[x] = ab;
+            };
+            auto reduce8 = [&](u32 e, const float (&f)[8]) {
+                float e2 = 0.0f, ab = 0.0f;
+#pragma unroll
+                for (int j = 0; j < 8; j++) {
+                    e2 = fmaf(f[j], f[j], e2);
+                    ab += fabsf(f[j]);
+                    mx = fmaxf(mx, fabsf(f[j]));
+                }
+                part[(size_t)(e / rows_pad) * rows_pad + e % rows_pad] = make_float2(e2, ab);
+            };
+            for (u32 e = pt; e < nitem8; e += 2 * kTcProdThreads) {
+                float f0[8], f1[8];
+                const u32 e1 = e + kTcProdThreads;
+                load8(e, f0);
+                if (e1 < nitem8) load8(e1, f1);
+                reduce8(e, f0);
+                if (e1 < nitem8) reduce8(e1, f1);
             }
             mx = warp_max_f(mx);
             if (lane == 0) pred[warp] = __float_as_uint(mx);
             named_bar(1, kTcProdThreads);
+            for (u32 x = pt; x < rows_pad; x += kTcProdThreads) {
+                float e2 = 0.0f, ab = 0.0f;
+                for (u32 cg = 0; cg < Cg2; cg++) {
+                    const float2 q = part[(size_t)cg * rows_pad + x];
+                    e2 += q.x;
+                    ab += q.y;
+                }
+                rowsq[x] = e2;
+                rowab[x] = ab;
+            }
+            named_bar(1, kTcProdThreads);                     // partial sums read before the strip overwrites them
             int kexp = 0;
             {
                 float m = 0.0f;
