@@ -98,14 +98,16 @@ int fbp_overlap_template_search(const float *templates, uint32_t n_templates, ui
                                 void *stream);
 
 /* Wiener filter arithmetic of wiener_filter.py:24-72 / :75-121 on device
- * spectra (the FFTs are the caller's): power[i] = |spec[i]|^2 (re^2 + im^2)
- * for interleaved complex128 spec [n_rows][n_bins]; the box-car smoothing of
- * :40-59 with the reference's running sums, per row, when smooth > 1; then
- * spec *= S / (S + N + 1e-9) (:126-129). */
-int fbp_power_spectrum(const double *spec, uint64_t n_rows, uint64_t n_bins, double *power, void *stream);
-int fbp_wiener_smooth(double *power, uint64_t n_rows, uint64_t n_bins, int64_t smooth, double *scratch,
+ * spectra (the FFTs are the caller's), in the spectra's precision dtype
+ * (FBP_F32: numpy transforms float32 voltage in single precision; FBP_F64
+ * otherwise): power[i] = |spec[i]|^2 (re^2 + im^2) for interleaved complex
+ * spec [n_rows][n_bins]; the box-car smoothing of :40-59 with the
+ * reference's running sums, per row, when smooth > 1 (scratch: n_rows *
+ * n_bins reals); then spec *= S / (S + N + 1e-9) (:124-129). */
+int fbp_power_spectrum(const void *spec, int dtype, uint64_t n_rows, uint64_t n_bins, void *power, void *stream);
+int fbp_wiener_smooth(void *power, int dtype, uint64_t n_rows, uint64_t n_bins, int64_t smooth, void *scratch,
                       void *stream);
-int fbp_wiener_apply(double *spec, const double *S, const double *N, uint64_t n_rows, uint64_t n_bins,
+int fbp_wiener_apply(void *spec, const void *S, const void *N, int dtype, uint64_t n_rows, uint64_t n_bins,
                      void *stream);
 
 /* get_noise_sampled_zca_matrix, preprocessing.py:104-169, the data passes:

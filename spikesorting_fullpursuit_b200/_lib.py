@@ -69,9 +69,9 @@ PREPOST_SIGNATURES = {
     "fbp_unit_mean_templates": (I, [P, U32, P, U32, P, P]),
     "fbp_overlap_template_scratch_bytes": (SZ, [U32, I32, I32]),
     "fbp_overlap_template_search": (I, [P, U32, U32, U32, I32, I32, P, U32, P, P, P, SZ, P]),
-    "fbp_power_spectrum": (I, [P, U64, U64, P, P]),
-    "fbp_wiener_smooth": (I, [P, U64, U64, I64, P, P]),
-    "fbp_wiener_apply": (I, [P, P, P, U64, U64, P]),
+    "fbp_power_spectrum": (I, [P, I, U64, U64, P, P]),
+    "fbp_wiener_smooth": (I, [P, I, U64, U64, I64, P, P]),
+    "fbp_wiener_apply": (I, [P, P, P, I, U64, U64, P]),
     "fbp_zca_scratch_bytes": (SZ, [U32]),
     "fbp_zca_covariance": (I, [P, I, U32, U64, P, I32, P, P, P, SZ, P]),
     "fbp_zca_apply": (I, [P, P, I, U32, U64, P, P]),

@@ -488,39 +488,42 @@ __global__ void k_overlap_tpl_pick(const double *__restrict__ part_ss, const int
 
 // ------------------------------------------------------------------ Wiener filter
 
-__global__ void k_power(const double2 *__restrict__ spec, u64 n, double *__restrict__ p) {
+template <typename R>
+__global__ void k_power(const R *__restrict__ spec, u64 n, R *__restrict__ p) {
     for (u64 i = (u64)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (u64)gridDim.x * blockDim.x) {
-        const double2 z = spec[i];
-        p[i] = z.x * z.x + z.y * z.y;
+        const R re = spec[2 * i], im = spec[2 * i + 1];
+        p[i] = mul_rn(re, re) + mul_rn(im, im);          // abs2: x.real**2 + x.imag**2
     }
 }
 
 // The rolling box-car of wiener_filter.py:40-59, one thread per row, the
-// reference's running sums in its order (np.sum of the first points is the
+// reference's running sums in its order and precision (the spectra's: float32
+// for float32 voltage, float64 otherwise; np.sum of the first points is the
 // pairwise sum), written to tmp then copied back.
-__global__ void k_smooth(double *__restrict__ P, u64 rows, u64 nb, long long smooth, double *__restrict__ tmp) {
+template <typename R>
+__global__ void k_smooth(R *__restrict__ P, u64 rows, u64 nb, long long smooth, R *__restrict__ tmp) {
     for (u64 r = (u64)blockIdx.x * blockDim.x + threadIdx.x; r < rows; r += (u64)gridDim.x * blockDim.x) {
-        double *x = P + r * nb, *o = tmp + r * nb;
+        R *x = P + r * nb, *o = tmp + r * nb;
         const long long half = smooth / 2;
         long long npts = half < (long long)nb ? half : (long long)nb;
-        double run = np_pairwise<double>(0, (u64)npts, [&](u64 i) { return x[i]; });
+        R run = np_pairwise<R>(0, (u64)npts, [&](u64 i) { return x[i]; });
         for (long long i = 0; i < (long long)nb; i++) {
             if (i + half < (long long)nb) { run += x[i + half]; npts += 1; }
             if (i - half > 0) { run -= x[i - half]; npts -= 1; }
-            o[i] = run / (double)npts;
+            o[i] = run / (R)npts;
         }
         for (u64 i = 0; i < nb; i++) x[i] = o[i];
     }
 }
 
-__global__ void k_wiener(double2 *__restrict__ spec, const double *__restrict__ S, const double *__restrict__ N,
-                         u64 n) {
+// spec *= S / (S + N + 1e-9), the filter in the spectra's precision
+// (wiener_optimal_filter, :124-129).
+template <typename R>
+__global__ void k_wiener(R *__restrict__ spec, const R *__restrict__ S, const R *__restrict__ N, u64 n) {
     for (u64 i = (u64)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (u64)gridDim.x * blockDim.x) {
-        const double f = S[i] / (S[i] + N[i] + 1e-9);
-        double2 z = spec[i];
-        z.x *= f;
-        z.y *= f;
-        spec[i] = z;
+        const R f = S[i] / ((S[i] + N[i]) + (R)1e-9);
+        spec[2 * i] = mul_rn(spec[2 * i], f);
+        spec[2 * i + 1] = mul_rn(spec[2 * i + 1], f);
     }
 }
 
@@ -909,31 +912,46 @@ int fbp_overlap_template_search(const float *templates, uint32_t K, uint32_t C, 
     return FBP_OK;
 }
 
-int fbp_power_spectrum(const double *spec, uint64_t rows, uint64_t nb, double *power, void *stream) {
+int fbp_power_spectrum(const void *spec, int dtype, uint64_t rows, uint64_t nb, void *power, void *stream) {
     fbp::set_last_error(0, "");
     if (!spec || !power) return fail(FBP_ERR_BAD_ARG, "fbp_power_spectrum: null pointer argument");
     const u64 n = rows * nb;
     if (n == 0) return FBP_OK;
-    k_power<<<grid_of(n, 256), 256, 0, (cudaStream_t)stream>>>((const double2 *)spec, n, power);
+    cudaStream_t st = (cudaStream_t)stream;
+    if (dtype == FBP_F32) k_power<float><<<grid_of(n, 256), 256, 0, st>>>((const float *)spec, n, (float *)power);
+    else if (dtype == FBP_F64) k_power<double><<<grid_of(n, 256), 256, 0, st>>>((const double *)spec, n, (double *)power);
+    else return fail(FBP_ERR_BAD_ARG, "fbp_power_spectrum: dtype must be FBP_F32 or FBP_F64");
     PP_LAUNCH_CHECK();
     return FBP_OK;
 }
 
-int fbp_wiener_smooth(double *power, uint64_t rows, uint64_t nb, int64_t smooth, double *scratch, void *stream) {
+int fbp_wiener_smooth(void *power, int dtype, uint64_t rows, uint64_t nb, int64_t smooth, void *scratch,
+                      void *stream) {
     fbp::set_last_error(0, "");
     if (smooth <= 1 || rows == 0 || nb == 0) return FBP_OK;
     if (!power || !scratch) return fail(FBP_ERR_BAD_ARG, "fbp_wiener_smooth: null pointer argument");
-    k_smooth<<<grid_of(rows, 32), 32, 0, (cudaStream_t)stream>>>(power, rows, nb, (long long)smooth, scratch);
+    cudaStream_t st = (cudaStream_t)stream;
+    if (dtype == FBP_F32)
+        k_smooth<float><<<grid_of(rows, 32), 32, 0, st>>>((float *)power, rows, nb, (long long)smooth, (float *)scratch);
+    else if (dtype == FBP_F64)
+        k_smooth<double><<<grid_of(rows, 32), 32, 0, st>>>((double *)power, rows, nb, (long long)smooth,
+                                                           (double *)scratch);
+    else return fail(FBP_ERR_BAD_ARG, "fbp_wiener_smooth: dtype must be FBP_F32 or FBP_F64");
     PP_LAUNCH_CHECK();
     return FBP_OK;
 }
 
-int fbp_wiener_apply(double *spec, const double *S, const double *N, uint64_t rows, uint64_t nb, void *stream) {
+int fbp_wiener_apply(void *spec, const void *S, const void *N, int dtype, uint64_t rows, uint64_t nb, void *stream) {
     fbp::set_last_error(0, "");
     if (!spec || !S || !N) return fail(FBP_ERR_BAD_ARG, "fbp_wiener_apply: null pointer argument");
     const u64 n = rows * nb;
     if (n == 0) return FBP_OK;
-    k_wiener<<<grid_of(n, 256), 256, 0, (cudaStream_t)stream>>>((double2 *)spec, S, N, n);
+    cudaStream_t st = (cudaStream_t)stream;
+    if (dtype == FBP_F32)
+        k_wiener<float><<<grid_of(n, 256), 256, 0, st>>>((float *)spec, (const float *)S, (const float *)N, n);
+    else if (dtype == FBP_F64)
+        k_wiener<double><<<grid_of(n, 256), 256, 0, st>>>((double *)spec, (const double *)S, (const double *)N, n);
+    else return fail(FBP_ERR_BAD_ARG, "fbp_wiener_apply: dtype must be FBP_F32 or FBP_F64");
     PP_LAUNCH_CHECK();
     return FBP_OK;
 }

@@ -4,11 +4,12 @@ prepost.npz by tests/golden/make_prepost_golden.py; inputs regenerated from
 their seeds by tests/_prepost_cases.py).
 
 Exact: clip gathers, robust templates (float32 and int16), duplicate keep
-masks, the template-sum search.  Within a stated tolerance (float64 sums in
-another order): the clip noise covariance (relative 1e-9 of its largest
-entry), the Wiener filter (1e-9 of the largest output; cuFFT against numpy's
-pocketfft) and the ZCA matrix (the reference sums the covariance in float32,
-this library in float64: 2e-4 of the largest entry)."""
+masks, the template-sum search.  Within a stated tolerance: the clip noise
+covariance (float64 sums in another order: 1e-9 of its largest entry), the
+Wiener filter (float32 throughout as numpy does it, cuFFT against numpy's
+pocketfft transform: 1e-5 of the largest output) and the ZCA matrix (the
+reference sums the covariance in float32, this library in float64: 2e-4 of
+the largest entry)."""
 import os
 
 import numpy as np
@@ -102,9 +103,10 @@ def test_wiener_filter_matches_reference(smooth):
     for fn, key in ((WF.wiener, "wiener_%d"), (WF.wiener_all, "wiener_all_%d")):
         got = fn(o, s, nz, smooth)
         ref = GOLD[key % smooth]
-        assert got.shape == ref.shape
-        err = np.abs(got - ref).max() / np.abs(ref).max()
-        assert err < 1e-9, (key, err)
+        assert got.shape == ref.shape and got.dtype == ref.dtype
+        err = np.abs(got.astype(np.float64) - ref).max() / np.abs(ref).max()
+        print("\n%s smooth=%d: max difference %.2e of the largest output" % (key % smooth, smooth, err))
+        assert err < 1e-5, (key, err)
 
 
 def test_zca_matrix_and_whitening_match_reference():
