@@ -183,14 +183,17 @@ def run_reference_arm(args, rank, world):
     slice_n = nwin * L
     nsteps = args.warmup + args.steps
     # one recording holding every step's slice (same generative model, sizes and seed as our arm)
-    rec = full if full is not None else workload(args.workload, nsteps * slice_n / fs + 1e-6, seed=1)
+    # slices start 10 ms in: the synthetic spike trains leave the first and
+    # last 5 ms of a recording empty
+    lead = int(round(0.01 * fs))
+    rec = full if full is not None else workload(args.workload, (lead + nsteps * slice_n) / fs + 0.006, seed=1)
     si = rec.sort_info()
     threads = os.cpu_count() or 1
     note = None
     crashes = [0]
 
     def one(i, use):
-        a = (i * slice_n) % max(1, rec.n_samples - slice_n + 1)
+        a = (lead + i * slice_n) % max(1, rec.n_samples - slice_n + 1)
         sl = np.ascontiguousarray(rec.voltage[:, a:a + slice_n])
         if use:
             try:
