@@ -69,6 +69,9 @@ def parse():
     ap.add_argument("--time-scale", type=float, default=0.05,
                     help="batch/serve: factor on the segment durations of the workload")
     ap.add_argument("--slots", type=int, default=4, help="batch/serve: concurrent requests on the GPU")
+    ap.add_argument("--fp32-segments", type=int, default=0,
+                    help="batch/serve: run the plain-FP32 comparison on the first N requests only "
+                         "(saturated, no Poisson sweep); 0: all of them")
     ap.add_argument("--rates", default="0.5,0.8,0.95",
                     help="serve: arrival rates as fractions of the measured saturated request rate")
     return ap.parse_args()
@@ -312,10 +315,14 @@ def run_mix(args):
     identical = True
     clocks.start()
     for prec in ("bf16", "fp32"):
+        # the plain-FP32 comparison may run on the first --fp32-segments
+        # requests only (a bounded call); its spikes are checked against the
+        # same requests of the bf16 run
+        run_segs = segs if (prec == "bf16" or not args.fp32_segments) else segs[: args.fp32_segments]
         with PursuitServer(slots=args.slots, precision=prec, overlap=args.overlap) as srv:
-            drive(srv, segs[: 2 * args.slots])                        # warm-up (untimed)
+            drive(srv, run_segs[: 2 * args.slots])                    # warm-up (untimed)
             torch.cuda.synchronize()
-            res, wall = drive(srv, segs)                                # saturated: all at once
+            res, wall = drive(srv, run_segs)                            # saturated: all at once
             torch.cuda.synchronize()
             summ = latency_summary(res, wall)
             summ.update({"wall_s": wall, "requests_per_s": len(res) / wall, "max_running": srv.max_running,
@@ -325,12 +332,17 @@ def run_mix(args):
                 reference_outputs = outs
             identical &= all(_same(a, b) for a, b in zip(outs, reference_outputs))
             entry = {"saturated": summ}
-            if serve:
+            if prec == "bf16" and args.fp32_segments:
+                # the same subset the FP32 run takes, for a like-for-like ratio
+                rs, ws_ = drive(srv, segs[: args.fp32_segments])
+                torch.cuda.synchronize()
+                entry["saturated_fp32_subset"] = latency_summary(rs, ws_)
+            if serve and (prec == "bf16" or not args.fp32_segments):
                 sweep = []
                 cap = len(res) / wall
                 for j, frac in enumerate(float(x) for x in args.rates.split(",")):
-                    arr = poisson_arrivals(frac * cap, len(segs), seed=100 + j)
-                    r2, w2 = drive(srv, segs, arr)
+                    arr = poisson_arrivals(frac * cap, len(run_segs), seed=100 + j)
+                    r2, w2 = drive(srv, run_segs, arr)
                     torch.cuda.synchronize()
                     s2 = latency_summary(r2, w2)
                     s2.update({"rate_fraction": frac, "rate_per_s": frac * cap, "max_running": srv.max_running})
@@ -343,7 +355,9 @@ def run_mix(args):
     line = {"metric": ("serving p50/p99 segment latency vs pursuit sample*template/s" if serve
                        else "batched pursuit sample*template/s"),
             "value": bf["throughput"], "unit": UNIT, "n_gpus": 1, "higher_is_better": True,
-            "fp32_value": fp["throughput"], "bf16_over_fp32": bf["throughput"] / fp["throughput"],
+            "fp32_value": fp["throughput"],
+            "bf16_over_fp32": (out["bf16"].get("saturated_fp32_subset", bf)["throughput"] / fp["throughput"]),
+            "fp32_requests": fp["requests"],
             "spikes_identical_bf16_fp32_and_across_runs": bool(identical),
             "data": "synthetic (seeded per request)",
             "config": {"workload": "serve_mix" if serve else "batch_mix", "requests": nseg,
