@@ -160,6 +160,16 @@ int fbp_pursuit_chunk(float *voltage, uint32_t n_samples, uint32_t n_chans,
                       uint32_t *n_passes_host, int profile, fbp_stage_stats *stats,
                       void *stream);
 
+/* Template group size of the tensor-core likelihood (no counterpart in the
+ * reference, whose kernels take one template per work-item).  0 (default):
+ * the planner's cost model picks, per chunk, the group size with the least
+ * padded MMA work that fits shared memory; 16..256 (multiples of 16): that
+ * size when its groups fit, else the cost model.  Applies to the calls the
+ * calling thread makes afterwards; set by the tuner
+ * (spikesorting_fullpursuit_b200.autotune) from timed trials per shape
+ * bucket.  Results do not depend on it. */
+int fbp_set_tc_group_size(uint32_t templates_per_group);
+
 /* ------------------------------------------------------------------------
  * Testing hooks (no counterpart in the reference).
  * ---------------------------------------------------------------------- */

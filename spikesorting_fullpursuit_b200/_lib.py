@@ -54,6 +54,7 @@ SIGNATURES = {
     "fbp_binary_pursuit_accept_noalloc": (I, [U32, U32, U32, P, P, P, U32, P, P, P, P, P, P, P, P]),
     "fbp_scan_scratch_bytes": (SZ, [U32]),
     "fbp_set_test_limits": (I, [P]),
+    "fbp_set_tc_group_size": (I, [U32]),
     "fbp_tc_likelihood_bounds": (I, [P, U32, U32, P, U32, U32, P, P, SZ, P, P, P]),
     "fbp_window_u8_bytes": (SZ, [U32]),
 }

@@ -66,6 +66,9 @@ namespace {
 // and the contender pool (0: the workspace's), polls of the tensor-core
 // kernel's pipeline waits.
 std::atomic<u32> g_lim_refine{0}, g_lim_pool{0}, g_lim_wait{FBP_DEFAULT_WAIT_POLLS};
+// Tensor-core template group size chosen by a tuner for the calling thread
+// (fbp_set_tc_group_size; 0: the planner's cost model).
+thread_local u32 t_tc_group_size = 0;
 
 int sm_count() {
     // initialised once, thread-safely (calls may come from several host threads)
@@ -188,8 +191,12 @@ bool plan_tc_groups(const std::vector<u32> &tsup, const std::vector<u32> &tperm,
     std::vector<TcGroup> cur;
     const u32 kall = (K + 15) / 16 * 16;
     const u32 sizes[] = {kall, 256, 128, 64, 32, 16};
+    const u32 forced = t_tc_group_size;
+    bool forced_fits = false;                        // a forced size that does not fit: the cost model
+    for (int pass = forced ? 0 : 1; pass < 2 && !forced_fits; pass++)
     for (u32 GS : sizes) {
         if (GS > 256 || GS == 0) continue;
+        if (pass == 0 && GS != std::min(forced, kall)) continue;
         if ((K + GS - 1) / GS > gmax) continue;
         cur.clear();
         double cost = 0;
@@ -226,6 +233,7 @@ bool plan_tc_groups(const std::vector<u32> &tsup, const std::vector<u32> &tperm,
         if (ok && cost < best) {
             best = cost;
             out = cur;
+            if (pass == 0) forced_fits = true;
         }
     }
     return best < 1e300;
@@ -1198,6 +1206,15 @@ int fbp_pursuit_chunk(float *voltage, uint32_t n, uint32_t C, const float *templ
     *n_passes_host = passes;
     S.passes = passes;
     return rc;
+}
+
+int fbp_set_tc_group_size(uint32_t templates_per_group) {
+    g_last_error.clear();
+    if (templates_per_group != 0 && (templates_per_group % 16 != 0 || templates_per_group > 256))
+        return fail(FBP_ERR_BAD_ARG, "fbp_set_tc_group_size: %u is not 0 or a multiple of 16 up to 256",
+                    templates_per_group);
+    t_tc_group_size = templates_per_group;
+    return FBP_OK;
 }
 
 int fbp_set_test_limits(const fbp_test_limits *lim) {

@@ -51,7 +51,7 @@ def _to_device_f32(torch, host_chunk, dev, stream):
 def binary_pursuit(voltage, v_dtype, sort_info, separability_metrics, n_max_shift_inds=None,
                    kernels_path=None, max_gpu_memory=None, *, precision="fp32",
                    chunk_samples=None, device=None, max_passes=1000000, stats=None, profile=False,
-                   overlap="fast"):
+                   overlap="fast", tune=False):
     """Full Binary Pursuit over `voltage` ([channels, samples], any real dtype).
 
     Returns (event_indices int64, neuron_labels int64, binary_pursuit_spike_bool
@@ -73,6 +73,10 @@ def binary_pursuit(voltage, v_dtype, sort_info, separability_metrics, n_max_shif
       stats          a list; one dict per chunk is appended (passes, spikes,
                      per-stage launches, work and, with profile=True, CUDA-event
                      milliseconds).
+      tune           precision "bf16": take the tensor-core template group size
+                     from the tuner's cache for this shape bucket, timing the
+                     candidates on a sample of the recording the first time
+                     (spikesorting_fullpursuit_b200.autotune); same spikes.
     """
     # The CUDA runtime is initialised inside the call, never at import time,
     # so callers may fork worker processes first (reference :166-170).
@@ -122,6 +126,11 @@ def binary_pursuit(voltage, v_dtype, sort_info, separability_metrics, n_max_shif
         raise ValueError("Cannot fit enough data on GPU to run binary pursuit. "
                          "Decrease template samples or get a new GPU.")
     onsets = chunk_onsets(n_samples, L, chunk_samples)
+    if tune and prec == _PRECISIONS["bf16"] and n_samples > 0:
+        from .. import autotune
+        first = np.ascontiguousarray(voltage[:, :min(n_samples, chunk_samples)], dtype=np.float32)
+        gs, _, _ = autotune.tune(first, templates_vector.reshape(K, -1), template_sum_squared, L)
+        autotune.apply(gs)
 
     stream = torch.cuda.current_stream(dev)
     sp = _lib.stream_ptr(stream)
@@ -187,5 +196,7 @@ def binary_pursuit(voltage, v_dtype, sort_info, separability_metrics, n_max_shif
     else:
         event_indices, neuron_labels, binary_pursuit_spike_bool, adjusted_clips = [], [], [], []
 
+    if tune:
+        _lib.check(lib.fbp_set_tc_group_size(0))
     add_n_spikes(separability_metrics, neuron_labels)
     return event_indices, neuron_labels, binary_pursuit_spike_bool, adjusted_clips

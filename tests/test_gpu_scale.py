@@ -217,3 +217,31 @@ def test_bounded_wait_gives_up_and_context_stays_usable(lib):
     got = bpp.binary_pursuit(rec.voltage, rec.voltage.dtype, si, rec.fresh_metrics(), n_max_shift_inds=40,
                              precision="bf16")
     assert_same_outputs(got, _as_tuple(exp))
+
+
+# ------------------------------------------------------------ tuned group size
+
+def test_tuned_group_size_gives_the_same_spikes(lib, tmp_path, monkeypatch):
+    """The tuner times the candidate template group sizes and caches the
+    fastest per shape bucket; a pursuit that uses it (and one with every
+    group size forced) returns the oracle's spikes."""
+    from spikesorting_fullpursuit_b200 import autotune
+    monkeypatch.setenv("FBP_TUNE_CACHE", str(tmp_path / "tune.json"))
+    rec = linear16_slice(0.1, 311)
+    si = rec.sort_info()
+    exp = O.binary_pursuit_oracle(rec.voltage, rec.voltage.dtype, si, rec.fresh_metrics(), n_max_shift_inds=100)
+    got = bpp.binary_pursuit(rec.voltage, rec.voltage.dtype, si, rec.fresh_metrics(), n_max_shift_inds=100,
+                             precision="bf16", tune=True)
+    assert_same_outputs(got, _as_tuple(exp))
+    table = autotune._load()
+    assert len(table) == 1
+    entry = next(iter(table.values()))
+    assert entry["group_size"] in autotune.CANDIDATES and len(entry["ms"]) == len(autotune.CANDIDATES)
+    for gs in (16, 32, 64):
+        autotune.apply(gs)
+        try:
+            got = bpp.binary_pursuit(rec.voltage, rec.voltage.dtype, si, rec.fresh_metrics(), n_max_shift_inds=100,
+                                     precision="bf16")
+        finally:
+            autotune.apply(0)
+        assert_same_outputs(got, _as_tuple(exp))
