@@ -99,3 +99,18 @@ def test_no_gpu_raises_runtime_error():
                             "get_adjusted_clips": False},
                            {"templates": np.zeros((1, 10)), "template_SS": np.zeros(1),
                             "neuron_lower_thresholds": np.zeros(1)})
+
+
+def test_tuner_bucket_and_cache(tmp_path, monkeypatch):
+    """The tuner's shape bucket and its JSON cache (no GPU: a cached bucket
+    is answered without timing)."""
+    from spikesorting_fullpursuit_b200 import autotune, synthetic
+    monkeypatch.setenv("FBP_TUNE_CACHE", str(tmp_path / "t.json"))
+    rec = synthetic.hd384(duration_s=0.01, seed=2)
+    T = rec.fresh_metrics()["templates"]
+    b = autotune.shape_bucket(rec.n_chans, T, rec.n_samples_per_chan)
+    assert b == "C384_K304_L61_w16"
+    autotune._store({b: {"group_size": 32, "ms": {"16": 2.0, "32": 1.0}}})
+    gs, bucket, times = autotune.tune(rec.voltage, T, -0.5 * rec.fresh_metrics()["template_SS"],
+                                      rec.n_samples_per_chan)
+    assert (gs, bucket, times) == (32, b, None)
