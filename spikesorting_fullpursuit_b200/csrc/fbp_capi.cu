@@ -678,6 +678,7 @@ int tc_likelihood_pass(const Workspace &w, const float *v, u32 n, u32 C, const f
                        Counters *cnt, cudaStream_t st, int *launches) {
     (void)max_windows;
     FBP_CUDA(cudaMemsetAsync(&cnt->tc_refseg, 0, 8, st));
+    FBP_CUDA(cudaMemsetAsync(&cnt->tc_overflow, 0, 4, st));   // set by the tiles when the list overflows
     (void)v; (void)n; (void)C; (void)T; (void)K; (void)L; (void)tss; (void)win; (void)n_win; (void)Lk;
     FBP_ALLOW_SMEM(k_lik_tc<0>);
     const u32 G = (u32)w.tcg.size();
@@ -702,7 +703,7 @@ int tc_refine_pass(const Workspace &w, const float *v, u32 n, u32 C, const float
     k_tc_refine<<<sm_count() * 8, kRefThreads, rsmem, st>>>(
         v, n, C, w.tc_cmax, T, K, L, tss, w.tc_ref_t, w.tc_ref_s, w.tc_seg_s0, w.tc_seg_base, w.tc_seg_cnt,
         w.tc_seg_grp, w.tc_gdesc, w.tperm, reinterpret_cast<const u32 *>(&cnt->tc_refseg), w.tc_seg_cap, Lk,
-        lazy_ctx(w, v, T, tss, C, L, 0), gamma, &cnt->tc_seq, w.wpos);
+        lazy_ctx(w, v, T, tss, C, L, 0), gamma, &cnt->tc_seq, w.wpos, &cnt->tc_overflow, w.tc_ref_cap);
     k_tc_gate<<<1, 1, 0, st>>>(cnt, w.tc_ref_cap, w.tc_seg_cap);
     FBP_LAUNCH_CHECK();
     int rc = launch_likelihood(v, n, C, T, K, L, tss, win, n_win, max_windows, Lk, st, &cnt->tc_overflow, w.apx,

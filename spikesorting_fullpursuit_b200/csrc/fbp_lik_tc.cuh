@@ -927,15 +927,20 @@ k_tc_refine(const float *__restrict__ vall, u32 n, u32 Call, u32 Cmax, const flo
             const u32 *__restrict__ seg_s0, const u32 *__restrict__ seg_base, const u32 *__restrict__ seg_cnt,
             const u32 *__restrict__ seg_grp, const u32 *__restrict__ gdesc, const u32 *__restrict__ tperm,
             const u32 *__restrict__ seg_count, u32 seg_cap, float *__restrict__ Lk, LazyLk z, double gamma,
-            u64 *__restrict__ n_seq, u8 *__restrict__ wpos) {
+            u64 *__restrict__ n_seq, u8 *__restrict__ wpos, const u32 *__restrict__ overflow, u32 ref_cap) {
     extern __shared__ float rsm[];
     const u32 lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     float *wbuf = rsm + (size_t)warp * kWarpChunk;
+    // A tile whose entries did not fit reserved its segment but wrote no
+    // record of it; the FP32 kernel then redoes the whole pass, so nothing
+    // here is needed (and the unwritten records must not be read).
+    if (*overflow) return;
     const u32 nseg = min(*seg_count, seg_cap);
     const u32 tstride = Call * L;          // floats between templates in T
     u32 nseq = 0;
     for (u32 sg = blockIdx.x; sg < nseg; sg += gridDim.x) {
         const u32 s0 = seg_s0[sg], base = seg_base[sg], cnt = seg_cnt[sg];
+        if (base > ref_cap || cnt > ref_cap - base) continue;   // never true for a written record
         // the segment's template group: columns t0.., channels [clo, clo + C)
         const u32 gi = seg_grp[sg];
         const u32 t0 = gdesc[3 * gi], clo = gdesc[3 * gi + 1], C = gdesc[3 * gi + 2];

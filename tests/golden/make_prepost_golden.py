@@ -77,7 +77,7 @@ def main():
     m = NS.compute_separability_metrics(T, covs, si)
     for k in ("template_SS", "neuron_variances", "neuron_lower_CI", "neuron_lower_thresholds", "peak_channel",
               "contamination", "channel_p_noise"):
-        out["sep_" + k] = np.asarray(m[k])
+        out["sep_" + k] = np.array(m[k], copy=True)       # set_bp_threshold changes some in place
     m = NS.set_bp_threshold(m)
     out["sep_bp_thresholds"] = np.asarray(m["neuron_lower_thresholds"])
     np.savez_compressed(os.path.join(HERE, "prepost", "prepost.npz"), **out)
