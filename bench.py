@@ -69,6 +69,9 @@ def parse():
     ap.add_argument("--time-scale", type=float, default=0.05,
                     help="batch/serve: factor on the segment durations of the workload")
     ap.add_argument("--slots", type=int, default=4, help="batch/serve: concurrent requests on the GPU")
+    ap.add_argument("--tune", action="store_true",
+                    help="batch/serve: tensor-core group size per shape bucket from the tuner (buckets tuned "
+                         "before the timed runs, untimed)")
     ap.add_argument("--fp32-segments", type=int, default=0,
                     help="batch/serve: run the plain-FP32 comparison on the first N requests only "
                          "(saturated, no Poisson sweep); 0: all of them")
@@ -309,6 +312,18 @@ def run_mix(args):
         B.build()
     torch.cuda.set_device(local)
     units = float(sum(sp.units for sp in specs))
+    tuned = None
+    if args.tune:
+        # one timed trial per shape bucket, before (and outside) the timed runs
+        from spikesorting_fullpursuit_b200 import autotune
+        t_tune = time.perf_counter()
+        seen = {}
+        for (v, si, m, nmax) in segs:
+            L = int(si["n_samples_per_chan"])
+            b = autotune.shape_bucket(v.shape[0], m["templates"], L)
+            if b not in seen:
+                seen[b] = autotune.tune(v, m["templates"], np.float32(-0.5 * m["template_SS"]), L)[0]
+        tuned = {"buckets": len(seen), "group_sizes": seen, "tuning_s": time.perf_counter() - t_tune}
     clocks = ClockSampler(local)
     out = {}
     reference_outputs = None
@@ -319,7 +334,8 @@ def run_mix(args):
         # requests only (a bounded call); its spikes are checked against the
         # same requests of the bf16 run
         run_segs = segs if (prec == "bf16" or not args.fp32_segments) else segs[: args.fp32_segments]
-        with PursuitServer(slots=args.slots, precision=prec, overlap=args.overlap) as srv:
+        with PursuitServer(slots=args.slots, precision=prec, overlap=args.overlap,
+                           tune=bool(args.tune) and prec == "bf16") as srv:
             drive(srv, run_segs[: 2 * args.slots])                    # warm-up (untimed)
             torch.cuda.synchronize()
             res, wall = drive(srv, run_segs)                            # saturated: all at once
@@ -357,7 +373,7 @@ def run_mix(args):
             "value": bf["throughput"], "unit": UNIT, "n_gpus": 1, "higher_is_better": True,
             "fp32_value": fp["throughput"],
             "bf16_over_fp32": (out["bf16"].get("saturated_fp32_subset", bf)["throughput"] / fp["throughput"]),
-            "fp32_requests": fp["requests"],
+            "fp32_requests": fp["requests"], "tuned": tuned,
             "spikes_identical_bf16_fp32_and_across_runs": bool(identical),
             "data": "synthetic (seeded per request)",
             "config": {"workload": "serve_mix" if serve else "batch_mix", "requests": nseg,

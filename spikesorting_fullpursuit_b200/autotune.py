@@ -28,15 +28,27 @@ def cache_path():
                                                             "tc_groups.json")
 
 
+def _up(x, m):
+    return (int(x) + m - 1) // m * m
+
+
 def shape_bucket(n_chans, templates, L):
-    """(C, K rounded up to 16, L, median template support width rounded up
-    to 8 channels): the quantities the group plan depends on."""
+    """The quantities the group plan depends on, rounded: channels up to 8,
+    templates up to 16, clip length up to 16, median template support width
+    up to 8 channels."""
     T = np.asarray(templates, dtype=np.float32).reshape(-1, n_chans, L)
     K = T.shape[0]
     nz = np.any(T != 0, axis=2)
     widths = [(np.nonzero(r)[0][-1] - np.nonzero(r)[0][0] + 1) if r.any() else 0 for r in nz]
     w = int(np.median(widths)) if widths else n_chans
-    return "C%d_K%d_L%d_w%d" % (n_chans, (K + 15) // 16 * 16, L, (w + 7) // 8 * 8)
+    return "C%d_K%d_L%d_w%d" % (_up(n_chans, 8), _up(K, 16), _up(L, 16), _up(w, 8))
+
+
+def candidates_for(n_templates):
+    """Group sizes that make distinct plans: up to the template count
+    rounded up to 16 (larger sizes give the same single group)."""
+    kall = _up(n_templates, 16)
+    return tuple(g for g in CANDIDATES if g <= kall) or (16,)
 
 
 def _load():
@@ -103,8 +115,12 @@ def tune(voltage, templates, neg_half_ss, L, sample_samples=120000, force=False)
     table = _load()
     if not force and bucket in table:
         return int(table[bucket]["group_size"]), bucket, None
+    K = int(np.asarray(templates).reshape(-1, C * L).shape[0])
+    cands = candidates_for(K)
+    if len(cands) == 1:                                      # nothing to choose
+        return cands[0], bucket, None
     sample = np.asarray(voltage)[:, :min(int(sample_samples), np.shape(voltage)[1])]
-    times = time_group_sizes(sample, templates, neg_half_ss, L)
+    times = time_group_sizes(sample, templates, neg_half_ss, L, cands)
     best = min(times, key=times.get)
     table[bucket] = {"group_size": int(best), "ms": {str(k): v for k, v in times.items()},
                      "sample_samples": int(sample.shape[1])}

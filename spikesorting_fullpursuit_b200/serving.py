@@ -191,7 +191,7 @@ class PursuitServer:
     streams.  `hbm_budget` defaults to 80 % of the device's free memory when
     the server starts."""
 
-    def __init__(self, slots=4, hbm_budget=None, device=None, precision="bf16", overlap="fast"):
+    def __init__(self, slots=4, hbm_budget=None, device=None, precision="bf16", overlap="fast", tune=False):
         import torch
         if not torch.cuda.is_available():
             raise RuntimeError("No GPU available")
@@ -201,6 +201,7 @@ class PursuitServer:
             hbm_budget = int(0.8 * free)
         self.precision = precision
         self.overlap = overlap
+        self.tune = tune                # tensor-core group size from the tuner's cache per shape bucket
         self.total_mem = torch.cuda.get_device_properties(self.device).total_memory
         self._streams = [None] * slots
         self._sched = AdmissionScheduler(slots, hbm_budget, self._run, self._init_worker)
@@ -226,6 +227,7 @@ class PursuitServer:
         kwargs.setdefault("precision", self.precision)
         kwargs.setdefault("overlap", self.overlap)
         kwargs.setdefault("device", self.device)
+        kwargs.setdefault("tune", self.tune)
         fp = request_footprint(voltage, sort_info, separability_metrics, n_max_shift_inds,
                                kwargs["precision"], kwargs["overlap"], kwargs.get("chunk_samples"),
                                self.total_mem, kwargs.get("max_gpu_memory"))

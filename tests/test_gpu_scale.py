@@ -236,7 +236,8 @@ def test_tuned_group_size_gives_the_same_spikes(lib, tmp_path, monkeypatch):
     table = autotune._load()
     assert len(table) == 1
     entry = next(iter(table.values()))
-    assert entry["group_size"] in autotune.CANDIDATES and len(entry["ms"]) == len(autotune.CANDIDATES)
+    assert entry["group_size"] in autotune.candidates_for(rec.n_templates)
+    assert len(entry["ms"]) == len(autotune.candidates_for(rec.n_templates))
     for gs in (16, 32, 64):
         autotune.apply(gs)
         try:

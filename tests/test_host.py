@@ -109,7 +109,9 @@ def test_tuner_bucket_and_cache(tmp_path, monkeypatch):
     rec = synthetic.hd384(duration_s=0.01, seed=2)
     T = rec.fresh_metrics()["templates"]
     b = autotune.shape_bucket(rec.n_chans, T, rec.n_samples_per_chan)
-    assert b == "C384_K304_L61_w16"
+    assert b == "C384_K304_L64_w16"
+    assert autotune.candidates_for(300) == autotune.CANDIDATES
+    assert autotune.candidates_for(20) == (16, 32)
     autotune._store({b: {"group_size": 32, "ms": {"16": 2.0, "32": 1.0}}})
     gs, bucket, times = autotune.tune(rec.voltage, T, -0.5 * rec.fresh_metrics()["template_SS"],
                                       rec.n_samples_per_chan)
