@@ -8,7 +8,7 @@ masks, the template-sum search.  Within a stated tolerance: the clip noise
 covariance (float64 sums in another order: 1e-9 of its largest entry), the
 Wiener filter (float32 throughout as numpy does it, cuFFT against numpy's
 pocketfft transform: 1e-5 of the largest output) and the ZCA matrix (the
-reference sums the covariance in float32, this library in float64: 2e-4 of
+reference sums the covariance in float32, this library in float64: 1e-5 of
 the largest entry)."""
 import os
 
@@ -115,7 +115,7 @@ def test_zca_matrix_and_whitening_match_reference():
     ref = GOLD["zca"]
     err = np.abs(Z - ref).max() / np.abs(ref).max()
     print("\nZCA matrix: max difference %.2e of the largest entry" % err)
-    assert err < 2e-4, err
+    assert err < 1e-5, err
     # the whitening itself against numpy's float64 product, rounded to float32
     out = PRE.zca_apply(ref, v)
     exp = (ref @ v).astype(np.float32)
