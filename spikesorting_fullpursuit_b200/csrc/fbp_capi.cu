@@ -129,6 +129,7 @@ struct Workspace {
     u32 slots;
     float *NT, *sNT, *tnorm, *Q, *XMr, *XM, *H, *vn, *cand_lb, *ga_lo, *ga_hi, *ga_max, *ga_abs, *pool_hi;
     u32 *ga_bits, *seed_a1;
+    float *pair_mb, *pair_mabs;
     Counters *snap;                  // counts of the last pass
     u32 *tsup, *tperm, *grange;      // template channel supports, order, group ranges
     u32 *grange32;                   // group ranges of 32 slots (masked overlap tables)
@@ -302,6 +303,8 @@ Workspace layout(char *base, u32 n, u32 K, u32 L, u32 nmax, bool want_fast, u32 
         w.ga_max = (float *)take(sl * 4);
         w.ga_abs = (float *)take(sl * 4);
         w.seed_a1 = (u32 *)take(sl * 4);
+        w.pair_mb = (float *)take(sl * K * 4);
+        w.pair_mabs = (float *)take(sl * K * 4);
         w.cand_lb = (float *)take(sl * 4);
         w.best_key = (u64 *)take(sl * 8);
         w.pool_cap = (u32)std::min<u64>(0x7fffffffull, std::max<u64>(1u << 22, (u64)sl * 128));
@@ -480,6 +483,7 @@ OvArgs ov_args(const Workspace &w, const float *v, u32 n, u32 C, const float *T,
     A.cand_lb = w.cand_lb;
     A.ga_lo = w.ga_lo; A.ga_hi = w.ga_hi; A.ga_bits = w.ga_bits; A.ga_max = w.ga_max; A.ga_abs = w.ga_abs;
     A.seed_a1 = w.seed_a1;
+    A.pair_mb = w.pair_mb; A.pair_mabs = w.pair_mabs;
     A.tsup = w.tsup;
     A.pool_slot = w.pool_slot; A.pool_item = w.pool_item; A.pool_hi = w.pool_hi; A.pool_cap = w.pool_cap;
     A.refined = &cnt->ov_ref;

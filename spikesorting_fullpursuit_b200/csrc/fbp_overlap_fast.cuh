@@ -63,6 +63,8 @@ struct OvArgs {
     float *ga_max, *ga_abs;          // [slot]     largest in-bounds hi(a), largest |hi(a)|
     unsigned long long *scan_next;   // next (candidate, template) pair of the scan
     u32 *seed_a1;                    // [slot]     in-bounds row a of largest lower bound
+    float *pair_mb, *pair_mabs;      // [slot][K]  per (candidate, template): largest in-bounds upper
+                                     //            bound of a row b and of its magnitude (from the seed)
     const u32 *tsup;                 // [K][2] non-zero channel range of each template (may be NULL)
     u32 *pool_total;                 // appended entries this pass
     u32 pool_cap;
@@ -600,7 +602,7 @@ k_ov_seed(OvArgs A) {
         ov_sub_b(A, g, t, subB0, subB1);
         const float eqt = 4.0f * kUnitRoundoff * A.tnorm[c.k0] * A.tnorm[t];
         const u32 xend = min(S, c.xhi_ex);
-        float v1 = -INFINITY, v2 = -INFINITY;
+        float v1 = -INFINITY, v2 = -INFINITY, mB = -INFINITY, mabs = 0.0f;
         u32 b1 = 0, b2 = 0;
         for (u32 x = c.xlo + lane; x < xend; x += 32) {
             float lo, hi;
@@ -608,9 +610,17 @@ k_ov_seed(OvArgs A) {
                             subB0, subB1, lo, hi);
             if (lo > v1) { v1 = lo; b1 = x; }
             if ((x > a1 ? x - a1 : a1 - x) <= L && lo > v2) { v2 = lo; b2 = x; }
+            mB = fmaxf(mB, hi);
+            mabs = fmaxf(mabs, fabsf(hi));
         }
         warp_argmax(v1, b1);
         warp_argmax(v2, b2);
+        mB = warp_max_f(mB);
+        mabs = warp_max_f(mabs);
+        if (lane == 0) {                                 // the scan's pair test, before its row pass
+            A.pair_mb[e] = mB;
+            A.pair_mabs[e] = mabs;
+        }
         float v3 = -INFINITY;
         u32 a3 = 0;
         for (u32 x = c.xlo + lane; x < xend; x += 32)
@@ -678,6 +688,14 @@ k_ov_scan(OvArgs A) {
         const float TH = fmaxf(LB, c.lbest);
         const size_t pair = (size_t)c.k0 * K + t;
         const float XM = A.XM[pair];
+        {
+            // the pair test below with the seed's row maxima (the same values
+            // the row pass computes): a pair that fails it needs no row pass
+            const float mB0 = A.pair_mb[e];
+            const float mabs0 = fmaxf(A.ga_abs[g], A.pair_mabs[e]);
+            const float slack0 = kPruneSlack * (2.0f * mabs0 + fabsf(TH) + fabsf(XM));
+            if (!(mA + mB0 + XM + slack0 >= TH)) continue;
+        }
         const float *Hg = A.H + ((size_t)g * K + t) * S;
         float subB0, subB1;
         ov_sub_b(A, g, t, subB0, subB1);
