@@ -145,6 +145,14 @@ class ClockSampler:
                 "samples": len(rows)}
 
 
+# DRAM bytes (read + write) per unit of algorithmic work of the tensor-core
+# likelihood tiles (k_lik_tc<0>), from one ncu capture of pass 1 of a 10 s
+# slice of each workload (every window listed; dram__bytes_read.sum +
+# dram__bytes_write.sum over sample x templates of the pass):
+# profiles/k_lik_tc_hd384_10s.md, profiles/k_lik_tc_linear16_10s.md.
+LIK_TC_DRAM_BYTES_PER_ST = {"hd384_300u": None, "linear16_64u": None}
+
+
 def measured_peaks():
     p = os.path.join(REPO, "MEASURED_PEAKS.json")
     if os.path.exists(p):
@@ -534,8 +542,17 @@ def main():
             per_stage["overlap"]["reference_equivalent_tflops"] = work[2] * 5.0 * Ct * L / secs / 1e12
     dom = max((k for k in per_stage if per_stage[k]["frac"] is not None), key=lambda k: per_stage[k]["ms"])
     d = per_stage[dom]
+    traffic = None
+    per_st = LIK_TC_DRAM_BYTES_PER_ST.get(rec.name)
+    if dom == "likelihood" and prec == 1 and per_st:
+        # algorithmic: every listed sample's voltage read once (4 C bytes,
+        # shared by the K templates) and 4 + 1 bytes written per entry
+        traffic = {"bytes_per_step": per_st * float(work[0]),
+                   "algorithmic_bytes_per_step": float(work[0]) * (5.0 + 4.0 * C / K),
+                   "source": "ncu dram__bytes_read.sum + dram__bytes_write.sum of k_lik_tc<0>, pass 1 of a 10 s "
+                             "slice (every window), per sample*template, times the step's sample*templates"}
     roofline = {"bound": d["bound"], "achieved": d["achieved"], "peak": d["peak"], "unit": d["unit"],
-                "frac": d["frac"], "traffic": None, "kernel": dom,
+                "frac": d["frac"], "traffic": traffic, "kernel": dom,
                 "peak_source": peak_src + (" sustained" if d["bound"] == "tensor" else ""),
                 "stages": per_stage,
                 "stage_ms_per_step": {_lib.STAGE_NAMES[i]: stage_ms[i] for i in range(_lib.N_STAGES)}}

@@ -419,57 +419,38 @@ k_lik_tc(const TcArgs *__restrict__ gargs, u32 ngroups) {
                     }
                 }
             }
-            // ---- row sums (energy, absolute) and the tile's largest magnitude:
-            // items (row x, group of 8 channels) over all producer threads,
-            // two items at a time; each item's partial sums go to the strip
-            // buffer (free until the strip is written below), then each row
-            // adds its groups in channel order
+            // ---- row sums (energy, absolute) and the tile's largest magnitude
             float mx = 0.0f;
-            float2 *part = reinterpret_cast<float2 *>(As);       // [cg][x]
-            const u32 nitem8 = rows_pad * Cg2;
-            auto load8 = [&](u32 e, float (&f)[8]) {
-                const u32 x = e % rows_pad, cg = e / rows_pad;
-                const long long pos = s0 + x;
-                const bool inside = pos >= m_lo && pos < m_hi && pos < n;
-                const float *vp = A.v + pos;
-#pragma unroll
-                for (int j = 0; j < 8; j++) {
-                    const u32 c = cg * 8 + j;
-                    f[j] = (inside && c < A.C) ? vp[(size_t)c * n] : 0.0f;
-                }
-            };
-            auto reduce8 = [&](u32 e, const float (&f)[8]) {
-                float e2 = 0.0f, ab = 0.0f;
-#pragma unroll
-                for (int j = 0; j < 8; j++) {
-                    e2 = fmaf(f[j], f[j], e2);
-                    ab += fabsf(f[j]);
-                    mx = fmaxf(mx, fabsf(f[j]));
-                }
-                part[(size_t)(e / rows_pad) * rows_pad + e % rows_pad] = make_float2(e2, ab);
-            };
-            for (u32 e = pt; e < nitem8; e += 2 * kTcProdThreads) {
-                float f0[8], f1[8];
-                const u32 e1 = e + kTcProdThreads;
-                load8(e, f0);
-                if (e1 < nitem8) load8(e1, f1);
-                reduce8(e, f0);
-                if (e1 < nitem8) reduce8(e1, f1);
-            }
-            mx = warp_max_f(mx);
-            if (lane == 0) pred[warp] = __float_as_uint(mx);
-            named_bar(1, kTcProdThreads);
             for (u32 x = pt; x < rows_pad; x += kTcProdThreads) {
+                const long long pos = s0 + x;
                 float e2 = 0.0f, ab = 0.0f;
-                for (u32 cg = 0; cg < Cg2; cg++) {
-                    const float2 q = part[(size_t)cg * rows_pad + x];
-                    e2 += q.x;
-                    ab += q.y;
+                if (pos >= m_lo && pos < m_hi && pos < n) {
+                    const float *vp = A.v + pos;
+                    u32 c = 0;
+                    for (; c + 8 <= A.C; c += 8) {
+                        float f[8];
+#pragma unroll
+                        for (int j = 0; j < 8; j++) f[j] = vp[(size_t)(c + j) * n];
+#pragma unroll
+                        for (int j = 0; j < 8; j++) {
+                            e2 = fmaf(f[j], f[j], e2);
+                            ab += fabsf(f[j]);
+                            mx = fmaxf(mx, fabsf(f[j]));
+                        }
+                    }
+                    for (; c < A.C; c++) {
+                        const float f = vp[(size_t)c * n];
+                        e2 = fmaf(f, f, e2);
+                        ab += fabsf(f);
+                        mx = fmaxf(mx, fabsf(f));
+                    }
                 }
                 rowsq[x] = e2;
                 rowab[x] = ab;
             }
-            named_bar(1, kTcProdThreads);                     // partial sums read before the strip overwrites them
+            mx = warp_max_f(mx);
+            if (lane == 0) pred[warp] = __float_as_uint(mx);
+            named_bar(1, kTcProdThreads);
             int kexp = 0;
             {
                 float m = 0.0f;
@@ -632,13 +613,19 @@ k_lik_tc(const TcArgs *__restrict__ gargs, u32 ngroups) {
             if (MODE == 1) {
                 // H[g][t][b] = correlation - 0.5 * clipped energy, b = shift row
                 const u32 brow = subi * kTcM + row;
-                auto table_cols = [&](auto cwc, u32 c0) {
-                    constexpr int CW = decltype(cwc)::value;
-                    u32 r[CW];
-                    tmem_ld<CW>(r, acc0 + c0);
+                for (u32 c0 = 16 * half; c0 < Np; c0 += 32) {
+                    u32 r[16];
+                    asm volatile(
+                        "tcgen05.ld.sync.aligned.32x32b.x16.b32 "
+                        "{%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, %15}, [%16];"
+                        : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]),
+                          "=r"(r[7]), "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]),
+                          "=r"(r[14]), "=r"(r[15])
+                        : "r"(acc0 + c0));
+                    asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
                     if (brow < A.S) {
 #pragma unroll
-                        for (int q = 0; q < CW; q++) {
+                        for (int q = 0; q < 16; q++) {
                             const u32 t = c0 + q;
                             if (t >= A.K) continue;
                             const u32 gt = ctrow[t];
@@ -648,11 +635,6 @@ k_lik_tc(const TcArgs *__restrict__ gargs, u32 ngroups) {
                             A.H[((size_t)g * A.Kall + gt) * A.S + brow] = x - 0.5f * A.NT[(size_t)gt * A.S + brow];
                         }
                     }
-                };
-                if (Np == 16) {
-                    table_cols(ColW<8>{}, 8 * half);       // both warps of the quadrant: 8 columns each
-                } else {
-                    for (u32 c0 = 16 * half; c0 < Np; c0 += 32) table_cols(ColW<16>{}, c0);
                 }
                 asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
                 __syncwarp();
@@ -690,21 +672,26 @@ k_lik_tc(const TcArgs *__restrict__ gargs, u32 ngroups) {
             const u32 whi = wpt > 1 ? ((u32)s0 + 32u * quad + 31u) / L : wlo;
             const u32 myw = s / L;
             bool anypos = false;
-            // One chunk of CW columns starting at c0; its uncertain entries
-            // set bits `shift`.. of `word`.  CW = 16: the two warps of a
-            // quadrant take alternate 16-column chunks; groups of exactly 16
-            // templates use CW = 8, so both warps drain 8 columns each.
-            auto chunk = [&](auto cwc, u32 c0, u32 &word, u32 shift) {
-                constexpr int CW = decltype(cwc)::value;
-                float uq[CW];
 #pragma unroll
-                for (int q = 0; q < CW; q++) uq[q] = 0.0f;
-                u32 r[CW];
-                tmem_ld<CW>(r, acc0 + c0);
+            for (int k = 0; k < 8; k++) {
+                const u32 c0 = 16 * half + 32 * k;
+                if (c0 >= Np) break;                     // uniform in the warp
+                float uq[16];
+#pragma unroll
+                for (int q = 0; q < 16; q++) uq[q] = 0.0f;
+                u32 r[16];
+                asm volatile(
+                    "tcgen05.ld.sync.aligned.32x32b.x16.b32 "
+                    "{%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, %15}, [%16];"
+                    : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]),
+                      "=r"(r[7]), "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]),
+                      "=r"(r[14]), "=r"(r[15])
+                    : "r"(acc0 + c0));
+                asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
                 u32 cw = 0;
                 if (in_win) {
 #pragma unroll
-                for (int q = 0; q < CW; q++) {
+                for (int q = 0; q < 16; q++) {
                     const u32 t = c0 + q;
                     // padding columns (t >= K) are computed and dropped, so the
                     // loop has no exit and its shared-memory reads can be issued early
@@ -734,41 +721,28 @@ k_lik_tc(const TcArgs *__restrict__ gargs, u32 ngroups) {
                     anypos |= real && !tail && pos;
                 }
                 if (tail) lomax = 0.0f, bmax = 0.0f;
-                word |= cw << shift;
+                wantbits[k] |= cw << (16 * half);
                 }
                 // per (window, template): the largest upper bound over the
-                // tile's rows -- the CW columns reduced over the warp together
+                // tile's rows -- the 16 columns reduced over the warp together
+                // (16 shuffles), column (lane >> 1) & 15 ending in lanes 2j, 2j+1
                 {
-                    constexpr u32 per = 32 / CW;               // lanes holding one column's result
-                    const u32 col = (lane / per) & (CW - 1);
-                    float vv[CW];
+                    const u32 col = (lane >> 1) & 15u;
+                    float vv[16];
 #pragma unroll
-                    for (int q = 0; q < CW; q++) vv[q] = myw == wlo ? uq[q] : 0.0f;
-                    float u;
-                    if constexpr (CW == 16) u = warp_max16(vv, lane); else u = warp_max8(vv, lane);
-                    if ((lane % per) == 0 && u > 0.0f && c0 + col < A.K)
+                    for (int q = 0; q < 16; q++) vv[q] = myw == wlo ? uq[q] : 0.0f;
+                    const float u = warp_max16(vv, lane);
+                    if ((lane & 1u) == 0 && u > 0.0f && c0 + col < A.K)
                         atomicMax(reinterpret_cast<int *>(A.umax) + (size_t)wlo * A.Kall + ctrow[c0 + col],
                                   __float_as_int(u));
                     if (whi != wlo) {                    // uniform in the warp
 #pragma unroll
-                        for (int q = 0; q < CW; q++) vv[q] = myw == whi ? uq[q] : 0.0f;
-                        float u2;
-                        if constexpr (CW == 16) u2 = warp_max16(vv, lane); else u2 = warp_max8(vv, lane);
-                        if ((lane % per) == 0 && u2 > 0.0f && c0 + col < A.K)
+                        for (int q = 0; q < 16; q++) vv[q] = myw == whi ? uq[q] : 0.0f;
+                        const float u2 = warp_max16(vv, lane);
+                        if ((lane & 1u) == 0 && u2 > 0.0f && c0 + col < A.K)
                             atomicMax(reinterpret_cast<int *>(A.umax) + (size_t)whi * A.Kall + ctrow[c0 + col],
                                       __float_as_int(u2));
                     }
-                }
-            };
-            if (Np == 16) {
-                // bit t of word 0 is column t, as phase 2 decodes it
-                chunk(ColW<8>{}, 8 * half, wantbits[0], 8 * half);
-            } else {
-#pragma unroll
-                for (int k = 0; k < 8; k++) {
-                    const u32 c0 = 16 * half + 32 * k;
-                    if (c0 >= Np) break;                 // uniform in the warp
-                    chunk(ColW<16>{}, c0, wantbits[k], 16 * half);
                 }
             }
             if (__any_sync(0xffffffffu, anypos && myw == wlo) && lane == 0) A.wpos[wlo] = 1;
@@ -952,16 +926,11 @@ k_tc_refine(const float *__restrict__ vall, u32 n, u32 Call, u32 Cmax, const flo
             const u32 t = trow ? trow[ref_t[base + e]] : ref_t[base + e], so = ref_s[base + e] - s0;
             const float *tp = T + (size_t)t * tstride;      // the group's channels of template t
             double X = 0.0, S = 0.0;
-            // element q = c * L + i of the template against voltage row c at
-            // sample s0 + so + i; (c, i) stepped by 32 without a division
-            const float *vs = v + s0 + so;
-            u32 c = lane / L, i = lane - c * L;
             for (u32 q = lane; q < CL; q += 32) {
-                const double p = (double)__ldg(tp + q) * (double)__ldg(vs + (size_t)c * n + i);
+                const u32 c = q / L, i = q - c * L;
+                const double p = (double)__ldg(tp + q) * (double)__ldg(v + (size_t)c * n + s0 + so + i);
                 X += p;
                 S += fabs(p);
-                i += 32;
-                while (i >= L) { i -= L; c++; }
             }
 #pragma unroll
             for (int o = 16; o > 0; o >>= 1) {
