@@ -613,19 +613,13 @@ k_lik_tc(const TcArgs *__restrict__ gargs, u32 ngroups) {
             if (MODE == 1) {
                 // H[g][t][b] = correlation - 0.5 * clipped energy, b = shift row
                 const u32 brow = subi * kTcM + row;
-                for (u32 c0 = 16 * half; c0 < Np; c0 += 32) {
-                    u32 r[16];
-                    asm volatile(
-                        "tcgen05.ld.sync.aligned.32x32b.x16.b32 "
-                        "{%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, %15}, [%16];"
-                        : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]),
-                          "=r"(r[7]), "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]),
-                          "=r"(r[14]), "=r"(r[15])
-                        : "r"(acc0 + c0));
-                    asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+                auto table_cols = [&](auto cwc, u32 c0) {
+                    constexpr int CW = decltype(cwc)::value;
+                    u32 r[CW];
+                    tmem_ld<CW>(r, acc0 + c0);
                     if (brow < A.S) {
 #pragma unroll
-                        for (int q = 0; q < 16; q++) {
+                        for (int q = 0; q < CW; q++) {
                             const u32 t = c0 + q;
                             if (t >= A.K) continue;
                             const u32 gt = ctrow[t];
@@ -635,6 +629,11 @@ k_lik_tc(const TcArgs *__restrict__ gargs, u32 ngroups) {
                             A.H[((size_t)g * A.Kall + gt) * A.S + brow] = x - 0.5f * A.NT[(size_t)gt * A.S + brow];
                         }
                     }
+                };
+                if (Np == 16) {
+                    table_cols(ColW<8>{}, 8 * half);       // both warps of the quadrant: 8 columns each
+                } else {
+                    for (u32 c0 = 16 * half; c0 < Np; c0 += 32) table_cols(ColW<16>{}, c0);
                 }
                 asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
                 __syncwarp();
@@ -672,26 +671,21 @@ k_lik_tc(const TcArgs *__restrict__ gargs, u32 ngroups) {
             const u32 whi = wpt > 1 ? ((u32)s0 + 32u * quad + 31u) / L : wlo;
             const u32 myw = s / L;
             bool anypos = false;
+            // One chunk of CW columns starting at c0; its uncertain entries
+            // set bits `shift`.. of `word`.  CW = 16: the two warps of a
+            // quadrant take alternate 16-column chunks; groups of exactly 16
+            // templates use CW = 8, so both warps drain 8 columns each.
+            auto chunk = [&](auto cwc, u32 c0, u32 &word, u32 shift) {
+                constexpr int CW = decltype(cwc)::value;
+                float uq[CW];
 #pragma unroll
-            for (int k = 0; k < 8; k++) {
-                const u32 c0 = 16 * half + 32 * k;
-                if (c0 >= Np) break;                     // uniform in the warp
-                float uq[16];
-#pragma unroll
-                for (int q = 0; q < 16; q++) uq[q] = 0.0f;
-                u32 r[16];
-                asm volatile(
-                    "tcgen05.ld.sync.aligned.32x32b.x16.b32 "
-                    "{%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, %15}, [%16];"
-                    : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]),
-                      "=r"(r[7]), "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]),
-                      "=r"(r[14]), "=r"(r[15])
-                    : "r"(acc0 + c0));
-                asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+                for (int q = 0; q < CW; q++) uq[q] = 0.0f;
+                u32 r[CW];
+                tmem_ld<CW>(r, acc0 + c0);
                 u32 cw = 0;
                 if (in_win) {
 #pragma unroll
-                for (int q = 0; q < 16; q++) {
+                for (int q = 0; q < CW; q++) {
                     const u32 t = c0 + q;
                     // padding columns (t >= K) are computed and dropped, so the
                     // loop has no exit and its shared-memory reads can be issued early
@@ -721,28 +715,41 @@ k_lik_tc(const TcArgs *__restrict__ gargs, u32 ngroups) {
                     anypos |= real && !tail && pos;
                 }
                 if (tail) lomax = 0.0f, bmax = 0.0f;
-                wantbits[k] |= cw << (16 * half);
+                word |= cw << shift;
                 }
                 // per (window, template): the largest upper bound over the
-                // tile's rows -- the 16 columns reduced over the warp together
-                // (16 shuffles), column (lane >> 1) & 15 ending in lanes 2j, 2j+1
+                // tile's rows -- the CW columns reduced over the warp together
                 {
-                    const u32 col = (lane >> 1) & 15u;
-                    float vv[16];
+                    constexpr u32 per = 32 / CW;               // lanes holding one column's result
+                    const u32 col = (lane / per) & (CW - 1);
+                    float vv[CW];
 #pragma unroll
-                    for (int q = 0; q < 16; q++) vv[q] = myw == wlo ? uq[q] : 0.0f;
-                    const float u = warp_max16(vv, lane);
-                    if ((lane & 1u) == 0 && u > 0.0f && c0 + col < A.K)
+                    for (int q = 0; q < CW; q++) vv[q] = myw == wlo ? uq[q] : 0.0f;
+                    float u;
+                    if constexpr (CW == 16) u = warp_max16(vv, lane); else u = warp_max8(vv, lane);
+                    if ((lane % per) == 0 && u > 0.0f && c0 + col < A.K)
                         atomicMax(reinterpret_cast<int *>(A.umax) + (size_t)wlo * A.Kall + ctrow[c0 + col],
                                   __float_as_int(u));
                     if (whi != wlo) {                    // uniform in the warp
 #pragma unroll
-                        for (int q = 0; q < 16; q++) vv[q] = myw == whi ? uq[q] : 0.0f;
-                        const float u2 = warp_max16(vv, lane);
-                        if ((lane & 1u) == 0 && u2 > 0.0f && c0 + col < A.K)
+                        for (int q = 0; q < CW; q++) vv[q] = myw == whi ? uq[q] : 0.0f;
+                        float u2;
+                        if constexpr (CW == 16) u2 = warp_max16(vv, lane); else u2 = warp_max8(vv, lane);
+                        if ((lane % per) == 0 && u2 > 0.0f && c0 + col < A.K)
                             atomicMax(reinterpret_cast<int *>(A.umax) + (size_t)whi * A.Kall + ctrow[c0 + col],
                                       __float_as_int(u2));
                     }
+                }
+            };
+            if (Np == 16) {
+                // bit t of word 0 is column t, as phase 2 decodes it
+                chunk(ColW<8>{}, 8 * half, wantbits[0], 8 * half);
+            } else {
+#pragma unroll
+                for (int k = 0; k < 8; k++) {
+                    const u32 c0 = 16 * half + 32 * k;
+                    if (c0 >= Np) break;                 // uniform in the warp
+                    chunk(ColW<16>{}, c0, wantbits[k], 16 * half);
                 }
             }
             if (__any_sync(0xffffffffu, anypos && myw == wlo) && lane == 0) A.wpos[wlo] = 1;
