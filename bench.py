@@ -50,6 +50,9 @@ def parse():
                     help="bf16: 16-bit tensor-core likelihood and overlap tables with exact fp32 refinement "
                          "(results identical to fp32); fp32: exact fp32 pipes only")
     ap.add_argument("--overlap", choices=["fast", "exact"], default="fast")
+    ap.add_argument("--tc-layout", choices=["auto", "wide", "samples"], default="auto",
+                    help="tensor-core likelihood layout (same spikes): wide tiles of the window stream, "
+                         "128-sample tiles, or the library's choice")
     ap.add_argument("--cpu-sample-s", type=float, default=0.05,
                     help="seconds of recording timed on the CPU baseline")
     ap.add_argument("--ref-windows", type=int, default=None,
@@ -70,7 +73,7 @@ def parse():
                     help="batch/serve: factor on the segment durations of the workload")
     ap.add_argument("--slots", type=int, default=4, help="batch/serve: concurrent requests on the GPU")
     ap.add_argument("--tune", action="store_true",
-                    help="batch/serve: tensor-core group size per shape bucket from the tuner (buckets tuned "
+                    help="batch/serve: tensor-core plan per shape bucket from the tuner (buckets tuned "
                          "before the timed runs, untimed)")
     ap.add_argument("--fp32-segments", type=int, default=0,
                     help="batch/serve: run the plain-FP32 comparison on the first N requests only "
@@ -146,11 +149,13 @@ class ClockSampler:
 
 
 # DRAM bytes (read + write) per unit of algorithmic work of the tensor-core
-# likelihood tiles (k_lik_tc<0>), from one ncu capture of pass 1 of a 10 s
+# likelihood kernel of each layout, from one ncu capture of pass 1 of a 10 s
 # slice of each workload (every window listed; dram__bytes_read.sum +
-# dram__bytes_write.sum over sample x templates of the pass):
-# profiles/k_lik_tc_hd384_10s.md, profiles/k_lik_tc_linear16_10s.md.
-LIK_TC_DRAM_BYTES_PER_ST = {"hd384_300u": None, "linear16_64u": None}
+# dram__bytes_write.sum over sample x templates of the pass); see the
+# k_lik_tc* summaries in profiles/.
+LIK_TC_DRAM_BYTES_PER_ST = {("hd384_300u", "wide"): None, ("linear16_64u", "wide"): None,
+                            ("hd384_300u", "samples"): 11.5, ("linear16_64u", "samples"): None}
+LIK_KERNEL = {"wide": "k_lik_tcw", "samples": "k_lik_tc<0>"}
 
 
 def measured_peaks():
@@ -331,7 +336,7 @@ def run_mix(args):
             b = autotune.shape_bucket(v.shape[0], m["templates"], L)
             if b not in seen:
                 seen[b] = autotune.tune(v, m["templates"], np.float32(-0.5 * m["template_SS"]), L)[0]
-        tuned = {"buckets": len(seen), "group_sizes": seen, "tuning_s": time.perf_counter() - t_tune}
+        tuned = {"buckets": len(seen), "plans": seen, "tuning_s": time.perf_counter() - t_tune}
     clocks = ClockSampler(local)
     out = {}
     reference_outputs = None
@@ -425,6 +430,9 @@ def main():
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600),
                                 device_id=dev)
     lib = _lib.lib() if not B.needs_build() else (B.build(), _lib.lib())[1]
+    # every pursuit this thread runs (timed steps, fp32 arm, end to end)
+    _lib.check(lib.fbp_set_tc_layout({"auto": _lib.TC_LAYOUT_AUTO, "wide": _lib.TC_LAYOUT_WIDE,
+                                      "samples": _lib.TC_LAYOUT_SAMPLES}[args.tc_layout]))
 
     t_gen = time.perf_counter()
     rec = workload(args.workload, args.duration, seed=1 + rank)
@@ -543,14 +551,16 @@ def main():
     dom = max((k for k in per_stage if per_stage[k]["frac"] is not None), key=lambda k: per_stage[k]["ms"])
     d = per_stage[dom]
     traffic = None
-    per_st = LIK_TC_DRAM_BYTES_PER_ST.get(rec.name)
+    layout = {1: "samples", 2: "wide"}.get(int(st_prof.tc_layout))
+    per_st = LIK_TC_DRAM_BYTES_PER_ST.get((rec.name, layout))
     if dom == "likelihood" and prec == 1 and per_st:
         # algorithmic: every listed sample's voltage read once (4 C bytes,
         # shared by the K templates) and 4 + 1 bytes written per entry
         traffic = {"bytes_per_step": per_st * float(work[0]),
                    "algorithmic_bytes_per_step": float(work[0]) * (5.0 + 4.0 * C / K),
-                   "source": "ncu dram__bytes_read.sum + dram__bytes_write.sum of k_lik_tc<0>, pass 1 of a 10 s "
-                             "slice (every window), per sample*template, times the step's sample*templates"}
+                   "source": "ncu dram__bytes_read.sum + dram__bytes_write.sum of %s, pass 1 of a 10 s "
+                             "slice (every window), per sample*template, times the step's sample*templates"
+                             % LIK_KERNEL[layout]}
     roofline = {"bound": d["bound"], "achieved": d["achieved"], "peak": d["peak"], "unit": d["unit"],
                 "frac": d["frac"], "traffic": traffic, "kernel": dom,
                 "peak_source": peak_src + (" sustained" if d["bound"] == "tensor" else ""),
@@ -630,6 +640,7 @@ def main():
                 "config": {"workload": rec.name, "n_chans": C, "n_samples": n, "n_templates": K,
                            "template_len": L, "n_max_shift": nmax, "precision": args.precision,
                            "overlap": args.overlap, "voltage_dtype": str(rec.voltage.dtype),
+                           "tc_layout": {1: "samples", 2: "wide"}.get(int(st_prof.tc_layout)),
                            "l2": "inputs larger than L2 (voltage %.2f GB, likelihood %.2f GB)"
                                  % (C * n * 4 / 1e9, K * n * 4 / 1e9),
                            "passes": int(st_prof.passes), "spikes": int(st_prof.spikes),

@@ -112,6 +112,9 @@ typedef struct fbp_stage_stats {
     uint64_t lik_seq_refined;   /* entries of lik_refined whose sign a double-precision
                                    interval could not settle, re-evaluated in the
                                    reference's order (FBP_PREC_BF16_REFINE) */
+    uint32_t tc_layout;         /* tensor-core likelihood layout the chunk used:
+                                   0 none (FP32 path), FBP_TC_LAYOUT_SAMPLES or FBP_TC_LAYOUT_WIDE */
+    uint32_t reserved;
 } fbp_stage_stats;
 
 /* Library version (major*10000 + minor*100 + patch). */
@@ -169,6 +172,16 @@ int fbp_pursuit_chunk(float *voltage, uint32_t n_samples, uint32_t n_chans,
  * (spikesorting_fullpursuit_b200.autotune) from timed trials per shape
  * bucket.  Results do not depend on it. */
 int fbp_set_tc_group_size(uint32_t templates_per_group);
+
+/* Layout of the tensor-core likelihood passes (no counterpart in the
+ * reference).  FBP_TC_LAYOUT_SAMPLES: tiles of 128 samples, template groups
+ * in the MMA's N (fbp_lik_tc.cuh); FBP_TC_LAYOUT_WIDE: tiles of 2048 positions
+ * of the pass's window stream, 16 templates x 8 sample shifts in the MMA's M
+ * and blocks of 8 samples in N (fbp_lik_tcw.cuh; needs 16 <= L <= 1024);
+ * FBP_TC_LAYOUT_AUTO (default): WIDE where it applies.  Applies to the calls
+ * the calling thread makes afterwards.  Results do not depend on it. */
+enum { FBP_TC_LAYOUT_AUTO = 0, FBP_TC_LAYOUT_SAMPLES = 1, FBP_TC_LAYOUT_WIDE = 2 };
+int fbp_set_tc_layout(int layout);
 
 /* ------------------------------------------------------------------------
  * Testing hooks (no counterpart in the reference).

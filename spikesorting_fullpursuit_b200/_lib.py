@@ -24,6 +24,9 @@ PREC_FP32 = 0
 PREC_BF16_REFINE = 1
 OVERLAP_FAST = 0
 OVERLAP_EXACT = 1
+TC_LAYOUT_AUTO = 0
+TC_LAYOUT_SAMPLES = 1
+TC_LAYOUT_WIDE = 2
 
 _lib = None
 
@@ -55,6 +58,7 @@ SIGNATURES = {
     "fbp_scan_scratch_bytes": (SZ, [U32]),
     "fbp_set_test_limits": (I, [P]),
     "fbp_set_tc_group_size": (I, [U32]),
+    "fbp_set_tc_layout": (I, [I]),
     "fbp_tc_likelihood_bounds": (I, [P, U32, U32, P, U32, U32, P, P, SZ, P, P, P]),
     "fbp_window_u8_bytes": (SZ, [U32]),
 }
@@ -93,7 +97,8 @@ class StageStats(ctypes.Structure):
                 ("refined_items", ctypes.c_uint64), ("fallback_candidates", ctypes.c_uint64),
                 ("lik_refined", ctypes.c_uint64), ("lik_exact_passes", ctypes.c_uint64),
                 ("passes", ctypes.c_uint32), ("spikes", ctypes.c_uint32),
-                ("lik_lazy_refined", ctypes.c_uint64), ("lik_seq_refined", ctypes.c_uint64)]
+                ("lik_lazy_refined", ctypes.c_uint64), ("lik_seq_refined", ctypes.c_uint64),
+                ("tc_layout", ctypes.c_uint32), ("reserved", ctypes.c_uint32)]
 
     def as_dict(self):
         return {"passes": self.passes, "spikes": self.spikes, "candidates": int(self.candidates),
@@ -101,6 +106,7 @@ class StageStats(ctypes.Structure):
                 "fallback_candidates": int(self.fallback_candidates),
                 "lik_refined": int(self.lik_refined), "lik_exact_passes": int(self.lik_exact_passes),
                 "lik_lazy_refined": int(self.lik_lazy_refined), "lik_seq_refined": int(self.lik_seq_refined),
+                "tc_layout": {0: None, 1: "samples", 2: "wide"}.get(int(self.tc_layout)),
                 "ms": {STAGE_NAMES[i]: self.ms[i] for i in range(N_STAGES)},
                 "launches": {STAGE_NAMES[i]: int(self.launches[i]) for i in range(N_STAGES)},
                 "work": {STAGE_NAMES[i]: int(self.work[i]) for i in range(N_STAGES)}}

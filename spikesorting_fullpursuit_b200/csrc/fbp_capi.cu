@@ -17,6 +17,7 @@
 #include "../../include/fbp_b200.h"
 #include "fbp_overlap_fast.cuh"
 #include "fbp_lik_tc.cuh"
+#include "fbp_lik_tcw.cuh"
 
 using namespace fbp;
 
@@ -69,6 +70,9 @@ std::atomic<u32> g_lim_refine{0}, g_lim_pool{0}, g_lim_wait{FBP_DEFAULT_WAIT_POL
 // Tensor-core template group size chosen by a tuner for the calling thread
 // (fbp_set_tc_group_size; 0: the planner's cost model).
 thread_local u32 t_tc_group_size = 0;
+// Layout of the tensor-core likelihood for the calling thread
+// (fbp_set_tc_layout): FBP_TC_LAYOUT_AUTO, _SAMPLES or _WIDE.
+thread_local int t_tc_layout = FBP_TC_LAYOUT_AUTO;
 
 int sm_count() {
     // initialised once, thread-safely (calls may come from several host threads)
@@ -164,6 +168,18 @@ struct Workspace {
     signed char *kx_s;
     u32 *tc_ref_t, *tc_ref_s, *tc_seg_s0, *tc_seg_base, *tc_seg_cnt;
     u32 tc_seg_cap;
+    // wide tiles (fbp_lik_tcw.cuh): groups of 16 templates, window streams
+    bool tcw = false;                // this chunk's likelihood passes use k_lik_tcw
+    u32 tcw_ns = 0;                  // ring stages
+    std::vector<TcGroup> tcwg;       // wide groups (tb_off: offset of its A tiles, 4 KB units)
+    float *vwmax;                    // [W + 2] bound on |v| per window (all channels)
+    u8 *ws_brk;                      // [window bytes] run starts of the pass's list
+    u32 *ws_runs, *ws_pos, *ws_first;
+    unsigned char *Aw;               // packed A tiles of every wide group
+    u32 *tgrp_w;                     // [K] wide group of each template
+    u32 *tcw_gdesc;                  // [group][3]: t0, clo, Cg (device)
+    TcwArgs *tcw_args;               // [group] (device)
+    size_t tcw_smem;
     u32 n;                           // samples of the chunk
     size_t bytes;
 };
@@ -238,6 +254,41 @@ bool plan_tc_groups(const std::vector<u32> &tsup, const std::vector<u32> &tperm,
         }
     }
     return best < 1e300;
+}
+
+// Wide-tile groups (fbp_lik_tcw.cuh): templates in support order (tperm)
+// cut into groups of 16 (M = 16 templates x 8 sample shifts); a group's
+// channels are the union of its templates' supports.  Returns the ring
+// stages that fit shared memory, 0 when the wide layout does not apply.
+u32 plan_tcw_groups(const std::vector<u32> &tsup, const std::vector<u32> &tperm, u32 K, u32 C, u32 L,
+                    std::vector<TcGroup> &out) {
+    out.clear();
+    if (L < kWMinL || L > 1024) return 0;
+    u32 ns = 0;
+    for (u32 s = kWMaxStages; s >= 2; s--)
+        if (tcw_smem_layout(L, s).total <= 227 * 1024) { ns = s; break; }
+    if (ns == 0) return 0;
+    size_t off = 0;
+    for (u32 t0 = 0; t0 < K; t0 += 16) {
+        TcGroup g{};
+        g.t0 = t0;
+        g.nt = std::min(16u, K - t0);
+        u32 lo = C, hi = 0;
+        for (u32 j = t0; j < t0 + g.nt; j++) {
+            const u32 t = tperm[j];
+            if (tsup[2 * t + 1] > tsup[2 * t]) {
+                lo = std::min(lo, tsup[2 * t]);
+                hi = std::max(hi, tsup[2 * t + 1]);
+            }
+        }
+        if (hi <= lo) { lo = 0; hi = 1; }               // all-zero templates: zero products
+        g.clo = lo;
+        g.Cg = hi - lo;
+        g.tb_off = off;
+        off += (size_t)g.Cg * tcw_nkc(L);
+        out.push_back(g);
+    }
+    return ns;
 }
 
 Workspace layout(char *base, u32 n, u32 K, u32 L, u32 nmax, bool want_fast, u32 C = 0, bool want_tc = false) {
@@ -344,6 +395,17 @@ Workspace layout(char *base, u32 n, u32 K, u32 L, u32 nmax, bool want_fast, u32 
         w.tgrp = (u32 *)take((size_t)K * 4);
         w.tc_args0 = (TcArgs *)take((size_t)w.tc_gmax * sizeof(TcArgs));
         w.tc_args1 = (TcArgs *)take((size_t)w.tc_gmax * sizeof(TcArgs));
+        // wide tiles: per-window |v| bound, the pass's stream, A tiles of
+        // every group of 16 templates (at most all C channels each)
+        w.vwmax = (float *)take(((size_t)W + 2) * 4);
+        w.ws_brk = (u8 *)take(window_bytes_u8(W));
+        w.ws_runs = (u32 *)take(Wp * 4);
+        w.ws_pos = (u32 *)take(Wp * 4);
+        w.ws_first = (u32 *)take(((size_t)W * (2 * (size_t)L) / kWPos + 4) * 4);
+        w.Aw = (unsigned char *)take((size_t)w.tc_gmax * C * tcw_nkc(L) * kWATile);
+        w.tgrp_w = (u32 *)take((size_t)K * 4);
+        w.tcw_gdesc = (u32 *)take((size_t)w.tc_gmax * 12);
+        w.tcw_args = (TcwArgs *)take((size_t)w.tc_gmax * sizeof(TcwArgs));
     }
     w.n = n;
     w.bytes = off;
@@ -402,7 +464,7 @@ int launch_argmax(u32 n, u32 L, u32 K, const u32 *win, const u32 *n_win_dev, u32
 int launch_overlap(const float *v, u32 n, u32 C, const float *T, u32 K, u32 L, const u32 *cand,
                    const u32 *n_cand_dev, u32 max_cand, const fbp_window_state &s, float *Lk,
                    u32 nmax, const float *thr, u64 *items_evaluated, cudaStream_t st,
-                   const LazyLk &z = LazyLk{}) {
+                   const LazyLk &z = LazyLk{}, const u32 *tsup = nullptr) {
     const size_t smem = (size_t)2 * C * L * sizeof(float);
     if (smem > 227 * 1024)
         return fail(FBP_ERR_BAD_ARG, "overlap recheck: C*L = %u too large for shared memory", C * L);
@@ -412,7 +474,7 @@ int launch_overlap(const float *v, u32 n, u32 C, const float *T, u32 K, u32 L, c
     const int grid = grid_for((u64)max_cand * kOvThreads, kOvThreads, 4);
     k_overlap_exact<<<grid, kOvThreads, smem, st>>>(v, n, C, T, K, L, cand, n_cand_dev, s.best_idx,
                                                     s.best_lab, s.best_ll, s.ov_idx, s.ov_lab,
-                                                    s.overlap_recheck, Lk, nmax, thr, items_evaluated, z);
+                                                    s.overlap_recheck, Lk, nmax, thr, items_evaluated, z, tsup);
     FBP_LAUNCH_CHECK();
     return FBP_OK;
 }
@@ -462,7 +524,7 @@ LazyLk lazy_ctx(const Workspace &w, const float *v, const float *T, const float 
     z.v = v; z.T = T; z.C = C; z.L = L;
     z.kappa_b = tc_kappa(w.tc_nz, L, ceil_div(w.tc_nz, 8));
     z.kappa_s = tc_kappa_s(w.tc_nz, L);
-    z.tgrp = w.tgrp; z.gstride = w.n; z.tsup = w.tsup;
+    z.tgrp = w.tcw ? w.tgrp_w : w.tgrp; z.gstride = w.n; z.tsup = w.tsup;
     z.refined = &w.cnt->lazy_ref;
     z.wlb = w.wlb; z.bm = w.bm_s;
     z.tag = 2u + (pass & 1u);
@@ -576,7 +638,7 @@ int ov_fast_pass(const Workspace &w, const OvArgs &A, Counters *cnt, cudaStream_
     FBP_LAUNCH_CHECK();
     fbp_window_state s{A.best_idx, A.best_lab, A.best_ll, A.ov_idx, A.ov_lab, nullptr, A.ovr};
     rc = launch_overlap(A.v, A.n, A.C, A.T, A.K, A.L, w.fb_list, &cnt->fb_count, slots, s, A.Lk, A.nmax, A.thr,
-                        A.items_evaluated, st, A.lazy);
+                        A.items_evaluated, st, A.lazy, w.tsup);
     *launches = 10;
     return rc;
 }
@@ -610,15 +672,54 @@ __global__ void k_tc_gate(Counters *cnt, u32 cap, u32 seg_cap) {
     cnt->tc_overflow = ((u32)(rs >> 32) > cap || (u32)rs > seg_cap) ? 1u : 0u;
 }
 
-int tc_chunk_setup(const Workspace &w, const float *T, u32 K, u32 C, u32 L, cudaStream_t st) {
+int tc_chunk_setup(const Workspace &w, const float *v, u32 n, const float *T, u32 K, u32 C, u32 L,
+                   cudaStream_t st) {
     k_tnorm<<<grid_for(K, 64), 64, 0, st>>>(T, K, C * L, w.tc_tnorm, w.tc_tabs, w.tc_texp);
     for (const TcGroup &g : w.tcg) {
         const u64 total = (u64)L * g.Cg2 * g.Np;
         k_tc_pack_templates<<<grid_for(total, 256), 256, 0, st>>>(T, g.nt, C, g.clo, g.Cg, L, g.Cg2, g.Np,
                                                                    w.tc_texp, w.tperm + g.t0, w.Tb + g.tb_off);
     }
+    if (w.tcw) {
+        const u32 nkc = tcw_nkc(L);
+        for (const TcGroup &g : w.tcwg) {
+            const u64 total = (u64)g.Cg * nkc * (kWATile / 2);
+            k_tcw_pack<<<grid_for(total, 256), 256, 0, st>>>(T, C, L, nkc, w.tperm + g.t0, g.nt, g.clo, g.Cg,
+                                                              w.tc_texp, (u16 *)(w.Aw + g.tb_off * kWATile));
+        }
+        const u32 W = ceil_div(n, L);
+        k_window_vmax<<<grid_for((u64)(W + 2) * 32, 256, 8), 256, 0, st>>>(v, n, C, L, W, w.vwmax);
+    }
     FBP_LAUNCH_CHECK();
     return FBP_OK;
+}
+
+// Launch arguments of one wide-tile group.
+TcwArgs tcw_group_args(const Workspace &w, u32 gi, const float *v, u32 n, u32 C, u32 K, u32 L, const float *tss,
+                       float *Lk, Counters *cnt) {
+    const TcGroup &g = w.tcwg[gi];
+    TcwArgs A{};
+    A.n = n; A.Cg = g.Cg; A.nt = g.nt; A.L = L;
+    A.nkc = tcw_nkc(L); A.ns = w.tcw_ns; A.px = tcw_px(L); A.Kall = K; A.W = ceil_div(n, L);
+    A.trow = w.tperm + g.t0;
+    A.kappa_b = tc_kappa(w.tc_nz, L, ceil_div(w.tc_nz, 8));
+    A.kappa_s = tc_kappa_s(w.tc_nz, L);
+    A.v = v + (size_t)g.clo * n;
+    A.tss = tss; A.tnorm = w.tc_tnorm; A.tabs = w.tc_tabs; A.texp = w.tc_texp;
+    A.Aw = w.Aw + g.tb_off * kWATile;
+    A.vwmax = w.vwmax;
+    A.win = w.win; A.n_win = &cnt->n_win;
+    A.pos = w.ws_pos; A.first = w.ws_first; A.n_stiles = &cnt->n_stiles;
+    A.Lk = Lk; A.apx = w.apx;
+    A.wn_s = w.wn_s + (size_t)gi * n; A.wa_s = w.wa_s + (size_t)gi * n; A.kx_s = w.kx_s + (size_t)gi * n;
+    A.bm_s = w.bm_s; A.wlb = w.wlb; A.umax = w.umax; A.wpos = w.wpos;
+    A.ref_t = w.tc_ref_t; A.ref_s = w.tc_ref_s; A.refseg = &cnt->tc_refseg; A.ref_cap = w.tc_ref_cap;
+    A.seg_s0 = w.tc_seg_s0; A.seg_base = w.tc_seg_base; A.seg_cnt = w.tc_seg_cnt; A.seg_grp = w.tc_seg_grp;
+    A.grp = gi;
+    A.seg_overflow = &cnt->tc_overflow; A.seg_cap = w.tc_seg_cap;
+    A.err = &cnt->tc_err;
+    A.wait_polls = g_lim_wait.load();
+    return A;
 }
 
 // Launch arguments of one template group of the tensor-core kernel.
@@ -683,7 +784,25 @@ int tc_likelihood_pass(const Workspace &w, const float *v, u32 n, u32 C, const f
     (void)max_windows;
     FBP_CUDA(cudaMemsetAsync(&cnt->tc_refseg, 0, 8, st));
     FBP_CUDA(cudaMemsetAsync(&cnt->tc_overflow, 0, 4, st));   // set by the tiles when the list overflows
-    (void)v; (void)n; (void)C; (void)T; (void)K; (void)L; (void)tss; (void)win; (void)n_win; (void)Lk;
+    (void)v; (void)C; (void)T; (void)K; (void)tss; (void)Lk;
+    if (w.tcw) {
+        // the pass's window stream: run starts, their list, stream positions
+        const u32 W = ceil_div(n, L);
+        const size_t wbb = window_bytes_u8(W);
+        k_ws_breaks<<<grid_for(wbb, 256), 256, 0, st>>>(win, n_win, (u32)wbb, w.ws_brk);
+        FBP_LAUNCH_CHECK();
+        if (int rc = compact(w.ws_brk, W, w.ws_runs, &cnt->n_runs, w.tile_counts, st)) return rc;
+        k_ws_pos<<<grid_for(W, 256), 256, 0, st>>>(n_win, w.ws_brk, w.ws_runs, &cnt->n_runs, L, w.ws_pos,
+                                                    w.ws_first, &cnt->n_stiles);
+        FBP_LAUNCH_CHECK();
+        FBP_ALLOW_SMEM(k_lik_tcw);
+        const u32 G = (u32)w.tcwg.size();
+        k_lik_tcw<<<std::max<u32>(sm_count(), G), kTcThreads, w.tcw_smem, st>>>(w.tcw_args, G);
+        FBP_LAUNCH_CHECK();
+        *launches = 6;
+        return FBP_OK;
+    }
+    (void)win; (void)n_win;
     FBP_ALLOW_SMEM(k_lik_tc<0>);
     const u32 G = (u32)w.tcg.size();
     k_lik_tc<0><<<std::max<u32>(sm_count(), G), kTcThreads, w.tc_smem, st>>>(w.tc_args0, G);
@@ -706,7 +825,7 @@ int tc_refine_pass(const Workspace &w, const float *v, u32 n, u32 C, const float
     const double gamma = 1.01 * (nr * u / (1.0 - nr * u)) + 4.0 * nr * 1.1102230246251565e-16;
     k_tc_refine<<<sm_count() * 8, kRefThreads, rsmem, st>>>(
         v, n, C, w.tc_cmax, T, K, L, tss, w.tc_ref_t, w.tc_ref_s, w.tc_seg_s0, w.tc_seg_base, w.tc_seg_cnt,
-        w.tc_seg_grp, w.tc_gdesc, w.tperm, reinterpret_cast<const u32 *>(&cnt->tc_refseg), w.tc_seg_cap, Lk,
+        w.tc_seg_grp, w.tcw ? w.tcw_gdesc : w.tc_gdesc, w.tperm, reinterpret_cast<const u32 *>(&cnt->tc_refseg), w.tc_seg_cap, Lk,
         lazy_ctx(w, v, T, tss, C, L, 0), gamma, &cnt->tc_seq, w.wpos, &cnt->tc_overflow, w.tc_ref_cap);
     k_tc_gate<<<1, 1, 0, st>>>(cnt, w.tc_ref_cap, w.tc_seg_cap);
     FBP_LAUNCH_CHECK();
@@ -868,6 +987,25 @@ int prepare_chunk(Workspace &w, float *voltage, u32 n, u32 C, const float *templ
                 }
                 FBP_CUDA(cudaMemcpyAsync(w.tc_gdesc, gdesc.data(), gdesc.size() * 4, cudaMemcpyHostToDevice, st));
                 FBP_CUDA(cudaMemcpyAsync(w.tgrp, tgrp.data(), tgrp.size() * 4, cudaMemcpyHostToDevice, st));
+                // the likelihood passes' layout: wide tiles where they apply
+                w.tcw = false;
+                if (t_tc_layout != FBP_TC_LAYOUT_SAMPLES) {
+                    w.tcw_ns = plan_tcw_groups(tsup, tperm, K, C, L, w.tcwg);
+                    w.tcw = w.tcw_ns > 0;
+                }
+                std::vector<u32> gdesc_w(3 * w.tcwg.size()), tgrp_w(K);
+                if (w.tcw) {
+                    for (u32 gi = 0; gi < (u32)w.tcwg.size(); gi++) {
+                        const TcGroup &g = w.tcwg[gi];
+                        w.tc_cmax = std::max(w.tc_cmax, g.Cg);
+                        gdesc_w[3 * gi] = g.t0; gdesc_w[3 * gi + 1] = g.clo; gdesc_w[3 * gi + 2] = g.Cg;
+                        for (u32 j = g.t0; j < g.t0 + g.nt; j++) tgrp_w[tperm[j]] = gi;
+                    }
+                    FBP_CUDA(cudaMemcpyAsync(w.tcw_gdesc, gdesc_w.data(), gdesc_w.size() * 4,
+                                             cudaMemcpyHostToDevice, st));
+                    FBP_CUDA(cudaMemcpyAsync(w.tgrp_w, tgrp_w.data(), tgrp_w.size() * 4, cudaMemcpyHostToDevice,
+                                             st));
+                }
                 FBP_CUDA(cudaStreamSynchronize(st));   // the host vectors go out of scope
             }
         }
@@ -885,7 +1023,7 @@ int prepare_chunk(Workspace &w, float *voltage, u32 n, u32 C, const float *templ
         timer.begin(FBP_STAGE_LIKELIHOOD);
         FBP_CUDA(cudaMemsetAsync(w.apx, 0, (size_t)K * n, st));
         FBP_CUDA(cudaMemsetAsync(w.bm_s, 0, (size_t)n * 4, st));
-        int rc0 = tc_chunk_setup(w, templates, K, C, L, st);
+        int rc0 = tc_chunk_setup(w, voltage, n, templates, K, C, L, st);
         if (rc0) return rc0;
         // launch arguments of every template group (constant for the chunk)
         {
@@ -911,8 +1049,19 @@ int prepare_chunk(Workspace &w, float *voltage, u32 n, u32 C, const float *templ
             }
             FBP_CUDA(cudaMemcpyAsync(w.tc_args0, a0.data(), G * sizeof(TcArgs), cudaMemcpyHostToDevice, st));
             FBP_CUDA(cudaMemcpyAsync(w.tc_args1, a1.data(), G * sizeof(TcArgs), cudaMemcpyHostToDevice, st));
+            std::vector<TcwArgs> aw(w.tcwg.size());
+            if (w.tcw) {
+                for (u32 gi = 0; gi < (u32)aw.size(); gi++) {
+                    aw[gi] = tcw_group_args(w, gi, voltage, n, C, K, L, neg_half_ss, w.Lk, w.cnt);
+                    aw[gi].dbgE = dbg_bound;
+                }
+                FBP_CUDA(cudaMemcpyAsync(w.tcw_args, aw.data(), aw.size() * sizeof(TcwArgs), cudaMemcpyHostToDevice,
+                                         st));
+                w.tcw_smem = tcw_smem_layout(L, w.tcw_ns).total;
+            }
             FBP_CUDA(cudaStreamSynchronize(st));   // the host vectors go out of scope
         }
+        S.tc_layout = w.tcw ? FBP_TC_LAYOUT_WIDE : FBP_TC_LAYOUT_SAMPLES;
         S.launches[FBP_STAGE_LIKELIHOOD] += 2;
         timer.end(FBP_STAGE_LIKELIHOOD);
     }
@@ -1051,7 +1200,7 @@ int fbp_pursuit_chunk(float *voltage, uint32_t n, uint32_t C, const float *templ
                 launched[FBP_STAGE_OVERLAP] += nl;
             } else {
                 if ((rc2 = launch_overlap(voltage, n, C, templates, K, L, w.cand, &w.cnt->n_cand, W, s, w.Lk,
-                                          nmax, thresholds, &w.cnt->ov_items, q, lz)))
+                                          nmax, thresholds, &w.cnt->ov_items, q, lz, w.tsup)))
                     return rc2;
                 launched[FBP_STAGE_OVERLAP] += 1;
             }
@@ -1094,7 +1243,8 @@ int fbp_pursuit_chunk(float *voltage, uint32_t n, uint32_t C, const float *templ
             launched[FBP_STAGE_RESIDUAL] += 1;
         }
         k_residual<<<grid_for((u64)W * 256, 256, 16), 256, 0, q>>>(voltage, n, C, templates, K, L, w.spk_idx,
-                                                                    w.spk_lab, &w.cnt->n_spk, 0, R, w.tsup);
+                                                                    w.spk_lab, &w.cnt->n_spk, 0, R, w.tsup,
+                                                                    w.tcw ? w.vwmax : nullptr);
         FBP_LAUNCH_CHECK();
         launched[FBP_STAGE_RESIDUAL] += 1;
         timer.end(FBP_STAGE_RESIDUAL);
@@ -1114,7 +1264,7 @@ int fbp_pursuit_chunk(float *voltage, uint32_t n, uint32_t C, const float *templ
                   (uint64_t)do_overlap_recheck, (uint64_t)precision, (uint64_t)overlap_method,
                   (uint64_t)(uintptr_t)workspace, (uint64_t)workspace_bytes, (uint64_t)(uintptr_t)spike_idx,
                   (uint64_t)(uintptr_t)spike_lab, spike_cap, (uint64_t)w.masked_tables, (uint64_t)w.tc,
-                  lim_refine, lim_pool, lim_wait};
+                  lim_refine, lim_pool, lim_wait, (uint64_t)w.tcw, w.tcw_ns};
         for (const TcGroup &g : w.tcg)               // the group plan follows the template supports
             if (w.tc) pg.key.insert(pg.key.end(), {g.t0, g.nt, g.clo, g.Cg, g.nbuf});
         std::lock_guard<std::mutex> lk(g_graph_mu);
@@ -1219,6 +1369,14 @@ int fbp_set_tc_group_size(uint32_t templates_per_group) {
         return fail(FBP_ERR_BAD_ARG, "fbp_set_tc_group_size: %u is not 0 or a multiple of 16 up to 256",
                     templates_per_group);
     t_tc_group_size = templates_per_group;
+    return FBP_OK;
+}
+
+int fbp_set_tc_layout(int layout) {
+    g_last_error.clear();
+    if (layout != FBP_TC_LAYOUT_AUTO && layout != FBP_TC_LAYOUT_SAMPLES && layout != FBP_TC_LAYOUT_WIDE)
+        return fail(FBP_ERR_BAD_ARG, "fbp_set_tc_layout: unknown layout %d", layout);
+    t_tc_layout = layout;
     return FBP_OK;
 }
 

@@ -40,7 +40,9 @@ struct Counters {
     u64 scan_next;    // work counter of the overlap scan
     u64 tc_refseg;    // tensor-core refinement list: entries queued (high half), tile segments (low half)
     u64 tc_seq;       // refinement entries whose sign needed the reference's own sum (whole chunk)
-    u32 pad[8];
+    u32 n_runs;       // runs of consecutive windows in the pass's list (wide tensor-core tiles)
+    u32 n_stiles;     // tiles of the pass's window stream (wide tensor-core tiles)
+    u32 pad[6];
 };
 static_assert(sizeof(Counters) == 128, "Counters is one 128-byte line");
 

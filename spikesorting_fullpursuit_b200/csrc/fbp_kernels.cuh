@@ -569,14 +569,21 @@ k_window_argmax(u32 n, u32 L, u32 K, const u32 *__restrict__ win,
 // the window's current best, which is what the parse kernel's strict-greater
 // scan over single-item groups returns.
 // ---------------------------------------------------------------------------
+// Channels outside both templates' non-zero ranges [lo1, hi1), [lo2, hi2)
+// add only exact zeros to the reference's sums (ss stays 0, so the -0.5 ss
+// step is skipped there too) and are left out; the others keep the
+// reference's channel order.
 __device__ __forceinline__ float overlap_pair_exact(const float *__restrict__ vwin,   // [C][L] at bidx
                                                     const float *__restrict__ tk0,    // [C][L]
                                                     const float *__restrict__ tt,     // [C][L]
-                                                    u32 C, u32 L, int fa, int sa) {
+                                                    u32 C, u32 L, int fa, int sa, u32 lo1 = 0, u32 hi1 = ~0u,
+                                                    u32 lo2 = 0, u32 hi2 = ~0u) {
     float cml = 0.0f;
     const u32 ffj = fa < 0 ? (u32)(-fa) : 0u;
     const u32 sfj = sa < 0 ? (u32)(-sa) : 0u;
-    for (u32 c = 0; c < C; c++) {
+    const u32 cend = min(C, max(hi1, hi2));
+    for (u32 c = min(lo1, lo2); c < cend; c++) {
+        if ((c < lo1 || c >= hi1) && (c < lo2 || c >= hi2)) continue;
         const float *f = tk0 + (size_t)c * L;
         const float *s = tt + (size_t)c * L;
         const float *vv = vwin + (size_t)c * L;
@@ -639,7 +646,7 @@ k_overlap_exact(const float *__restrict__ v, u32 n, u32 C, const float *__restri
                 u32 *__restrict__ best_idx, u32 *__restrict__ best_lab, float *__restrict__ best_ll,
                 u32 *__restrict__ ov_idx, u32 *__restrict__ ov_lab, u8 *__restrict__ ovr,
                 const float *__restrict__ Lk, u32 nmax, const float *__restrict__ thr,
-                u64 *__restrict__ items_evaluated, LazyLk z) {
+                u64 *__restrict__ items_evaluated, LazyLk z, const u32 *__restrict__ tsup) {
     extern __shared__ float sm[];          // vwin [C*L], tk0 [C*L]
     __shared__ float red_v[kOvThreads / 32];
     __shared__ u64 red_i[kOvThreads / 32];
@@ -650,6 +657,7 @@ k_overlap_exact(const float *__restrict__ v, u32 n, u32 C, const float *__restri
     for (u32 g = blockIdx.x; g < n_cand; g += gridDim.x) {
         const u32 id = cand[g];
         const u32 lab = best_lab[id], bidx = best_idx[id];
+        const u32 lo_lab = tsup && lab < K ? tsup[2 * lab] : 0u, hi_lab = tsup && lab < K ? tsup[2 * lab + 1] : C;
         const float start_ll = best_ll[id];
         const float bll = Lk[(size_t)lab * n + bidx];
         const bool skip_all = (bll < thr[lab]) || (bidx >= n - L);   // .cl:518-527
@@ -679,7 +687,8 @@ k_overlap_exact(const float *__restrict__ v, u32 n, u32 C, const float *__restri
                 const float ls = Lk[(size_t)t * n + ashift];
                 if (lf <= 0.0f && ls <= 0.0f) continue;                       // .cl:572-576
                 const float ll = overlap_pair_exact(vwin, tk0, T + (size_t)t * C * L, C, L,
-                                                    (int)bidx - (int)afix, (int)bidx - (int)ashift);
+                                                    (int)bidx - (int)afix, (int)bidx - (int)ashift, lo_lab, hi_lab,
+                                                    tsup ? tsup[2 * t] : 0u, tsup ? tsup[2 * t + 1] : C);
                 evaluated++;
                 if (ll > bv) { bv = ll; bi = it; }
             }
@@ -886,7 +895,7 @@ constexpr u32 kResNb = 128;
 __global__ void __launch_bounds__(256)
 k_residual(float *__restrict__ v, u32 n, u32 C, const float *__restrict__ T, u32 K, u32 L,
            const u32 *__restrict__ idx, const u32 *__restrict__ lab, const u32 *__restrict__ n_spk_dev,
-           u32 n_spk_host, u32 R, const u32 *__restrict__ tsup) {
+           u32 n_spk_host, u32 R, const u32 *__restrict__ tsup, float *__restrict__ vwmax = nullptr) {
     __shared__ u32 nb_p[kResNb], nb_lab[kResNb], nb_lo[kResNb], nb_hi[kResNb];
     const u32 m = n_spk_dev ? *n_spk_dev : n_spk_host;
     const u32 warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nw = blockDim.x >> 5;
@@ -924,6 +933,7 @@ k_residual(float *__restrict__ v, u32 n, u32 C, const float *__restrict__ T, u32
         };
         const u32 p = idx[s];
         const u32 clo = tsup ? tsup[2 * ls] : 0u, chi = tsup ? tsup[2 * ls + 1] : C;
+        float mx = 0.0f;                                                 // largest |value| written
         for (u32 c = clo + warp; c < chi; c += nw) {
             for (u32 i = lane; i < L; i += 32) {
                 const u32 x = p + i;
@@ -940,6 +950,16 @@ k_residual(float *__restrict__ v, u32 n, u32 C, const float *__restrict__ T, u32
                     }
                 }
                 v[(size_t)c * n + x] = val;
+                mx = fmaxf(mx, fabsf(val));
+            }
+        }
+        // the per-window bound on |v| of the wide tensor-core tiles stays an
+        // upper bound (the clip covers windows p / L and (p + L - 1) / L)
+        if (vwmax) {
+            mx = warp_max_float(mx);
+            if (lane == 0 && mx > 0.0f) {
+                atomicMax(reinterpret_cast<int *>(vwmax) + p / L, __float_as_int(mx));
+                atomicMax(reinterpret_cast<int *>(vwmax) + (p + L - 1) / L, __float_as_int(mx));
             }
         }
     }

@@ -14,6 +14,7 @@ import numpy as np
 from .chunking import chunk_onsets, num_indices_per_chunk
 
 _PRECISIONS = {"fp32": 0, "bf16": 1, "bf16_refine": 1}
+_TC_LAYOUTS = {"auto": 0, "samples": 1, "wide": 2}   # FBP_TC_LAYOUT_* of include/fbp_b200.h
 
 
 def time_window_to_samples(time_window, sampling_rate):
@@ -51,7 +52,7 @@ def _to_device_f32(torch, host_chunk, dev, stream):
 def binary_pursuit(voltage, v_dtype, sort_info, separability_metrics, n_max_shift_inds=None,
                    kernels_path=None, max_gpu_memory=None, *, precision="fp32",
                    chunk_samples=None, device=None, max_passes=1000000, stats=None, profile=False,
-                   overlap="fast", tune=False):
+                   overlap="fast", tune=False, tc_layout=None):
     """Full Binary Pursuit over `voltage` ([channels, samples], any real dtype).
 
     Returns (event_indices int64, neuron_labels int64, binary_pursuit_spike_bool
@@ -73,10 +74,17 @@ def binary_pursuit(voltage, v_dtype, sort_info, separability_metrics, n_max_shif
       stats          a list; one dict per chunk is appended (passes, spikes,
                      per-stage launches, work and, with profile=True, CUDA-event
                      milliseconds).
-      tune           precision "bf16": take the tensor-core template group size
-                     from the tuner's cache for this shape bucket, timing the
-                     candidates on a sample of the recording the first time
+      tune           precision "bf16": take the tensor-core plan (layout and
+                     template group size) from the tuner's cache for this
+                     shape bucket, timing the candidates on a sample of the
+                     recording the first time
                      (spikesorting_fullpursuit_b200.autotune); same spikes.
+      tc_layout      precision "bf16", for this call: "auto" (wide tiles where
+                     they apply), "wide" (2048-position tiles of the pass's
+                     window stream, 16 templates x 8 shifts per MMA) or
+                     "samples" (128-sample tiles, template groups per MMA);
+                     None (default): the calling thread's setting
+                     (autotune.apply); same spikes.
     """
     # The CUDA runtime is initialised inside the call, never at import time,
     # so callers may fork worker processes first (reference :166-170).
@@ -91,6 +99,8 @@ def binary_pursuit(voltage, v_dtype, sort_info, separability_metrics, n_max_shif
     if overlap not in ("fast", "exact"):
         raise ValueError("overlap must be 'fast' or 'exact'")
     ov_method = _lib.OVERLAP_FAST if overlap == "fast" else _lib.OVERLAP_EXACT
+    if tc_layout is not None and tc_layout not in _TC_LAYOUTS:
+        raise ValueError("tc_layout must be one of %s" % sorted(_TC_LAYOUTS))
 
     n_chans = int(voltage.shape[0])
     n_samples = int(voltage.shape[1])
@@ -129,8 +139,10 @@ def binary_pursuit(voltage, v_dtype, sort_info, separability_metrics, n_max_shif
     if tune and prec == _PRECISIONS["bf16"] and n_samples > 0:
         from .. import autotune
         first = np.ascontiguousarray(voltage[:, :min(n_samples, chunk_samples)], dtype=np.float32)
-        gs, _, _ = autotune.tune(first, templates_vector.reshape(K, -1), template_sum_squared, L)
-        autotune.apply(gs)
+        plan, _, _ = autotune.tune(first, templates_vector.reshape(K, -1), template_sum_squared, L)
+        autotune.apply(plan)
+    elif tc_layout is not None:
+        _lib.check(lib.fbp_set_tc_layout(_TC_LAYOUTS[tc_layout]))
 
     stream = torch.cuda.current_stream(dev)
     sp = _lib.stream_ptr(stream)
@@ -196,7 +208,8 @@ def binary_pursuit(voltage, v_dtype, sort_info, separability_metrics, n_max_shif
     else:
         event_indices, neuron_labels, binary_pursuit_spike_bool, adjusted_clips = [], [], [], []
 
-    if tune:
+    if tune or tc_layout is not None:           # back to the library's own choice
         _lib.check(lib.fbp_set_tc_group_size(0))
+        _lib.check(lib.fbp_set_tc_layout(_lib.TC_LAYOUT_AUTO))
     add_n_spikes(separability_metrics, neuron_labels)
     return event_indices, neuron_labels, binary_pursuit_spike_bool, adjusted_clips

@@ -66,14 +66,19 @@ def P(t):
 
 # ----------------------------------------------------------------- whole pursuit
 
-@pytest.mark.parametrize("precision", ["fp32", "bf16"])
+# precision, and for the tensor cores the likelihood layout
+MODES = {"fp32": ("fp32", None), "bf16-samples": ("bf16", "samples"), "bf16-wide": ("bf16", "wide")}
+
+
+@pytest.mark.parametrize("mode", sorted(MODES))
 @pytest.mark.parametrize("path", golden_paths(), ids=lambda p: p.split("/")[-1][:-4])
-def test_binary_pursuit_matches_reference_golden(lib, path, precision):
+def test_binary_pursuit_matches_reference_golden(lib, path, mode):
+    precision, layout = MODES[mode]
     c = GoldenCase(path)
     m = c.metrics()
     out = bpp.binary_pursuit(c.voltage, c.voltage.dtype, c.sort_info, m,
                              n_max_shift_inds=c.n_max_shift_inds, chunk_samples=c.chunk_samples,
-                             precision=precision)
+                             precision=precision, tc_layout=layout)
     assert_same_outputs(out, c.expected, c.empty)
     assert np.array_equal(m["n_spikes"], c.n_spikes)
 
@@ -89,9 +94,10 @@ LIVE = [
 ]
 
 
-@pytest.mark.parametrize("precision", ["fp32", "bf16"])
+@pytest.mark.parametrize("mode", sorted(MODES))
 @pytest.mark.parametrize("cfg", LIVE, ids=lambda c: "%s-%d" % (c["kind"], c["seed"]))
-def test_binary_pursuit_matches_oracle(lib, cfg, precision):
+def test_binary_pursuit_matches_oracle(lib, cfg, mode):
+    precision, layout = MODES[mode]
     kw = dict(duration_s=cfg["dur"], seed=cfg["seed"], L=cfg["L"])
     if "K" in cfg:
         kw["n_templates"] = cfg["K"]
@@ -107,12 +113,13 @@ def test_binary_pursuit_matches_oracle(lib, cfg, precision):
     stats = []
     got = bpp.binary_pursuit(rec.voltage, rec.voltage.dtype, si, rec.fresh_metrics(),
                              n_max_shift_inds=cfg["nmax"], chunk_samples=chunk, precision=precision,
-                             stats=stats)
+                             stats=stats, tc_layout=layout)
     assert_same_outputs(got, tuple(np.asarray(x) for x in exp), isinstance(exp[0], list))
     if precision == "bf16":
-        # the tensor-core path ran (the 64-channel case as template groups
-        # on their channel ranges)
+        # the tensor-core path ran, in the layout asked for (the 64-channel
+        # case as template groups on their channel ranges)
         assert stats[0]["launches"]["lik_refine"] >= 3 * stats[0]["passes"]
+        assert all(s["tc_layout"] == layout for s in stats)
 
 
 @pytest.mark.parametrize("overlap", ["fast", "exact"])

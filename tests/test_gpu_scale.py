@@ -93,7 +93,7 @@ def test_linear16_full_overlap_range_matches_oracle(lib, precision):
 
 # ------------------------------------------------------------ long recordings, GPU only
 
-@pytest.mark.parametrize("kind,duration_s,nmax", [("linear16", 10.0, 100), ("hd384", 2.0, 60)])
+@pytest.mark.parametrize("kind,duration_s,nmax", [("linear16", 10.0, 100), ("hd384", 1.0, 60)])
 def test_tensor_core_fast_equals_fp32_exhaustive(lib, kind, duration_s, nmax):
     """bf16 + fast overlap against fp32 + the reference's exhaustive overlap
     recheck (the oracle-pinned plain path), every output array equal."""
@@ -114,8 +114,8 @@ def test_tensor_core_fast_equals_fp32_exhaustive(lib, kind, duration_s, nmax):
 
 # ------------------------------------------------------------ overflow paths
 
-@pytest.mark.parametrize("kind", ["linear16", "hd384"])
-def test_overflowing_refinement_list_and_pool_match_oracle(lib, kind):
+@pytest.mark.parametrize("kind,layout", [("linear16", "wide"), ("linear16", "samples"), ("hd384", "wide")])
+def test_overflowing_refinement_list_and_pool_match_oracle(lib, kind, layout):
     """A refinement list of 64 entries and a contender pool of 8 overflow on
     almost every pass: the FP32 kernel redoes the likelihood of the pass and
     the candidates go to the exact overlap kernel."""
@@ -128,9 +128,10 @@ def test_overflowing_refinement_list_and_pool_match_oracle(lib, kind):
     _lib.set_test_limits(refine_list_cap=64, contender_pool_cap=8)
     stats = []
     got = bpp.binary_pursuit(rec.voltage, rec.voltage.dtype, si, rec.fresh_metrics(), n_max_shift_inds=nmax,
-                             precision="bf16", overlap="fast", stats=stats)
+                             precision="bf16", overlap="fast", stats=stats, tc_layout=layout)
     _lib.reset_test_limits()
     assert_same_outputs(got, _as_tuple(exp))
+    assert stats[0]["tc_layout"] == layout
     assert stats[0]["lik_exact_passes"] > 0
     assert stats[0]["fallback_candidates"] > 0
 
@@ -159,8 +160,9 @@ def _likelihood_f64(v64, T, tss32, L):
     return out
 
 
+@pytest.mark.parametrize("layout", ["samples", "wide"])
 @pytest.mark.parametrize("case", sorted(BOUND_CASES))
-def test_tensor_core_bound_holds_for_every_entry(lib, case):
+def test_tensor_core_bound_holds_for_every_entry(lib, case, layout):
     fn, kw = BOUND_CASES[case]
     rec = fn(**kw)
     C, n, K, L = rec.n_chans, rec.n_samples, rec.n_templates, rec.n_samples_per_chan
@@ -176,8 +178,13 @@ def test_tensor_core_bound_holds_for_every_entry(lib, case):
     approx_d = torch.zeros((K, n), dtype=torch.float32, device=dev)
     bound_d = torch.zeros((K, n), dtype=torch.float32, device=dev)
     sp = _lib.stream_ptr(torch.cuda.current_stream(dev))
-    _lib.check(lib.fbp_tc_likelihood_bounds(_lib.ptr(v_d), n, C, _lib.ptr(T_d), K, L, _lib.ptr(tss_d),
-                                            _lib.ptr(ws), ws.numel(), _lib.ptr(approx_d), _lib.ptr(bound_d), sp))
+    _lib.check(lib.fbp_set_tc_layout(_lib.TC_LAYOUT_WIDE if layout == "wide" else _lib.TC_LAYOUT_SAMPLES))
+    try:
+        _lib.check(lib.fbp_tc_likelihood_bounds(_lib.ptr(v_d), n, C, _lib.ptr(T_d), K, L, _lib.ptr(tss_d),
+                                                _lib.ptr(ws), ws.numel(), _lib.ptr(approx_d), _lib.ptr(bound_d),
+                                                sp))
+    finally:
+        _lib.check(lib.fbp_set_tc_layout(_lib.TC_LAYOUT_AUTO))
     torch.cuda.synchronize()
     approx, E = approx_d.cpu().numpy(), bound_d.cpu().numpy()
     # the reference's binary32 values (oracle) and float64 values
@@ -195,21 +202,23 @@ def test_tensor_core_bound_holds_for_every_entry(lib, case):
     err64 = np.abs(approx.astype(np.float64) - ref64)
     ref_err64 = np.abs(ref32.astype(np.float64) - ref64)
     scale = np.abs(ref64[live]).max()
-    print("\nlikelihood error %s (C=%d, K=%d, L=%d, %d samples, %d entries): tensor-core vs fp64 max %.3e "
-          "(%.2e of max |L|), reference fp32 vs fp64 max %.3e, max |approx - fp32| / E = %.3f, median E %.3e"
-          % (case, C, K, L, n, int(live.sum()), err64[live].max(), err64[live].max() / scale,
+    print("\nlikelihood error %s, %s layout (C=%d, K=%d, L=%d, %d samples, %d entries): tensor-core vs fp64 "
+          "max %.3e (%.2e of max |L|), reference fp32 vs fp64 max %.3e, max |approx - fp32| / E = %.3f, "
+          "median E %.3e"
+          % (case, layout, C, K, L, n, int(live.sum()), err64[live].max(), err64[live].max() / scale,
              ref_err64[live].max(), float((err32[live] / E[live]).max()), float(np.median(E[live]))))
 
 
 # ------------------------------------------------------------ bounded waits
 
-def test_bounded_wait_gives_up_and_context_stays_usable(lib):
+@pytest.mark.parametrize("layout", ["samples", "wide"])
+def test_bounded_wait_gives_up_and_context_stays_usable(lib, layout):
     rec = synthetic.tetrode(duration_s=0.2, seed=310, L=41)
     si = rec.sort_info()
     _lib.set_test_limits(wait_polls=0)
     with pytest.raises(_lib.PursuitError) as ei:
         bpp.binary_pursuit(rec.voltage, rec.voltage.dtype, si, rec.fresh_metrics(), n_max_shift_inds=40,
-                           precision="bf16")
+                           precision="bf16", tc_layout=layout)
     assert ei.value.code == _lib.FBP_ERR_TIMEOUT
     _lib.reset_test_limits()
     torch.cuda.synchronize()
@@ -221,10 +230,11 @@ def test_bounded_wait_gives_up_and_context_stays_usable(lib):
 
 # ------------------------------------------------------------ tuned group size
 
-def test_tuned_group_size_gives_the_same_spikes(lib, tmp_path, monkeypatch):
-    """The tuner times the candidate template group sizes and caches the
-    fastest per shape bucket; a pursuit that uses it (and one with every
-    group size forced) returns the oracle's spikes."""
+def test_tuned_plan_gives_the_same_spikes(lib, tmp_path, monkeypatch):
+    """The tuner times the candidate plans (wide tiles, 128-sample tiles with
+    each template group size) and caches the fastest per shape bucket; a
+    pursuit that uses it (and one with every plan forced) returns the
+    oracle's spikes."""
     from spikesorting_fullpursuit_b200 import autotune
     monkeypatch.setenv("FBP_TUNE_CACHE", str(tmp_path / "tune.json"))
     rec = linear16_slice(0.1, 311)
@@ -236,13 +246,16 @@ def test_tuned_group_size_gives_the_same_spikes(lib, tmp_path, monkeypatch):
     table = autotune._load()
     assert len(table) == 1
     entry = next(iter(table.values()))
-    assert entry["group_size"] in autotune.candidates_for(rec.n_templates)
-    assert len(entry["ms"]) == len(autotune.candidates_for(rec.n_templates))
-    for gs in (16, 32, 64):
-        autotune.apply(gs)
+    plans = autotune.plans_for(rec.n_templates, rec.n_samples_per_chan)
+    assert entry["plan"] in plans
+    assert sorted(entry["ms"]) == sorted(plans)
+    for plan in plans:
+        autotune.apply(plan)
         try:
+            st = []
             got = bpp.binary_pursuit(rec.voltage, rec.voltage.dtype, si, rec.fresh_metrics(), n_max_shift_inds=100,
-                                     precision="bf16")
+                                     precision="bf16", stats=st)
         finally:
-            autotune.apply(0)
+            autotune.apply(None)
         assert_same_outputs(got, _as_tuple(exp))
+        assert st[0]["tc_layout"] == plan.split(":")[0]

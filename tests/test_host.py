@@ -112,7 +112,9 @@ def test_tuner_bucket_and_cache(tmp_path, monkeypatch):
     assert b == "C384_K304_L64_w16"
     assert autotune.candidates_for(300) == autotune.CANDIDATES
     assert autotune.candidates_for(20) == (16, 32)
-    autotune._store({b: {"group_size": 32, "ms": {"16": 2.0, "32": 1.0}}})
-    gs, bucket, times = autotune.tune(rec.voltage, T, -0.5 * rec.fresh_metrics()["template_SS"],
-                                      rec.n_samples_per_chan)
-    assert (gs, bucket, times) == (32, b, None)
+    assert autotune.plans_for(20, 61) == ("wide", "samples:16", "samples:32")
+    assert autotune.plans_for(20, 8) == ("samples:16", "samples:32")
+    autotune._store({b: {"plan": "samples:32", "ms": {"wide": 2.0, "samples:32": 1.0}}})
+    plan, bucket, times = autotune.tune(rec.voltage, T, -0.5 * rec.fresh_metrics()["template_SS"],
+                                        rec.n_samples_per_chan)
+    assert (plan, bucket, times) == ("samples:32", b, None)
