@@ -50,6 +50,7 @@ constexpr u32 kWTwMax = 136;             // listed windows a tile can touch (L >
 constexpr u32 kWMinL = 16;
 constexpr u32 kWMaxStages = 8;
 constexpr u32 kWATile = 4096;            // one A tile: 128 rows x 16 lags x fp16
+constexpr u32 kWDepth = 3;               // channels of voltage in flight (fp32 staging slots)
 
 __host__ __device__ inline u32 tcw_nkc(u32 L) { return (L + 7 + 15) / 16; }
 __host__ __device__ inline u32 tcw_px(u32 L) { return kWPos + 16 * tcw_nkc(L); }   // staged positions
@@ -84,9 +85,10 @@ struct TcwArgs {
     u32 wait_polls;
 };
 
+static_assert(sizeof(TcwArgs) % 4 == 0, "TcwArgs is copied as 32-bit words");
 struct TcwSmem {
-    size_t ring, stage, a_bytes, spos, wnwa, wrel, tw, cw, tf, ti, psq, pab, tpos, twin, xs, xe, ct, bars, misc,
-        tcnt, total;
+    size_t args, ring, stage, a_bytes, vst, spos, wnwa, wrel, tw, cw, tf, ti, psq, pab, tpos, twin, xs, xe, ct, bars,
+        misc, tcnt, total;
 };
 __host__ __device__ inline TcwSmem tcw_smem_layout(u32 L, u32 ns) {
     const size_t nkc = tcw_nkc(L), px = tcw_px(L);
@@ -94,7 +96,9 @@ __host__ __device__ inline TcwSmem tcw_smem_layout(u32 L, u32 ns) {
     m.a_bytes = nkc * kWATile;
     m.stage = align_up(m.a_bytes + align_up(px * 2, 16), 128);
     size_t o = 0;
+    m.args = o;  o += align_up(sizeof(TcwArgs), 128);     // the launch arguments (shared-memory copy)
     m.ring = o;  o += ns * m.stage;                       // A tiles + voltage stream per channel
+    m.vst = o;   o += (size_t)kWDepth * px * 4;            // producers: fp32 voltage of the next channels
     m.spos = o;  o += 2 * (size_t)kWPos * 4;               // per tile: sample of a kept output, else ~0
     m.wnwa = o;  o += 2 * (size_t)kWPos * 8;               // per tile: window L2 / L1 norms
     m.wrel = o;  o += 2 * (size_t)kWPos;                   // per tile: table entry of a kept output, else 0xff
@@ -138,6 +142,14 @@ __device__ __forceinline__ double warp_incl_scan_d(double v, u32 lane) {
     }
     return v;
 }
+// 4-byte asynchronous copy global -> shared; src_bytes 0 writes a zero
+// (nothing is read)
+__device__ __forceinline__ void cp_async4(u32 dst, const float *src, u32 src_bytes) {
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 4, %2;" ::"r"(dst), "l"(src), "r"(src_bytes) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory"); }
 __device__ __forceinline__ u16 half_bits_clamped(float f) {
     return __half_as_ushort(__float2half_rn(fminf(fmaxf(f, -65504.0f), 65504.0f)));
 }
@@ -167,11 +179,16 @@ k_lik_tcw(const TcwArgs *__restrict__ gargs, u32 ngroups) {
         }
         if (gi >= ngroups) return;
     }
-    const TcwArgs &A = gargs[gi];
-    const u32 ntiles = *A.n_stiles;
+    const TcwArgs &Ag = gargs[gi];
+    const u32 ntiles = *Ag.n_stiles;
     if (bi >= ntiles) return;                        // no tile for this CTA: no set-up at all
     extern __shared__ __align__(128) unsigned char wsm[];
-    const u32 L = A.L, nkc = A.nkc, ns = A.ns, px = A.px, n = A.n, Cg = A.Cg;
+    // the roles read their arguments from a shared-memory copy (a reload
+    // costs a shared-memory access, not a global one)
+    for (u32 i = threadIdx.x; i < (u32)(sizeof(TcwArgs) / 4); i += blockDim.x)
+        reinterpret_cast<u32 *>(wsm)[i] = reinterpret_cast<const u32 *>(&Ag)[i];
+    const TcwArgs &A = *reinterpret_cast<const TcwArgs *>(wsm);   // valid after the first __syncthreads
+    const u32 L = Ag.L, nkc = Ag.nkc, ns = Ag.ns, px = Ag.px, n = Ag.n, Cg = Ag.Cg;
     const TcwSmem lay = tcw_smem_layout(L, ns);
     unsigned char *ring = wsm + lay.ring;
     u32 *spos_all = (u32 *)(wsm + lay.spos);
@@ -195,7 +212,7 @@ k_lik_tcw(const TcwArgs *__restrict__ gargs, u32 ngroups) {
     double *dsum = (double *)(misc + 16);            // [16] producer warp sums (two arrays)
     u32 *tcnt = (u32 *)(wsm + lay.tcnt);
     const u32 tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-    const u32 wlim = A.wait_polls;
+    const u32 wlim = Ag.wait_polls;
     auto bar_sfull = [&](u32 s) { return smem_u32(&bars[s]); };
     auto bar_sempty = [&](u32 s) { return smem_u32(&bars[ns + s]); };
     auto bar_afull = [&](u32 b) { return smem_u32(&bars[2 * ns + b]); };
@@ -226,13 +243,13 @@ k_lik_tcw(const TcwArgs *__restrict__ gargs, u32 ngroups) {
     }
     for (u32 t = tid; t < 16; t += blockDim.x) {
         tcnt[t] = 0;
-        const bool real = t < A.nt;
-        const u32 gt = real ? A.trow[t] : 0u;
+        const bool real = t < Ag.nt;
+        const u32 gt = real ? Ag.trow[t] : 0u;
         ctrow[t] = gt;
-        ctk[t] = real ? A.kappa_b * A.tnorm[gt] : 0.0f;
-        ctb[t] = real ? 2.98023223876953125e-08f * 1.001f * ldexpf(1.0f, -A.texp[gt]) : 0.0f;
-        ctss[t] = real ? A.tss[gt] : 0.0f;
-        cta[t] = real ? A.kappa_s * fabsf(A.tss[gt]) : 0.0f;
+        ctk[t] = real ? Ag.kappa_b * Ag.tnorm[gt] : 0.0f;
+        ctb[t] = real ? 2.98023223876953125e-08f * 1.001f * ldexpf(1.0f, -Ag.texp[gt]) : 0.0f;
+        ctss[t] = real ? Ag.tss[gt] : 0.0f;
+        cta[t] = real ? Ag.kappa_s * fabsf(Ag.tss[gt]) : 0.0f;
     }
     __syncthreads();
     asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
@@ -243,12 +260,15 @@ k_lik_tcw(const TcwArgs *__restrict__ gargs, u32 ngroups) {
         // =========================== producers ===========================
         const u32 pt = tid;                          // 0..255
         const u32 m = *A.n_win;
-        const bool hasB = 8 * (kWPos / 8 + pt) < px; // a second group of 8 positions past 2048
-        u32 use[2] = {0u, 0u};
+        const u32 nB = px - kWPos;                   // staged positions past 2048
+        const bool hasB = 8 * pt < nB;               // this thread packs 8 of them
+        float *vst = (float *)(wsm + lay.vst);       // [kWDepth][px] fp32 voltage (cp.async)
+        u32 use0 = 0u, use1 = 0u;
         u32 it = 0;
         for (u32 q = bi; q < ntiles; q += cnt, it++) {
             const u32 b = it & 1u;
-            if (use[b] > 0 && !mbar_wait_bounded(bar_bempty(b), (use[b] - 1) & 1u, wlim)) {
+            const u32 ub = b ? use1 : use0;
+            if (ub > 0 && !mbar_wait_bounded(bar_bempty(b), (ub - 1) & 1u, wlim)) {
                 atomicExch(A.err, 13u);
                 atomicExch(abort_flag, 1u);
             }
@@ -285,7 +305,6 @@ k_lik_tcw(const TcwArgs *__restrict__ gargs, u32 ngroups) {
             // ---- positions -> samples (this thread: 8pt.. in registers and,
             //      past 2048, 2048 + 8pt.. in shared memory)
             u32 smpA[8], smpB[8];
-            u32 usefulA = 0;
             auto map8 = [&](u32 x0, u32 (&smp)[8], bool kept_out) -> u32 {
                 // last entry with tpos <= x0 (binary search), then step
                 u32 lo = 0, hi = nw - 1;
@@ -310,7 +329,7 @@ k_lik_tcw(const TcwArgs *__restrict__ gargs, u32 ngroups) {
                 }
                 return kept;
             };
-            usefulA = map8(8 * pt, smpA, true);
+            map8(8 * pt, smpA, true);              // spos / wrel of this thread's positions
             if (hasB) {
                 map8(kWPos + 8 * pt, smpB, false);
 #pragma unroll
@@ -362,13 +381,85 @@ k_lik_tcw(const TcwArgs *__restrict__ gargs, u32 ngroups) {
                 tsc[pt] = sc;
                 tsa[pt] = sa;
             }
-            // ---- the voltage stream, one channel per ring stage
+            // ---- the voltage stream, one channel per ring stage.  Each channel
+            //      is copied (fp32) into a staging slot by coalesced 4-byte
+            //      asynchronous copies -- thread pt copies positions pt + 256 e --
+            //      kWDepth - 1 channels ahead of the one being packed; a thread
+            //      packs positions 8 pt .. 8 pt + 7 (and 2048 + 8 pt .. when hasB).
+            u32 lidx[8];                             // sample of position pt + 256 e, ~0 past the recording
+#pragma unroll
+            for (int e = 0; e < 8; e++) {
+                const int x = (int)(pt + 256u * e);
+                u32 lo = 0, hi = nw - 1;             // last entry with tpos <= x
+                while (lo < hi) {
+                    const u32 mid = (lo + hi + 1) >> 1;
+                    if (tpos[mid] <= x) lo = mid; else hi = mid - 1;
+                }
+                const u32 sx = twin[lo] * L + (u32)(x - tpos[lo]);
+                lidx[e] = sx < n ? sx : 0xffffffffu;
+            }
+            auto issue = [&](u32 c) {
+                float *dst = vst + (size_t)(c % kWDepth) * px;
+                const float *vc = A.v + (size_t)c * n;
+#pragma unroll
+                for (int e = 0; e < 8; e++) {
+                    const bool ok = lidx[e] != 0xffffffffu;
+                    cp_async4(smem_u32(dst + pt + 256u * e), vc + (ok ? lidx[e] : 0u), ok ? 4u : 0u);
+                }
+                for (u32 x = pt; x < nB; x += kTcProdThreads) {
+                    const u32 sb = xs[x];
+                    cp_async4(smem_u32(dst + kWPos + x), vc + (sb < n ? sb : 0u), sb < n ? 4u : 0u);
+                }
+            };
             const float kscale = ldexpf(1.0f, kexp);     // exact: |kexp| <= 126
             float e2A[8], abA[8];
 #pragma unroll
             for (int e = 0; e < 8; e++) e2A[e] = abA[e] = 0.0f;
+#pragma unroll
+            for (u32 j = 0; j + 1 < kWDepth; j++) {
+                if (j < Cg) issue(j);
+                cp_async_commit();
+            }
+            cp_async_wait<kWDepth - 2>();            // channel 0: this thread's copies
+            named_bar(1, kTcProdThreads);            // and every thread's
             bool stop = false;
             for (u32 c = 0; c < Cg; c++) {
+                if (c + kWDepth - 1 < Cg) issue(c + kWDepth - 1);
+                cp_async_commit();                   // one group per channel (empty past the last)
+                const float *src = vst + (size_t)(c % kWDepth) * px;
+                uint4 qa, qb = make_uint4(0u, 0u, 0u, 0u);
+                {
+                    const float4 f0 = *reinterpret_cast<const float4 *>(src + 8 * pt);
+                    const float4 f1 = *reinterpret_cast<const float4 *>(src + 8 * pt + 4);
+                    const float f[8] = {f0.x, f0.y, f0.z, f0.w, f1.x, f1.y, f1.z, f1.w};
+                    u16 h[8];
+#pragma unroll
+                    for (int e = 0; e < 8; e++) {
+                        e2A[e] = fmaf(f[e], f[e], e2A[e]);
+                        abA[e] += fabsf(f[e]);
+                        h[e] = half_bits_clamped(__fmul_rn(f[e], kscale));
+                    }
+                    qa.x = ((u32)h[1] << 16) | h[0];
+                    qa.y = ((u32)h[3] << 16) | h[2];
+                    qa.z = ((u32)h[5] << 16) | h[4];
+                    qa.w = ((u32)h[7] << 16) | h[6];
+                }
+                if (hasB) {
+                    const float4 f0 = *reinterpret_cast<const float4 *>(src + kWPos + 8 * pt);
+                    const float4 f1 = *reinterpret_cast<const float4 *>(src + kWPos + 8 * pt + 4);
+                    const float f[8] = {f0.x, f0.y, f0.z, f0.w, f1.x, f1.y, f1.z, f1.w};
+                    u16 h[8];
+#pragma unroll
+                    for (int e = 0; e < 8; e++) {
+                        xe2[8 * pt + e] = fmaf(f[e], f[e], xe2[8 * pt + e]);
+                        xab[8 * pt + e] += fabsf(f[e]);
+                        h[e] = half_bits_clamped(__fmul_rn(f[e], kscale));
+                    }
+                    qb.x = ((u32)h[1] << 16) | h[0];
+                    qb.y = ((u32)h[3] << 16) | h[2];
+                    qb.z = ((u32)h[5] << 16) | h[4];
+                    qb.w = ((u32)h[7] << 16) | h[6];
+                }
                 const u32 s = gstage % ns, u = gstage / ns;
                 if (u > 0 && !mbar_wait_bounded(bar_sempty(s), (u - 1) & 1u, wlim)) {
                     atomicExch(A.err, 11u);
@@ -385,44 +476,14 @@ k_lik_tcw(const TcwArgs *__restrict__ gargs, u32 ngroups) {
                         ::"r"(smem_u32(stg)), "l"(A.Aw + (size_t)c * bytes), "r"(bytes), "r"(bar_sfull(s))
                         : "memory");
                 }
-                const float *vc = A.v + (size_t)c * n;
-                {
-                    u16 h[8];
-#pragma unroll
-                    for (int e = 0; e < 8; e++) {
-                        const float f = smpA[e] < n ? __ldg(vc + smpA[e]) : 0.0f;
-                        e2A[e] = fmaf(f, f, e2A[e]);
-                        abA[e] += fabsf(f);
-                        h[e] = half_bits_clamped(__fmul_rn(f, kscale));
-                    }
-                    uint4 v4;
-                    v4.x = ((u32)h[1] << 16) | h[0];
-                    v4.y = ((u32)h[3] << 16) | h[2];
-                    v4.z = ((u32)h[5] << 16) | h[4];
-                    v4.w = ((u32)h[7] << 16) | h[6];
-                    *reinterpret_cast<uint4 *>(stg + lay.a_bytes + 16 * (size_t)pt) = v4;
-                }
-                if (hasB) {
-                    u16 h[8];
-#pragma unroll
-                    for (int e = 0; e < 8; e++) {
-                        const u32 sb = xs[8 * pt + e];
-                        const float f = sb < n ? __ldg(vc + sb) : 0.0f;
-                        xe2[8 * pt + e] = fmaf(f, f, xe2[8 * pt + e]);
-                        xab[8 * pt + e] += fabsf(f);
-                        h[e] = half_bits_clamped(__fmul_rn(f, kscale));
-                    }
-                    uint4 v4;
-                    v4.x = ((u32)h[1] << 16) | h[0];
-                    v4.y = ((u32)h[3] << 16) | h[2];
-                    v4.z = ((u32)h[5] << 16) | h[4];
-                    v4.w = ((u32)h[7] << 16) | h[6];
-                    *reinterpret_cast<uint4 *>(stg + lay.a_bytes + 16 * (size_t)(kWN + pt)) = v4;
-                }
+                *reinterpret_cast<uint4 *>(stg + lay.a_bytes + 16 * (size_t)pt) = qa;
+                if (hasB) *reinterpret_cast<uint4 *>(stg + lay.a_bytes + 16 * (size_t)(kWN + pt)) = qb;
                 asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-                named_bar(1, kTcProdThreads);
+                cp_async_wait<kWDepth - 2>();        // channel c + 1: this thread's copies
+                named_bar(1, kTcProdThreads);        // every thread's; the stage is written
                 if (pt == 0) mbar_arrive(bar_sfull(s));  // release: the barrier ordered every write
             }
+            cp_async_wait<0>();                      // no copy lands after the loop (abort path)
             if (stop) break;
             // ---- window norms: prefix sums (double) over the staged positions
 #pragma unroll
@@ -453,22 +514,22 @@ k_lik_tcw(const TcwArgs *__restrict__ gargs, u32 ngroups) {
             named_bar(1, kTcProdThreads);
 #pragma unroll
             for (int e = 0; e < 8; e++) {
-                if (!((usefulA >> e) & 1u)) continue;
                 const u32 x = 8 * pt + e, hi_x = x + L - 1;    // < px
+                const u32 smp = spos[x];             // the sample of a kept output
+                if (smp == 0xffffffffu) continue;
                 const double pa = psq[hi_x], pb = pab[hi_x];
                 const double da = pa - (x ? psq[x - 1] : 0.0), db = pb - (x ? pab[x - 1] : 0.0);
                 // the double sums' own rounding (< 2 px 2^-53 of the prefix) is added back
                 const float wn = (float)sqrt(fmax(da, 0.0) + 1e-12 * pa) * 1.0001f + 1e-30f;
                 const float wa = (float)(fmax(db, 0.0) + 1e-12 * pb) * 1.0001f + 1e-30f;
                 wnwa[x] = make_float2(wn, wa);
-                const u32 smp = smpA[e];
                 A.wn_s[smp] = wn;
                 A.wa_s[smp] = wa;
                 A.kx_s[smp] = (signed char)kexp;
             }
             named_bar(1, kTcProdThreads);
             if (pt == 0) mbar_arrive(bar_ifull(b));
-            use[b]++;
+            if (b) use1++; else use0++;
         }
         // the last copies into the ring land before the CTA exits
         if (pt == 0) {
@@ -484,14 +545,15 @@ k_lik_tcw(const TcwArgs *__restrict__ gargs, u32 ngroups) {
         const u64 a0 = umma_desc(smem_u32(ring), kWATile / 2, 128);       // K halves 2048 B apart
         const u64 b0 = umma_desc(smem_u32(ring) + (u32)lay.a_bytes, 16, 128);   // rows 8 samples apart
         const u64 sstep = (u64)(lay.stage >> 4);
-        u32 use[2] = {0u, 0u};
+        u32 use0 = 0u, use1 = 0u;
         u32 it = 0;
         bool issued = false;
         for (u32 q = bi; q < ntiles; q += cnt, it++) {
             const u32 b = it & 1u;
+            const u32 ub = b ? use1 : use0;
             u32 ok = 1;
             if (lane == 0) {
-                if (use[b] > 0 && !mbar_wait_bounded(bar_aempty(b), (use[b] - 1) & 1u, wlim)) {
+                if (ub > 0 && !mbar_wait_bounded(bar_aempty(b), (ub - 1) & 1u, wlim)) {
                     atomicExch(A.err, 12u);
                     ok = 0;
                 }
@@ -535,7 +597,7 @@ k_lik_tcw(const TcwArgs *__restrict__ gargs, u32 ngroups) {
                 asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];"
                              ::"r"(bar_afull(b)) : "memory");
             __syncwarp();
-            use[b]++;
+            if (b) use1++; else use0++;
         }
         // every MMA issued here is done before TMEM and the ring are released
         if (lane == 0 && issued) {
@@ -555,12 +617,16 @@ k_lik_tcw(const TcwArgs *__restrict__ gargs, u32 ngroups) {
         const u32 gt = ctrow[tl];
         const float ck = ctk[tl], cb = ctb[tl], css = ctss[tl], ca = cta[tl];
         const int texp_t = real ? A.texp[gt] : 0;
-        u32 use[2] = {0u, 0u};
+        float *const Lk = A.Lk;
+        u8 *const apx = A.apx;
+        float *const dbgE = A.dbgE;
+        u32 use0 = 0u, use1 = 0u;
         u32 it = 0;
         for (u32 q = bi; q < ntiles; q += cnt, it++) {
             const u32 b = it & 1u;
-            bool ok = mbar_wait_bounded(bar_afull(b), use[b] & 1u, wlim);
-            ok = ok && mbar_wait_bounded(bar_ifull(b), use[b] & 1u, wlim);
+            const u32 ub = b ? use1 : use0;
+            bool ok = mbar_wait_bounded(bar_afull(b), ub & 1u, wlim);
+            ok = ok && mbar_wait_bounded(bar_ifull(b), ub & 1u, wlim);
             if (!ok) { atomicExch(A.err, 10u); atomicExch(abort_flag, 1u); }
             if (named_bar_or(2, kTcEpiThreads, *(volatile u32 *)abort_flag != 0)) break;
             asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
@@ -588,7 +654,9 @@ k_lik_tcw(const TcwArgs *__restrict__ gargs, u32 ngroups) {
                     const bool kept = real && s != 0xffffffffu;
                     const float2 nwa = wnwa[x];
                     const float a = __uint_as_float(r[j]);
-                    const float approx = __fadd_rn(tsc != 0.0f ? __fmul_rn(a, tsc) : ldexpf(a, -(kexp + texp_t)), css);
+                    float sa = __fmul_rn(a, tsc);
+                    if (tsc == 0.0f) sa = ldexpf(a, -(kexp + texp_t));   // scale outside the normal range
+                    const float approx = __fadd_rn(sa, css);
                     // E = kappa ||t|| ||w|| + 2^-25 (|t|_1 / s_v + |w|_1 / s_t) * 1.001
                     //     + kappa_s |SS/2| + 2^-22 |approx|
                     const float E = fmaf(ck, nwa.x, fmaf(cb, nwa.y, tsa) + ca + 2.384185791015625e-07f * fabsf(approx));
@@ -597,9 +665,9 @@ k_lik_tcw(const TcwArgs *__restrict__ gargs, u32 ngroups) {
                     const bool neg = approx + E <= 0.0f;       // certainly <= 0: only its sign is read
                     if (kept) {
                         const size_t e = (size_t)gt * n + s;
-                        A.Lk[e] = tail ? 0.0f : approx;
-                        A.apx[e] = (!tail && pos) ? (u8)1 : (u8)0;
-                        if (A.dbgE) A.dbgE[e] = tail ? 0.0f : E;
+                        Lk[e] = tail ? 0.0f : approx;
+                        apx[e] = (!tail && pos) ? (u8)1 : (u8)0;
+                        if (dbgE) dbgE[e] = tail ? 0.0f : E;
                         if (!tail && pos) atomicMax(reinterpret_cast<int *>(A.bm_s) + s, __float_as_int(E));
                     }
                     const bool live = kept && !tail;
@@ -692,7 +760,7 @@ k_lik_tcw(const TcwArgs *__restrict__ gargs, u32 ngroups) {
             // the tile's tables are no longer needed
             __syncwarp();
             if (lane == 0) mbar_arrive(bar_bempty(b));
-            use[b]++;
+            if (b) use1++; else use0++;
         }
     }
     __syncthreads();
