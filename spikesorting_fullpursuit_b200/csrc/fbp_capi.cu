@@ -991,7 +991,8 @@ int prepare_chunk(Workspace &w, float *voltage, u32 n, u32 C, const float *templ
                 w.tcw = false;
                 if (t_tc_layout != FBP_TC_LAYOUT_SAMPLES) {
                     w.tcw_ns = plan_tcw_groups(tsup, tperm, K, C, L, w.tcwg);
-                    w.tcw = w.tcw_ns > 0;
+                    // the stream table marks tail outputs in bit 31 of a sample
+                    w.tcw = w.tcw_ns > 0 && n < 0x80000000u;
                 }
                 std::vector<u32> gdesc_w(3 * w.tcwg.size()), tgrp_w(K);
                 if (w.tcw) {

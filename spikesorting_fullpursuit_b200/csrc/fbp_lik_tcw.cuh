@@ -40,6 +40,7 @@
 // to the fp16 range, so no inf reaches a product with a zero template value.
 #pragma once
 #include <cuda_fp16.h>
+#include <type_traits>
 #include "fbp_lik_tc.cuh"
 
 namespace fbp {
@@ -51,6 +52,7 @@ constexpr u32 kWMinL = 16;
 constexpr u32 kWMaxStages = 8;
 constexpr u32 kWATile = 4096;            // one A tile: 128 rows x 16 lags x fp16
 constexpr u32 kWDepth = 3;               // channels of voltage in flight (fp32 staging slots)
+constexpr u32 kWTail = 0x80000000u;      // stream table: a kept output in the zeroed tail (n < 2^31)
 
 __host__ __device__ inline u32 tcw_nkc(u32 L) { return (L + 7 + 15) / 16; }
 __host__ __device__ inline u32 tcw_px(u32 L) { return kWPos + 16 * tcw_nkc(L); }   // staged positions
@@ -322,7 +324,8 @@ k_lik_tcw(const TcwArgs *__restrict__ gargs, u32 ngroups) {
                     smp[e] = s;
                     if (kept_out) {
                         const bool k = o < L && s < n;
-                        spos[x] = k ? s : 0xffffffffu;
+                        // bit 31: the output is the reference's zeroed tail (.cl:231-234)
+                        spos[x] = k ? (s | (s + L >= n ? kWTail : 0u)) : 0xffffffffu;
                         wrel[x] = k ? (u8)j : (u8)0xff;
                         kept |= k ? (1u << e) : 0u;
                     }
@@ -515,8 +518,9 @@ k_lik_tcw(const TcwArgs *__restrict__ gargs, u32 ngroups) {
 #pragma unroll
             for (int e = 0; e < 8; e++) {
                 const u32 x = 8 * pt + e, hi_x = x + L - 1;    // < px
-                const u32 smp = spos[x];             // the sample of a kept output
-                if (smp == 0xffffffffu) continue;
+                const u32 sp = spos[x];              // the sample of a kept output
+                if (sp == 0xffffffffu) continue;
+                const u32 smp = sp & ~kWTail;
                 const double pa = psq[hi_x], pb = pab[hi_x];
                 const double da = pa - (x ? psq[x - 1] : 0.0), db = pb - (x ? pab[x - 1] : 0.0);
                 // the double sums' own rounding (< 2 px 2^-53 of the prefix) is added back
@@ -617,9 +621,11 @@ k_lik_tcw(const TcwArgs *__restrict__ gargs, u32 ngroups) {
         const u32 gt = ctrow[tl];
         const float ck = ctk[tl], cb = ctb[tl], css = ctss[tl], ca = cta[tl];
         const int texp_t = real ? A.texp[gt] : 0;
-        float *const Lk = A.Lk;
-        u8 *const apx = A.apx;
-        float *const dbgE = A.dbgE;
+        // this lane's template row of the likelihood and flag buffers
+        float *const Lk_t = A.Lk + (size_t)gt * n;
+        u8 *const apx_t = A.apx + (size_t)gt * n;
+        float *const dbg_t = A.dbgE ? A.dbgE + (size_t)gt * n : nullptr;
+        int *const bm_i = reinterpret_cast<int *>(A.bm_s);
         u32 use0 = 0u, use1 = 0u;
         u32 it = 0;
         for (u32 q = bi; q < ntiles; q += cnt, it++) {
@@ -638,9 +644,15 @@ k_lik_tcw(const TcwArgs *__restrict__ gargs, u32 ngroups) {
             const int kexp = ti_all[b * 4];
             const float tsc = tf_all[b * 32 + tl], tsa = tf_all[b * 32 + 16 + tl];
             const u32 acc0 = tmem + ((quad * 32u) << 16) + b * kWN;
+            // the rare cases (a scale outside the float range, the testing
+            // output of E) take a separate, warp-uniform copy of the loop
+            const bool rare = __any_sync(0xffffffffu, tsc == 0.0f) || dbg_t != nullptr;
             u32 want[8];
-#pragma unroll
-            for (int k = 0; k < 8; k++) {
+            // one 16-column chunk: classify and store its entries; per
+            // (window, template) the largest upper bound, per window the
+            // largest lower bound and whether some entry is > 0
+            auto chunk = [&](const int k, auto RARE) {
+                constexpr bool kRare = decltype(RARE)::value;
                 const u32 c0 = 128 * half + 16 * k;
                 u32 r[16];
                 tmem_ld<16>(r, acc0 + c0);
@@ -650,27 +662,27 @@ k_lik_tcw(const TcwArgs *__restrict__ gargs, u32 ngroups) {
 #pragma unroll
                 for (int j = 0; j < 16; j++) {
                     const u32 x = 8 * (c0 + j) + d;
-                    const u32 s = spos[x];
-                    const bool kept = real && s != 0xffffffffu;
+                    const u32 sp = spos[x];
+                    const bool kept = real && sp != 0xffffffffu;
+                    const bool tail = (sp & kWTail) != 0u;          // .cl:231-234 (kept outputs only)
+                    const u32 s = sp & ~kWTail;
                     const float2 nwa = wnwa[x];
                     const float a = __uint_as_float(r[j]);
                     float sa = __fmul_rn(a, tsc);
-                    if (tsc == 0.0f) sa = ldexpf(a, -(kexp + texp_t));   // scale outside the normal range
+                    if (kRare && tsc == 0.0f) sa = ldexpf(a, -(kexp + texp_t));
                     const float approx = __fadd_rn(sa, css);
                     // E = kappa ||t|| ||w|| + 2^-25 (|t|_1 / s_v + |w|_1 / s_t) * 1.001
                     //     + kappa_s |SS/2| + 2^-22 |approx|
                     const float E = fmaf(ck, nwa.x, fmaf(cb, nwa.y, tsa) + ca + 2.384185791015625e-07f * fabsf(approx));
-                    const bool tail = kept && s + L >= n;      // .cl:231-234
                     const bool pos = approx - E > 0.0f;        // certainly > 0: refined when a decision needs it
                     const bool neg = approx + E <= 0.0f;       // certainly <= 0: only its sign is read
-                    if (kept) {
-                        const size_t e = (size_t)gt * n + s;
-                        Lk[e] = tail ? 0.0f : approx;
-                        apx[e] = (!tail && pos) ? (u8)1 : (u8)0;
-                        if (dbgE) dbgE[e] = tail ? 0.0f : E;
-                        if (!tail && pos) atomicMax(reinterpret_cast<int *>(A.bm_s) + s, __float_as_int(E));
-                    }
                     const bool live = kept && !tail;
+                    if (kept) {
+                        Lk_t[s] = tail ? 0.0f : approx;
+                        apx_t[s] = (live && pos) ? (u8)1 : (u8)0;
+                        if (kRare && dbg_t) dbg_t[s] = tail ? 0.0f : E;
+                    }
+                    if (live && pos) atomicMax(bm_i + s, __float_as_int(E));
                     wbits |= (live && !pos && !neg) ? (1u << j) : 0u;
                     pbits |= (live && pos) ? (1u << j) : 0u;
                     uq[j] = live ? fmaxf(0.0f, approx + E) : 0.0f;
@@ -678,8 +690,6 @@ k_lik_tcw(const TcwArgs *__restrict__ gargs, u32 ngroups) {
                     any |= live && !neg;
                 }
                 want[k] = wbits;
-                // per (window, template): the largest upper bound; per window:
-                // the largest lower bound and whether some entry is > 0
                 if (__any_sync(0xffffffffu, any)) {
                     const u32 cwv = cw[half * 8 + k];
                     const u32 wf = cwv & 0xffffu, wl = cwv >> 16;
@@ -704,6 +714,13 @@ k_lik_tcw(const TcwArgs *__restrict__ gargs, u32 ngroups) {
                         if (__any_sync(0xffffffffu, mp) && lane == 0) A.wpos[wa] = 1;
                     }
                 }
+            };
+            if (rare) {
+#pragma unroll
+                for (int k = 0; k < 8; k++) chunk(k, std::true_type{});
+            } else {
+#pragma unroll
+                for (int k = 0; k < 8; k++) chunk(k, std::false_type{});
             }
             // accumulator b is no longer needed
             asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
@@ -750,7 +767,7 @@ k_lik_tcw(const TcwArgs *__restrict__ gargs, u32 ngroups) {
                             const u32 x = 8 * (128 * half + 16 * k + j) + d;
                             const u32 p = seg_base + atomicAdd(&tcnt[tl], 1u);
                             A.ref_t[p] = tl;
-                            A.ref_s[p] = spos[x];
+                            A.ref_s[p] = spos[x] & ~kWTail;
                         }
                     }
                 }
