@@ -153,7 +153,7 @@ class ClockSampler:
 # slice of each workload (every window listed; dram__bytes_read.sum +
 # dram__bytes_write.sum over sample x templates of the pass); see the
 # k_lik_tc* summaries in profiles/.
-LIK_TC_DRAM_BYTES_PER_ST = {("hd384_300u", "wide"): None, ("linear16_64u", "wide"): None,
+LIK_TC_DRAM_BYTES_PER_ST = {("hd384_300u", "wide"): 12.23, ("linear16_64u", "wide"): None,
                             ("hd384_300u", "samples"): 11.5, ("linear16_64u", "samples"): None}
 LIK_KERNEL = {"wide": "k_lik_tcw", "samples": "k_lik_tc<0>"}
 
