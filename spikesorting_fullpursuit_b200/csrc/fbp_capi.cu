@@ -644,26 +644,37 @@ int ov_fast_pass(const Workspace &w, const OvArgs &A, Counters *cnt, cudaStream_
 }
 
 // Per template: ||t||_2, ||t||_1 (rounded up) and the power-of-two scale that
-// brings its largest magnitude just under 2^14 in fp16.
+// brings its largest magnitude just under 2^14 in fp16.  One warp per
+// template: lanes stride over its C*L values, double sums reduced over the
+// warp (the 1e-6 margin covers any summation order's rounding).
 __global__ void k_tnorm(const float *__restrict__ T, u32 K, u32 CL, float *__restrict__ out,
                         float *__restrict__ out1, int *__restrict__ texp) {
-    for (u32 t = blockIdx.x * blockDim.x + threadIdx.x; t < K; t += gridDim.x * blockDim.x) {
+    const u32 lane = threadIdx.x & 31u, nwarps = (gridDim.x * blockDim.x) >> 5;
+    for (u32 t = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; t < K; t += nwarps) {
         double ss = 0.0, s1 = 0.0;
         float mx = 0.0f;
-        for (u32 i = 0; i < CL; i++) {
+        for (u32 i = lane; i < CL; i += 32) {
             const float x = T[(size_t)t * CL + i];
             ss += (double)x * x;
             s1 += fabs((double)x);
             mx = fmaxf(mx, fabsf(x));
         }
-        out[t] = (float)(sqrt(ss) * (1.0 + 1e-6));
-        out1[t] = (float)(s1 * (1.0 + 1e-6));
-        int e = 0;
-        if (mx > 0.0f) {
-            frexpf(mx, &e);
-            e = 14 - e;
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+            ss += __shfl_xor_sync(0xffffffffu, ss, o);
+            s1 += __shfl_xor_sync(0xffffffffu, s1, o);
+            mx = fmaxf(mx, __shfl_xor_sync(0xffffffffu, mx, o));
         }
-        texp[t] = e;
+        if (lane == 0) {
+            out[t] = (float)(sqrt(ss) * (1.0 + 1e-6));
+            out1[t] = (float)(s1 * (1.0 + 1e-6));
+            int e = 0;
+            if (mx > 0.0f) {
+                frexpf(mx, &e);
+                e = 14 - e;
+            }
+            texp[t] = e;
+        }
     }
 }
 
@@ -674,7 +685,7 @@ __global__ void k_tc_gate(Counters *cnt, u32 cap, u32 seg_cap) {
 
 int tc_chunk_setup(const Workspace &w, const float *v, u32 n, const float *T, u32 K, u32 C, u32 L,
                    cudaStream_t st) {
-    k_tnorm<<<grid_for(K, 64), 64, 0, st>>>(T, K, C * L, w.tc_tnorm, w.tc_tabs, w.tc_texp);
+    k_tnorm<<<grid_for((u64)K * 32, 256), 256, 0, st>>>(T, K, C * L, w.tc_tnorm, w.tc_tabs, w.tc_texp);
     for (const TcGroup &g : w.tcg) {
         const u64 total = (u64)L * g.Cg2 * g.Np;
         k_tc_pack_templates<<<grid_for(total, 256), 256, 0, st>>>(T, g.nt, C, g.clo, g.Cg, L, g.Cg2, g.Np,
