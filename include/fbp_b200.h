@@ -177,8 +177,9 @@ int fbp_set_tc_group_size(uint32_t templates_per_group);
  * reference).  FBP_TC_LAYOUT_SAMPLES: tiles of 128 samples, template groups
  * in the MMA's N (fbp_lik_tc.cuh); FBP_TC_LAYOUT_WIDE: tiles of 2048 positions
  * of the pass's window stream, 16 templates x 8 sample shifts in the MMA's M
- * and blocks of 8 samples in N (fbp_lik_tcw.cuh; needs 16 <= L <= 1024);
- * FBP_TC_LAYOUT_AUTO (default): WIDE where it applies.  Applies to the calls
+ * and blocks of 8 samples in N (fbp_lik_tcw.cuh; applies when L >= 16, its
+ * shared-memory plan fits -- L up to about 190 -- and the chunk has fewer than
+ * 2^31 samples); FBP_TC_LAYOUT_AUTO (default): WIDE where it applies.  Applies to the calls
  * the calling thread makes afterwards.  Results do not depend on it. */
 enum { FBP_TC_LAYOUT_AUTO = 0, FBP_TC_LAYOUT_SAMPLES = 1, FBP_TC_LAYOUT_WIDE = 2 };
 int fbp_set_tc_layout(int layout);
