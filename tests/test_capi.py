@@ -73,3 +73,19 @@ def test_bounds_entry_rejects_null_arguments(lib):
     rc = lib.fbp_tc_likelihood_bounds(None, 100, 4, None, 8, 31, None, None, 0, None, None, None)
     assert rc == _lib.FBP_ERR_BAD_ARG
     assert b"null pointer" in lib.fbp_last_error()
+
+
+def test_plan_knobs_are_host_only_and_checked(lib):
+    """The per-thread tensor-core plan knobs take their documented values and
+    reject others with FBP_ERR_BAD_ARG, without touching a device."""
+    for layout in (_lib.TC_LAYOUT_AUTO, _lib.TC_LAYOUT_SAMPLES, _lib.TC_LAYOUT_WIDE):
+        assert lib.fbp_set_tc_layout(layout) == 0
+    assert lib.fbp_set_tc_layout(3) == _lib.FBP_ERR_BAD_ARG
+    assert b"unknown layout" in lib.fbp_last_error()
+    assert lib.fbp_set_tc_layout(_lib.TC_LAYOUT_AUTO) == 0
+    for gs in (0, 16, 32, 256):
+        assert lib.fbp_set_tc_group_size(gs) == 0
+    for gs in (8, 24, 272):
+        assert lib.fbp_set_tc_group_size(gs) == _lib.FBP_ERR_BAD_ARG
+    assert lib.fbp_set_tc_group_size(0) == 0
+    assert lib.fbp_last_error() == b""
