@@ -50,7 +50,7 @@ def _to_device_f32(torch, host_chunk, dev, stream):
 
 
 def binary_pursuit(voltage, v_dtype, sort_info, separability_metrics, n_max_shift_inds=None,
-                   kernels_path=None, max_gpu_memory=None, *, precision="fp32",
+                   kernels_path=None, max_gpu_memory=None, *, precision="bf16",
                    chunk_samples=None, device=None, max_passes=1000000, stats=None, profile=False,
                    overlap="fast", tune=False, tc_layout=None):
     """Full Binary Pursuit over `voltage` ([channels, samples], any real dtype).
@@ -61,9 +61,9 @@ def binary_pursuit(voltage, v_dtype, sort_info, separability_metrics, n_max_shif
     ignored (there are no OpenCL sources to load).
 
     Extra keyword-only arguments (not in the reference):
-      precision      "fp32" (likelihoods on the FP32 pipes in the reference's
-                     order) or "bf16" (tensor cores with exact refinement);
-                     both give the same spikes.
+      precision      "bf16" (default: tensor cores with exact refinement) or
+                     "fp32" (likelihoods on the FP32 pipes in the reference's
+                     order); both give the same spikes.
       chunk_samples  override the chunk length (the reference derives it from
                      device memory, :276-341); needed to reproduce a given
                      chunking exactly.

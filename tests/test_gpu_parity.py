@@ -144,7 +144,8 @@ def test_fast_overlap_exact_ties_between_duplicate_templates(lib):
     m2 = {k: (v.copy() if isinstance(v, np.ndarray) else v) for k, v in m.items()}
     exp = O.binary_pursuit_oracle(rec.voltage, rec.voltage.dtype, si, m, n_max_shift_inds=40)
     stats = []
-    got = bpp.binary_pursuit(rec.voltage, rec.voltage.dtype, si, m2, n_max_shift_inds=40, stats=stats)
+    got = bpp.binary_pursuit(rec.voltage, rec.voltage.dtype, si, m2, n_max_shift_inds=40, stats=stats,
+                             precision="fp32")
     assert_same_outputs(got, tuple(np.asarray(x) for x in exp))
     assert stats[0]["candidates"] > 0
 
@@ -353,8 +354,9 @@ def test_iteration_cap_returns_error_status(lib):
     si = rec.sort_info()
     with pytest.raises(_lib.PursuitError) as e:
         bpp.binary_pursuit(rec.voltage, rec.voltage.dtype, si, rec.fresh_metrics(), n_max_shift_inds=5,
-                           max_passes=1)
+                           max_passes=1, precision="fp32")
     assert e.value.code == _lib.FBP_ERR_ITER_CAP
     # the context is still usable afterwards
-    out = bpp.binary_pursuit(rec.voltage, rec.voltage.dtype, si, rec.fresh_metrics(), n_max_shift_inds=5)
+    out = bpp.binary_pursuit(rec.voltage, rec.voltage.dtype, si, rec.fresh_metrics(), n_max_shift_inds=5,
+                             precision="fp32")
     assert len(out[0]) > 0
