@@ -16,8 +16,10 @@
 // sample-major kernel (fbp_lik_tc.cuh) does 128 x (templates in a group) x 16.
 // A (the shifted templates) is packed once per chunk (k_tcw_pack) and
 // streamed per channel into a ring of shared-memory stages with one bulk
-// asynchronous copy.  Accumulators are FP32 in tensor memory (two tiles of
-// 256 columns).
+// asynchronous copy.  The channel's fp32 voltage reaches a staging slot by
+// coalesced 4-byte asynchronous copies, kWDepth - 1 channels ahead, and the
+// producers convert it to fp16 into the stage.  Accumulators are FP32 in
+// tensor memory (two tiles of 256 columns).
 //
 // The stream.  A pass lists windows w (ascending).  Their outputs are laid
 // end to end: listed window i of the list starts at stream position
@@ -158,7 +160,8 @@ __device__ __forceinline__ u16 half_bits_clamped(float f) {
 
 // Persistent, one CTA per SM, 17 warps: 8 producers (tile tables, voltage
 // stream per channel, window norms), 1 MMA warp, 8 epilogue warps (two per
-// TMEM lane quadrant, one half of the 256 columns each).  Barriers:
+// TMEM lane quadrant, one half of the 256 columns each).  The launch
+// arguments are copied into shared memory first.  Barriers:
 //   stage_full[s]  producers wrote the stream (one arrive) and the A copy landed (tx);
 //   stage_empty[s] the MMAs that read stage s are done (tcgen05.commit);
 //   acc_full[b]    the tile's MMAs are done (commit);
